@@ -1,0 +1,341 @@
+#!/usr/bin/env python
+"""bench.py -- grid-cell time steps per second of the PaScaL_TCS step on B200.
+
+One "step" is one full time step of main.f90:129-223 (energy ADI, momentum
+ADI, FFT pressure Poisson solve, projection, Div/CFL/Nu/KE) on one
+HBM-resident case.  Default workload: the 256^3 plain-FP64 case with
+temperature-dependent water properties (Ra = 1e8, Pr = 7, dt = 2e-4, tanh
+y-stretching gamma = 1.5, seeded conduction profile + 0.01 noise, seed 1).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME] [--impl ours|reference]
+
+With N > 1 (torchrun, one process per GPU) every rank advances its own
+replica of the case: a single case does not shard on this path, so there is
+no data-path collective; the barrier and the max-over-ranks timing use NCCL.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    # the plain FP64 256^3 water case the headline metric is quoted on
+    "rb256_water_fp64": dict(n1m=256, n2m=256, n3m=256, gamma2=1.5, property_set=1, Pr=7.0, Ra=1e8,
+                             DeltaT=10.0, dtStart=2e-4, fixed_dt=1, seed=1, noise_amp=0.01),
+    "rb64_const_fp64": dict(n1m=64, n2m=64, n3m=64, gamma2=1.5, property_set=0, Pr=0.71, Ra=1e5,
+                            dtStart=1e-3, fixed_dt=1, seed=0, noise_amp=0.01),
+    "rb512_water_fp64": dict(n1m=512, n2m=512, n3m=512, gamma2=2.0, property_set=1, Pr=7.0, Ra=1e9,
+                             DeltaT=10.0, dtStart=5e-5, fixed_dt=1, seed=2, noise_amp=0.01),
+}
+
+# Compulsory-traffic model: FP64 arrays each kernel must stream once (reads +
+# writes) per interior cell; properties and tridiagonal coefficients are
+# recomputed, 1-D metrics and ghosts ignored.  Whole step: 109 arrays = 872 B.
+STEP_ARRAYS_FP64 = 109
+KERNEL_ARRAYS = {"thermal_z": 5, "thermal_x": 4, "thermal_y": 4,
+                 "du_z": 6, "du_x": 4, "du_y": 4, "dv_z": 7, "dv_x": 4, "dv_y": 4,
+                 "dw_z": 8, "dw_x": 4, "dw_y": 4, "blockld_v": 5, "blockld_u": 6,
+                 "prhs_fftx": 11, "fftz_fwd": 2, "modal_tdma": 2, "fftz_inv": 2, "ifftx": 2,
+                 "projection": 14, "post": 4}
+
+
+def kernel_bytes(name: str, n1: int, n2: int, n3: int) -> float:
+    cells = n1 * n2 * n3
+    h1p = n1 // 2 + 1
+    spec = 16.0 * h1p * n2 * n3                       # one pass over the complex half-spectrum
+    if name in ("fftz_fwd", "modal_tdma", "fftz_inv"):
+        return 2 * spec
+    if name == "ifftx":
+        return spec + 8.0 * cells
+    if name == "prhs_fftx":
+        return 10 * 8.0 * cells + spec
+    if name.startswith("dv_") or name == "blockld_v":
+        cells = n1 * (n2 - 1) * n3
+    return KERNEL_ARRAYS[name] * 8.0 * cells
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic(kernel: str, workload: str):
+    """dram__bytes_read.sum + dram__bytes_write.sum per launch from the committed
+    ncu summary (profiles/traffic.json), or None."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        d = json.load(f)
+    return d.get(workload, {}).get(kernel)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device, self.proc, self.lines = device, None, []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.device)],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.t.join(timeout=2)
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1])); mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup(n_gpus: int):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    return ws, rank, local
+
+
+def dist_max(x: float, ws: int) -> float:
+    """Max over ranks (the slowest replica sets the job time)."""
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def dist_barrier(ws: int):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def cpu_baseline(cfg: dict, target_s: float = 20.0, threads: int | None = None) -> dict:
+    """The oracle (one-rank C restatement of the reference's CPU path; the
+    Fortran/MPI/FFTW reference has no toolchain here) on the host cores."""
+    from oracle import oracle as O
+    threads = threads or os.cpu_count() or 1
+    O.set_threads(threads)
+    o = O.Oracle(**{k: v for k, v in cfg.items() if k != "device"})
+    t0 = time.perf_counter(); o.step(1); t1 = time.perf_counter()
+    first = t1 - t0
+    n = max(1, min(20, int(target_s / max(first, 1e-3))))
+    t0 = time.perf_counter(); o.step(n); t1 = time.perf_counter()
+    cells = cfg["n1m"] * cfg["n2m"] * cfg["n3m"]
+    return {"value": cells * n / (t1 - t0), "unit": "cell-steps/s", "cores": threads, "kind": "port",
+            "sample": f"{n} full time steps of the same {cfg['n1m']}x{cfg['n2m']}x{cfg['n3m']} case "
+                      f"(after 1 untimed), oracle C restatement with OpenMP",
+            "seconds": t1 - t0}
+
+
+def run_reference(args, cfg, workload):
+    ws, rank, _ = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
+    if rank != 0:
+        return 0
+    from oracle import oracle as O
+    threads = os.cpu_count() or 1
+    O.set_threads(threads)
+    o = O.Oracle(**{k: v for k, v in cfg.items() if k != "device"})
+    if args.warmup:
+        o.step(args.warmup)
+    t0 = time.perf_counter()
+    o.step(args.steps)
+    el = time.perf_counter() - t0
+    cells = cfg["n1m"] * cfg["n2m"] * cfg["n3m"]
+    v = cells * args.steps / el
+    line = {"impl": "reference", "metric": "cell-steps/s (FP64 plain, one case per process)", "value": v,
+            "unit": "cell-steps/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded conduction profile + noise)",
+            "config": {"workload": workload, **{k: cfg[k] for k in ("n1m", "n2m", "n3m", "Ra", "Pr", "dtStart")},
+                       "properties": "water", "cpu_threads": threads},
+            "cpu_baseline": {"value": v, "unit": "cell-steps/s", "cores": threads, "kind": "port",
+                             "sample": f"{args.steps} full time steps after {args.warmup} warm-up steps; the Fortran/MPI/"
+                                       "FFTW reference has no toolchain on this image, so its one-rank C restatement runs"},
+            "e2e": {"value": v, "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--workload", default="rb256_water_fp64", choices=sorted(WORKLOADS))
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    workload = args.workload
+    cfg = dict(WORKLOADS[workload])
+    if args.impl == "reference":
+        return run_reference(args, cfg, workload)
+
+    ws, rank, local = dist_setup(args.gpus)
+    import torch
+    import pascal_tcs_b200 as P
+
+    torch.cuda.set_device(local)
+    stream = torch.cuda.Stream()
+    cfg["device"] = local
+    n1, n2, n3 = cfg["n1m"], cfg["n2m"], cfg["n3m"]
+    cells = n1 * n2 * n3
+    s = P.Solver(**cfg)
+    s.set_stream(stream.cuda_stream)
+
+    # warm-up; the last warm-up step probes every kernel to find the dominant one
+    s.step(max(0, args.warmup - 1))
+    names = P.kernel_names()
+    s.probe(names)
+    s.step(1)
+    per = {k: s.probe_read(k) for k in names}
+    s.probe_reset()
+    top = max((k for k in per if per[k][1] > 0 and k in KERNEL_ARRAYS), key=lambda k: per[k][0])
+    s.probe([top])
+    torch.cuda.synchronize()
+
+    # timed region: K steps, device events on the launching stream
+    launches0 = P.launch_count()
+    with ClockSampler(local) as clk:
+        dist_barrier(ws)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        done = s.step(args.steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        dist_barrier(ws)
+    launches = P.launch_count() - launches0
+    ms_local = e0.elapsed_time(e1)
+    ms = dist_max(ms_local, ws)
+    assert done == args.steps
+    value = ws * cells * args.steps / (ms * 1e-3)
+    tk, nk = s.probe_read(top)
+    s.probe([])
+    peak, peak_kind = measured_peaks()
+    kb = kernel_bytes(top, n1, n2, n3)
+    achieved = kb / (tk / nk * 1e-3) / 1e9 if nk else None
+    roof = {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak if achieved else None, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+            "algorithmic_bytes_per_launch": kb, "launches": nk, "avg_launch_ms": tk / nk if nk else None,
+            "traffic": profiled_traffic(top, workload)}
+    step_bytes = STEP_ARRAYS_FP64 * 8.0 * cells
+    whole = {"algorithmic_bytes_per_step": step_bytes, "achieved_gbs": step_bytes / (ms / args.steps * 1e-3) / 1e9}
+    whole["frac_of_peak"] = whole["achieved_gbs"] / peak
+    kernel_split = {k: round(v[0], 4) for k, v in sorted(per.items(), key=lambda kv: -kv[1][0]) if v[1]}
+
+    # end to end through the C ABI with host buffers: fields uploaded from pinned
+    # host memory, K steps driven one reference routine at a time (each step
+    # returns maxDivU, CFL and dt to the host), fields downloaded back.
+    e2e = None
+    if not args.no_e2e:
+        host = {f: torch.empty(s.shape, dtype=torch.float64, pin_memory=True) for f in ("T", "U", "V", "W", "P")}
+        for f, t in host.items():
+            t.numpy()[...] = s.get(f)
+        dist_barrier(ws)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for f, t in host.items():
+            s.upload_async(f, t.data_ptr())
+        for _ in range(args.steps):
+            s.driver_step()
+        for f, t in host.items():
+            s.download_async(f, t.data_ptr())
+        s.synchronize()
+        el = dist_max(time.perf_counter() - t0, ws)
+        nbytes = 8 * int(np.prod(s.shape))
+        e2e = {"value": ws * cells * args.steps / el, "unit": "cell-steps/s",
+               "h2d_bytes_per_step": 5 * nbytes / args.steps,
+               "d2h_bytes_per_step": 5 * nbytes / args.steps + 2 * 11 * 8,
+               "what": "upload T,U,V,W,P from pinned host memory, K steps through the per-routine C-ABI "
+                       "entry points (maxDivU, CFL, dt read back every step), download T,U,V,W,P"}
+
+    base = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        base = cpu_baseline(cfg)
+        base.pop("seconds", None)
+
+    if rank == 0:
+        line = {"metric": "cell-steps/s (FP64 plain, one 256^3 case per GPU)", "value": value,
+                "unit": "cell-steps/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic: seeded conduction profile + uniform noise 0.01, zero velocity",
+                "config": {"workload": workload, "grid": [n1, n2, n3], "properties": "water",
+                           "Ra": cfg["Ra"], "Pr": cfg["Pr"], "dt": cfg["dtStart"],
+                           "parallelism": "replicas" if ws > 1 else "single",
+                           "l2": "inputs larger than L2 (each field %.0f MB)" % (8 * np.prod(s.shape) / 1e6),
+                           "timing": "eager launches with one event-probed kernel; CUDA events on the solver stream"},
+                "gpu_launches": launches, "roofline": roof, "whole_step": whole,
+                "kernel_ms_one_step": kernel_split, "clocks": clk.summary(), "e2e": e2e,
+                "cpu_baseline": base}
+        print(json.dumps(line))
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

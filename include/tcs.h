@@ -1,0 +1,141 @@
+/*
+ * tcs.h -- C ABI of libtcs: the PaScaL_TCS per-timestep path on one B200.
+ *
+ * Every entry point takes plain pointers, sizes and a context handle, returns
+ * an int status (TCS_OK = 0), and never blocks the host except where a scalar
+ * or a host buffer is returned.  All names mirror the reference routine they
+ * replace; the citation after each declaration is the reference interface
+ * (path:line within the PaScaL_TCS source tree).
+ *
+ * Fields are the reference's padded arrays (0:n1sub, 0:n2sub, 0:n3sub),
+ * n_sub = n_m + 1, Fortran order (i fastest), FP64.  They live on the device;
+ * host arrays cross only through tcs_upload_field / tcs_download_field (the
+ * continue-file reader and writer, and the instantaneous-field dump, are the
+ * only reference call sites that need host data: main.f90:121-125, 209, 226-228).
+ */
+#ifndef TCS_H
+#define TCS_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define TCS_OK              0
+#define TCS_ERR_ARG         1   /* bad argument, shape or handle */
+#define TCS_ERR_CUDA        2   /* a CUDA call failed (see tcs_last_error) */
+#define TCS_ERR_UNSUPPORTED 3   /* size or option outside what the kernels support */
+#define TCS_ERR_BLOWUP      4   /* max divergence >= 1e-3 (main.f90:208-212) */
+#define TCS_ERR_NOMEM       5   /* device allocation failed */
+#define TCS_ERR_NONFINITE   6   /* a returned scalar is NaN or Inf */
+
+/* Run configuration: the PARA_INPUT.dat namelists (module_global.f90:83-105)
+ * plus the options of the seeded benchmark cases.  The layout of the leading
+ * members is shared with the test oracle's parameter block. */
+typedef struct tcs_config {
+    int n1m, n2m, n3m;                /* &meshes */
+    int uniform1, uniform2, uniform3; /* &uniform_mesh (x and z must be periodic) */
+    double gamma1, gamma2, gamma3;    /* &mesh_stretch */
+    double aspect1, H, aspect3;       /* &aspect_ratio */
+    double Ra, Pr, DeltaT, MaxCFL;    /* &sim_parameter */
+    double dtStart, tStart;           /* &sim_control */
+    int property_set;                 /* 0 constant (module_global.f90:117-120), 1 water (:113-116), 2 glycerol (:129-132) */
+    int fixed_dt;                     /* 0: dt = min(MaxCFL / max|u|/dx, dtMax) after every step (module_post.f90:222-226); 1: keep dtStart */
+    uint64_t seed;                    /* initial temperature noise seed */
+    double noise_amp;                 /* noise amplitude (0.01 in the benchmark cases) */
+    int init_mode;                    /* 0: T = 0.5 - y + noise; 1: T = 0 interior (mpi_thermal_initial) */
+    int top_wall_mode;                /* 0: top ghost row of T stays 0 as on one y rank (module_solve_thermal.f90:102-110); 1: = Tup */
+    int device;                       /* CUDA device ordinal */
+} tcs_config;
+
+/* field identifiers */
+enum {
+    TCS_F_T = 0, TCS_F_U, TCS_F_V, TCS_F_W, TCS_F_P, TCS_F_DPHAT, TCS_F_DP0,
+    TCS_F_DU, TCS_F_DV, TCS_F_DW, TCS_F_DP, TCS_F_MU, TCS_F_INVRHO, TCS_F_COUNT
+};
+
+/* device scalars returned by tcs_get_scalars */
+enum {
+    TCS_S_DT = 0, TCS_S_TIME, TCS_S_CFL, TCS_S_MAXDIV, TCS_S_NUBOT, TCS_S_NUTOP, TCS_S_KE,
+    TCS_S_BLOWUP, TCS_S_AVER, TCS_S_STEP, TCS_S_FIXED_DT, TCS_S_COUNT
+};
+
+typedef struct tcs_ctx tcs_ctx;
+typedef struct tcs_tdma_plan tcs_tdma_plan;
+
+/* ---- set-up: main.f90:82-125 ------------------------------------------- */
+/* global_inputpara + mpi_subdomain_make/mesh/indices + *_allocation/initial/boundary +
+ * mpi_pressure_wave_number + the initial ghost updates (main.f90:82-109). */
+int tcs_create(const tcs_config *cfg, tcs_ctx **out);
+int tcs_destroy(tcs_ctx *ctx);                                     /* *_clean (main.f90:234-241) */
+int tcs_set_stream(tcs_ctx *ctx, void *cuda_stream);               /* NULL: library-owned stream */
+void *tcs_get_stream(tcs_ctx *ctx);
+int tcs_dims(const tcs_ctx *ctx, int *padded3);                    /* (n1m+2, n2m+2, n3m+2) */
+int tcs_upload_field(tcs_ctx *ctx, int field, const double *host); /* blocking copy of a padded host array */
+int tcs_download_field(tcs_ctx *ctx, int field, double *host);
+int tcs_upload_field_async(tcs_ctx *ctx, int field, const double *pinned_host);   /* on the context stream */
+int tcs_download_field_async(tcs_ctx *ctx, int field, double *pinned_host);
+int tcs_field_device_ptr(tcs_ctx *ctx, int field, double **dev);   /* current device buffer */
+int tcs_synchronize(tcs_ctx *ctx);
+int tcs_set_dt(tcs_ctx *ctx, double dt);
+int tcs_get_metric(const tcs_ctx *ctx, int which, double *out);    /* x1,dx1,dmx1,x2,...,dmx3 (0..8) */
+
+/* ---- one time step, reference order (main.f90:133-221) ---------------- */
+int tcs_thermal_coeffi(tcs_ctx *ctx);                  /* module_solve_thermal.f90:116  (fused: no work) */
+int tcs_thermal_solver(tcs_ctx *ctx);                  /* module_solve_thermal.f90:175  (U,V,W are the context's) */
+int tcs_thermal_coeffi_clean(tcs_ctx *ctx);            /* module_solve_thermal.f90:161  (no work) */
+int tcs_subdomain_ghostcell_update(tcs_ctx *ctx, int field); /* module_mpi_subdomain.f90:758 */
+int tcs_momentum_coeffi(tcs_ctx *ctx);                 /* module_solve_momentum.f90:145 */
+int tcs_momentum_solvedU(tcs_ctx *ctx);                /* module_solve_momentum.f90:225 */
+int tcs_momentum_solvedV(tcs_ctx *ctx);                /* module_solve_momentum.f90:569 */
+int tcs_momentum_solvedW(tcs_ctx *ctx);                /* module_solve_momentum.f90:930 */
+int tcs_momentum_blockLdV(tcs_ctx *ctx);               /* module_solve_momentum.f90:1278 */
+int tcs_momentum_blockLdU(tcs_ctx *ctx);               /* module_solve_momentum.f90:1362 */
+int tcs_momentum_pseudoupdateUVW(tcs_ctx *ctx);        /* module_solve_momentum.f90:178 */
+int tcs_momentum_coeffi_clean(tcs_ctx *ctx);           /* module_solve_momentum.f90:213 (no work) */
+int tcs_pressure_RHS(tcs_ctx *ctx);                    /* module_solve_pressure.f90:140 */
+int tcs_pressure_Poisson_FFT2(tcs_ctx *ctx);           /* module_solve_pressure.f90:489 */
+int tcs_pressure_Projection(tcs_ctx *ctx);             /* module_solve_pressure.f90:756 */
+int tcs_post_div(tcs_ctx *ctx, double *maxDivU);       /* module_post.f90:100 (also computes CFL, Nu, KE) */
+int tcs_post_cfl(tcs_ctx *ctx, double *CFL, double *dt); /* module_post.f90:168 */
+
+/* Whole steps (main.f90:129-223) replayed from a CUDA graph; stops early on
+ * blow-up.  *done receives the number of completed steps. */
+int tcs_step(tcs_ctx *ctx, int nsteps, int *done);
+int tcs_get_scalars(tcs_ctx *ctx, double *out);        /* TCS_S_COUNT doubles */
+/* Per-step series recorded by tcs_step: 7 doubles per step
+ * (dt used, time, max divergence, CFL, Nu bottom, Nu top, kinetic energy). */
+int tcs_get_history(tcs_ctx *ctx, int first, int count, double *out);
+
+/* ---- PaScaL_TDMA many-systems interface (pascal_tdma.f90) ------------- */
+/* pascal_tdma.f90:185 PaScaL_TDMA_plan_many_create(plan, n_sys, myrank, nprocs, mpi_world).
+ * Only nprocs == 1 exists on one GPU; other values return TCS_ERR_UNSUPPORTED. */
+int tcs_tdma_plan_many_create(tcs_tdma_plan **plan, int n_sys, int myrank, int nprocs);
+/* pascal_tdma.f90:272 PaScaL_TDMA_plan_many_destroy(plan, nprocs) */
+int tcs_tdma_plan_many_destroy(tcs_tdma_plan *plan);
+/* pascal_tdma.f90:487 PaScaL_TDMA_many_solve(plan, A, B, C, D, n_sys, n_row): A,B,C,D are
+ * (n_sys, n_row), system index fastest, host or device pointers; D := solution,
+ * A and C are clobbered. */
+int tcs_tdma_many_solve(tcs_tdma_plan *plan, double *A, double *B, double *C, double *D, int n_sys, int n_row);
+/* pascal_tdma.f90:715 PaScaL_TDMA_many_solve_cycle(plan, A, B, C, D, n_sys, n_row) */
+int tcs_tdma_many_solve_cycle(tcs_tdma_plan *plan, double *A, double *B, double *C, double *D, int n_sys, int n_row);
+
+/* ---- measurement --------------------------------------------------------- */
+int tcs_kernel_count(void);
+unsigned long long tcs_launch_count(void);           /* kernels this library has launched so far */
+const char *tcs_kernel_name(int kernel_id);
+/* Record a CUDA event pair around every launch of the kernels in mask (bit =
+ * kernel id) on the launching stream; tcs_probe_read returns their summed
+ * device time.  Probed steps run without the CUDA graph. */
+int tcs_probe_enable(tcs_ctx *ctx, uint64_t mask);
+int tcs_probe_read(tcs_ctx *ctx, int kernel_id, double *total_ms, int *launches);
+int tcs_probe_reset(tcs_ctx *ctx);
+int tcs_set_use_graph(tcs_ctx *ctx, int on);
+const char *tcs_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,8 @@
+"""pascal_tcs_b200 -- the PaScaL_TCS per-timestep hot path (energy and momentum
+ADI sweeps, FFT pressure Poisson solve, projection and diagnostics) as CUDA
+kernels for one B200, behind the C ABI of include/tcs.h."""
+from .tcs import (EXPORTS, FIELDS, HISTORY, LIB_PATH, SCALARS, Solver, TcsConfig,  # noqa: F401
+                  TcsError, TdmaPlan, default_config, kernel_names, launch_count, load)
+
+__all__ = ["Solver", "TdmaPlan", "TcsError", "TcsConfig", "default_config", "kernel_names", "launch_count", "load",
+           "FIELDS", "SCALARS", "HISTORY", "EXPORTS", "LIB_PATH"]

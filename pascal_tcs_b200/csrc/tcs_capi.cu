@@ -1,0 +1,899 @@
+// tcs_capi.cu -- host runtime and C ABI of libtcs (declared in include/tcs.h).
+//
+// Owns one case: the host-side mesh (mpi_subdomain_mesh), the device fields,
+// the stage sequence of main.f90:129-223, CUDA-graph replay of whole steps,
+// CUDA-event probes and the PaScaL_TDMA many-systems plans.
+#include "tcs_kernels.h"
+#include "tcs.h"
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <utility>
+#include <vector>
+
+namespace tcs {
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+static thread_local std::string g_err;
+static thread_local int g_launch_err = 0;
+static unsigned long long g_launches = 0;   // kernels launched by this library (graph replays included)
+
+static int set_err(int code, const std::string &msg)
+{
+    g_err = msg;
+    return code;
+}
+
+int record_launch_error(const char *what)
+{
+    g_launches++;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        g_launch_err = 1;
+        g_err = std::string("launch of ") + what + " failed: " + cudaGetErrorString(e);
+    }
+    return e == cudaSuccess ? 0 : 1;
+}
+
+static int take_launch_error()
+{
+    const int e = g_launch_err;
+    g_launch_err = 0;
+    return e ? TCS_ERR_CUDA : TCS_OK;
+}
+
+#define CK(call)                                                                                   \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess)                                                                     \
+            return set_err(TCS_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));      \
+    } while (0)
+
+static const char *const k_names[K_COUNT] = {
+    "thermal_z", "thermal_x", "thermal_y", "momentum_coeffi",
+    "du_z", "du_x", "du_y", "dv_z", "dv_x", "dv_y", "dw_z", "dw_x", "dw_y",
+    "blockld_v", "blockld_u", "pseudo_update", "prhs_fftx", "fftz_fwd", "modal_tdma", "mean",
+    "fftz_inv", "ifftx", "dp_wall", "projection", "post", "finalize", "tdma_api"};
+
+const char *kernel_name(int kid) { return (kid >= 0 && kid < K_COUNT) ? k_names[kid] : "?"; }
+
+// ---------------------------------------------------------------------------
+// probes: CUDA event pairs on the launching stream
+// ---------------------------------------------------------------------------
+struct ProbeState {
+    uint64_t mask = 0;
+    std::vector<cudaEvent_t> pool;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> rec[K_COUNT];
+    cudaEvent_t pending[K_COUNT] = {};
+    cudaEvent_t take()
+    {
+        if (!pool.empty()) { cudaEvent_t e = pool.back(); pool.pop_back(); return e; }
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        return e;
+    }
+};
+
+void probe_begin(const Ctx &cx, int kid, cudaStream_t s)
+{
+    ProbeState *p = cx.probe;
+    if (!p || !(p->mask & (1ull << kid))) return;
+    p->pending[kid] = p->take();
+    cudaEventRecord(p->pending[kid], s);
+}
+
+void probe_end(const Ctx &cx, int kid, cudaStream_t s)
+{
+    ProbeState *p = cx.probe;
+    if (!p || !(p->mask & (1ull << kid)) || !p->pending[kid]) return;
+    cudaEvent_t e = p->take();
+    cudaEventRecord(e, s);
+    p->rec[kid].push_back({p->pending[kid], e});
+    p->pending[kid] = nullptr;
+}
+
+// ---------------------------------------------------------------------------
+// plans
+// ---------------------------------------------------------------------------
+LinePlan make_line_plan(int n, bool cyclic, int TL)
+{
+    LinePlan lp;
+    int P;
+    if (cyclic) { P = 1; while (P * 2 <= 32 && n / (P * 2) >= 2) P *= 2; }
+    else { P = n / 2; if (P > 32) P = 32; if (P < 1) P = 1; }
+    lp.n = n; lp.P = P; lp.m0 = n / P; lp.rem = n % P;
+    const int mmax = lp.m0 + (lp.rem > 0 ? 1 : 0);
+    lp.PS = mmax | 1;
+    lp.LS = (P * lp.PS) | 1;
+    lp.TL = TL;
+    lp.cyclic = cyclic ? 1 : 0;
+    return lp;
+}
+
+static int choose_tl(int n, bool cyclic, int nrhs, int want)
+{
+    LinePlan lp = make_line_plan(n, cyclic, want);
+    int tl = want;
+    while (tl > 2 && (size_t)(2 + nrhs) * tl * lp.LS * sizeof(double) > 112 * 1024) tl /= 2;
+    return tl;
+}
+
+bool make_fft_plan(int n, FFTPlan &fp)
+{
+    fp.n = n; fp.npass = 0;
+    int m = n;
+    while (m % 4 == 0 && fp.npass < 24) { fp.radix[fp.npass++] = 4; m /= 4; }
+    while (m % 2 == 0 && fp.npass < 24) { fp.radix[fp.npass++] = 2; m /= 2; }
+    while (m % 3 == 0 && fp.npass < 24) { fp.radix[fp.npass++] = 3; m /= 3; }
+    while (m % 5 == 0 && fp.npass < 24) { fp.radix[fp.npass++] = 5; m /= 5; }
+    return m == 1;
+}
+
+} // namespace tcs
+
+using namespace tcs;
+
+// ---------------------------------------------------------------------------
+// the context
+// ---------------------------------------------------------------------------
+struct tcs_ctx {
+    tcs_config cfg;
+    Ctx cx;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    std::vector<double> hm[9];           // x1, dx1, dmx1, x2, dx2, dmx2, x3, dx3, dmx3
+    std::vector<void *> allocs;
+    uint32_t ghost_ok = 0;               // bit per field id: periodic ghosts are current
+    bool pending_pseudo = false;
+    bool use_graph = true;
+    struct GraphEntry { const double *T, *U, *dPhat; cudaGraphExec_t exec; unsigned long long kernels; };
+    std::vector<GraphEntry> graphs;
+    ProbeState probe;
+    int partials = 0;
+};
+
+namespace tcs {
+int post_partial_count();
+void launch_tdma_many(double *A, const double *B, double *C, double *D, int n_sys, int n_row, int cyclic, cudaStream_t s);
+} // namespace tcs
+
+static void mesh_periodic(int uniform, double L, double gamma, int nm, std::vector<double> &x, std::vector<double> &dx, std::vector<double> &dmx)
+{
+    // mpi_subdomain_mesh for a periodic direction on one rank (module_mpi_subdomain.f90:167-209)
+    const int nsub = nm + 1;
+    x.assign(nsub + 1, 0.0); dx.assign(nsub + 1, 0.0); dmx.assign(nsub + 1, 0.0);
+    for (int i = 0; i <= nsub; i++) {
+        if (uniform == 1) x[i] = (double)(i - 1) * L / (double)nm + 0.0;
+        else x[i] = L * 0.5 * (1.0 + std::tanh(0.5 * gamma * (2.0 * (double)(i - 1) / (double)nm - 1.0)) / std::tanh(gamma * 0.5)) + 0.0;
+    }
+    for (int i = 1; i <= nsub - 1; i++) dx[i] = x[i + 1] - x[i];
+    dx[0] = dx[nsub - 1]; dx[nsub] = dx[1];
+    for (int i = 1; i <= nsub - 1; i++) dmx[i] = 0.5 * (dx[i - 1] + dx[i]);
+    dmx[0] = dmx[nsub - 1]; dmx[nsub] = dmx[1];
+}
+
+static void mesh_wall(int uniform, double L, double gamma, int nm, std::vector<double> &x, std::vector<double> &dx, std::vector<double> &dmx)
+{
+    // the wall-bounded y direction (module_mpi_subdomain.f90:211-253)
+    const int nsub = nm + 1;
+    x.assign(nsub + 1, 0.0); dx.assign(nsub + 1, 0.0); dmx.assign(nsub + 1, 0.0);
+    for (int j = 0; j <= nsub; j++) {
+        if (uniform == 1) x[j] = (double)(j - 1) * L / (double)nm + 0.0;
+        else x[j] = L * 0.5 * (1. + std::tanh(0.5 * gamma * (2. * (double)(j - 1) / (double)nm - 1.0)) / std::tanh(gamma * 0.5)) + 0.0;
+    }
+    x[0] = x[1];
+    for (int j = 1; j <= nsub - 1; j++) dx[j] = x[j + 1] - x[j];
+    dx[0] = 0.0; dx[nsub] = 0.0;
+    for (int j = 1; j <= nsub - 1; j++) dmx[j] = 0.5 * (dx[j - 1] + dx[j]);
+    dmx[0] = 0.0;
+    dmx[nsub] = 0.5 * (dx[nsub - 1] + dx[nsub]);
+}
+
+static void set_properties(const tcs_config &c, Phys &p)
+{
+    // module_global.f90:107-141
+    p.Uup = p.Ubt = p.Vup = p.Vbt = p.Wup = p.Wbt = 0.0;
+    p.Tup = -0.5; p.Tbt = 0.5;
+    if (c.property_set == 1) {
+        p.a10 = 0.9922e+3; p.a11 = -3.736e-4; p.a12 = -3.98e-6; p.a13 = 0.; p.a14 = 0.; p.a15 = 0.;
+        p.b10 = 4.1690e+3; p.b11 = 0.084e-4; p.b12 = 4.60e-6; p.b13 = 0.; p.b14 = 0.; p.b15 = 0.;
+        p.c10 = (double)0.6297f; p.c11 = 21.99e-4; p.c12 = -17.8e-6; p.c13 = 0.; p.c14 = 0.; p.c15 = 0.;
+        p.d10 = 0.6690e-6; p.d11 = -175.9e-4; p.d12 = 295.8e-6; p.d13 = -460.e-8; p.d14 = 0.; p.d15 = 0.;
+    } else if (c.property_set == 2) {
+        p.a10 = 1.2477e+3; p.a11 = -4.789e-4; p.a12 = -0.3795e-6; p.a13 = 0.; p.a14 = 0.; p.a15 = 0.;
+        p.b10 = 2.5108e+3; p.b11 = 22.511e-4; p.b12 = 0.; p.b13 = 0.; p.b14 = 0.; p.b15 = 0.;
+        p.c10 = 2.9351e-3; p.c11 = 3.863e-4; p.c12 = 0.; p.c13 = 0.; p.c14 = 0.; p.c15 = 0.;
+        p.d10 = 238.71e-6; p.d11 = -702.83e-4; p.d12 = 2393.1e-6; p.d13 = -6923.0e-8; p.d14 = 33131.3e-10; p.d15 = -71517.5e-12;
+    } else {
+        p.a10 = 1.0; p.a11 = 0.0; p.a12 = 0.0; p.a13 = 0.0; p.a14 = 0.; p.a15 = 0.;
+        p.b10 = 1.0; p.b11 = 0.0; p.b12 = 0.0; p.b13 = 0.0; p.b14 = 0.; p.b15 = 0.;
+        p.c10 = 1.0; p.c11 = 0.0; p.c12 = 0.0; p.c13 = 0.0; p.c14 = 0.; p.c15 = 0.;
+        p.d10 = 1.0; p.d11 = 0.0; p.d12 = 0.0; p.d13 = 0.0; p.d14 = 0.; p.d15 = 0.;
+    }
+    p.a12pera11 = (p.a12 < 1.0e-14) ? 0.0 : p.a12 / p.a11;
+    p.Rho0 = p.a10; p.Cp0 = p.b10; p.KPP0 = p.c10; p.Mu0 = p.a10 * p.d10;
+    p.Cmu = std::sqrt(c.Pr / c.Ra); p.Cmt = 1.0; p.Ct = 1.0 / std::sqrt(c.Ra * c.Pr); p.Cmp = 1.0;
+    p.DeltaT = c.DeltaT; p.MaxCFL = c.MaxCFL;
+    p.L1 = c.H * c.aspect1; p.L2 = c.H; p.L3 = c.H * c.aspect3;
+    const double t1 = p.L1 / (double)c.n1m, t2 = p.L2 / (double)c.n2m, t3 = p.L3 / (double)c.n3m;
+    double mn = t1; if (t2 < mn) mn = t2; if (t3 < mn) mn = t3;
+    p.dtMax = mn * 100;
+}
+
+static uint64_t splitmix64_mix(uint64_t z)
+{
+    z += 0x9E3779B97F4A7C15ULL;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    return z ^ (z >> 31);
+}
+
+template <class T>
+static int dalloc(tcs_ctx *c, T **p, size_t n)
+{
+    void *q = nullptr;
+    cudaError_t e = cudaMalloc(&q, n * sizeof(T) ? n * sizeof(T) : 16);
+    if (e != cudaSuccess) return set_err(TCS_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    c->allocs.push_back(q);
+    cudaMemsetAsync(q, 0, n * sizeof(T), c->stream);
+    *p = (T *)q;
+    return TCS_OK;
+}
+
+template <class T>
+static int upload_vec(tcs_ctx *c, const std::vector<T> &v, const T **out)
+{
+    T *d;
+    int r = dalloc(c, &d, v.size());
+    if (r) return r;
+    CK(cudaMemcpyAsync(d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, c->stream));
+    *out = d;
+    return TCS_OK;
+}
+
+static void host_ghost(std::vector<double> &a, int N1, int N2, int N3)
+{
+    const size_t P1 = N1 + 2, P2 = N2 + 2;
+    auto I = [&](int i, int j, int k) { return (size_t)i + P1 * ((size_t)j + P2 * (size_t)k); };
+    for (int k = 0; k <= N3 + 1; k++)
+        for (int j = 0; j <= N2 + 1; j++) { a[I(0, j, k)] = a[I(N1, j, k)]; a[I(N1 + 1, j, k)] = a[I(1, j, k)]; }
+    for (int j = 0; j <= N2 + 1; j++)
+        for (int i = 0; i <= N1 + 1; i++) { a[I(i, j, 0)] = a[I(i, j, N3)]; a[I(i, j, N3 + 1)] = a[I(i, j, 1)]; }
+}
+
+static double *field_ptr(tcs_ctx *c, int f)
+{
+    Fields &F = c->cx.f;
+    switch (f) {
+    case TCS_F_T: return F.T; case TCS_F_U: return F.U; case TCS_F_V: return F.V; case TCS_F_W: return F.W;
+    case TCS_F_P: return F.P; case TCS_F_DPHAT: return F.dPhat; case TCS_F_DP0: return F.dP0;
+    case TCS_F_DU: return F.dU; case TCS_F_DV: return F.dV; case TCS_F_DW: return F.dW; case TCS_F_DP: return F.dP;
+    default: return nullptr;
+    }
+}
+
+static int flush_pending(tcs_ctx *c)
+{
+    if (!c->pending_pseudo) return TCS_OK;
+    launch_pseudo_update(c->cx, c->stream);
+    std::swap(c->cx.f.U, c->cx.f.Un); std::swap(c->cx.f.V, c->cx.f.Vn); std::swap(c->cx.f.W, c->cx.f.Wn);
+    c->pending_pseudo = false;
+    return take_launch_error();
+}
+
+extern "C" {
+
+const char *tcs_last_error(void) { return g_err.c_str(); }
+int tcs_kernel_count(void) { return K_COUNT; }
+unsigned long long tcs_launch_count(void) { return g_launches; }
+const char *tcs_kernel_name(int kid) { return kernel_name(kid); }
+
+int tcs_create(const tcs_config *cfg, tcs_ctx **out)
+{
+    if (!cfg || !out) return set_err(TCS_ERR_ARG, "null argument");
+    *out = nullptr;
+    if (cfg->n1m < 4 || cfg->n2m < 4 || cfg->n3m < 4) return set_err(TCS_ERR_ARG, "every n_m must be >= 4");
+    if ((long long)(cfg->n1m + 2) * (cfg->n2m + 2) * (cfg->n3m + 2) > (1ll << 31))
+        return set_err(TCS_ERR_UNSUPPORTED, "padded grid exceeds 2^31 cells");
+    if (cfg->n1m > 4096 || cfg->n3m > 4096 || cfg->n2m > 4096) return set_err(TCS_ERR_UNSUPPORTED, "an axis exceeds 4096 cells");
+    FFTPlan fp1, fp3;
+    if (!make_fft_plan(cfg->n1m, fp1) || !make_fft_plan(cfg->n3m, fp3))
+        return set_err(TCS_ERR_UNSUPPORTED, "n1m and n3m must factor into 2, 3 and 5 (FFT radices)");
+    CK(cudaSetDevice(cfg->device));
+    tcs_ctx *c = new tcs_ctx();
+    c->cfg = *cfg;
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) { delete c; return set_err(TCS_ERR_CUDA, "stream"); }
+    c->own_stream = true;
+    const int N1 = cfg->n1m, N2 = cfg->n2m, N3 = cfg->n3m;
+    Grid &g = c->cx.g;
+    g.N1 = N1; g.N2 = N2; g.N3 = N3; g.P1 = N1 + 2; g.P2 = N2 + 2;
+    g.NP = (long long)(N1 + 2) * (N2 + 2) * (N3 + 2);
+    set_properties(*cfg, g.ph);
+    mesh_periodic(cfg->uniform1, g.ph.L1, cfg->gamma1, N1, c->hm[0], c->hm[1], c->hm[2]);
+    mesh_wall(cfg->uniform2, g.ph.L2, cfg->gamma2, N2, c->hm[3], c->hm[4], c->hm[5]);
+    mesh_periodic(cfg->uniform3, g.ph.L3, cfg->gamma3, N3, c->hm[6], c->hm[7], c->hm[8]);
+    // fix dtMax with the reference formula on n - 1 = n_m (module_global.f90:161-165)
+    int r = TCS_OK;
+    Metric *ms[3] = {&g.m1, &g.m2, &g.m3};
+    for (int d = 0; d < 3 && !r; d++) {
+        const std::vector<double> &dx = c->hm[3 * d + 1], &dmx = c->hm[3 * d + 2];
+        std::vector<double> rdx(dx.size()), rdmx(dmx.size());
+        for (size_t q = 0; q < dx.size(); q++) { rdx[q] = dx[q] != 0.0 ? 1.0 / dx[q] : 0.0; rdmx[q] = dmx[q] != 0.0 ? 1.0 / dmx[q] : 0.0; }
+        r = r ? r : upload_vec(c, dx, &ms[d]->dx);
+        r = r ? r : upload_vec(c, dmx, &ms[d]->dmx);
+        r = r ? r : upload_vec(c, rdx, &ms[d]->rdx);
+        r = r ? r : upload_vec(c, rdmx, &ms[d]->rdmx);
+    }
+    Fields &F = c->cx.f;
+    const size_t NP = (size_t)g.NP;
+    double **fl[] = {&F.T, &F.U, &F.V, &F.W, &F.P, &F.dPhat, &F.dP0, &F.Tn, &F.Un, &F.Vn, &F.Wn, &F.dPhatn, &F.dP0n,
+                     &F.dU, &F.dV, &F.dW, &F.dP, &F.R};
+    for (double **p : fl) if (!r) r = dalloc(c, p, NP);
+    if (!r) r = dalloc(c, &F.Mu2, (size_t)(N2 + 2) * (N3 + 2));
+    if (!r) r = dalloc(c, &F.iR2, (size_t)(N2 + 2) * (N3 + 2));
+    c->cx.h1p = N1 / 2 + 1;
+    if (!r) r = dalloc(c, &F.S, (size_t)c->cx.h1p * N2 * N3);
+    if (!r) r = dalloc(c, &g.scal, (size_t)S_NSCAL);
+    c->partials = post_partial_count();
+    if (!r) r = dalloc(c, &F.part, (size_t)c->partials);
+    F.hist_cap = 100000;
+    if (!r) r = dalloc(c, &F.hist, (size_t)F.hist_cap * 7);
+    if (r) { tcs_destroy(c); return r; }
+
+    // wavenumbers (module_solve_pressure.f90:93-129) and modal y coefficients (:599-609)
+    const double PI = std::acos(-1.0), ddx = g.ph.L1 / (double)N1, ddz = g.ph.L3 / (double)N3;
+    const int h3p = N3 / 2 + 1;
+    std::vector<double> dzk(N3), dxk2(c->cx.h1p), fam(N2 + 2, 0.0), fap(N2 + 2, 0.0);
+    for (int k = 1; k <= N3; k++) {
+        const int km = (k <= h3p) ? k - 1 : N3 - k + 1;
+        dzk[k - 1] = 2.0 * (1.0 - std::cos(2.0 * PI * (double)km * ddz / g.ph.L3)) / (ddz * ddz);
+    }
+    for (int i = 1; i <= c->cx.h1p; i++) dxk2[i - 1] = 2.0 * (1.0 - std::cos(2.0 * PI * (double)(i - 1) * ddx / g.ph.L1)) / (ddx * ddx);
+    const std::vector<double> &dx2 = c->hm[4], &dmx2 = c->hm[5];
+    for (int j = 1; j <= N2; j++) {
+        fam[j] = (j == 1) ? 0.0 : 1.0 / dx2[j] / dmx2[j];
+        fap[j] = (j == N2) ? 0.0 : 1.0 / dx2[j] / dmx2[j + 1];
+    }
+    r = r ? r : upload_vec(c, dzk, &F.dzk);
+    r = r ? r : upload_vec(c, dxk2, &F.dxk2);
+    r = r ? r : upload_vec(c, fam, &F.fam);
+    r = r ? r : upload_vec(c, fap, &F.fap);
+    auto twid = [](int n) {
+        std::vector<double2> w(n);
+        for (int e = 0; e < n; e++) w[e] = make_double2(std::cos(2.0 * M_PI * (double)e / (double)n), -std::sin(2.0 * M_PI * (double)e / (double)n));
+        return w;
+    };
+    r = r ? r : upload_vec(c, twid(N1), &F.tw1);
+    r = r ? r : upload_vec(c, twid(N3), &F.tw3);
+    {   // Pbc_a, Pbc_b (module_solve_pressure.f90:720-730)
+        const int n2sub = N2 + 1, n2msub = N2;
+        const double s1 = (dmx2[1] + dmx2[2]) * (dmx2[1] + dmx2[2]);
+        c->cx.wall_ab = s1 / (s1 - dmx2[1] * dmx2[1]);
+        c->cx.wall_bb = dmx2[1] * dmx2[1] / (s1 - dmx2[1] * dmx2[1]);
+        const double s2 = (dmx2[n2sub] + dmx2[n2msub]) * (dmx2[n2sub] + dmx2[n2msub]);
+        c->cx.wall_at = s2 / (s2 - dmx2[n2sub] * dmx2[n2sub]);
+        c->cx.wall_bt = dmx2[n2sub] * dmx2[n2sub] / (s2 - dmx2[n2sub] * dmx2[n2sub]);
+    }
+    c->cx.fp1 = fp1; c->cx.fp3 = fp3;
+    c->cx.tl_strided = 8;
+    c->cx.tl_contig = choose_tl(N1, true, 1, 8);
+    c->cx.tl_modal = choose_tl(N2, false, 2, 8);
+    {
+        const int tz = choose_tl(N3, true, 1, 8), ty = choose_tl(N2, false, 1, 8);
+        c->cx.tl_strided = tz < ty ? tz : ty;
+    }
+    c->cx.fft_lines_x = N1 <= 256 ? 8 : (N1 <= 512 ? 4 : 2);
+    c->cx.fft_lines_z = N3 <= 256 ? 8 : (N3 <= 512 ? 4 : 2);
+    c->cx.probe = &c->probe;
+
+    // initial fields: mpi_thermal_initial/boundary, mpi_momentum_initial/boundary,
+    // mpi_pressure_initial, then ghost(T,U,V,W,P) (main.f90:92-109)
+    std::vector<double> T(NP, 0.0);
+    const size_t P1 = N1 + 2, P2 = N2 + 2;
+    auto I = [&](int i, int j, int k) { return (size_t)i + P1 * ((size_t)j + P2 * (size_t)k); };
+    for (int k = 0; k <= N3 + 1; k++)
+        for (int i = 0; i <= N1 + 1; i++) {
+            T[I(i, 0, k)] = g.ph.Tbt;
+            if (cfg->top_wall_mode) T[I(i, N2 + 1, k)] = g.ph.Tup;
+        }
+    if (cfg->init_mode == 0) {
+        const uint64_t base = splitmix64_mix(cfg->seed);
+        const std::vector<double> &x2 = c->hm[3];
+        for (int k = 1; k <= N3; k++)
+            for (int j = 1; j <= N2; j++) {
+                const double yc = 0.5 * (x2[j] + x2[j + 1]);
+                for (int i = 1; i <= N1; i++) {
+                    const uint64_t z = splitmix64_mix(base ^ (uint64_t)I(i, j, k));
+                    const double u = (double)(z >> 11) * (1.0 / 9007199254740992.0);
+                    T[I(i, j, k)] = 0.5 - yc + cfg->noise_amp * (2.0 * u - 1.0);
+                }
+            }
+    }
+    host_ghost(T, N1, N2, N3);
+    if (!r) {
+        cudaMemcpyAsync(F.T, T.data(), NP * sizeof(double), cudaMemcpyHostToDevice, c->stream);
+        cudaMemcpyAsync(F.Tn, T.data(), NP * sizeof(double), cudaMemcpyHostToDevice, c->stream);
+        double sc[S_NSCAL] = {0};
+        sc[S_DT] = cfg->dtStart; sc[S_TIME] = cfg->tStart; sc[S_CFL] = cfg->MaxCFL;
+        sc[S_FIXED_DT] = cfg->fixed_dt ? 1.0 : 0.0;
+        cudaMemcpyAsync(g.scal, sc, sizeof(sc), cudaMemcpyHostToDevice, c->stream);
+        if (cudaStreamSynchronize(c->stream) != cudaSuccess) r = set_err(TCS_ERR_CUDA, "initial upload");
+    }
+    if (r) { tcs_destroy(c); return r; }
+    c->ghost_ok = 0xffffffffu;
+    *out = c;
+    return TCS_OK;
+}
+
+int tcs_destroy(tcs_ctx *c)
+{
+    if (!c) return TCS_ERR_ARG;
+    cudaSetDevice(c->cfg.device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    for (auto &ge : c->graphs) cudaGraphExecDestroy(ge.exec);
+    for (void *p : c->allocs) cudaFree(p);
+    for (auto &v : c->probe.rec) for (auto &pr : v) { cudaEventDestroy(pr.first); cudaEventDestroy(pr.second); }
+    for (cudaEvent_t e : c->probe.pool) cudaEventDestroy(e);
+    if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return TCS_OK;
+}
+
+int tcs_set_stream(tcs_ctx *c, void *s)
+{
+    if (!c) return set_err(TCS_ERR_ARG, "null context");
+    CK(cudaStreamSynchronize(c->stream));
+    if (c->own_stream) cudaStreamDestroy(c->stream);
+    if (s) { c->stream = (cudaStream_t)s; c->own_stream = false; }
+    else { CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)); c->own_stream = true; }
+    for (auto &ge : c->graphs) cudaGraphExecDestroy(ge.exec);
+    c->graphs.clear();
+    return TCS_OK;
+}
+
+void *tcs_get_stream(tcs_ctx *c) { return c ? (void *)c->stream : nullptr; }
+
+int tcs_dims(const tcs_ctx *c, int *d)
+{
+    if (!c || !d) return set_err(TCS_ERR_ARG, "null argument");
+    d[0] = c->cx.g.N1 + 2; d[1] = c->cx.g.N2 + 2; d[2] = c->cx.g.N3 + 2;
+    return TCS_OK;
+}
+
+int tcs_get_metric(const tcs_ctx *c, int which, double *out)
+{
+    if (!c || !out || which < 0 || which > 8) return set_err(TCS_ERR_ARG, "bad metric");
+    std::memcpy(out, c->hm[which].data(), c->hm[which].size() * sizeof(double));
+    return TCS_OK;
+}
+
+static int copy_field(tcs_ctx *c, int f, double *host, bool up, bool async)
+{
+    if (!c || !host) return set_err(TCS_ERR_ARG, "null argument");
+    cudaSetDevice(c->cfg.device);
+    int r = flush_pending(c);
+    if (r) return r;
+    const size_t NP = (size_t)c->cx.g.NP;
+    const Grid &g = c->cx.g;
+    if (f == TCS_F_MU || f == TCS_F_INVRHO) {
+        if (up) return set_err(TCS_ERR_ARG, "Mu and invRho are derived from T");
+        std::vector<double> t((size_t)(g.N2 + 2) * (g.N3 + 2));
+        CK(cudaMemcpyAsync(t.data(), f == TCS_F_MU ? c->cx.f.Mu2 : c->cx.f.iR2, t.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        for (int k = 0; k < g.N3 + 2; k++)
+            for (int j = 0; j < g.N2 + 2; j++)
+                for (int i = 0; i < g.N1 + 2; i++) host[(size_t)i + (size_t)g.P1 * ((size_t)j + (size_t)g.P2 * k)] = t[j + (size_t)g.P2 * k];
+        return TCS_OK;
+    }
+    double *d = field_ptr(c, f);
+    if (!d) return set_err(TCS_ERR_ARG, "unknown field");
+    if (up) {
+        CK(cudaMemcpyAsync(d, host, NP * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        if (f == TCS_F_T) CK(cudaMemcpyAsync(c->cx.f.Tn, host, NP * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        c->ghost_ok &= ~(1u << f);
+    } else {
+        CK(cudaMemcpyAsync(host, d, NP * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    }
+    if (!async) CK(cudaStreamSynchronize(c->stream));
+    return TCS_OK;
+}
+
+int tcs_upload_field(tcs_ctx *c, int f, const double *h) { return copy_field(c, f, (double *)h, true, false); }
+int tcs_download_field(tcs_ctx *c, int f, double *h) { return copy_field(c, f, h, false, false); }
+int tcs_upload_field_async(tcs_ctx *c, int f, const double *h) { return copy_field(c, f, (double *)h, true, true); }
+int tcs_download_field_async(tcs_ctx *c, int f, double *h) { return copy_field(c, f, h, false, true); }
+
+int tcs_field_device_ptr(tcs_ctx *c, int f, double **dev)
+{
+    if (!c || !dev) return set_err(TCS_ERR_ARG, "null argument");
+    int r = flush_pending(c);
+    if (r) return r;
+    *dev = field_ptr(c, f);
+    return *dev ? TCS_OK : set_err(TCS_ERR_ARG, "unknown field");
+}
+
+int tcs_synchronize(tcs_ctx *c)
+{
+    if (!c) return set_err(TCS_ERR_ARG, "null context");
+    CK(cudaStreamSynchronize(c->stream));
+    return TCS_OK;
+}
+
+int tcs_set_dt(tcs_ctx *c, double dt)
+{
+    if (!c || !(dt > 0.0)) return set_err(TCS_ERR_ARG, "dt must be positive");
+    CK(cudaMemcpyAsync(c->cx.g.scal + S_DT, &dt, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return TCS_OK;
+}
+
+// ---- stages ---------------------------------------------------------------
+#define ENTER(c)                                                   \
+    if (!(c)) return set_err(TCS_ERR_ARG, "null context");        \
+    cudaSetDevice((c)->cfg.device);
+
+int tcs_thermal_coeffi(tcs_ctx *c) { ENTER(c); return TCS_OK; }
+int tcs_thermal_coeffi_clean(tcs_ctx *c) { ENTER(c); return TCS_OK; }
+int tcs_momentum_coeffi_clean(tcs_ctx *c) { ENTER(c); return TCS_OK; }
+
+static void ensure_ghosts(tcs_ctx *c, int f)
+{
+    if (c->ghost_ok & (1u << f)) return;
+    launch_ghost(c->cx, field_ptr(c, f), c->stream);
+    c->ghost_ok |= (1u << f);
+}
+
+int tcs_subdomain_ghostcell_update(tcs_ctx *c, int f)
+{
+    ENTER(c);
+    if (f < 0 || f >= TCS_F_MU) return set_err(TCS_ERR_ARG, "unknown field");
+    // while the pseudo-update is deferred into the pressure RHS, U/V/W ghosts
+    // are written by that fused kernel
+    if (c->pending_pseudo && (f == TCS_F_U || f == TCS_F_V || f == TCS_F_W)) return TCS_OK;
+    int r = flush_pending(c);
+    if (r) return r;
+    ensure_ghosts(c, f);
+    return take_launch_error();
+}
+
+int tcs_thermal_solver(tcs_ctx *c)
+{
+    ENTER(c);
+    int r = flush_pending(c);
+    if (r) return r;
+    ensure_ghosts(c, TCS_F_T); ensure_ghosts(c, TCS_F_U); ensure_ghosts(c, TCS_F_V); ensure_ghosts(c, TCS_F_W);
+    launch_thermal(c->cx, c->stream);
+    std::swap(c->cx.f.T, c->cx.f.Tn);
+    return take_launch_error();
+}
+
+int tcs_momentum_coeffi(tcs_ctx *c)
+{
+    ENTER(c);
+    int r = flush_pending(c);
+    if (r) return r;
+    ensure_ghosts(c, TCS_F_T);
+    launch_momentum_coeffi(c->cx, c->stream);
+    return take_launch_error();
+}
+
+#define SIMPLE_STAGE(name, launcher, outfield)                  \
+    int name(tcs_ctx *c)                                        \
+    {                                                           \
+        ENTER(c);                                               \
+        int r = flush_pending(c);                               \
+        if (r) return r;                                        \
+        launcher(c->cx, c->stream);                             \
+        if ((outfield) >= 0) c->ghost_ok |= (1u << (outfield)); \
+        return take_launch_error();                             \
+    }
+SIMPLE_STAGE(tcs_momentum_solvedU, launch_solve_du, TCS_F_DU)
+SIMPLE_STAGE(tcs_momentum_solvedV, launch_solve_dv, TCS_F_DV)
+SIMPLE_STAGE(tcs_momentum_solvedW, launch_solve_dw, TCS_F_DW)
+SIMPLE_STAGE(tcs_momentum_blockLdV, launch_blockld_v, TCS_F_DV)
+#undef SIMPLE_STAGE
+
+int tcs_momentum_blockLdU(tcs_ctx *c)
+{
+    ENTER(c);
+    int r = flush_pending(c);
+    if (r) return r;
+    launch_blockld_u(c->cx, c->stream);
+    c->ghost_ok &= ~(1u << TCS_F_DU);   // the reference leaves dU's ghosts stale here
+    return take_launch_error();
+}
+
+int tcs_momentum_pseudoupdateUVW(tcs_ctx *c)
+{
+    ENTER(c);
+    int r = flush_pending(c);
+    if (r) return r;
+    c->pending_pseudo = true;          // executed inside tcs_pressure_RHS
+    c->ghost_ok |= (1u << TCS_F_U) | (1u << TCS_F_V) | (1u << TCS_F_W);
+    return TCS_OK;
+}
+
+int tcs_pressure_RHS(tcs_ctx *c)
+{
+    ENTER(c);
+    ensure_ghosts(c, TCS_F_DPHAT);
+    if (c->pending_pseudo) {
+        launch_pseudo_prhs_fftx(c->cx, c->stream, true);
+        std::swap(c->cx.f.U, c->cx.f.Un); std::swap(c->cx.f.V, c->cx.f.Vn); std::swap(c->cx.f.W, c->cx.f.Wn);
+        c->pending_pseudo = false;
+    } else {
+        ensure_ghosts(c, TCS_F_U); ensure_ghosts(c, TCS_F_V); ensure_ghosts(c, TCS_F_W);
+        launch_pseudo_prhs_fftx(c->cx, c->stream, false);
+    }
+    return take_launch_error();
+}
+
+int tcs_pressure_Poisson_FFT2(tcs_ctx *c)
+{
+    ENTER(c);
+    int r = flush_pending(c);
+    if (r) return r;
+    launch_poisson_rest(c->cx, c->stream);
+    c->ghost_ok |= (1u << TCS_F_DP);
+    return take_launch_error();
+}
+
+int tcs_pressure_Projection(tcs_ctx *c)
+{
+    ENTER(c);
+    int r = flush_pending(c);
+    if (r) return r;
+    ensure_ghosts(c, TCS_F_DPHAT);
+    launch_projection(c->cx, c->stream);
+    std::swap(c->cx.f.dPhat, c->cx.f.dPhatn); std::swap(c->cx.f.dP0, c->cx.f.dP0n);
+    c->ghost_ok |= (1u << TCS_F_U) | (1u << TCS_F_V) | (1u << TCS_F_W) | (1u << TCS_F_P) | (1u << TCS_F_DPHAT);
+    return take_launch_error();
+}
+
+int tcs_post_div(tcs_ctx *c, double *maxDivU)
+{
+    ENTER(c);
+    int r = flush_pending(c);
+    if (r) return r;
+    launch_post(c->cx, c->stream, 1);
+    if ((r = take_launch_error())) return r;
+    double sc[S_NSCAL];
+    CK(cudaMemcpyAsync(sc, c->cx.g.scal, sizeof(sc), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (maxDivU) *maxDivU = sc[S_MAXDIV];
+    return sc[S_BLOWUP] != 0.0 ? set_err(TCS_ERR_BLOWUP, "BLOW UP: max divergence >= 1e-3") : TCS_OK;
+}
+
+int tcs_post_cfl(tcs_ctx *c, double *CFL, double *dt)
+{
+    ENTER(c);
+    double sc[S_NSCAL];
+    CK(cudaMemcpyAsync(sc, c->cx.g.scal, sizeof(sc), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (CFL) *CFL = sc[S_CFL];
+    if (dt) *dt = sc[S_DT];
+    return std::isfinite(sc[S_DT]) ? TCS_OK : set_err(TCS_ERR_NONFINITE, "dt is not finite");
+}
+
+static void launch_step(tcs_ctx *c)
+{
+    Ctx &cx = c->cx;
+    cudaStream_t s = c->stream;
+    launch_thermal(cx, s);
+    std::swap(cx.f.T, cx.f.Tn);
+    launch_momentum_coeffi(cx, s);
+    launch_solve_du(cx, s);
+    launch_solve_dv(cx, s);
+    launch_solve_dw(cx, s);
+    launch_blockld_v(cx, s);
+    launch_blockld_u(cx, s);
+    launch_pseudo_prhs_fftx(cx, s, true);
+    std::swap(cx.f.U, cx.f.Un); std::swap(cx.f.V, cx.f.Vn); std::swap(cx.f.W, cx.f.Wn);
+    launch_poisson_rest(cx, s);
+    launch_projection(cx, s);
+    std::swap(cx.f.dPhat, cx.f.dPhatn); std::swap(cx.f.dP0, cx.f.dP0n);
+    launch_post(cx, s, 1);
+}
+
+int tcs_set_use_graph(tcs_ctx *c, int on)
+{
+    ENTER(c);
+    c->use_graph = on != 0;
+    return TCS_OK;
+}
+
+int tcs_step(tcs_ctx *c, int nsteps, int *done)
+{
+    ENTER(c);
+    if (done) *done = 0;
+    if (nsteps < 0) return set_err(TCS_ERR_ARG, "nsteps < 0");
+    int r = flush_pending(c);
+    if (r) return r;
+    const int fl[] = {TCS_F_T, TCS_F_U, TCS_F_V, TCS_F_W, TCS_F_P, TCS_F_DPHAT};
+    for (int f : fl) ensure_ghosts(c, f);
+    if ((r = take_launch_error())) return r;
+    double sc0[S_NSCAL];
+    CK(cudaMemcpyAsync(sc0, c->cx.g.scal, sizeof(sc0), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (sc0[S_BLOWUP] != 0.0) return set_err(TCS_ERR_BLOWUP, "the case has already blown up");
+    const bool graph = c->use_graph && c->probe.mask == 0;
+    for (int n = 0; n < nsteps; n++) {
+        if (!graph) {
+            launch_step(c);
+            if ((r = take_launch_error())) return r;
+            continue;
+        }
+        const double *T0 = c->cx.f.T, *U0 = c->cx.f.U, *P0 = c->cx.f.dPhat;
+        cudaGraphExec_t exec = nullptr;
+        unsigned long long kernels_this = 0;
+        for (auto &ge : c->graphs) if (ge.T == T0 && ge.U == U0 && ge.dPhat == P0) { exec = ge.exec; kernels_this = ge.kernels; break; }
+        if (!exec) {
+            cudaGraph_t gr;
+            const unsigned long long before = g_launches;
+            CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+            launch_step(c);
+            const unsigned long long nk = g_launches - before;
+            g_launches = before;
+            cudaError_t ec = cudaStreamEndCapture(c->stream, &gr);
+            if (ec != cudaSuccess || take_launch_error()) return set_err(TCS_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ec));
+            CK(cudaGraphInstantiate(&exec, gr, 0));
+            cudaGraphDestroy(gr);
+            c->graphs.push_back({T0, U0, P0, exec, nk});
+            kernels_this = nk;
+            // capture swapped the buffers already; the launch below performs that step
+        } else {
+            std::swap(c->cx.f.T, c->cx.f.Tn);
+            std::swap(c->cx.f.U, c->cx.f.Un); std::swap(c->cx.f.V, c->cx.f.Vn); std::swap(c->cx.f.W, c->cx.f.Wn);
+            std::swap(c->cx.f.dPhat, c->cx.f.dPhatn); std::swap(c->cx.f.dP0, c->cx.f.dP0n);
+        }
+        CK(cudaGraphLaunch(exec, c->stream));
+        g_launches += kernels_this;
+    }
+    double sc[S_NSCAL];
+    CK(cudaMemcpyAsync(sc, c->cx.g.scal, sizeof(sc), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    c->ghost_ok |= (1u << TCS_F_T) | (1u << TCS_F_U) | (1u << TCS_F_V) | (1u << TCS_F_W) | (1u << TCS_F_P) | (1u << TCS_F_DPHAT) | (1u << TCS_F_DP);
+    const int steps_now = (int)sc[S_STEP] - (int)sc0[S_STEP];
+    if (done) *done = steps_now;
+    if (sc[S_BLOWUP] != 0.0) return set_err(TCS_ERR_BLOWUP, "BLOW UP: max divergence >= 1e-3");
+    return TCS_OK;
+}
+
+int tcs_get_scalars(tcs_ctx *c, double *out)
+{
+    ENTER(c);
+    if (!out) return set_err(TCS_ERR_ARG, "null argument");
+    CK(cudaMemcpyAsync(out, c->cx.g.scal, sizeof(double) * S_NSCAL, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return TCS_OK;
+}
+
+int tcs_get_history(tcs_ctx *c, int first, int count, double *out)
+{
+    ENTER(c);
+    if (!out || first < 0 || count < 0 || first + count > c->cx.f.hist_cap) return set_err(TCS_ERR_ARG, "history range");
+    CK(cudaMemcpyAsync(out, c->cx.f.hist + (size_t)first * 7, sizeof(double) * 7 * (size_t)count, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return TCS_OK;
+}
+
+// ---- probes ---------------------------------------------------------------
+int tcs_probe_enable(tcs_ctx *c, uint64_t mask)
+{
+    ENTER(c);
+    c->probe.mask = mask;
+    return TCS_OK;
+}
+
+int tcs_probe_read(tcs_ctx *c, int kid, double *total_ms, int *launches)
+{
+    ENTER(c);
+    if (kid < 0 || kid >= K_COUNT) return set_err(TCS_ERR_ARG, "kernel id");
+    CK(cudaStreamSynchronize(c->stream));
+    double t = 0.0;
+    for (auto &pr : c->probe.rec[kid]) {
+        float ms = 0.0f;
+        CK(cudaEventElapsedTime(&ms, pr.first, pr.second));
+        t += ms;
+    }
+    if (total_ms) *total_ms = t;
+    if (launches) *launches = (int)c->probe.rec[kid].size();
+    return TCS_OK;
+}
+
+int tcs_probe_reset(tcs_ctx *c)
+{
+    ENTER(c);
+    CK(cudaStreamSynchronize(c->stream));
+    for (auto &v : c->probe.rec) {
+        for (auto &pr : v) { c->probe.pool.push_back(pr.first); c->probe.pool.push_back(pr.second); }
+        v.clear();
+    }
+    return TCS_OK;
+}
+
+// ---- PaScaL_TDMA ------------------------------------------------------------
+} // extern "C"
+
+struct tcs_tdma_plan {
+    int n_sys;
+    int device;
+    cudaStream_t stream;
+    double *buf;
+    size_t cap;
+};
+
+extern "C" {
+
+int tcs_tdma_plan_many_create(tcs_tdma_plan **plan, int n_sys, int myrank, int nprocs)
+{
+    if (!plan || n_sys < 1) return set_err(TCS_ERR_ARG, "bad plan arguments");
+    if (nprocs != 1 || myrank != 0) return set_err(TCS_ERR_UNSUPPORTED, "one GPU holds the whole line: nprocs must be 1");
+    tcs_tdma_plan *p = new tcs_tdma_plan();
+    p->n_sys = n_sys; p->buf = nullptr; p->cap = 0;
+    cudaGetDevice(&p->device);
+    if (cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking) != cudaSuccess) { delete p; return set_err(TCS_ERR_CUDA, "stream"); }
+    *plan = p;
+    return TCS_OK;
+}
+
+int tcs_tdma_plan_many_destroy(tcs_tdma_plan *p)
+{
+    if (!p) return set_err(TCS_ERR_ARG, "null plan");
+    cudaStreamSynchronize(p->stream);
+    if (p->buf) cudaFree(p->buf);
+    cudaStreamDestroy(p->stream);
+    delete p;
+    return TCS_OK;
+}
+
+static int tdma_solve(tcs_tdma_plan *p, double *A, double *B, double *C, double *D, int n_sys, int n_row, int cyclic)
+{
+    if (!p || !A || !B || !C || !D) return set_err(TCS_ERR_ARG, "null argument");
+    if (n_sys != p->n_sys || n_row < 2) return set_err(TCS_ERR_ARG, "n_sys must match the plan and n_row >= 2");
+    cudaSetDevice(p->device);
+    cudaPointerAttributes at;
+    bool dev = cudaPointerGetAttributes(&at, D) == cudaSuccess && at.type == cudaMemoryTypeDevice;
+    cudaGetLastError();
+    const size_t n = (size_t)n_sys * n_row;
+    if (dev) {
+        launch_tdma_many(A, B, C, D, n_sys, n_row, cyclic, p->stream);
+        if (take_launch_error()) return TCS_ERR_CUDA;
+        CK(cudaStreamSynchronize(p->stream));
+        return TCS_OK;
+    }
+    if (p->cap < 4 * n) {
+        if (p->buf) cudaFree(p->buf);
+        p->buf = nullptr; p->cap = 0;
+        CK(cudaMalloc(&p->buf, 4 * n * sizeof(double)));
+        p->cap = 4 * n;
+    }
+    double *dA = p->buf, *dB = dA + n, *dC = dB + n, *dD = dC + n;
+    CK(cudaMemcpyAsync(dA, A, n * sizeof(double), cudaMemcpyHostToDevice, p->stream));
+    CK(cudaMemcpyAsync(dB, B, n * sizeof(double), cudaMemcpyHostToDevice, p->stream));
+    CK(cudaMemcpyAsync(dC, C, n * sizeof(double), cudaMemcpyHostToDevice, p->stream));
+    CK(cudaMemcpyAsync(dD, D, n * sizeof(double), cudaMemcpyHostToDevice, p->stream));
+    launch_tdma_many(dA, dB, dC, dD, n_sys, n_row, cyclic, p->stream);
+    if (take_launch_error()) return TCS_ERR_CUDA;
+    CK(cudaMemcpyAsync(A, dA, n * sizeof(double), cudaMemcpyDeviceToHost, p->stream));
+    CK(cudaMemcpyAsync(C, dC, n * sizeof(double), cudaMemcpyDeviceToHost, p->stream));
+    CK(cudaMemcpyAsync(D, dD, n * sizeof(double), cudaMemcpyDeviceToHost, p->stream));
+    CK(cudaStreamSynchronize(p->stream));
+    return TCS_OK;
+}
+
+int tcs_tdma_many_solve(tcs_tdma_plan *p, double *A, double *B, double *C, double *D, int n_sys, int n_row)
+{
+    return tdma_solve(p, A, B, C, D, n_sys, n_row, 0);
+}
+
+int tcs_tdma_many_solve_cycle(tcs_tdma_plan *p, double *A, double *B, double *C, double *D, int n_sys, int n_row)
+{
+    return tdma_solve(p, A, B, C, D, n_sys, n_row, 1);
+}
+
+} // extern "C"

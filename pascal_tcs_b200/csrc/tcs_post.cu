@@ -1,0 +1,148 @@
+// tcs_post.cu -- per-step diagnostics: mpi_Post_Div and mpi_Post_CFL
+// (module_post.f90:100-158, 168-230) with the adaptive time step, the
+// blow-up test of main.f90:208-212, and the Nusselt / kinetic-energy series.
+// Two kernels: block partials in a fixed order, then one block that combines
+// them and updates dt, time and CFL on the device (deterministic).
+#include "tcs_kernels.h"
+
+#include <math.h>
+
+namespace tcs {
+
+enum { PT_DIV = 0, PT_CFL, PT_KE, PT_NUB, PT_NUT, PT_N };
+static const int POST_BLOCKS = 592;   // 4 x 148 SMs
+
+__global__ void __launch_bounds__(256) post_kernel(Grid g, Fields f)
+{
+    __shared__ double red[PT_N][256];
+    if (blown(g)) return;
+    const long long n = (long long)g.N1 * g.N2 * g.N3;
+    double mdiv = -INFINITY, mcfl = -INFINITY, ke = 0.0, nub = 0.0, nut = 0.0;
+    const double *dx1 = g.m1.dx, *dx2 = g.m2.dx, *dx3 = g.m3.dx;
+    const double *rdx1 = g.m1.rdx, *rdx2 = g.m2.rdx, *rdx3 = g.m3.rdx;
+    const long long sj = g.P1, sk = (long long)g.P1 * g.P2;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const int i = 1 + (int)(t % g.N1);
+        const long long q = t / g.N1;
+        const int j = 1 + (int)(q % g.N2), k = 1 + (int)(q / g.N2);
+        const long long c = ix(g, i, j, k);
+        const double Uc = ld(f.U + c), Vc = ld(f.V + c), Wc = ld(f.W + c);
+        const double Ux = ld(f.U + c + 1), Vy = ld(f.V + c + sj), Wz = ld(f.W + c + sk);
+        const double dv = (Ux - Uc) * rdx1[i] + (Vy - Vc) * rdx2[j] + (Wz - Wc) * rdx3[k];
+        const double cf = (fabs(Ux + Uc) / 2.0) * rdx1[i] + (fabs(Vy + Vc) / 2.0) * rdx2[j] + (fabs(Wz + Wc) / 2.0) * rdx3[k];
+        mdiv = fmax(mdiv, dv);
+        mcfl = fmax(mcfl, cf);
+        ke += (Uc * Uc + Vc * Vc + Wc * Wc) * dx1[i] * dx2[j] * dx3[k];
+        if (j == 1) nub += -(ld(f.T + c) - g.ph.Tbt) / g.m2.dmx[1];
+        if (j == g.N2) nut += -(g.ph.Tup - ld(f.T + c)) / g.m2.dmx[g.N2 + 1];
+    }
+    red[PT_DIV][threadIdx.x] = mdiv; red[PT_CFL][threadIdx.x] = mcfl;
+    red[PT_KE][threadIdx.x] = ke; red[PT_NUB][threadIdx.x] = nub; red[PT_NUT][threadIdx.x] = nut;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) {
+            red[PT_DIV][threadIdx.x] = fmax(red[PT_DIV][threadIdx.x], red[PT_DIV][threadIdx.x + w]);
+            red[PT_CFL][threadIdx.x] = fmax(red[PT_CFL][threadIdx.x], red[PT_CFL][threadIdx.x + w]);
+            red[PT_KE][threadIdx.x] += red[PT_KE][threadIdx.x + w];
+            red[PT_NUB][threadIdx.x] += red[PT_NUB][threadIdx.x + w];
+            red[PT_NUT][threadIdx.x] += red[PT_NUT][threadIdx.x + w];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x < PT_N) f.part[blockIdx.x * PT_N + threadIdx.x] = red[threadIdx.x][0];
+}
+
+__global__ void __launch_bounds__(256) finalize_kernel(Grid g, Fields f, int nblocks, int record_hist)
+{
+    __shared__ double red[PT_N][256];
+    if (blown(g)) return;
+    double mdiv = -INFINITY, mcfl = -INFINITY, ke = 0.0, nub = 0.0, nut = 0.0;
+    for (int b = threadIdx.x; b < nblocks; b += blockDim.x) {
+        const double *p = f.part + b * PT_N;
+        mdiv = fmax(mdiv, p[PT_DIV]); mcfl = fmax(mcfl, p[PT_CFL]);
+        ke += p[PT_KE]; nub += p[PT_NUB]; nut += p[PT_NUT];
+    }
+    red[PT_DIV][threadIdx.x] = mdiv; red[PT_CFL][threadIdx.x] = mcfl;
+    red[PT_KE][threadIdx.x] = ke; red[PT_NUB][threadIdx.x] = nub; red[PT_NUT][threadIdx.x] = nut;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) {
+            red[PT_DIV][threadIdx.x] = fmax(red[PT_DIV][threadIdx.x], red[PT_DIV][threadIdx.x + w]);
+            red[PT_CFL][threadIdx.x] = fmax(red[PT_CFL][threadIdx.x], red[PT_CFL][threadIdx.x + w]);
+            red[PT_KE][threadIdx.x] += red[PT_KE][threadIdx.x + w];
+            red[PT_NUB][threadIdx.x] += red[PT_NUB][threadIdx.x + w];
+            red[PT_NUT][threadIdx.x] += red[PT_NUT][threadIdx.x + w];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x != 0) return;
+    double *sc = g.scal;
+    const double dt_used = sc[S_DT];
+    const double maxdiv = red[PT_DIV][0], mx = red[PT_CFL][0];
+    const double cnt = (double)g.N1 * (double)g.N3;
+    sc[S_MAXDIV] = maxdiv;
+    sc[S_NUBOT] = red[PT_NUB][0] / cnt;
+    sc[S_NUTOP] = red[PT_NUT][0] / cnt;
+    sc[S_KE] = 0.5 * red[PT_KE][0] / (g.ph.L1 * g.ph.L2 * g.ph.L3);
+    if (maxdiv >= 1.0e-3 || maxdiv != maxdiv) {
+        sc[S_BLOWUP] = sc[S_STEP] + 1.0;          // the step (1-based) that blew up
+        return;
+    }
+    if (sc[S_FIXED_DT] != 0.0) {
+        sc[S_CFL] = dt_used * mx;
+    } else {
+        double nd = g.ph.MaxCFL / mx;              // +Inf for a resting fluid
+        if (nd > g.ph.dtMax) nd = g.ph.dtMax;
+        sc[S_DT] = nd;
+        sc[S_CFL] = nd * mx;
+    }
+    sc[S_TIME] = sc[S_TIME] + sc[S_DT];
+    const int step = (int)sc[S_STEP];
+    if (record_hist && step < f.hist_cap) {
+        double *h = f.hist + (long long)step * 7;
+        h[0] = dt_used; h[1] = sc[S_TIME]; h[2] = maxdiv; h[3] = sc[S_CFL];
+        h[4] = sc[S_NUBOT]; h[5] = sc[S_NUTOP]; h[6] = sc[S_KE];
+    }
+    sc[S_STEP] = step + 1;
+}
+
+void launch_post(const Ctx &cx, cudaStream_t s, int record_hist)
+{
+    probe_begin(cx, K_POST, s);
+    post_kernel<<<POST_BLOCKS, 256, 0, s>>>(cx.g, cx.f);
+    probe_end(cx, K_POST, s);
+    record_launch_error("post");
+    probe_begin(cx, K_FINAL, s);
+    finalize_kernel<<<1, 256, 0, s>>>(cx.g, cx.f, POST_BLOCKS, record_hist);
+    probe_end(cx, K_FINAL, s);
+    record_launch_error("finalize");
+}
+
+int post_partial_count() { return POST_BLOCKS * PT_N; }
+
+// Periodic ghost update of one padded field (module_mpi_subdomain.f90:758-791):
+// x faces first, then z faces including the x-ghost columns.
+__global__ void ghost_x_kernel(Grid g, double *a)
+{
+    const int j = blockIdx.x * blockDim.x + threadIdx.x, k = blockIdx.y;
+    if (j > g.N2 + 1) return;
+    a[ix(g, 0, j, k)] = a[ix(g, g.N1, j, k)];
+    a[ix(g, g.N1 + 1, j, k)] = a[ix(g, 1, j, k)];
+}
+__global__ void ghost_z_kernel(Grid g, double *a)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
+    if (i > g.N1 + 1) return;
+    a[ix(g, i, j, 0)] = a[ix(g, i, j, g.N3)];
+    a[ix(g, i, j, g.N3 + 1)] = a[ix(g, i, j, 1)];
+}
+
+void launch_ghost(const Ctx &cx, double *a, cudaStream_t s)
+{
+    const Grid &g = cx.g;
+    ghost_x_kernel<<<dim3((g.N2 + 2 + 127) / 128, g.N3 + 2), 128, 0, s>>>(g, a);
+    ghost_z_kernel<<<dim3((g.N1 + 2 + 127) / 128, g.N2 + 2), 128, 0, s>>>(g, a);
+    record_launch_error("ghost");
+}
+
+} // namespace tcs

@@ -1,0 +1,345 @@
+"""Python host binding of libtcs (include/tcs.h).
+
+The reference's host side is the Fortran driver main.f90; this module mirrors
+its call sequence and the module interfaces it uses (mpi_thermal,
+mpi_momentum, mpi_pressure, mpi_subdomain, mpi_Post, PaScaL_TDMA) one call per
+C-ABI entry point.  There is no CPU path: every method calls the CUDA library,
+and loading fails loudly if libtcs.so has not been built.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libtcs.so")
+
+FIELDS = {"T": 0, "U": 1, "V": 2, "W": 3, "P": 4, "dPhat": 5, "dP0": 6,
+          "dU": 7, "dV": 8, "dW": 9, "dP": 10, "Mu": 11, "invRho": 12}
+SCALARS = ["dt", "time", "CFL", "maxDivU", "Nu_bot", "Nu_top", "KE", "blowup",
+           "aver", "step", "fixed_dt"]
+HISTORY = ["dt", "time", "maxDivU", "CFL", "Nu_bot", "Nu_top", "KE"]
+METRICS = ["x1", "dx1", "dmx1", "x2", "dx2", "dmx2", "x3", "dx3", "dmx3"]
+ERRORS = {1: "bad argument", 2: "CUDA error", 3: "unsupported", 4: "BLOW UP",
+          5: "out of device memory", 6: "non-finite scalar"}
+
+# Every symbol include/tcs.h declares (checked by the CPU test suite).
+EXPORTS = [
+    "tcs_create", "tcs_destroy", "tcs_set_stream", "tcs_get_stream", "tcs_dims",
+    "tcs_upload_field", "tcs_download_field", "tcs_upload_field_async",
+    "tcs_download_field_async", "tcs_field_device_ptr", "tcs_synchronize", "tcs_set_dt",
+    "tcs_get_metric", "tcs_thermal_coeffi", "tcs_thermal_solver", "tcs_thermal_coeffi_clean",
+    "tcs_subdomain_ghostcell_update", "tcs_momentum_coeffi", "tcs_momentum_solvedU",
+    "tcs_momentum_solvedV", "tcs_momentum_solvedW", "tcs_momentum_blockLdV",
+    "tcs_momentum_blockLdU", "tcs_momentum_pseudoupdateUVW", "tcs_momentum_coeffi_clean",
+    "tcs_pressure_RHS", "tcs_pressure_Poisson_FFT2", "tcs_pressure_Projection",
+    "tcs_post_div", "tcs_post_cfl", "tcs_step", "tcs_get_scalars", "tcs_get_history",
+    "tcs_tdma_plan_many_create", "tcs_tdma_plan_many_destroy", "tcs_tdma_many_solve",
+    "tcs_tdma_many_solve_cycle", "tcs_kernel_count", "tcs_launch_count", "tcs_kernel_name", "tcs_probe_enable",
+    "tcs_probe_read", "tcs_probe_reset", "tcs_set_use_graph", "tcs_last_error",
+]
+
+
+class TcsError(RuntimeError):
+    def __init__(self, code: int, where: str, msg: str):
+        super().__init__(f"{where}: {ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class TcsConfig(ctypes.Structure):
+    _fields_ = [("n1m", ctypes.c_int), ("n2m", ctypes.c_int), ("n3m", ctypes.c_int),
+                ("uniform1", ctypes.c_int), ("uniform2", ctypes.c_int), ("uniform3", ctypes.c_int),
+                ("gamma1", ctypes.c_double), ("gamma2", ctypes.c_double), ("gamma3", ctypes.c_double),
+                ("aspect1", ctypes.c_double), ("H", ctypes.c_double), ("aspect3", ctypes.c_double),
+                ("Ra", ctypes.c_double), ("Pr", ctypes.c_double), ("DeltaT", ctypes.c_double),
+                ("MaxCFL", ctypes.c_double), ("dtStart", ctypes.c_double), ("tStart", ctypes.c_double),
+                ("property_set", ctypes.c_int), ("fixed_dt", ctypes.c_int),
+                ("seed", ctypes.c_uint64), ("noise_amp", ctypes.c_double),
+                ("init_mode", ctypes.c_int), ("top_wall_mode", ctypes.c_int), ("device", ctypes.c_int)]
+
+
+def default_config(**kw) -> dict:
+    """The 64^3 constant-property Boussinesq case: Lx = Lz = 2, Ly = 1,
+    tanh-stretched y (gamma 1.5), Ra = 1e5, Pr = 0.71, dt = 1e-3."""
+    c = dict(n1m=64, n2m=64, n3m=64, uniform1=1, uniform2=0, uniform3=1,
+             gamma1=3.0, gamma2=1.5, gamma3=3.0, aspect1=2.0, H=1.0, aspect3=2.0,
+             Ra=1e5, Pr=0.71, DeltaT=10.0, MaxCFL=1.0, dtStart=1e-3, tStart=0.0,
+             property_set=0, fixed_dt=1, seed=0, noise_amp=0.01, init_mode=0,
+             top_wall_mode=0, device=0)
+    c.update(kw)
+    return c
+
+
+_lib = None
+
+
+def load() -> ctypes.CDLL:
+    """Load libtcs.so (built in-tree by pascal_tcs_b200.build)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: run `python -m pascal_tcs_b200.build` (there is no CPU fallback)")
+    L = ctypes.CDLL(LIB_PATH)
+    vp, ip, dp = ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double)
+    sig = {
+        "tcs_create": ([ctypes.POINTER(TcsConfig), ctypes.POINTER(vp)], ip),
+        "tcs_destroy": ([vp], ip),
+        "tcs_set_stream": ([vp, vp], ip),
+        "tcs_get_stream": ([vp], vp),
+        "tcs_dims": ([vp, ctypes.POINTER(ip)], ip),
+        "tcs_upload_field": ([vp, ip, vp], ip),
+        "tcs_download_field": ([vp, ip, vp], ip),
+        "tcs_upload_field_async": ([vp, ip, vp], ip),
+        "tcs_download_field_async": ([vp, ip, vp], ip),
+        "tcs_field_device_ptr": ([vp, ip, ctypes.POINTER(vp)], ip),
+        "tcs_synchronize": ([vp], ip),
+        "tcs_set_dt": ([vp, ctypes.c_double], ip),
+        "tcs_get_metric": ([vp, ip, dp], ip),
+        "tcs_subdomain_ghostcell_update": ([vp, ip], ip),
+        "tcs_post_div": ([vp, dp], ip),
+        "tcs_post_cfl": ([vp, dp, dp], ip),
+        "tcs_step": ([vp, ip, ctypes.POINTER(ip)], ip),
+        "tcs_get_scalars": ([vp, dp], ip),
+        "tcs_get_history": ([vp, ip, ip, dp], ip),
+        "tcs_tdma_plan_many_create": ([ctypes.POINTER(vp), ip, ip, ip], ip),
+        "tcs_tdma_plan_many_destroy": ([vp], ip),
+        "tcs_tdma_many_solve": ([vp, vp, vp, vp, vp, ip, ip], ip),
+        "tcs_tdma_many_solve_cycle": ([vp, vp, vp, vp, vp, ip, ip], ip),
+        "tcs_kernel_count": ([], ip),
+        "tcs_launch_count": ([], ctypes.c_ulonglong),
+        "tcs_kernel_name": ([ip], ctypes.c_char_p),
+        "tcs_probe_enable": ([vp, ctypes.c_uint64], ip),
+        "tcs_probe_read": ([vp, ip, dp, ctypes.POINTER(ip)], ip),
+        "tcs_probe_reset": ([vp], ip),
+        "tcs_set_use_graph": ([vp, ip], ip),
+        "tcs_last_error": ([], ctypes.c_char_p),
+    }
+    for name in ("tcs_thermal_coeffi", "tcs_thermal_solver", "tcs_thermal_coeffi_clean",
+                 "tcs_momentum_coeffi", "tcs_momentum_solvedU", "tcs_momentum_solvedV",
+                 "tcs_momentum_solvedW", "tcs_momentum_blockLdV", "tcs_momentum_blockLdU",
+                 "tcs_momentum_pseudoupdateUVW", "tcs_momentum_coeffi_clean", "tcs_pressure_RHS",
+                 "tcs_pressure_Poisson_FFT2", "tcs_pressure_Projection"):
+        sig[name] = ([vp], ip)
+    for name, (args, res) in sig.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = res
+    _lib = L
+    return L
+
+
+def _check(r: int, where: str) -> None:
+    if r != 0:
+        raise TcsError(r, where, load().tcs_last_error().decode())
+
+
+def launch_count() -> int:
+    """Kernels launched by libtcs in this process (CUDA-graph replays included)."""
+    return int(load().tcs_launch_count())
+
+
+def kernel_names() -> list[str]:
+    L = load()
+    return [L.tcs_kernel_name(i).decode() for i in range(L.tcs_kernel_count())]
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+class Solver:
+    """One case resident on one GPU, driven with the reference's call sequence."""
+
+    def __init__(self, **cfg):
+        self.config = default_config(**cfg)
+        L = load()
+        h = ctypes.c_void_p()
+        _check(L.tcs_create(ctypes.byref(TcsConfig(**self.config)), ctypes.byref(h)), "tcs_create")
+        self._h = h
+        d = (ctypes.c_int * 3)()
+        _check(L.tcs_dims(h, d), "tcs_dims")
+        self.shape = (d[2], d[1], d[0])
+        self.n1m, self.n2m, self.n3m = (self.config[k] for k in ("n1m", "n2m", "n3m"))
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.tcs_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # -- data -----------------------------------------------------------------
+    def get(self, name: str) -> np.ndarray:
+        a = np.empty(self.shape, dtype=np.float64)
+        _check(load().tcs_download_field(self._h, FIELDS[name], a.ctypes.data), f"download {name}")
+        return a
+
+    def set(self, name: str, a: np.ndarray) -> None:
+        a = np.ascontiguousarray(a, dtype=np.float64).reshape(self.shape)
+        _check(load().tcs_upload_field(self._h, FIELDS[name], a.ctypes.data), f"upload {name}")
+
+    def upload_async(self, name: str, pinned_ptr: int) -> None:
+        _check(load().tcs_upload_field_async(self._h, FIELDS[name], pinned_ptr), f"upload {name}")
+
+    def download_async(self, name: str, pinned_ptr: int) -> None:
+        _check(load().tcs_download_field_async(self._h, FIELDS[name], pinned_ptr), f"download {name}")
+
+    def device_ptr(self, name: str) -> int:
+        p = ctypes.c_void_p()
+        _check(load().tcs_field_device_ptr(self._h, FIELDS[name], ctypes.byref(p)), "device_ptr")
+        return p.value
+
+    def metric(self, name: str) -> np.ndarray:
+        n = {"1": self.shape[2], "2": self.shape[1], "3": self.shape[0]}[name[-1]]
+        a = np.empty(n, dtype=np.float64)
+        _check(load().tcs_get_metric(self._h, METRICS.index(name), _dptr(a)), "metric")
+        return a
+
+    def set_stream(self, stream_handle: int | None) -> None:
+        _check(load().tcs_set_stream(self._h, stream_handle or None), "set_stream")
+
+    @property
+    def stream(self) -> int:
+        return load().tcs_get_stream(self._h) or 0
+
+    def synchronize(self) -> None:
+        _check(load().tcs_synchronize(self._h), "synchronize")
+
+    def set_dt(self, dt: float) -> None:
+        _check(load().tcs_set_dt(self._h, float(dt)), "set_dt")
+
+    def scalars(self) -> dict:
+        a = np.zeros(len(SCALARS))
+        _check(load().tcs_get_scalars(self._h, _dptr(a)), "scalars")
+        return dict(zip(SCALARS, a.tolist()))
+
+    def history(self, first: int, count: int) -> np.ndarray:
+        a = np.zeros((count, len(HISTORY)))
+        _check(load().tcs_get_history(self._h, int(first), int(count), _dptr(a)), "history")
+        return a
+
+    # -- the reference's step, one call per routine (main.f90:133-221) ---------
+    def _call(self, name: str) -> None:
+        _check(getattr(load(), name)(self._h), name)
+
+    def thermal_coeffi(self): self._call("tcs_thermal_coeffi")
+    def thermal_solver(self): self._call("tcs_thermal_solver")
+    def thermal_coeffi_clean(self): self._call("tcs_thermal_coeffi_clean")
+    def momentum_coeffi(self): self._call("tcs_momentum_coeffi")
+    def momentum_solvedU(self): self._call("tcs_momentum_solvedU")
+    def momentum_solvedV(self): self._call("tcs_momentum_solvedV")
+    def momentum_solvedW(self): self._call("tcs_momentum_solvedW")
+    def momentum_blockLdV(self): self._call("tcs_momentum_blockLdV")
+    def momentum_blockLdU(self): self._call("tcs_momentum_blockLdU")
+    def momentum_pseudoupdateUVW(self): self._call("tcs_momentum_pseudoupdateUVW")
+    def momentum_coeffi_clean(self): self._call("tcs_momentum_coeffi_clean")
+    def pressure_RHS(self): self._call("tcs_pressure_RHS")
+    def pressure_Poisson_FFT2(self): self._call("tcs_pressure_Poisson_FFT2")
+    def pressure_Projection(self): self._call("tcs_pressure_Projection")
+
+    def ghostcell_update(self, name: str) -> None:
+        _check(load().tcs_subdomain_ghostcell_update(self._h, FIELDS[name]), "ghostcell_update")
+
+    def post_div(self) -> float:
+        v = ctypes.c_double()
+        _check(load().tcs_post_div(self._h, ctypes.byref(v)), "post_div")
+        return v.value
+
+    def post_cfl(self) -> tuple[float, float]:
+        c, d = ctypes.c_double(), ctypes.c_double()
+        _check(load().tcs_post_cfl(self._h, ctypes.byref(c), ctypes.byref(d)), "post_cfl")
+        return c.value, d.value
+
+    def driver_step(self) -> float:
+        """One iteration of main.f90:129-223 through the stage entry points."""
+        self.thermal_coeffi(); self.thermal_solver(); self.thermal_coeffi_clean()
+        self.ghostcell_update("T")
+        self.momentum_coeffi()
+        self.momentum_solvedU(); self.ghostcell_update("dU")
+        self.momentum_solvedV(); self.ghostcell_update("dV")
+        self.momentum_solvedW(); self.ghostcell_update("dW")
+        self.momentum_blockLdV(); self.ghostcell_update("dV")
+        self.momentum_blockLdU()
+        self.momentum_pseudoupdateUVW()
+        for f in ("U", "V", "W"):
+            self.ghostcell_update(f)
+        self.pressure_RHS()
+        self.pressure_Poisson_FFT2()
+        self.ghostcell_update("dP")
+        self.pressure_Projection()
+        for f in ("U", "V", "W", "P", "dPhat"):
+            self.ghostcell_update(f)
+        self.momentum_coeffi_clean()
+        div = self.post_div()
+        self.post_cfl()
+        return div
+
+    def step(self, n: int = 1) -> int:
+        done = ctypes.c_int()
+        _check(load().tcs_step(self._h, int(n), ctypes.byref(done)), "tcs_step")
+        return done.value
+
+    def use_graph(self, on: bool) -> None:
+        _check(load().tcs_set_use_graph(self._h, int(bool(on))), "use_graph")
+
+    # -- measurement ----------------------------------------------------------
+    def probe(self, kernels) -> None:
+        names = kernel_names()
+        mask = 0
+        for k in kernels:
+            mask |= 1 << (names.index(k) if isinstance(k, str) else int(k))
+        _check(load().tcs_probe_enable(self._h, ctypes.c_uint64(mask)), "probe_enable")
+
+    def probe_read(self, kernel) -> tuple[float, int]:
+        kid = kernel_names().index(kernel) if isinstance(kernel, str) else int(kernel)
+        t, n = ctypes.c_double(), ctypes.c_int()
+        _check(load().tcs_probe_read(self._h, kid, ctypes.byref(t), ctypes.byref(n)), "probe_read")
+        return t.value, n.value
+
+    def probe_reset(self) -> None:
+        _check(load().tcs_probe_reset(self._h), "probe_reset")
+
+
+class TdmaPlan:
+    """PaScaL_TDMA_plan_many_create / many_solve / many_solve_cycle / destroy
+    (pascal_tdma.f90:185-290, 487-578, 715-806) on one GPU."""
+
+    def __init__(self, n_sys: int, myrank: int = 0, nprocs: int = 1):
+        h = ctypes.c_void_p()
+        _check(load().tcs_tdma_plan_many_create(ctypes.byref(h), int(n_sys), int(myrank), int(nprocs)),
+               "PaScaL_TDMA_plan_many_create")
+        self._h, self.n_sys = h, int(n_sys)
+
+    def destroy(self) -> None:
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.tcs_tdma_plan_many_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.destroy()
+
+    def _solve(self, fn: str, A, B, C, D, n_sys: int, n_row: int) -> None:
+        ptrs = []
+        for x in (A, B, C, D):
+            if isinstance(x, np.ndarray):
+                assert x.dtype == np.float64 and x.flags["C_CONTIGUOUS"]
+                ptrs.append(x.ctypes.data)
+            else:                           # device tensor (data_ptr) or raw pointer
+                ptrs.append(int(x.data_ptr()) if hasattr(x, "data_ptr") else int(x))
+        _check(getattr(load(), fn)(self._h, *ptrs, int(n_sys), int(n_row)), fn)
+
+    def many_solve(self, A, B, C, D, n_sys: int, n_row: int) -> None:
+        self._solve("tcs_tdma_many_solve", A, B, C, D, n_sys, n_row)
+
+    def many_solve_cycle(self, A, B, C, D, n_sys: int, n_row: int) -> None:
+        self._solve("tcs_tdma_many_solve_cycle", A, B, C, D, n_sys, n_row)

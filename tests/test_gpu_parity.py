@@ -1,0 +1,202 @@
+"""CUDA path vs the CPU oracle, through the C ABI (needs a B200).
+
+Tolerances (FP64 plain form): every stage <= 1e-11 relative L2 against the
+oracle from identical inputs; the full 100-step run of the 64^3 constant-
+property case <= 1e-10 relative L2 on u, v, w, T, p and on the Nusselt and
+kinetic-energy series (the bar BASELINE.json sets for the FP64 form); the
+PaScaL_TDMA interface is bit-exact.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+STAGE_TOL = 1e-11
+RUN_TOL = 1e-10
+
+
+def rel_l2(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    nb = np.linalg.norm(b)
+    d = np.linalg.norm(a - b)
+    return d / nb if nb > 0 else d
+
+
+@pytest.fixture(scope="module")
+def tcs():
+    import pascal_tcs_b200 as P
+    P.load()
+    return P
+
+
+def _pair(tcs, oracle_mod, **cfg):
+    g = tcs.Solver(**cfg)
+    o = oracle_mod.Oracle(**{k: v for k, v in g.config.items() if k != "device"})
+    return g, o
+
+
+def _check_fields(g, o, names, tol=STAGE_TOL, where=""):
+    for n in names:
+        a, b = g.get(n), o.get(n)
+        assert np.all(np.isfinite(a)), f"{where}: {n} not finite"
+        e = rel_l2(a, b)
+        assert e <= tol, f"{where}: {n} rel L2 {e:.3e} > {tol:.1e}"
+
+
+CASES = [
+    dict(n1m=32, n2m=24, n3m=16, property_set=0),
+    dict(n1m=48, n2m=20, n3m=40, property_set=1, Pr=7.0, Ra=1e6, dtStart=5e-4, top_wall_mode=1),
+    dict(n1m=30, n2m=17, n3m=24, property_set=2, Pr=7.0, Ra=1e5, dtStart=5e-4, uniform1=0, gamma1=1.2),
+]
+
+
+@pytest.mark.parametrize("case", range(len(CASES)))
+def test_stage_by_stage_parity(tcs, oracle_mod, case):
+    g, o = _pair(tcs, oracle_mod, **CASES[case])
+    _check_fields(g, o, ["T", "U", "V", "W", "P"], tol=0.0, where="initial")
+    for step in range(3):
+        w = f"step {step}"
+        g.thermal_solver(); o.stage("thermal"); o.stage("ghost_T")
+        _check_fields(g, o, ["T"], where=w + " thermal")
+        g.momentum_coeffi(); o.stage("mom_coeffi")
+        _check_fields(g, o, ["Mu", "invRho"], where=w + " mom_coeffi")
+        g.momentum_solvedU(); o.stage("dU")
+        _check_fields(g, o, ["dU"], where=w + " solvedU")
+        g.momentum_solvedV(); o.stage("dV")
+        _check_fields(g, o, ["dV"], where=w + " solvedV")
+        g.momentum_solvedW(); o.stage("dW")
+        _check_fields(g, o, ["dW"], where=w + " solvedW")
+        g.momentum_blockLdV(); o.stage("blockLdV")
+        _check_fields(g, o, ["dV"], where=w + " blockLdV")
+        g.momentum_blockLdU(); o.stage("blockLdU")
+        _check_fields(g, o, ["dU"], where=w + " blockLdU")
+        g.momentum_pseudoupdateUVW(); g.pressure_RHS(); g.pressure_Poisson_FFT2()
+        o.stage("pseudo"); o.stage("prhs"); o.stage("poisson")
+        _check_fields(g, o, ["U", "V", "W", "dP"], where=w + " pseudo+poisson")
+        g.pressure_Projection(); o.stage("project")
+        _check_fields(g, o, ["U", "V", "W", "P", "dPhat", "dP0"], where=w + " projection")
+        div = g.post_div(); cfl, dt = g.post_cfl(); o.stage("post")
+        so = o.scalars()
+        assert abs(div - so["maxDivU"]) <= 1e-12 + 1e-9 * abs(so["maxDivU"]), (div, so["maxDivU"])
+        assert rel_l2(cfl, so["CFL"]) < 1e-12 and rel_l2(dt, so["dt"]) < 1e-12
+
+
+def _run_compare(tcs, oracle_mod, steps, **cfg):
+    g, o = _pair(tcs, oracle_mod, **cfg)
+    g.step(steps)
+    hd = o.step(steps)
+    hg = g.history(0, steps)
+    out = {n: rel_l2(g.get(n)[1:-1, 1:-1, 1:-1], o.get(n)[1:-1, 1:-1, 1:-1]) for n in ("U", "V", "W", "T", "P")}
+    for col, n in ((4, "Nu_bot"), (5, "Nu_top"), (6, "KE")):
+        out[n] = rel_l2(hg[:, col], hd[:, col])
+    out["dt"] = rel_l2(hg[:, 0], hd[:, 0])
+    return out, g, o
+
+
+def test_64cube_constant_properties_100_steps(tcs, oracle_mod):
+    # The plain FP64 Rayleigh-Benard channel case: 64^3, Ra=1e5, Pr=0.71, dt=1e-3, seed 0.
+    err, g, _ = _run_compare(tcs, oracle_mod, 100, n1m=64, n2m=64, n3m=64, Ra=1e5, Pr=0.71,
+                             dtStart=1e-3, fixed_dt=1, seed=0, property_set=0)
+    for k, v in err.items():
+        assert v <= RUN_TOL, f"{k}: rel L2 {v:.3e}"
+    assert g.scalars()["step"] == 100
+
+
+def test_water_adaptive_dt_run(tcs, oracle_mod):
+    # Temperature-dependent water properties with the reference's CFL-adaptive dt.
+    err, _, _ = _run_compare(tcs, oracle_mod, 40, n1m=32, n2m=32, n3m=32, property_set=1, Pr=7.0,
+                             Ra=1e7, DeltaT=10.0, dtStart=2e-4, fixed_dt=0, MaxCFL=0.5, seed=1,
+                             top_wall_mode=1)
+    for k, v in err.items():
+        assert v <= RUN_TOL, f"{k}: rel L2 {v:.3e}"
+
+
+def test_driver_sequence_matches_graph_step(tcs):
+    cfg = dict(n1m=32, n2m=16, n3m=24, property_set=1, Pr=7.0, Ra=1e6, dtStart=5e-4)
+    a = tcs.Solver(**cfg)
+    b = tcs.Solver(**cfg)
+    for _ in range(4):
+        a.driver_step()
+    b.step(4)
+    for n in ("T", "U", "V", "W", "P", "dPhat", "dP0"):
+        np.testing.assert_array_equal(a.get(n), b.get(n), err_msg=n)
+    np.testing.assert_array_equal(a.history(0, 4), b.history(0, 4))
+
+
+def test_graph_and_eager_steps_identical(tcs):
+    cfg = dict(n1m=24, n2m=16, n3m=20)
+    a = tcs.Solver(**cfg)
+    b = tcs.Solver(**cfg)
+    b.use_graph(False)
+    a.step(5); b.step(5)
+    for n in ("T", "U", "V", "W", "P"):
+        np.testing.assert_array_equal(a.get(n), b.get(n), err_msg=n)
+
+
+@pytest.mark.parametrize("n_row", [3, 7, 64, 255])
+@pytest.mark.parametrize("cyclic", [False, True])
+def test_tdma_interface_bitexact_host(tcs, oracle_mod, n_row, cyclic):
+    rng = np.random.default_rng(n_row + 10 * cyclic)
+    n_sys = 333
+    ratio = 0.45 if n_row < 10 else 0.3        # weakly dominant: the one-rank closure is visible
+    A = rng.uniform(-1, 1, (n_row, n_sys)) * ratio
+    C = rng.uniform(-1, 1, (n_row, n_sys)) * ratio
+    B = 1.0 + rng.uniform(0, 1, (n_row, n_sys))
+    D = rng.uniform(-1, 1, (n_row, n_sys))
+    ref = oracle_mod.tdma_many(A, B, C, D, cyclic=cyclic)
+    plan = tcs.TdmaPlan(n_sys)
+    Ag, Bg, Cg, Dg = A.copy(), B.copy(), C.copy(), D.copy()
+    (plan.many_solve_cycle if cyclic else plan.many_solve)(Ag, Bg, Cg, Dg, n_sys, n_row)
+    np.testing.assert_array_equal(Dg, ref)
+    np.testing.assert_array_equal(Bg, B)
+
+
+def test_tdma_interface_device_pointers(tcs, oracle_mod):
+    torch = pytest.importorskip("torch")
+    rng = np.random.default_rng(4)
+    n_sys, n_row = 4096, 96
+    A = rng.uniform(-0.3, 0.3, (n_row, n_sys)); C = rng.uniform(-0.3, 0.3, (n_row, n_sys))
+    B = 1.0 + rng.uniform(0, 1, (n_row, n_sys)); D = rng.uniform(-1, 1, (n_row, n_sys))
+    ref = oracle_mod.tdma_many(A, B, C, D, cyclic=True)
+    t = [torch.tensor(x, device="cuda") for x in (A, B, C, D)]
+    plan = tcs.TdmaPlan(n_sys)
+    plan.many_solve_cycle(*t, n_sys, n_row)
+    np.testing.assert_array_equal(t[3].cpu().numpy(), ref)
+
+
+def test_tdma_plan_rejects_multirank(tcs):
+    with pytest.raises(tcs.TcsError):
+        tcs.TdmaPlan(16, myrank=0, nprocs=2)
+
+
+def test_blowup_is_reported_and_freezes_fields(tcs):
+    # A time step far beyond the stability limit makes the fields grow until the
+    # round-off divergence after projection passes 1e-3 (main.f90:208-212).
+    g = tcs.Solver(n1m=16, n2m=16, n3m=16)
+    rng = np.random.default_rng(0)
+    U = g.get("U")
+    U[1:-1, 1:-1, 1:-1] = rng.uniform(-50, 50, U[1:-1, 1:-1, 1:-1].shape)
+    g.set("U", U)
+    g.set_dt(5.0)
+    blew = None
+    for n in range(40):
+        try:
+            g.step(1)
+        except tcs.TcsError as e:
+            assert e.code == 4
+            blew = n + 1
+            break
+    assert blew is not None, "no blow-up detected"
+    s = g.scalars()
+    assert s["blowup"] == blew and s["step"] == blew - 1
+    T1 = g.get("T")
+    with pytest.raises(tcs.TcsError):
+        g.step(1)
+    np.testing.assert_array_equal(g.get("T"), T1)
+
+
+def test_unsupported_fft_size_is_rejected(tcs):
+    with pytest.raises(tcs.TcsError) as ei:
+        tcs.Solver(n1m=14, n2m=8, n3m=8)      # 14 = 2 * 7: no radix-7 FFT
+    assert ei.value.code == 3

@@ -105,6 +105,11 @@ int tcs_post_cfl(tcs_ctx *ctx, double *CFL, double *dt); /* module_post.f90:168 
  * blow-up.  *done receives the number of completed steps. */
 int tcs_step(tcs_ctx *ctx, int nsteps, int *done);
 int tcs_get_scalars(tcs_ctx *ctx, double *out);        /* TCS_S_COUNT doubles */
+/* On-device checkpoint of the step state (T, U, V, W, P, dPhat, dP0, scalars) and
+ * its restore: the continue-file write/read of module_post.f90:1264-1454 without
+ * leaving the device (and, unlike those files, including dPhat and dP0). */
+int tcs_snapshot(tcs_ctx *ctx);
+int tcs_restore(tcs_ctx *ctx);
 /* Per-step series recorded by tcs_step: 7 doubles per step
  * (dt used, time, max divergence, CFL, Nu bottom, Nu top, kinetic energy). */
 int tcs_get_history(tcs_ctx *ctx, int first, int count, double *out);

@@ -154,6 +154,9 @@ struct tcs_ctx {
     std::vector<GraphEntry> graphs;
     ProbeState probe;
     int partials = 0;
+    double *snap[7] = {};                // on-device copy of T, U, V, W, P, dPhat, dP0
+    double snap_scal[S_NSCAL] = {};
+    bool have_snap = false;
 };
 
 namespace tcs {
@@ -760,6 +763,40 @@ int tcs_step(tcs_ctx *c, int nsteps, int *done)
     const int steps_now = (int)sc[S_STEP] - (int)sc0[S_STEP];
     if (done) *done = steps_now;
     if (sc[S_BLOWUP] != 0.0) return set_err(TCS_ERR_BLOWUP, "BLOW UP: max divergence >= 1e-3");
+    return TCS_OK;
+}
+
+// On-device checkpoint of the state a time step reads (T, U, V, W, P, dPhat,
+// dP0 and the scalars): a restart that needs no host round trip.
+int tcs_snapshot(tcs_ctx *c)
+{
+    ENTER(c);
+    int r = flush_pending(c);
+    if (r) return r;
+    const size_t bytes = (size_t)c->cx.g.NP * sizeof(double);
+    const int fl[7] = {TCS_F_T, TCS_F_U, TCS_F_V, TCS_F_W, TCS_F_P, TCS_F_DPHAT, TCS_F_DP0};
+    for (int q = 0; q < 7; q++) {
+        if (!c->snap[q] && (r = dalloc(c, &c->snap[q], (size_t)c->cx.g.NP))) return r;
+        CK(cudaMemcpyAsync(c->snap[q], field_ptr(c, fl[q]), bytes, cudaMemcpyDeviceToDevice, c->stream));
+    }
+    CK(cudaMemcpyAsync(c->snap_scal, c->cx.g.scal, sizeof(c->snap_scal), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    c->have_snap = true;
+    return TCS_OK;
+}
+
+int tcs_restore(tcs_ctx *c)
+{
+    ENTER(c);
+    if (!c->have_snap) return set_err(TCS_ERR_ARG, "no snapshot");
+    int r = flush_pending(c);
+    if (r) return r;
+    const size_t bytes = (size_t)c->cx.g.NP * sizeof(double);
+    const int fl[7] = {TCS_F_T, TCS_F_U, TCS_F_V, TCS_F_W, TCS_F_P, TCS_F_DPHAT, TCS_F_DP0};
+    for (int q = 0; q < 7; q++)
+        CK(cudaMemcpyAsync(field_ptr(c, fl[q]), c->snap[q], bytes, cudaMemcpyDeviceToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->cx.g.scal, c->snap_scal, sizeof(c->snap_scal), cudaMemcpyHostToDevice, c->stream));
+    c->ghost_ok |= (1u << TCS_F_T) | (1u << TCS_F_U) | (1u << TCS_F_V) | (1u << TCS_F_W) | (1u << TCS_F_P) | (1u << TCS_F_DPHAT);
     return TCS_OK;
 }
 

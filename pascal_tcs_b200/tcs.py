@@ -36,6 +36,7 @@ EXPORTS = [
     "tcs_momentum_blockLdU", "tcs_momentum_pseudoupdateUVW", "tcs_momentum_coeffi_clean",
     "tcs_pressure_RHS", "tcs_pressure_Poisson_FFT2", "tcs_pressure_Projection",
     "tcs_post_div", "tcs_post_cfl", "tcs_step", "tcs_get_scalars", "tcs_get_history",
+    "tcs_snapshot", "tcs_restore",
     "tcs_tdma_plan_many_create", "tcs_tdma_plan_many_destroy", "tcs_tdma_many_solve",
     "tcs_tdma_many_solve_cycle", "tcs_kernel_count", "tcs_launch_count", "tcs_kernel_name", "tcs_probe_enable",
     "tcs_probe_read", "tcs_probe_reset", "tcs_set_use_graph", "tcs_last_error",
@@ -121,7 +122,7 @@ def load() -> ctypes.CDLL:
                  "tcs_momentum_coeffi", "tcs_momentum_solvedU", "tcs_momentum_solvedV",
                  "tcs_momentum_solvedW", "tcs_momentum_blockLdV", "tcs_momentum_blockLdU",
                  "tcs_momentum_pseudoupdateUVW", "tcs_momentum_coeffi_clean", "tcs_pressure_RHS",
-                 "tcs_pressure_Poisson_FFT2", "tcs_pressure_Projection"):
+                 "tcs_pressure_Poisson_FFT2", "tcs_pressure_Projection", "tcs_snapshot", "tcs_restore"):
         sig[name] = ([vp], ip)
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -163,6 +164,7 @@ class Solver:
         _check(L.tcs_dims(h, d), "tcs_dims")
         self.shape = (d[2], d[1], d[0])
         self.n1m, self.n2m, self.n3m = (self.config[k] for k in ("n1m", "n2m", "n3m"))
+        self._since_restore = 0
 
     def close(self) -> None:
         if getattr(self, "_h", None) and _lib is not None:
@@ -282,12 +284,28 @@ class Solver:
         self.momentum_coeffi_clean()
         div = self.post_div()
         self.post_cfl()
+        self._since_restore += 1
         return div
 
     def step(self, n: int = 1) -> int:
         done = ctypes.c_int()
         _check(load().tcs_step(self._h, int(n), ctypes.byref(done)), "tcs_step")
+        self._since_restore += done.value
         return done.value
+
+    def scalars_step_mod(self, m: int) -> int:
+        """Completed steps since the last restore, modulo m (host-side counter)."""
+        return self._since_restore % m if m else 0
+
+    def snapshot(self) -> None:
+        """Keep an on-device copy of the step state (fields read by a step + scalars)."""
+        self._call("tcs_snapshot")
+        self._since_restore = 0
+
+    def restore(self) -> None:
+        """Return to the last snapshot (device-to-device copies on the solver stream)."""
+        self._call("tcs_restore")
+        self._since_restore = 0
 
     def use_graph(self, on: bool) -> None:
         _check(load().tcs_set_use_graph(self._h, int(bool(on))), "use_graph")

@@ -57,7 +57,7 @@ static const char *const k_names[K_COUNT] = {
     "thermal_z", "thermal_x", "thermal_y", "momentum_coeffi",
     "du_z", "du_x", "du_y", "dv_z", "dv_x", "dv_y", "dw_z", "dw_x", "dw_y",
     "blockld_v", "blockld_u", "pseudo_update", "prhs_fftx", "fftz_fwd", "modal_tdma", "mean",
-    "fftz_inv", "ifftx", "dp_wall", "projection", "post", "finalize", "tdma_api"};
+    "fftz_inv", "ifftx", "dp_wall", "projection", "p_wall", "post", "finalize", "tdma_api"};
 
 const char *kernel_name(int kid) { return (kid >= 0 && kid < K_COUNT) ? k_names[kid] : "?"; }
 
@@ -118,7 +118,7 @@ static int choose_tl(int n, bool cyclic, int nrhs, int want)
 {
     LinePlan lp = make_line_plan(n, cyclic, want);
     int tl = want;
-    while (tl > 2 && (size_t)(2 + nrhs) * tl * lp.LS * sizeof(double) > 112 * 1024) tl /= 2;
+    while (tl > 2 && (size_t)(2 + nrhs) * tl * lp.LS * sizeof(double) + (size_t)n * sizeof(int) > 112 * 1024) tl /= 2;
     return tl;
 }
 
@@ -219,6 +219,16 @@ static void set_properties(const tcs_config &c, Phys &p)
     }
     p.a12pera11 = (p.a12 < 1.0e-14) ? 0.0 : p.a12 / p.a11;
     p.Rho0 = p.a10; p.Cp0 = p.b10; p.KPP0 = p.c10; p.Mu0 = p.a10 * p.d10;
+    p.cK = p.c10 / p.KPP0;
+    p.cRC = p.Rho0 * p.Cp0 / (p.a10 * p.b10);
+    p.k2 = 2.0 * p.c12; p.k3 = 3.0 * p.c13; p.k4 = 4.0 * p.c14; p.k5 = 5.0 * p.c15;
+    // numerator of d(invRhoCp)/dT (module_solve_thermal.f90:144-148) in powers of t
+    p.n0 = p.a11 + p.b11;
+    p.n1 = 2.0 * p.a11 * p.b11 + 2.0 * p.b12 + 2.0 * p.a12;
+    p.n2 = 3.0 * p.a12 * p.b11 + 3.0 * p.a11 * p.b12 + 3.0 * (p.a13 + p.b13);
+    p.n3 = 4.0 * p.a13 * p.b11 + 4.0 * p.a11 * p.b13 + 4.0 * p.a12 * p.b12;
+    p.n4 = 5.0 * p.a13 * p.b12 + 5.0 * p.a12 * p.b13;
+    p.n5 = 6.0 * p.a13 * p.b13;
     p.Cmu = std::sqrt(c.Pr / c.Ra); p.Cmt = 1.0; p.Ct = 1.0 / std::sqrt(c.Ra * c.Pr); p.Cmp = 1.0;
     p.DeltaT = c.DeltaT; p.MaxCFL = c.MaxCFL;
     p.L1 = c.H * c.aspect1; p.L2 = c.H; p.L3 = c.H * c.aspect3;

@@ -32,6 +32,10 @@ struct Phys {
     double Tup, Tbt, Uup, Ubt, Vup, Vbt, Wup, Wbt;
     double MaxCFL, dtMax;
     double L1, L2, L3;
+    double cK;       // c10 / KPP0
+    double cRC;      // Rho0 * Cp0 / (a10 * b10)
+    double k2, k3, k4, k5;               // 2 c12, 3 c13, 4 c14, 5 c15 (dKPP in Horner form)
+    double n0, n1, n2, n3, n4, n5;       // d(invRhoCp)/dT numerator collected in powers of DeltaT*T
 };
 
 // Device scalar block (one per case).  dt is read by every kernel so the
@@ -87,33 +91,33 @@ __device__ __forceinline__ int wrap3(const Grid &g, int k) { return k < 1 ? k + 
 // (module_solve_thermal.f90:129-154), evaluated at the point where the
 // stencil needs them instead of being stored.
 // ---------------------------------------------------------------------------
+// Horner forms of KPP = c10 (1 + c11 t + ... + c15 t^5) / KPP0 and its derivative.
 __device__ __forceinline__ void kpp_eval(const Phys &p, double T, double &kpp, double &dkpp)
 {
-    const double t1 = p.DeltaT * T, t2 = t1 * t1, t3 = t2 * t1, t4 = t3 * t1, t5 = t4 * t1;
-    kpp = p.c10 * (1.0 + p.c11 * t1 + p.c12 * t2 + p.c13 * t3 + p.c14 * t4 + p.c15 * t5) / p.KPP0;
-    dkpp = p.c10 * (p.c11 + 2.0 * p.c12 * t1 + 3.0 * p.c13 * t2 + 4.0 * p.c14 * t3 + 5.0 * p.c15 * t4) / p.KPP0;
+    const double t = p.DeltaT * T;
+    kpp = p.cK * (1.0 + t * (p.c11 + t * (p.c12 + t * (p.c13 + t * (p.c14 + t * p.c15)))));
+    dkpp = p.cK * (p.c11 + t * (p.k2 + t * (p.k3 + t * (p.k4 + t * p.k5))));
 }
 
 __device__ __forceinline__ double kpp_only(const Phys &p, double T)
 {
-    const double t1 = p.DeltaT * T, t2 = t1 * t1, t3 = t2 * t1, t4 = t3 * t1, t5 = t4 * t1;
-    return p.c10 * (1.0 + p.c11 * t1 + p.c12 * t2 + p.c13 * t3 + p.c14 * t4 + p.c15 * t5) / p.KPP0;
+    const double t = p.DeltaT * T;
+    return p.cK * (1.0 + t * (p.c11 + t * (p.c12 + t * (p.c13 + t * (p.c14 + t * p.c15)))));
 }
 
+// invRhoCp = Rho0 Cp0 / (a10 (1 + A)) / (b10 (1 + B)) and its T-derivative
+// share one reciprocal of q1 q2 = (1 + A)(1 + B): every property set of
+// module_global.f90 has a14 = a15 = b14 = b15 = 0, so 1 + A is the q1 of
+// module_solve_thermal.f90:149.  The derivative's numerator (:144-148) is
+// collected into a polynomial in t = DeltaT*T with coefficients n0..n5.
 __device__ __forceinline__ void rhocp_eval(const Phys &p, double T, double &irc, double &dirc)
 {
-    const double t1 = p.DeltaT * T, t2 = t1 * t1, t3 = t2 * t1, t4 = t3 * t1, t5 = t4 * t1;
-    irc = p.Rho0 * p.Cp0
-        / (p.a10 + p.a10 * (p.a11 * t1 + p.a12 * t2 + p.a13 * t3 + p.a14 * t4 + p.a15 * t5))
-        / (p.b10 + p.b10 * (p.b11 * t1 + p.b12 * t2 + p.b13 * t3 + p.b14 * t4 + p.b15 * t5));
-    const double q1 = (1.0 + p.a11 * t1 + p.a12 * t2 + p.a13 * t3);
-    const double q2 = (1.0 + p.b11 * t1 + p.b12 * t2 + p.b13 * t3);
-    dirc = -(p.b11 * (1.0 + 3.0 * p.a12 * t2 + 4.0 * p.a13 * t3)
-             + p.a11 * (1.0 + 2.0 * p.b11 * t1 + 3.0 * p.b12 * t2 + 4.0 * p.b13 * t3)
-             + t1 * (p.b12 * (2.0 + 5.0 * p.a13 * t3)
-                     + p.a12 * (2.0 + 4.0 * p.b12 * t2 + 5.0 * p.b13 * t3)
-                     + 3.0 * t1 * (p.a13 + p.b13 + 2.0 * p.a13 * p.b13 * t3)))
-         / (q1 * q1) / (q2 * q2);
+    const double t = p.DeltaT * T;
+    const double q1 = 1.0 + t * (p.a11 + t * (p.a12 + t * p.a13));
+    const double q2 = 1.0 + t * (p.b11 + t * (p.b12 + t * p.b13));
+    const double rq = 1.0 / (q1 * q2);
+    irc = p.cRC * rq;
+    dirc = -(p.n0 + t * (p.n1 + t * (p.n2 + t * (p.n3 + t * (p.n4 + t * p.n5))))) * (rq * rq);
 }
 
 // ---------------------------------------------------------------------------
@@ -277,35 +281,64 @@ __device__ __forceinline__ void warp_solve_line(double *A, double *C, double *D,
 
 // The kernel.  Prob supplies:
 //   static constexpr int NRHS;  static constexpr bool CONTIG (rows contiguous in memory);
-//   __device__ bool tile(int l)            -> line l of this block exists
-//   __device__ Coef<NRHS> build(int l, int r)
-//   __device__ void emit(int l, int r, const double *x)
+//   struct State; __device__ State prepare()   -> per-block scalars (dt, stale values)
+//   __device__ bool skip(), line_ok(int l)
+//   __device__ Coef<NRHS> build(int l, int r, const State &)
+//   __device__ void emit(int l, int r, const double *x, const State &)
+// TL (lines per block) is a power of two; blockDim.x is 256.
 template <class Prob>
 __global__ void __launch_bounds__(256, 2) line_solve_kernel(Prob prob, LinePlan lp)
 {
     constexpr int NR = Prob::NRHS;
     extern __shared__ double sm[];
     if (prob.skip()) return;
+    const typename Prob::State st = prob.prepare();
     const int TL = lp.TL, n = lp.n, LS = lp.LS;
+    const int lgTL = __ffs(TL) - 1;
     double *sA = sm, *sC = sA + TL * LS, *sD = sC + TL * LS;
+    int *spos = (int *)(sD + NR * TL * LS);
     const int DS = TL * LS;
-    const int nitems = TL * n;
-    for (int t = threadIdx.x; t < nitems; t += blockDim.x) {
-        int l, r;
-        if (Prob::CONTIG) { l = t / n; r = t - l * n; }
-        else { r = t / TL; l = t - r * TL; }
-        const int pos = l * LS + lp_pos(lp, r);
-        if (prob.line_ok(l)) {
-            Coef<NR> cf = prob.build(l, r);
-            const double rb = 1.0 / cf.b;
-            sA[pos] = cf.a * rb;
-            sC[pos] = cf.c * rb;
+    // row -> shared-memory position: partition p holds rows start_p .. start_p + m_p - 1
+    if (threadIdx.x < lp.P) {
+        const int p = threadIdx.x, m = lp.m0 + (p < lp.rem ? 1 : 0);
+        const int start = p * lp.m0 + (p < lp.rem ? p : lp.rem);
+        for (int q = 0; q < m; q++) spos[start + q] = p * lp.PS + q;
+    }
+    __syncthreads();
+    if (Prob::CONTIG) {
+        for (int l = 0; l < TL; l++) {
+            const bool ok = prob.line_ok(l);
+            for (int r = threadIdx.x; r < n; r += blockDim.x) {
+                const int pos = l * LS + spos[r];
+                if (ok) {
+                    const Coef<NR> cf = prob.build(l, r, st);
+                    const double rb = 1.0 / cf.b;
+                    sA[pos] = cf.a * rb; sC[pos] = cf.c * rb;
 #pragma unroll
-            for (int q = 0; q < NR; q++) sD[q * DS + pos] = cf.d[q] * rb;
-        } else {
-            sA[pos] = 0.0; sC[pos] = 0.0;
+                    for (int q = 0; q < NR; q++) sD[q * DS + pos] = cf.d[q] * rb;
+                } else {
+                    sA[pos] = 0.0; sC[pos] = 0.0;
 #pragma unroll
-            for (int q = 0; q < NR; q++) sD[q * DS + pos] = 0.0;
+                    for (int q = 0; q < NR; q++) sD[q * DS + pos] = 0.0;
+                }
+            }
+        }
+    } else {
+        const int nitems = TL * n;
+        for (int t = threadIdx.x; t < nitems; t += blockDim.x) {
+            const int r = t >> lgTL, l = t & (TL - 1);
+            const int pos = l * LS + spos[r];
+            if (prob.line_ok(l)) {
+                const Coef<NR> cf = prob.build(l, r, st);
+                const double rb = 1.0 / cf.b;
+                sA[pos] = cf.a * rb; sC[pos] = cf.c * rb;
+#pragma unroll
+                for (int q = 0; q < NR; q++) sD[q * DS + pos] = cf.d[q] * rb;
+            } else {
+                sA[pos] = 0.0; sC[pos] = 0.0;
+#pragma unroll
+                for (int q = 0; q < NR; q++) sD[q * DS + pos] = 0.0;
+            }
         }
     }
     __syncthreads();
@@ -313,16 +346,28 @@ __global__ void __launch_bounds__(256, 2) line_solve_kernel(Prob prob, LinePlan 
     for (int l = warp; l < TL; l += nw)
         warp_solve_line<NR>(sA + l * LS, sC + l * LS, sD + l * LS, DS, lp, lane);
     __syncthreads();
-    for (int t = threadIdx.x; t < nitems; t += blockDim.x) {
-        int l, r;
-        if (Prob::CONTIG) { l = t / n; r = t - l * n; }
-        else { r = t / TL; l = t - r * TL; }
-        if (!prob.line_ok(l)) continue;
-        const int pos = l * LS + lp_pos(lp, r);
-        double x[NR];
+    if (Prob::CONTIG) {
+        for (int l = 0; l < TL; l++) {
+            if (!prob.line_ok(l)) continue;
+            for (int r = threadIdx.x; r < n; r += blockDim.x) {
+                const int pos = l * LS + spos[r];
+                double x[NR];
 #pragma unroll
-        for (int q = 0; q < NR; q++) x[q] = sD[q * DS + pos];
-        prob.emit(l, r, x);
+                for (int q = 0; q < NR; q++) x[q] = sD[q * DS + pos];
+                prob.emit(l, r, x, st);
+            }
+        }
+    } else {
+        const int nitems = TL * n;
+        for (int t = threadIdx.x; t < nitems; t += blockDim.x) {
+            const int r = t >> lgTL, l = t & (TL - 1);
+            if (!prob.line_ok(l)) continue;
+            const int pos = l * LS + spos[r];
+            double x[NR];
+#pragma unroll
+            for (int q = 0; q < NR; q++) x[q] = sD[q * DS + pos];
+            prob.emit(l, r, x, st);
+        }
     }
 }
 

@@ -14,7 +14,7 @@ enum KernelId : int {
     K_THERMAL_Z = 0, K_THERMAL_X, K_THERMAL_Y, K_MOM_COEFFI,
     K_DU_Z, K_DU_X, K_DU_Y, K_DV_Z, K_DV_X, K_DV_Y, K_DW_Z, K_DW_X, K_DW_Y,
     K_BLOCKLDV, K_BLOCKLDU, K_PSEUDO, K_PRHS_FFTX, K_FFTZ_FWD, K_MODAL, K_MEAN,
-    K_FFTZ_INV, K_IFFTX, K_DP_WALL, K_PROJECT, K_POST, K_FINAL, K_TDMA_API,
+    K_FFTZ_INV, K_IFFTX, K_DP_WALL, K_PROJECT, K_P_WALL, K_POST, K_FINAL, K_TDMA_API,
     K_COUNT
 };
 
@@ -47,7 +47,7 @@ int record_launch_error(const char *what);
 template <class Prob>
 inline void launch_lines(const Prob &p, const LinePlan &lp, dim3 grid, cudaStream_t s, int kid, const Ctx &cx)
 {
-    const size_t smem = (size_t)(2 + Prob::NRHS) * lp.TL * lp.LS * sizeof(double);
+    const size_t smem = (size_t)(2 + Prob::NRHS) * lp.TL * lp.LS * sizeof(double) + (size_t)lp.n * sizeof(int);
     static size_t configured = 0;
     if (smem > configured) {
         cudaFuncSetAttribute(line_solve_kernel<Prob>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

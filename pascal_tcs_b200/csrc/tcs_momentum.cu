@@ -47,9 +47,11 @@ struct DUZ {
     static constexpr bool CONTIG = false;
     Grid g; Fields f; int TL;
     __device__ bool skip() const { return blown(g); }
+    struct State { double dt; };
+    __device__ State prepare() const { return State{g.scal[S_DT]}; }
     __device__ int li(int l) const { return 1 + blockIdx.x * TL + l; }
     __device__ bool line_ok(int l) const { return li(l) <= g.N1; }
-    __device__ Coef<1> build(int l, int r) const
+    __device__ Coef<1> build(int l, int r, const State &st) const
     {
         const int i = li(l), j = 1 + blockIdx.y, k = r + 1;
         const int im = i - 1, ip = i + 1, jm = j - 1, jp = j + 1, km = k - 1, kp = k + 1;
@@ -115,12 +117,12 @@ struct DUZ {
         rhs = rhs - (mAPI * Uxp + mACI * Uc + mAMI * Uxm + mAPJ * Uyp + mACJ * Uc + mAMJ * Uym + mAPK * Uzp + mACK * Uc + mAMK * Uzm);
         rhs = rhs - (0.25 * (v4 * jup * dudy4 + v3 * jum * dudy3) - ih * rdx2[j] * (mu4 * dvdx4 * jup - mu3 * dvdx3 * jum));
         rhs = rhs - (0.25 * (w6 * dudz6 + w5 * dudz5) - ih * rdx3[k] * (mu6 * dwdx6 - mu5 * dwdx5));
-        const double dt = g.scal[S_DT];
+        const double dt = st.dt;
         Coef<1> cf;
         cf.b = mACK * dt + 1.0; cf.c = mAPK * dt; cf.a = mAMK * dt; cf.d[0] = rhs * dt;
         return cf;
     }
-    __device__ void emit(int l, int r, const double *x) const { f.R[ix(g, li(l), 1 + blockIdx.y, r + 1)] = x[0]; }
+    __device__ void emit(int l, int r, const double *x, const State &st) const { f.R[ix(g, li(l), 1 + blockIdx.y, r + 1)] = x[0]; }
 };
 
 struct DUX {
@@ -128,9 +130,11 @@ struct DUX {
     static constexpr bool CONTIG = true;
     Grid g; Fields f; int TL;
     __device__ bool skip() const { return blown(g); }
+    struct State { double dt; };
+    __device__ State prepare() const { return State{g.scal[S_DT]}; }
     __device__ int lj(int l) const { return 1 + blockIdx.x * TL + l; }
     __device__ bool line_ok(int l) const { return lj(l) <= g.N2; }
-    __device__ Coef<1> build(int l, int r) const
+    __device__ Coef<1> build(int l, int r, const State &st) const
     {
         const int i = r + 1, j = lj(l), k = 1 + blockIdx.y, im = i - 1;
         const Phys &p = g.ph;
@@ -145,12 +149,12 @@ struct DUX {
         const double mACI = ih * rdmx1[i] * (Mjk * rdx1[i] + Mjk * rdx1[im]) * 2.0 + 0.25 * (dudx2 * 0.5 + dudx1 * 0.5 - u2 * rdx1[i] + u1 * rdx1[im]);
         const double mAPI = -ih * rdmx1[i] * Mjk * rdx1[i] * 2.0 + 0.25 * (u2 * rdx1[i] + dudx2 * 0.5);
         const double mAMI = -ih * rdmx1[i] * Mjk * rdx1[im] * 2.0 + 0.25 * (-u1 * rdx1[im] + dudx1 * 0.5);
-        const double dt = g.scal[S_DT];
+        const double dt = st.dt;
         Coef<1> cf;
         cf.b = mACI * dt + 1.0; cf.c = mAPI * dt; cf.a = mAMI * dt; cf.d[0] = ld(f.R + c);
         return cf;
     }
-    __device__ void emit(int l, int r, const double *x) const { f.R[ix(g, r + 1, lj(l), 1 + blockIdx.y)] = x[0]; }
+    __device__ void emit(int l, int r, const double *x, const State &st) const { f.R[ix(g, r + 1, lj(l), 1 + blockIdx.y)] = x[0]; }
 };
 
 struct DUY {
@@ -158,9 +162,11 @@ struct DUY {
     static constexpr bool CONTIG = false;
     Grid g; Fields f; int TL;
     __device__ bool skip() const { return blown(g); }
+    struct State { double dt; };
+    __device__ State prepare() const { return State{g.scal[S_DT]}; }
     __device__ int li(int l) const { return 1 + blockIdx.x * TL + l; }
     __device__ bool line_ok(int l) const { return li(l) <= g.N1; }
-    __device__ Coef<1> build(int l, int r) const
+    __device__ Coef<1> build(int l, int r, const State &st) const
     {
         const int i = li(l), j = r + 1, k = 1 + blockIdx.y, im = i - 1, jm = j - 1, jp = j + 1;
         const Phys &p = g.ph;
@@ -181,12 +187,12 @@ struct DUY {
         const double mACJ = ih * rdx2[j] * (mu4 * rdmx2[jp] + mu3 * rdmx2[j]) + 0.25 * (-v4 * rdmx2[jp] + v3 * rdmx2[j]);
         const double mAPJ = (-ih * rdx2[j] * mu4 * rdmx2[jp] + 0.25 * (v4 * rdmx2[jp])) * jup;
         const double mAMJ = (-ih * rdx2[j] * mu3 * rdmx2[j] + 0.25 * (-v3 * rdmx2[j])) * jum;
-        const double dt = g.scal[S_DT];
+        const double dt = st.dt;
         Coef<1> cf;
         cf.b = mACJ * dt + 1.0; cf.c = mAPJ * dt; cf.a = mAMJ * dt; cf.d[0] = ld(f.R + c);
         return cf;
     }
-    __device__ void emit(int l, int r, const double *x) const { store_periodic(g, f.dU, li(l), r + 1, 1 + blockIdx.y, x[0]); }
+    __device__ void emit(int l, int r, const double *x, const State &st) const { store_periodic(g, f.dU, li(l), r + 1, 1 + blockIdx.y, x[0]); }
 };
 
 // ---------------------------------------------------------------------------
@@ -199,9 +205,11 @@ struct DVZ {
     static constexpr bool CONTIG = false;
     Grid g; Fields f; int TL;
     __device__ bool skip() const { return blown(g); }
+    struct State { double dt; };
+    __device__ State prepare() const { return State{g.scal[S_DT]}; }
     __device__ int li(int l) const { return 1 + blockIdx.x * TL + l; }
     __device__ bool line_ok(int l) const { return li(l) <= g.N1; }
-    __device__ Coef<1> build(int l, int r) const
+    __device__ Coef<1> build(int l, int r, const State &st) const
     {
         const int i = li(l), j = 2 + blockIdx.y, k = r + 1;
         const int im = i - 1, ip = i + 1, jm = j - 1, jp = j + 1, km = k - 1, kp = k + 1;
@@ -268,12 +276,12 @@ struct DVZ {
         rhs = rhs - (0.25 * (u2 * dvdx2 + u1 * dvdx1) - ih * rdx1[i] * (mu2 * dudy2 - mu1 * dudy1));
         rhs = rhs - (0.25 * (w6 * dvdz6 + w5 * dvdz5) - ih * rdx3[k] * (mu6 * dwdy6 - mu5 * dwdy5));
         rhs = rhs - (0.25 * (ddu2 * dvdx2 + ddu1 * dvdx1) - ih * rdx1[i] * (mu2 * ddudy2 - mu1 * ddudy1));
-        const double dt = g.scal[S_DT];
+        const double dt = st.dt;
         Coef<1> cf;
         cf.b = mACK * dt + 1.0; cf.c = mAPK * dt; cf.a = mAMK * dt; cf.d[0] = rhs * dt;
         return cf;
     }
-    __device__ void emit(int l, int r, const double *x) const { f.R[ix(g, li(l), 2 + blockIdx.y, r + 1)] = x[0]; }
+    __device__ void emit(int l, int r, const double *x, const State &st) const { f.R[ix(g, li(l), 2 + blockIdx.y, r + 1)] = x[0]; }
 };
 
 // mu1, mu2 of solvedV's last stage-1 iteration (i = N1, j = N2, k = N3).
@@ -291,16 +299,23 @@ struct DVX {
     static constexpr bool CONTIG = true;
     Grid g; Fields f; int TL;
     __device__ bool skip() const { return blown(g); }
+    struct State { double dt, mu1, mu2; };
+    __device__ State prepare() const
+    {
+        State s;
+        s.dt = g.scal[S_DT];
+        dv_stale_mu12(g, f, s.mu1, s.mu2);
+        return s;
+    }
     __device__ int lj(int l) const { return 2 + blockIdx.x * TL + l; }
     __device__ bool line_ok(int l) const { return lj(l) <= g.N2; }
-    __device__ Coef<1> build(int l, int r) const
+    __device__ Coef<1> build(int l, int r, const State &st) const
     {
         const int i = r + 1, j = lj(l), k = 1 + blockIdx.y, ip = i + 1, jm = j - 1;
         const Phys &p = g.ph;
         const double *dx2 = g.m2.dx, *rdx1 = g.m1.rdx, *rdmx1 = g.m1.rdmx, *rdmx2 = g.m2.rdmx;
         const long long c = ix(g, i, j, k), sj = g.P1;
-        double mu1, mu2;
-        dv_stale_mu12(g, f, mu1, mu2);
+        const double mu1 = st.mu1, mu2 = st.mu2;
         const double u1 = (dx2[jm] * ld(f.U + c) + dx2[j] * ld(f.U + c - sj)) * rdmx2[j] * 0.5;
         const double u2 = (dx2[jm] * ld(f.U + c + 1) + dx2[j] * ld(f.U + c + 1 - sj)) * rdmx2[j] * 0.5;
         const double invRhoc = 0.5 * (dx2[jm] * IR(j, k) + dx2[j] * IR(jm, k)) * rdmx2[j];
@@ -308,12 +323,12 @@ struct DVX {
         const double mACI = ih * rdx1[i] * (mu2 * rdmx1[ip] + mu1 * rdmx1[i]) + 0.25 * (-u2 * rdmx1[ip] + u1 * rdmx1[i]);
         const double mAPI = -ih * rdx1[i] * mu2 * rdmx1[ip] + 0.25 * (u2 * rdmx1[ip]);
         const double mAMI = -ih * rdx1[i] * mu1 * rdmx1[i] + 0.25 * (-u1 * rdmx1[i]);
-        const double dt = g.scal[S_DT];
+        const double dt = st.dt;
         Coef<1> cf;
         cf.b = mACI * dt + 1.0; cf.c = mAPI * dt; cf.a = mAMI * dt; cf.d[0] = ld(f.R + c);
         return cf;
     }
-    __device__ void emit(int l, int r, const double *x) const { f.R[ix(g, r + 1, lj(l), 1 + blockIdx.y)] = x[0]; }
+    __device__ void emit(int l, int r, const double *x, const State &st) const { f.R[ix(g, r + 1, lj(l), 1 + blockIdx.y)] = x[0]; }
 };
 
 struct DVY {
@@ -321,9 +336,11 @@ struct DVY {
     static constexpr bool CONTIG = false;
     Grid g; Fields f; int TL;
     __device__ bool skip() const { return blown(g); }
+    struct State { double dt; };
+    __device__ State prepare() const { return State{g.scal[S_DT]}; }
     __device__ int li(int l) const { return 1 + blockIdx.x * TL + l; }
     __device__ bool line_ok(int l) const { return li(l) <= g.N1; }
-    __device__ Coef<1> build(int l, int r) const
+    __device__ Coef<1> build(int l, int r, const State &st) const
     {
         const int i = li(l), j = r + 2, k = 1 + blockIdx.y, jm = j - 1, jp = j + 1;
         const Phys &p = g.ph;
@@ -339,12 +356,12 @@ struct DVY {
         const double mACJ = ih * rdmx2[j] * (Mjk * rdx2[j] + Mjmk * rdx2[jm]) * 2.0 + 0.25 * (dvdy4 * 0.5 + dvdy3 * 0.5 - v4 * rdx2[j] + v3 * rdx2[jm]);
         const double mAPJ = (-ih * rdmx2[j] * Mjk * rdx2[j] * 2.0 + 0.25 * (v4 * rdx2[j] + dvdy4 * 0.5)) * jvp;
         const double mAMJ = (-ih * rdmx2[j] * Mjmk * rdx2[jm] * 2.0 + 0.25 * (-v3 * rdx2[jm] + dvdy3 * 0.5)) * jvm;
-        const double dt = g.scal[S_DT];
+        const double dt = st.dt;
         Coef<1> cf;
         cf.b = mACJ * dt + 1.0; cf.c = mAPJ * dt; cf.a = mAMJ * dt; cf.d[0] = ld(f.R + c);
         return cf;
     }
-    __device__ void emit(int l, int r, const double *x) const { store_periodic(g, f.dV, li(l), r + 2, 1 + blockIdx.y, x[0]); }
+    __device__ void emit(int l, int r, const double *x, const State &st) const { store_periodic(g, f.dV, li(l), r + 2, 1 + blockIdx.y, x[0]); }
 };
 
 // ---------------------------------------------------------------------------
@@ -356,9 +373,11 @@ struct DWZ {
     static constexpr bool CONTIG = false;
     Grid g; Fields f; int TL;
     __device__ bool skip() const { return blown(g); }
+    struct State { double dt; };
+    __device__ State prepare() const { return State{g.scal[S_DT]}; }
     __device__ int li(int l) const { return 1 + blockIdx.x * TL + l; }
     __device__ bool line_ok(int l) const { return li(l) <= g.N1; }
-    __device__ Coef<1> build(int l, int r) const
+    __device__ Coef<1> build(int l, int r, const State &st) const
     {
         const int i = li(l), j = 1 + blockIdx.y, k = r + 1;
         const int im = i - 1, ip = i + 1, jm = j - 1, jp = j + 1, km = k - 1, kp = k + 1;
@@ -430,12 +449,12 @@ struct DWZ {
         rhs = rhs - (0.25 * (v3 * jwm * dwdy3 + v4 * jwp * dwdy4) - ih * rdx2[j] * (mu4 * dvdz4 * jwp - mu3 * dvdz3 * jwm));
         rhs = rhs - (0.25 * (ddu2 * dwdx2 + ddu1 * dwdx1) - ih * rdx1[i] * (mu2 * ddudz2 - mu1 * ddudz1));
         rhs = rhs - (0.25 * (ddv3 * jwm * dwdy3 + ddv4 * jwp * dwdy4) - ih * rdx2[j] * (mu4 * ddvdz4 * jwp - mu3 * ddvdz3 * jwm));
-        const double dt = g.scal[S_DT];
+        const double dt = st.dt;
         Coef<1> cf;
         cf.b = mACK * dt + 1.0; cf.c = mAPK * dt; cf.a = mAMK * dt; cf.d[0] = rhs * dt;
         return cf;
     }
-    __device__ void emit(int l, int r, const double *x) const { f.R[ix(g, li(l), 1 + blockIdx.y, r + 1)] = x[0]; }
+    __device__ void emit(int l, int r, const double *x, const State &st) const { f.R[ix(g, li(l), 1 + blockIdx.y, r + 1)] = x[0]; }
 };
 
 // mu1..mu4 of solvedW's last stage-1 iteration (i = N1, j = N2, k = N3).
@@ -458,16 +477,24 @@ struct DWX {
     static constexpr bool CONTIG = true;
     Grid g; Fields f; int TL;
     __device__ bool skip() const { return blown(g); }
+    struct State { double dt, mu1, mu2, mu3, mu4; };
+    __device__ State prepare() const
+    {
+        State s;
+        s.dt = g.scal[S_DT];
+        dw_stale_mu(g, f, s.mu1, s.mu2, s.mu3, s.mu4);
+        return s;
+    }
     __device__ int lj(int l) const { return 1 + blockIdx.x * TL + l; }
     __device__ bool line_ok(int l) const { return lj(l) <= g.N2; }
-    __device__ Coef<1> build(int l, int r) const
+    __device__ Coef<1> build(int l, int r, const State &st) const
     {
         const int i = r + 1, j = lj(l), k = 1 + blockIdx.y, ip = i + 1, km = k - 1;
         const Phys &p = g.ph;
         const double *dx3 = g.m3.dx, *rdx1 = g.m1.rdx, *rdmx1 = g.m1.rdmx, *rdmx3 = g.m3.rdmx;
         const long long c = ix(g, i, j, k), sk = (long long)g.P1 * g.P2;
-        double mu1, mu2, mu3, mu4;
-        dw_stale_mu(g, f, mu1, mu2, mu3, mu4);
+        const double mu1 = st.mu1, mu2 = st.mu2, mu3 = st.mu3, mu4 = st.mu4;
+        (void)mu1; (void)mu2; (void)mu3; (void)mu4;
         const double u1 = (dx3[km] * ld(f.U + c) + dx3[k] * ld(f.U + c - sk)) * rdmx3[k] * 0.5;
         const double u2 = (dx3[km] * ld(f.U + c + 1) + dx3[k] * ld(f.U + c + 1 - sk)) * rdmx3[k] * 0.5;
         const double invRhoc = 0.5 * (dx3[km] * IR(j, k) + dx3[k] * IR(j, km)) * rdmx3[k];
@@ -475,12 +502,12 @@ struct DWX {
         const double mACI = ih * rdx1[i] * (mu2 * rdmx1[ip] + mu1 * rdmx1[i]) + 0.25 * (-u2 * rdmx1[ip] + u1 * rdmx1[i]);
         const double mAPI = -ih * rdx1[i] * mu2 * rdmx1[ip] + 0.25 * (u2 * rdmx1[ip]);
         const double mAMI = -ih * rdx1[i] * mu1 * rdmx1[i] + 0.25 * (-u1 * rdmx1[i]);
-        const double dt = g.scal[S_DT];
+        const double dt = st.dt;
         Coef<1> cf;
         cf.b = mACI * dt + 1.0; cf.c = mAPI * dt; cf.a = mAMI * dt; cf.d[0] = ld(f.R + c);
         return cf;
     }
-    __device__ void emit(int l, int r, const double *x) const { f.R[ix(g, r + 1, lj(l), 1 + blockIdx.y)] = x[0]; }
+    __device__ void emit(int l, int r, const double *x, const State &st) const { f.R[ix(g, r + 1, lj(l), 1 + blockIdx.y)] = x[0]; }
 };
 
 struct DWY {
@@ -488,17 +515,25 @@ struct DWY {
     static constexpr bool CONTIG = false;
     Grid g; Fields f; int TL;
     __device__ bool skip() const { return blown(g); }
+    struct State { double dt, mu1, mu2, mu3, mu4; };
+    __device__ State prepare() const
+    {
+        State s;
+        s.dt = g.scal[S_DT];
+        dw_stale_mu(g, f, s.mu1, s.mu2, s.mu3, s.mu4);
+        return s;
+    }
     __device__ int li(int l) const { return 1 + blockIdx.x * TL + l; }
     __device__ bool line_ok(int l) const { return li(l) <= g.N1; }
-    __device__ Coef<1> build(int l, int r) const
+    __device__ Coef<1> build(int l, int r, const State &st) const
     {
         const int i = li(l), j = r + 1, k = 1 + blockIdx.y, jp = j + 1, km = g.N3 - 1;
         const Phys &p = g.ph;
         const double *dx3 = g.m3.dx, *rdx2 = g.m2.rdx, *rdmx2 = g.m2.rdmx, *rdmx3 = g.m3.rdmx;
         const long long c = ix(g, i, j, k), sj = g.P1;
         const double jwm = (j == 1) ? 0.0 : 1.0, jwp = (j == g.N2) ? 0.0 : 1.0;
-        double mu1, mu2, mu3, mu4;
-        dw_stale_mu(g, f, mu1, mu2, mu3, mu4);
+        const double mu1 = st.mu1, mu2 = st.mu2, mu3 = st.mu3, mu4 = st.mu4;
+        (void)mu1; (void)mu2; (void)mu3; (void)mu4;
         const long long ckm = ix(g, i, j, km);
         const double v3 = (dx3[km] * ld(f.V + c) + dx3[k] * ld(f.V + ckm)) * rdmx3[k] * 0.5;
         const double v4 = (dx3[km] * ld(f.V + c + sj) + dx3[k] * ld(f.V + ckm + sj)) * rdmx3[k] * 0.5;
@@ -507,12 +542,12 @@ struct DWY {
         const double mACJ = ih * rdx2[j] * (mu4 * rdmx2[jp] + mu3 * rdmx2[j]) + 0.25 * (-v4 * rdmx2[jp] + v3 * rdmx2[j]);
         const double mAPJ = (-ih * rdx2[j] * mu4 * rdmx2[jp] + 0.25 * (v4 * rdmx2[jp])) * jwp;
         const double mAMJ = (-ih * rdx2[j] * mu3 * rdmx2[j] + 0.25 * (-v3 * rdmx2[j])) * jwm;
-        const double dt = g.scal[S_DT];
+        const double dt = st.dt;
         Coef<1> cf;
         cf.b = mACJ * dt + 1.0; cf.c = mAPJ * dt; cf.a = mAMJ * dt; cf.d[0] = ld(f.R + c);
         return cf;
     }
-    __device__ void emit(int l, int r, const double *x) const { store_periodic(g, f.dW, li(l), r + 1, 1 + blockIdx.y, x[0]); }
+    __device__ void emit(int l, int r, const double *x, const State &st) const { store_periodic(g, f.dW, li(l), r + 1, 1 + blockIdx.y, x[0]); }
 };
 
 void launch_solve_du(const Ctx &cx, cudaStream_t s)

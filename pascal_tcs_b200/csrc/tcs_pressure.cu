@@ -232,9 +232,11 @@ struct Modal {
     static constexpr bool CONTIG = false;
     Grid g; Fields f; int TL; int h1p;
     __device__ bool skip() const { return blown(g); }
+    struct State { double dt; };
+    __device__ State prepare() const { return State{g.scal[S_DT]}; }
     __device__ int lk(int l) const { return blockIdx.x * TL + l; }
     __device__ bool line_ok(int l) const { return lk(l) < h1p; }
-    __device__ Coef<2> build(int l, int r) const
+    __device__ Coef<2> build(int l, int r, const State &st) const
     {
         const int kx = lk(l), kz = blockIdx.y, j = r + 1;
         const double am = f.fam[j], ap = f.fap[j];
@@ -249,7 +251,7 @@ struct Modal {
         }
         return cf;
     }
-    __device__ void emit(int l, int r, const double *x) const
+    __device__ void emit(int l, int r, const double *x, const State &st) const
     {
         const int kx = lk(l), kz = blockIdx.y, j = r + 1;
         const bool zi = (kx == 0) && (kz == 0 || kz == g.N3 / 2);
@@ -319,13 +321,14 @@ __global__ void dp_wall_kernel(Grid g, Fields f, double ab, double bb, double at
 }
 
 // ---------------------------------------------------------------------------
-// mpi_pressure_Projection (:756-874) + ghost(U,V,W,P,dPhat).  One thread per
-// (i,k) column.  The reference sweeps k, then j = 2..N2, then j = 1, with i
+// mpi_pressure_Projection (:756-874) + ghost(U,V,W,P,dPhat), one thread per
+// cell.  The reference sweeps k, then j = 2..N2, then j = 1, with i
 // innermost, updating dPhat in place, so the pressure-correction term of a
 // cell reads the NEW dPhat of its x-lower neighbour (i >= 2), of its y-lower
 // neighbour (j >= 3) and of its z-lower neighbour (k >= 2), and the old value
-// otherwise.  New values are recomputed here from the old ones with the same
-// arithmetic: dP0n = (dPhat + dP0)/2, dPhatn = 2 dP - dP0n.
+// otherwise.  New values are recomputed from the old ones with the same
+// arithmetic (dP0n = (dPhat + dP0)/2, dPhatn = 2 dP - dP0n) and written to
+// the second buffers.  The P wall rows (:853-869) follow in p_wall_kernel.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ double new_phat(const Fields &f, long long n)
 {
@@ -333,52 +336,48 @@ __device__ __forceinline__ double new_phat(const Fields &f, long long n)
     return 2.0 * ld(f.dP + n) - dp0n;
 }
 
-__global__ void projection_kernel(Grid g, Fields f, double ab, double bb, double at, double bt)
+__global__ void __launch_bounds__(256) projection_kernel(Grid g, Fields f)
+{
+    const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x, j = 1 + blockIdx.y, k = 1 + blockIdx.z;
+    if (i > g.N1 || blown(g)) return;
+    const int im = i - 1, jm = j - 1, km = k - 1;
+    const double *dx1 = g.m1.dx, *dx2 = g.m2.dx, *dx3 = g.m3.dx;
+    const double *rdmx1 = g.m1.rdmx, *rdmx2 = g.m2.rdmx, *rdmx3 = g.m3.rdmx;
+    const long long c = ix(g, i, j, k), sj = g.P1, sk = (long long)g.P1 * g.P2;
+    const double dtc = g.scal[S_DT] * g.ph.Cmp;
+    const double dPc = ld(f.dP + c), ph = ld(f.dPhat + c), p0 = ld(f.dP0 + c);
+    const double dp0n = (ph + p0) / 2.0;
+    const double phn = 2.0 * dPc - dp0n;
+    const double iRjk = IR(j, k);
+    const double Xim = (i >= 2) ? new_phat(f, c - 1) : ld(f.dPhat + c - 1);
+    double invRhoc = 0.5 * rdmx1[i] * (dx1[i] * iRjk + dx1[im] * iRjk);
+    const double un = f.U[c] - dtc * ((dPc - ld(f.dP + c - 1)) * rdmx1[i] + (invRhoc - 1.0) * (ph - Xim) * rdmx1[i]);
+    double vn = f.V[c];
+    if (j >= 2) {   // the lower wall plane keeps V: dble(2 - j_indexS) = 0
+        const double Xjm = (j >= 3) ? new_phat(f, c - sj) : ld(f.dPhat + c - sj);
+        invRhoc = 0.5 * rdmx2[j] * (dx2[j] * IR(jm, k) + dx2[jm] * iRjk);
+        vn = vn - dtc * ((dPc - ld(f.dP + c - sj)) * rdmx2[j] + (invRhoc - 1.0) * (ph - Xjm) * rdmx2[j]);
+    }
+    const double Xkm = (k >= 2) ? new_phat(f, c - sk) : ld(f.dPhat + c - sk);
+    invRhoc = 0.5 * rdmx3[k] * (dx3[k] * IR(j, km) + dx3[km] * iRjk);
+    const double wn = f.W[c] - dtc * ((dPc - ld(f.dP + c - sk)) * rdmx3[k] + (invRhoc - 1.0) * (ph - Xkm) * rdmx3[k]);
+    store_periodic(g, f.U, i, j, k, un);
+    store_periodic(g, f.V, i, j, k, vn);
+    store_periodic(g, f.W, i, j, k, wn);
+    store_periodic(g, f.P, i, j, k, f.P[c] + dPc);
+    store_periodic(g, f.dPhatn, i, j, k, phn);
+    f.dP0n[c] = dp0n;
+}
+
+// P(i,0,k) = Pbc_a P(i,1,k) - Pbc_b P(i,2,k) and the top-wall counterpart
+// (:853-869), then ghost(P).
+__global__ void p_wall_kernel(Grid g, Fields f, double ab, double bb, double at, double bt)
 {
     const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x, k = 1 + blockIdx.y;
     if (i > g.N1 || blown(g)) return;
-    const int im = i - 1, km = k - 1;
-    const double *dx1 = g.m1.dx, *dx2 = g.m2.dx, *dx3 = g.m3.dx;
-    const double *rdmx1 = g.m1.rdmx, *rdmx2 = g.m2.rdmx, *rdmx3 = g.m3.rdmx;
-    const long long sj = g.P1, sk = (long long)g.P1 * g.P2;
-    const double dtc = g.scal[S_DT] * g.ph.Cmp;
-    double phat_prev = 0.0, p1 = 0.0, p2 = 0.0, pN = 0.0, pNm = 0.0;
-    for (int j = 1; j <= g.N2; j++) {
-        const long long c = ix(g, i, j, k);
-        const double dPc = ld(f.dP + c), ph = ld(f.dPhat + c), p0 = ld(f.dP0 + c);
-        const double dp0n = (ph + p0) / 2.0;
-        const double phn = 2.0 * dPc - dp0n;
-        const double iRjk = IR(j, k);
-        // U
-        const double Xim = (i >= 2) ? new_phat(f, c - 1) : ld(f.dPhat + c - 1);
-        double invRhoc = 0.5 * rdmx1[i] * (dx1[i] * iRjk + dx1[im] * iRjk);
-        const double un = f.U[c] - dtc * ((dPc - ld(f.dP + c - 1)) * rdmx1[i] + (invRhoc - 1.0) * (ph - Xim) * rdmx1[i]);
-        // V (the lower wall plane j = 1 is left unchanged: dble(2 - j_indexS) = 0)
-        double vn = f.V[c];
-        if (j >= 2) {
-            const double Xjm = (j >= 3) ? phat_prev : ld(f.dPhat + c - sj);
-            invRhoc = 0.5 * rdmx2[j] * (dx2[j] * IR(j - 1, k) + dx2[j - 1] * iRjk);
-            vn = vn - dtc * ((dPc - ld(f.dP + c - sj)) * rdmx2[j] + (invRhoc - 1.0) * (ph - Xjm) * rdmx2[j]);
-        }
-        // W
-        const double Xkm = (k >= 2) ? new_phat(f, c - sk) : ld(f.dPhat + c - sk);
-        invRhoc = 0.5 * rdmx3[k] * (dx3[k] * IR(j, km) + dx3[km] * iRjk);
-        const double wn = f.W[c] - dtc * ((dPc - ld(f.dP + c - sk)) * rdmx3[k] + (invRhoc - 1.0) * (ph - Xkm) * rdmx3[k]);
-        const double pn = f.P[c] + dPc;
-        store_periodic(g, f.U, i, j, k, un);
-        store_periodic(g, f.V, i, j, k, vn);
-        store_periodic(g, f.W, i, j, k, wn);
-        store_periodic(g, f.P, i, j, k, pn);
-        store_periodic(g, f.dPhatn, i, j, k, phn);
-        f.dP0n[c] = dp0n;
-        phat_prev = phn;
-        if (j == 1) p1 = pn;
-        if (j == 2) p2 = pn;
-        if (j == g.N2 - 1) pNm = pn;
-        if (j == g.N2) pN = pn;
-    }
-    store_periodic(g, f.P, i, 0, k, ab * p1 - bb * p2);
-    store_periodic(g, f.P, i, g.N2 + 1, k, at * pN - bt * pNm);
+    const double *P = f.P;
+    store_periodic(g, f.P, i, 0, k, ab * P[ix(g, i, 1, k)] - bb * P[ix(g, i, 2, k)]);
+    store_periodic(g, f.P, i, g.N2 + 1, k, at * P[ix(g, i, g.N2, k)] - bt * P[ix(g, i, g.N2 - 1, k)]);
 }
 
 static size_t fftx_smem(const Ctx &cx) { return (size_t)cx.fft_lines_x * cx.g.N1 * (2 * sizeof(double2) + sizeof(double)); }
@@ -438,9 +437,13 @@ void launch_projection(const Ctx &cx, cudaStream_t s)
 {
     const Grid &g = cx.g;
     probe_begin(cx, K_PROJECT, s);
-    projection_kernel<<<dim3((g.N1 + 63) / 64, g.N3), 64, 0, s>>>(g, cx.f, cx.wall_ab, cx.wall_bb, cx.wall_at, cx.wall_bt);
+    projection_kernel<<<dim3((g.N1 + 255) / 256, g.N2, g.N3), 256, 0, s>>>(g, cx.f);
     probe_end(cx, K_PROJECT, s);
     record_launch_error("projection");
+    probe_begin(cx, K_P_WALL, s);
+    p_wall_kernel<<<dim3((g.N1 + 127) / 128, g.N3), 128, 0, s>>>(g, cx.f, cx.wall_ab, cx.wall_bb, cx.wall_at, cx.wall_bt);
+    probe_end(cx, K_P_WALL, s);
+    record_launch_error("p_wall");
 }
 
 #undef IR

@@ -18,9 +18,11 @@ struct ThermalZ {
     static constexpr bool CONTIG = false;
     Grid g; Fields f; int TL;
     __device__ bool skip() const { return blown(g); }
+    struct State { double dt; };
+    __device__ State prepare() const { return State{g.scal[S_DT]}; }
     __device__ int li(int l) const { return 1 + blockIdx.x * TL + l; }
     __device__ bool line_ok(int l) const { return li(l) <= g.N1; }
-    __device__ Coef<1> build(int l, int r) const
+    __device__ Coef<1> build(int l, int r, const State &st) const
     {
         const int i = li(l), j = 1 + blockIdx.y, k = r + 1;
         const int im = i - 1, ip = i + 1, jm = j - 1, jp = j + 1, km = k - 1, kp = k + 1;
@@ -80,7 +82,7 @@ struct ThermalZ {
         const double eAMJ = (-h * rdx2[j] * (kPP3 * rdmx2[j] - dx2[j] * (0.5 * rdmx2[j]) * dkPP3 * dedy3) - 0.25 * Vc * rdmx2[j]) * jem;
         rhs = rhs - (eAPK * Tzp + eACK * Tc + eAMK * Tzm + eAPJ * Typ + eACJ * Tc + eAMJ * Tym
                      + eAPI * Txp + eACI * Tc + eAMI * Txm - dh * Tc * dv);
-        const double dt = g.scal[S_DT];
+        const double dt = st.dt;
         Coef<1> cf;
         cf.b = eACK * dt - 0.5 * dh * dv * dt + 1.0;
         cf.c = eAPK * dt;
@@ -88,7 +90,7 @@ struct ThermalZ {
         cf.d[0] = rhs * dt;
         return cf;
     }
-    __device__ void emit(int l, int r, const double *x) const
+    __device__ void emit(int l, int r, const double *x, const State &st) const
     {
         f.R[ix(g, li(l), 1 + blockIdx.y, r + 1)] = x[0];
     }
@@ -101,9 +103,11 @@ struct ThermalX {
     static constexpr bool CONTIG = true;
     Grid g; Fields f; int TL;
     __device__ bool skip() const { return blown(g); }
+    struct State { double dt; };
+    __device__ State prepare() const { return State{g.scal[S_DT]}; }
     __device__ int lj(int l) const { return 1 + blockIdx.x * TL + l; }
     __device__ bool line_ok(int l) const { return lj(l) <= g.N2; }
-    __device__ Coef<1> build(int l, int r) const
+    __device__ Coef<1> build(int l, int r, const State &st) const
     {
         const int i = r + 1, j = lj(l), k = 1 + blockIdx.y;
         const int im = i - 1, ip = i + 1, jm = g.N2 - 1, jp = g.N2 + 1, km = g.N3 - 1, kp = g.N3 + 1;
@@ -134,7 +138,7 @@ struct ThermalX {
                           - 0.5 * h * ((kPP2 * dedx2 - kPP1 * dedx1) * rdx1[i] + (kPP4 * dedy4 - kPP3 * dedy3) * rdx2[j] + (kPP6 * dedz6 - kPP5 * dedz5) * rdx3[k]);
         const double eAPI = -h * rdx1[i] * (kPP2 * rdmx1[ip] + dx1[i] * (0.5 * rdmx1[ip]) * dkPP2 * dedx2) + 0.25 * Uxp * rdmx1[ip];
         const double eAMI = -h * rdx1[i] * (kPP1 * rdmx1[i] - dx1[i] * (0.5 * rdmx1[i]) * dkPP1 * dedx1) - 0.25 * Uc * rdmx1[i];
-        const double dt = g.scal[S_DT];
+        const double dt = st.dt;
         Coef<1> cf;
         cf.b = eACI * dt + 1.0;
         cf.c = eAPI * dt;
@@ -142,7 +146,7 @@ struct ThermalX {
         cf.d[0] = ld(f.R + c);
         return cf;
     }
-    __device__ void emit(int l, int r, const double *x) const
+    __device__ void emit(int l, int r, const double *x, const State &st) const
     {
         f.R[ix(g, r + 1, lj(l), 1 + blockIdx.y)] = x[0];
     }
@@ -154,9 +158,11 @@ struct ThermalY {
     static constexpr bool CONTIG = false;
     Grid g; Fields f; int TL;
     __device__ bool skip() const { return blown(g); }
+    struct State { double dt; };
+    __device__ State prepare() const { return State{g.scal[S_DT]}; }
     __device__ int li(int l) const { return 1 + blockIdx.x * TL + l; }
     __device__ bool line_ok(int l) const { return li(l) <= g.N1; }
-    __device__ Coef<1> build(int l, int r) const
+    __device__ Coef<1> build(int l, int r, const State &st) const
     {
         const int i = li(l), j = r + 1, k = 1 + blockIdx.y;
         const int im = i - 1, ip = i + 1, jm = j - 1, jp = j + 1, km = g.N3 - 1, kp = g.N3 + 1;
@@ -187,7 +193,7 @@ struct ThermalY {
                           - 0.5 * h * ((KPP2 * dedx2 - KPP1 * dedx1) * rdx1[i] + (kPP4 * dedy4 - kPP3 * dedy3) * rdx2[j] + (KPP6 * dedz6 - KPP5 * dedz5) * rdx3[k]);
         const double eAPJ = (-h * rdx2[j] * (kPP4 * rdmx2[jp] + dx2[j] * (0.5 * rdmx2[jp]) * dkPP4 * dedy4) + 0.25 * Vyp * rdmx2[jp]) * jep;
         const double eAMJ = (-h * rdx2[j] * (kPP3 * rdmx2[j] - dx2[j] * (0.5 * rdmx2[j]) * dkPP3 * dedy3) - 0.25 * Vc * rdmx2[j]) * jem;
-        const double dt = g.scal[S_DT];
+        const double dt = st.dt;
         Coef<1> cf;
         cf.b = eACJ * dt + 1.0;
         cf.c = eAPJ * dt;
@@ -195,7 +201,7 @@ struct ThermalY {
         cf.d[0] = ld(f.R + c);
         return cf;
     }
-    __device__ void emit(int l, int r, const double *x) const
+    __device__ void emit(int l, int r, const double *x, const State &st) const
     {
         const int i = li(l), j = r + 1, k = 1 + blockIdx.y;
         store_periodic(g, f.Tn, i, j, k, ld(f.T + ix(g, i, j, k)) + x[0]);

@@ -138,6 +138,10 @@ int tcs_probe_enable(tcs_ctx *ctx, uint64_t mask);
 int tcs_probe_read(tcs_ctx *ctx, int kernel_id, double *total_ms, int *launches);
 int tcs_probe_reset(tcs_ctx *ctx);
 int tcs_set_use_graph(tcs_ctx *ctx, int on);
+/* launch-shape knobs: lines per thread block (powers of two) */
+enum { TCS_TUNE_TL_STRIDED = 0, TCS_TUNE_TL_CONTIG, TCS_TUNE_TL_MODAL, TCS_TUNE_FFT_LINES_X, TCS_TUNE_FFT_LINES_Z, TCS_TUNE_COUNT };
+int tcs_set_tuning(tcs_ctx *ctx, int knob, int value);
+int tcs_get_tuning(tcs_ctx *ctx, int knob, int *value);
 const char *tcs_last_error(void);
 
 #ifdef __cplusplus

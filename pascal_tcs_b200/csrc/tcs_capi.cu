@@ -399,8 +399,9 @@ int tcs_create(const tcs_config *cfg, tcs_ctx **out)
         const int tz = choose_tl(N3, true, 1, 8), ty = choose_tl(N2, false, 1, 8);
         c->cx.tl_strided = tz < ty ? tz : ty;
     }
-    c->cx.fft_lines_x = N1 <= 256 ? 8 : (N1 <= 512 ? 4 : 2);
-    c->cx.fft_lines_z = N3 <= 256 ? 8 : (N3 <= 512 ? 4 : 2);
+    // measured on B200 at 256^3: 4 lines per block beats 1, 2, 8 and 16 for both FFT kernels
+    c->cx.fft_lines_x = N1 <= 256 ? 4 : (N1 <= 512 ? 2 : 1);
+    c->cx.fft_lines_z = N3 <= 256 ? 4 : (N3 <= 512 ? 2 : 1);
     c->cx.probe = &c->probe;
 
     // initial fields: mpi_thermal_initial/boundary, mpi_momentum_initial/boundary,
@@ -710,6 +711,57 @@ static void launch_step(tcs_ctx *c)
     launch_projection(cx, s);
     std::swap(cx.f.dPhat, cx.f.dPhatn); std::swap(cx.f.dP0, cx.f.dP0n);
     launch_post(cx, s, 1);
+}
+
+// Launch-shape knobs (lines per block of the line-solver families and of the
+// FFT kernels).  Values are validated against the shared-memory budget.
+int tcs_set_tuning(tcs_ctx *c, int knob, int value)
+{
+    ENTER(c);
+    if (value < 1 || value > 64 || (value & (value - 1))) return set_err(TCS_ERR_ARG, "tuning value must be a power of two in 1..64");
+    Ctx &x = c->cx;
+    const Grid &g = x.g;
+    switch (knob) {
+    case TCS_TUNE_TL_STRIDED: {
+        LinePlan a = make_line_plan(g.N3, true, value), b = make_line_plan(g.N2, false, value);
+        const int LS = a.LS > b.LS ? a.LS : b.LS;
+        if ((size_t)3 * value * LS * 8 + 4096 * 4 > 200 * 1024) return set_err(TCS_ERR_ARG, "too many lines for shared memory");
+        x.tl_strided = value; break; }
+    case TCS_TUNE_TL_CONTIG: {
+        LinePlan a = make_line_plan(g.N1, true, value);
+        if ((size_t)3 * value * a.LS * 8 + 4096 * 4 > 200 * 1024) return set_err(TCS_ERR_ARG, "too many lines for shared memory");
+        x.tl_contig = value; break; }
+    case TCS_TUNE_TL_MODAL: {
+        LinePlan a = make_line_plan(g.N2, false, value);
+        if ((size_t)4 * value * a.LS * 8 + 4096 * 4 > 200 * 1024) return set_err(TCS_ERR_ARG, "too many lines for shared memory");
+        x.tl_modal = value; break; }
+    case TCS_TUNE_FFT_LINES_X:
+        if ((size_t)value * g.N1 * 40 > 200 * 1024) return set_err(TCS_ERR_ARG, "too many lines for shared memory");
+        x.fft_lines_x = value; break;
+    case TCS_TUNE_FFT_LINES_Z:
+        if ((size_t)value * g.N3 * 32 > 200 * 1024) return set_err(TCS_ERR_ARG, "too many lines for shared memory");
+        x.fft_lines_z = value; break;
+    default: return set_err(TCS_ERR_ARG, "unknown tuning knob");
+    }
+    for (auto &ge : c->graphs) cudaGraphExecDestroy(ge.exec);
+    c->graphs.clear();
+    return TCS_OK;
+}
+
+int tcs_get_tuning(tcs_ctx *c, int knob, int *value)
+{
+    ENTER(c);
+    if (!value) return set_err(TCS_ERR_ARG, "null argument");
+    const Ctx &x = c->cx;
+    switch (knob) {
+    case TCS_TUNE_TL_STRIDED: *value = x.tl_strided; break;
+    case TCS_TUNE_TL_CONTIG: *value = x.tl_contig; break;
+    case TCS_TUNE_TL_MODAL: *value = x.tl_modal; break;
+    case TCS_TUNE_FFT_LINES_X: *value = x.fft_lines_x; break;
+    case TCS_TUNE_FFT_LINES_Z: *value = x.fft_lines_z; break;
+    default: return set_err(TCS_ERR_ARG, "unknown tuning knob");
+    }
+    return TCS_OK;
 }
 
 int tcs_set_use_graph(tcs_ctx *c, int on)

@@ -22,6 +22,7 @@ SCALARS = ["dt", "time", "CFL", "maxDivU", "Nu_bot", "Nu_top", "KE", "blowup",
            "aver", "step", "fixed_dt"]
 HISTORY = ["dt", "time", "maxDivU", "CFL", "Nu_bot", "Nu_top", "KE"]
 METRICS = ["x1", "dx1", "dmx1", "x2", "dx2", "dmx2", "x3", "dx3", "dmx3"]
+TUNING = ["tl_strided", "tl_contig", "tl_modal", "fft_lines_x", "fft_lines_z"]
 ERRORS = {1: "bad argument", 2: "CUDA error", 3: "unsupported", 4: "BLOW UP",
           5: "out of device memory", 6: "non-finite scalar"}
 
@@ -39,7 +40,8 @@ EXPORTS = [
     "tcs_snapshot", "tcs_restore",
     "tcs_tdma_plan_many_create", "tcs_tdma_plan_many_destroy", "tcs_tdma_many_solve",
     "tcs_tdma_many_solve_cycle", "tcs_kernel_count", "tcs_launch_count", "tcs_kernel_name", "tcs_probe_enable",
-    "tcs_probe_read", "tcs_probe_reset", "tcs_set_use_graph", "tcs_last_error",
+    "tcs_probe_read", "tcs_probe_reset", "tcs_set_use_graph", "tcs_set_tuning", "tcs_get_tuning",
+    "tcs_last_error",
 ]
 
 
@@ -116,6 +118,8 @@ def load() -> ctypes.CDLL:
         "tcs_probe_read": ([vp, ip, dp, ctypes.POINTER(ip)], ip),
         "tcs_probe_reset": ([vp], ip),
         "tcs_set_use_graph": ([vp, ip], ip),
+        "tcs_set_tuning": ([vp, ip, ip], ip),
+        "tcs_get_tuning": ([vp, ip, ctypes.POINTER(ip)], ip),
         "tcs_last_error": ([], ctypes.c_char_p),
     }
     for name in ("tcs_thermal_coeffi", "tcs_thermal_solver", "tcs_thermal_coeffi_clean",
@@ -306,6 +310,17 @@ class Solver:
         """Return to the last snapshot (device-to-device copies on the solver stream)."""
         self._call("tcs_restore")
         self._since_restore = 0
+
+    def set_tuning(self, knob: str, value: int) -> None:
+        _check(load().tcs_set_tuning(self._h, TUNING.index(knob), int(value)), f"set_tuning {knob}")
+
+    def tuning(self) -> dict:
+        out = {}
+        for i, k in enumerate(TUNING):
+            v = ctypes.c_int()
+            _check(load().tcs_get_tuning(self._h, i, ctypes.byref(v)), "get_tuning")
+            out[k] = v.value
+        return out
 
     def use_graph(self, on: bool) -> None:
         _check(load().tcs_set_use_graph(self._h, int(bool(on))), "use_graph")

@@ -127,6 +127,20 @@ int tcs_tdma_many_solve(tcs_tdma_plan *plan, double *A, double *B, double *C, do
 /* pascal_tdma.f90:715 PaScaL_TDMA_many_solve_cycle(plan, A, B, C, D, n_sys, n_row) */
 int tcs_tdma_many_solve_cycle(tcs_tdma_plan *plan, double *A, double *B, double *C, double *D, int n_sys, int n_row);
 
+/* No counterpart in the reference.  The PaScaL_TDMA many-systems solve
+ * (cyclic != 0: the _cycle form) for callers that cannot allocate device
+ * memory when they solve: host arrays A, B, C, D (n_sys, n_row) are staged
+ * through a fixed device array compiled into the library, with no plan, no
+ * cudaMalloc and no cudaFree.  n_sys * n_row must not exceed
+ * TCS_TDMA_NOALLOC_MAX_ELEMS (TCS_ERR_UNSUPPORTED otherwise).  The array costs
+ * 4 * TCS_TDMA_NOALLOC_MAX_ELEMS doubles (8 MiB) on every GPU that loads the
+ * library, for the life of the process.  The first call on a device looks up
+ * the array's address; make that first call before any stream capture.  All
+ * calls share the array: calls that overlap on the GPU race.  Blocking; runs
+ * on the legacy default stream of the current device. */
+#define TCS_TDMA_NOALLOC_MAX_ELEMS (1 << 18)
+int tcs_tdma_many_solve_noalloc(double *A, double *B, double *C, double *D, int n_sys, int n_row, int cyclic);
+
 /* ---- measurement --------------------------------------------------------- */
 int tcs_kernel_count(void);
 unsigned long long tcs_launch_count(void);           /* kernels this library has launched so far */

@@ -39,6 +39,8 @@ int record_launch_error(const char *what)
     return e == cudaSuccess ? 0 : 1;
 }
 
+int set_error(int code, const std::string &msg) { return set_err(code, msg); }
+
 static int take_launch_error()
 {
     const int e = g_launch_err;

@@ -6,6 +6,7 @@
 
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <string>
 
 namespace tcs {
 
@@ -43,6 +44,7 @@ bool make_fft_plan(int n, FFTPlan &fp);
 void probe_begin(const Ctx &cx, int kid, cudaStream_t s);
 void probe_end(const Ctx &cx, int kid, cudaStream_t s);
 int record_launch_error(const char *what);
+int set_error(int code, const std::string &msg);
 
 template <class Prob>
 inline void launch_lines(const Prob &p, const LinePlan &lp, dim3 grid, cudaStream_t s, int kid, const Ctx &cx)

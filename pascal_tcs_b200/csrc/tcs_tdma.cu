@@ -12,6 +12,9 @@
 // e(n2) = -c(2)).  D receives the solution; A and C are clobbered as in the
 // reference.
 #include "tcs_kernels.h"
+#include "tcs.h"
+
+#include <mutex>
 
 namespace tcs {
 
@@ -86,4 +89,66 @@ void launch_tdma_many(double *A, const double *B, double *C, double *D, int n_sy
     record_launch_error("tdma_many");
 }
 
+// ---------------------------------------------------------------------------
+// Allocation-free variant of the many-systems solve.
+//
+// Some callers cannot allocate device memory at the point where they solve:
+// code that runs while a memory budget forbids further cudaMalloc after
+// start-up (a solver embedded in a host application that owns the device
+// memory pool), callers on a path where a cudaMalloc/cudaFree would
+// synchronise the device and stall other work, and Fortran drivers that only
+// hand over host arrays and must not create per-call plans.  They stage their
+// systems through this file-scope device array instead.  It is statically
+// sized, so every GPU that loads the library holds TCS_TDMA_NOALLOC_MAX_ELEMS
+// x 4 doubles (8 MiB) until the process exits.  All calls share it and it
+// keeps the last call's contents; calls that overlap on the GPU (other host
+// threads, other streams) race on it.
+// ---------------------------------------------------------------------------
+static __device__ __align__(256) double g_tdma_noalloc[4 * TCS_TDMA_NOALLOC_MAX_ELEMS];
+
+static std::mutex g_noalloc_mu;
+static double *g_noalloc_ptr[64] = {};
+
 } // namespace tcs
+
+extern "C" int tcs_tdma_many_solve_noalloc(double *A, double *B, double *C, double *D, int n_sys, int n_row, int cyclic)
+{
+    using namespace tcs;
+    if (!A || !B || !C || !D) return set_error(TCS_ERR_ARG, "null argument");
+    if (n_sys < 1 || n_row < 2) return set_error(TCS_ERR_ARG, "n_sys >= 1 and n_row >= 2 required");
+    const size_t n = (size_t)n_sys * (size_t)n_row;
+    if (n > (size_t)TCS_TDMA_NOALLOC_MAX_ELEMS)
+        return set_error(TCS_ERR_UNSUPPORTED, "n_sys * n_row exceeds TCS_TDMA_NOALLOC_MAX_ELEMS");
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return set_error(TCS_ERR_CUDA, cudaGetErrorString(e));
+    if (dev < 0 || dev >= 64) return set_error(TCS_ERR_UNSUPPORTED, "device ordinal >= 64");
+    double *base;
+    {
+        // First call on this device: host code needs the array's device address
+        // (the symbol name itself is only a host-side stand-in).
+        std::lock_guard<std::mutex> lk(g_noalloc_mu);
+        if (!g_noalloc_ptr[dev]) {
+            void *p = nullptr;
+            e = cudaGetSymbolAddress(&p, g_tdma_noalloc);
+            if (e != cudaSuccess) return set_error(TCS_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+            g_noalloc_ptr[dev] = (double *)p;
+        }
+        base = g_noalloc_ptr[dev];
+    }
+    double *dA = base, *dB = base + n, *dC = base + 2 * n, *dD = base + 3 * n;
+    const size_t bytes = n * sizeof(double);
+    // Every element the kernel reads is copied in first, so nothing needs clearing.
+    if ((e = cudaMemcpy(dA, A, bytes, cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMemcpy(dB, B, bytes, cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMemcpy(dC, C, bytes, cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMemcpy(dD, D, bytes, cudaMemcpyHostToDevice)) != cudaSuccess)
+        return set_error(TCS_ERR_CUDA, std::string("cudaMemcpy to the static scratch: ") + cudaGetErrorString(e));
+    tdma_many_kernel<<<(n_sys + 127) / 128, 128, 0, 0>>>(dA, dB, dC, dD, n_sys, n_row, cyclic ? 1 : 0);
+    if ((e = cudaGetLastError()) != cudaSuccess) return set_error(TCS_ERR_CUDA, std::string("tdma_many launch: ") + cudaGetErrorString(e));
+    if ((e = cudaMemcpy(A, dA, bytes, cudaMemcpyDeviceToHost)) != cudaSuccess ||
+        (e = cudaMemcpy(C, dC, bytes, cudaMemcpyDeviceToHost)) != cudaSuccess ||
+        (e = cudaMemcpy(D, dD, bytes, cudaMemcpyDeviceToHost)) != cudaSuccess)
+        return set_error(TCS_ERR_CUDA, std::string("cudaMemcpy from the static scratch: ") + cudaGetErrorString(e));
+    return TCS_OK;
+}

@@ -39,7 +39,7 @@ EXPORTS = [
     "tcs_post_div", "tcs_post_cfl", "tcs_step", "tcs_get_scalars", "tcs_get_history",
     "tcs_snapshot", "tcs_restore",
     "tcs_tdma_plan_many_create", "tcs_tdma_plan_many_destroy", "tcs_tdma_many_solve",
-    "tcs_tdma_many_solve_cycle", "tcs_kernel_count", "tcs_launch_count", "tcs_kernel_name", "tcs_probe_enable",
+    "tcs_tdma_many_solve_cycle", "tcs_tdma_many_solve_noalloc", "tcs_kernel_count", "tcs_launch_count", "tcs_kernel_name", "tcs_probe_enable",
     "tcs_probe_read", "tcs_probe_reset", "tcs_set_use_graph", "tcs_set_tuning", "tcs_get_tuning",
     "tcs_last_error",
 ]
@@ -111,6 +111,7 @@ def load() -> ctypes.CDLL:
         "tcs_tdma_plan_many_destroy": ([vp], ip),
         "tcs_tdma_many_solve": ([vp, vp, vp, vp, vp, ip, ip], ip),
         "tcs_tdma_many_solve_cycle": ([vp, vp, vp, vp, vp, ip, ip], ip),
+        "tcs_tdma_many_solve_noalloc": ([vp, vp, vp, vp, ip, ip, ip], ip),
         "tcs_kernel_count": ([], ip),
         "tcs_launch_count": ([], ctypes.c_ulonglong),
         "tcs_kernel_name": ([ip], ctypes.c_char_p),
@@ -376,3 +377,20 @@ class TdmaPlan:
 
     def many_solve_cycle(self, A, B, C, D, n_sys: int, n_row: int) -> None:
         self._solve("tcs_tdma_many_solve_cycle", A, B, C, D, n_sys, n_row)
+
+
+# Largest n_sys * n_row accepted by tdma_many_solve_noalloc (TCS_TDMA_NOALLOC_MAX_ELEMS).
+TDMA_NOALLOC_MAX_ELEMS = 1 << 18
+
+
+def tdma_many_solve_noalloc(A: np.ndarray, B: np.ndarray, C: np.ndarray, D: np.ndarray,
+                            n_sys: int, n_row: int, cyclic: bool = False) -> None:
+    """PaScaL_TDMA many-systems solve for callers that cannot allocate device
+    memory: host arrays are staged through a fixed device array inside the
+    library (no plan, no cudaMalloc).  D receives the solution, A and C are
+    clobbered.  Calls that overlap on the GPU share the array and race."""
+    for x in (A, B, C, D):
+        assert isinstance(x, np.ndarray) and x.dtype == np.float64 and x.flags["C_CONTIGUOUS"]
+    _check(load().tcs_tdma_many_solve_noalloc(A.ctypes.data, B.ctypes.data, C.ctypes.data, D.ctypes.data,
+                                              int(n_sys), int(n_row), int(bool(cyclic))),
+           "tcs_tdma_many_solve_noalloc")

@@ -48,7 +48,15 @@ typedef struct tcs_config {
     int init_mode;                    /* 0: T = 0.5 - y + noise; 1: T = 0 interior (mpi_thermal_initial) */
     int top_wall_mode;                /* 0: top ghost row of T stays 0 as on one y rank (module_solve_thermal.f90:102-110); 1: = Tup */
     int device;                       /* CUDA device ordinal */
+    int precision;                    /* TCS_PREC_FP64 (the reference's arithmetic) or TCS_PREC_FP32_MIXED */
 } tcs_config;
+
+/* numerical forms (tcs_config.precision).  FP32_MIXED stores the fields in FP32
+ * and runs stencils, ADI sweeps and FFTs in FP32 with one FP64-residual
+ * refinement pass per tridiagonal system; the modal pressure solves, the
+ * pressure right-hand side, the projection and every reduction compute in
+ * FP64.  The host interface moves FP64 arrays in both forms. */
+enum { TCS_PREC_FP64 = 0, TCS_PREC_FP32_MIXED = 1 };
 
 /* field identifiers */
 enum {
@@ -77,7 +85,8 @@ int tcs_upload_field(tcs_ctx *ctx, int field, const double *host); /* blocking c
 int tcs_download_field(tcs_ctx *ctx, int field, double *host);
 int tcs_upload_field_async(tcs_ctx *ctx, int field, const double *pinned_host);   /* on the context stream */
 int tcs_download_field_async(tcs_ctx *ctx, int field, double *pinned_host);
-int tcs_field_device_ptr(tcs_ctx *ctx, int field, double **dev);   /* current device buffer */
+int tcs_field_device_ptr(tcs_ctx *ctx, int field, void **dev);     /* current device buffer: double (FP64) or float (FP32_MIXED) */
+int tcs_precision(const tcs_ctx *ctx);                             /* tcs_config.precision of the context */
 int tcs_synchronize(tcs_ctx *ctx);
 int tcs_set_dt(tcs_ctx *ctx, double dt);
 int tcs_get_metric(const tcs_ctx *ctx, int which, double *out);    /* x1,dx1,dmx1,x2,...,dmx3 (0..8) */

@@ -80,7 +80,7 @@ struct ProbeState {
     }
 };
 
-void probe_begin(const Ctx &cx, int kid, cudaStream_t s)
+void probe_begin(const Shapes &cx, int kid, cudaStream_t s)
 {
     ProbeState *p = cx.probe;
     if (!p || !(p->mask & (1ull << kid))) return;
@@ -88,7 +88,7 @@ void probe_begin(const Ctx &cx, int kid, cudaStream_t s)
     cudaEventRecord(p->pending[kid], s);
 }
 
-void probe_end(const Ctx &cx, int kid, cudaStream_t s)
+void probe_end(const Shapes &cx, int kid, cudaStream_t s)
 {
     ProbeState *p = cx.probe;
     if (!p || !(p->mask & (1ull << kid)) || !p->pending[kid]) return;
@@ -116,11 +116,18 @@ LinePlan make_line_plan(int n, bool cyclic, int TL)
     return lp;
 }
 
-static int choose_tl(int n, bool cyclic, int nrhs, int want)
+// Shared-memory bytes per row of a line-solver block: A, C, D[nrhs] of the
+// row type, plus the kept rows A0, B0, C0, D0[nrhs] when FP32 rows are refined.
+static size_t row_bytes(int nrhs, bool fp32_refined)
+{
+    return fp32_refined ? (size_t)(5 + 2 * nrhs) * sizeof(float) : (size_t)(2 + nrhs) * sizeof(double);
+}
+
+static int choose_tl(int n, bool cyclic, size_t rowb, int want)
 {
     LinePlan lp = make_line_plan(n, cyclic, want);
     int tl = want;
-    while (tl > 2 && (size_t)(2 + nrhs) * tl * lp.LS * sizeof(double) + (size_t)n * sizeof(int) > 112 * 1024) tl /= 2;
+    while (tl > 2 && rowb * tl * lp.LS + (size_t)n * sizeof(int) > 112 * 1024) tl /= 2;
     return tl;
 }
 
@@ -144,7 +151,12 @@ using namespace tcs;
 // ---------------------------------------------------------------------------
 struct tcs_ctx {
     tcs_config cfg;
-    Ctx cx;
+    bool fp32 = false;                   // TCS_PREC_FP32_MIXED
+    // The grid, scalars, history and launch shapes live in cx in both forms;
+    // the fields are allocated in the context of the active form only.
+    Ctx<double> cx;
+    Ctx<float> cf;
+    double *stage = nullptr;             // FP64 staging copy of one field (FP32 form)
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     std::vector<double> hm[9];           // x1, dx1, dmx1, x2, dx2, dmx2, x3, dx3, dmx3
@@ -152,14 +164,30 @@ struct tcs_ctx {
     uint32_t ghost_ok = 0;               // bit per field id: periodic ghosts are current
     bool pending_pseudo = false;
     bool use_graph = true;
-    struct GraphEntry { const double *T, *U, *dPhat; cudaGraphExec_t exec; unsigned long long kernels; };
+    struct GraphEntry { const void *T, *U, *dPhat; cudaGraphExec_t exec; unsigned long long kernels; };
     std::vector<GraphEntry> graphs;
     ProbeState probe;
     int partials = 0;
-    double *snap[7] = {};                // on-device copy of T, U, V, W, P, dPhat, dP0
+    void *snap[7] = {};                  // on-device copy of T, U, V, W, P, dPhat, dP0
     double snap_scal[S_NSCAL] = {};
     bool have_snap = false;
 };
+
+// Run fn on the context of the active form.
+template <class Fn>
+static auto on_ctx(tcs_ctx *c, Fn &&fn) -> decltype(fn(c->cx))
+{
+    if (c->fp32) return fn(c->cf);
+    return fn(c->cx);
+}
+
+// The shapes are decided once on cx; the FP32 context runs with the same ones.
+static void sync_shapes(tcs_ctx *c)
+{
+    static_cast<Shapes &>(c->cf) = static_cast<const Shapes &>(c->cx);
+}
+
+static size_t esize(const tcs_ctx *c) { return c->fp32 ? sizeof(float) : sizeof(double); }
 
 namespace tcs {
 int post_partial_count();
@@ -280,9 +308,9 @@ static void host_ghost(std::vector<double> &a, int N1, int N2, int N3)
         for (int i = 0; i <= N1 + 1; i++) { a[I(i, j, 0)] = a[I(i, j, N3)]; a[I(i, j, N3 + 1)] = a[I(i, j, 1)]; }
 }
 
-static double *field_ptr(tcs_ctx *c, int f)
+template <class R>
+static R *field_ptr_t(FieldsT<R> &F, int f)
 {
-    Fields &F = c->cx.f;
     switch (f) {
     case TCS_F_T: return F.T; case TCS_F_U: return F.U; case TCS_F_V: return F.V; case TCS_F_W: return F.W;
     case TCS_F_P: return F.P; case TCS_F_DPHAT: return F.dPhat; case TCS_F_DP0: return F.dP0;
@@ -291,11 +319,19 @@ static double *field_ptr(tcs_ctx *c, int f)
     }
 }
 
+static void *field_ptr(tcs_ctx *c, int f)
+{
+    return on_ctx(c, [&](auto &x) -> void * { return field_ptr_t(x.f, f); });
+}
+
+template <class R> static void swap_T(Ctx<R> &x) { std::swap(x.f.T, x.f.Tn); }
+template <class R> static void swap_UVW(Ctx<R> &x) { std::swap(x.f.U, x.f.Un); std::swap(x.f.V, x.f.Vn); std::swap(x.f.W, x.f.Wn); }
+template <class R> static void swap_phat(Ctx<R> &x) { std::swap(x.f.dPhat, x.f.dPhatn); std::swap(x.f.dP0, x.f.dP0n); }
+
 static int flush_pending(tcs_ctx *c)
 {
     if (!c->pending_pseudo) return TCS_OK;
-    launch_pseudo_update(c->cx, c->stream);
-    std::swap(c->cx.f.U, c->cx.f.Un); std::swap(c->cx.f.V, c->cx.f.Vn); std::swap(c->cx.f.W, c->cx.f.Wn);
+    on_ctx(c, [&](auto &x) { launch_pseudo_update(x, c->stream); swap_UVW(x); });
     c->pending_pseudo = false;
     return take_launch_error();
 }
@@ -318,22 +354,28 @@ int tcs_create(const tcs_config *cfg, tcs_ctx **out)
     FFTPlan fp1, fp3;
     if (!make_fft_plan(cfg->n1m, fp1) || !make_fft_plan(cfg->n3m, fp3))
         return set_err(TCS_ERR_UNSUPPORTED, "n1m and n3m must factor into 2, 3 and 5 (FFT radices)");
+    if (cfg->precision != TCS_PREC_FP64 && cfg->precision != TCS_PREC_FP32_MIXED)
+        return set_err(TCS_ERR_ARG, "precision must be TCS_PREC_FP64 or TCS_PREC_FP32_MIXED");
     CK(cudaSetDevice(cfg->device));
     tcs_ctx *c = new tcs_ctx();
     c->cfg = *cfg;
+    c->fp32 = cfg->precision == TCS_PREC_FP32_MIXED;
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) { delete c; return set_err(TCS_ERR_CUDA, "stream"); }
     c->own_stream = true;
     const int N1 = cfg->n1m, N2 = cfg->n2m, N3 = cfg->n3m;
-    Grid &g = c->cx.g;
+    GridT<double> &g = c->cx.g;
     g.N1 = N1; g.N2 = N2; g.N3 = N3; g.P1 = N1 + 2; g.P2 = N2 + 2;
     g.NP = (long long)(N1 + 2) * (N2 + 2) * (N3 + 2);
     set_properties(*cfg, g.ph);
+    g.phd = g.ph;
     mesh_periodic(cfg->uniform1, g.ph.L1, cfg->gamma1, N1, c->hm[0], c->hm[1], c->hm[2]);
     mesh_wall(cfg->uniform2, g.ph.L2, cfg->gamma2, N2, c->hm[3], c->hm[4], c->hm[5]);
     mesh_periodic(cfg->uniform3, g.ph.L3, cfg->gamma3, N3, c->hm[6], c->hm[7], c->hm[8]);
     // fix dtMax with the reference formula on n - 1 = n_m (module_global.f90:161-165)
     int r = TCS_OK;
-    Metric *ms[3] = {&g.m1, &g.m2, &g.m3};
+    MetricT<double> *ms[3] = {&g.m1, &g.m2, &g.m3};
+    MetricT<float> *mf[3] = {&c->cf.g.m1, &c->cf.g.m2, &c->cf.g.m3};
+    auto to_f = [](const std::vector<double> &v) { return std::vector<float>(v.begin(), v.end()); };
     for (int d = 0; d < 3 && !r; d++) {
         const std::vector<double> &dx = c->hm[3 * d + 1], &dmx = c->hm[3 * d + 2];
         std::vector<double> rdx(dx.size()), rdmx(dmx.size());
@@ -342,22 +384,36 @@ int tcs_create(const tcs_config *cfg, tcs_ctx **out)
         r = r ? r : upload_vec(c, dmx, &ms[d]->dmx);
         r = r ? r : upload_vec(c, rdx, &ms[d]->rdx);
         r = r ? r : upload_vec(c, rdmx, &ms[d]->rdmx);
+        if (c->fp32) {   // the same tables rounded once to FP32
+            r = r ? r : upload_vec(c, to_f(dx), &mf[d]->dx);
+            r = r ? r : upload_vec(c, to_f(dmx), &mf[d]->dmx);
+            r = r ? r : upload_vec(c, to_f(rdx), &mf[d]->rdx);
+            r = r ? r : upload_vec(c, to_f(rdmx), &mf[d]->rdmx);
+        }
     }
-    Fields &F = c->cx.f;
+    g.d1 = g.m1; g.d2 = g.m2; g.d3 = g.m3;
     const size_t NP = (size_t)g.NP;
-    double **fl[] = {&F.T, &F.U, &F.V, &F.W, &F.P, &F.dPhat, &F.dP0, &F.Tn, &F.Un, &F.Vn, &F.Wn, &F.dPhatn, &F.dP0n,
-                     &F.dU, &F.dV, &F.dW, &F.dP, &F.R};
-    for (double **p : fl) if (!r) r = dalloc(c, p, NP);
-    if (!r) r = dalloc(c, &F.Mu2, (size_t)(N2 + 2) * (N3 + 2));
-    if (!r) r = dalloc(c, &F.iR2, (size_t)(N2 + 2) * (N3 + 2));
     c->cx.h1p = N1 / 2 + 1;
-    if (!r) r = dalloc(c, &F.S, (size_t)c->cx.h1p * N2 * N3);
     if (!r) r = dalloc(c, &g.scal, (size_t)S_NSCAL);
     c->partials = post_partial_count();
-    if (!r) r = dalloc(c, &F.part, (size_t)c->partials);
-    F.hist_cap = 100000;
-    if (!r) r = dalloc(c, &F.hist, (size_t)F.hist_cap * 7);
+    if (!r) r = dalloc(c, &c->cx.f.part, (size_t)c->partials);
+    c->cx.f.hist_cap = 100000;
+    if (!r) r = dalloc(c, &c->cx.f.hist, (size_t)c->cx.f.hist_cap * 7);
+    // the fields of the active form
+    auto alloc_fields = [&](auto &x) {
+        auto &F = x.f;
+        using R = std::remove_pointer_t<decltype(F.T)>;
+        R **fl[] = {&F.T, &F.U, &F.V, &F.W, &F.P, &F.dPhat, &F.dP0, &F.Tn, &F.Un, &F.Vn, &F.Wn, &F.dPhatn, &F.dP0n,
+                    &F.dU, &F.dV, &F.dW, &F.dP, &F.scr};
+        for (R **p : fl) if (!r) r = dalloc(c, p, NP);
+        if (!r) r = dalloc(c, &F.Mu2, (size_t)(N2 + 2) * (N3 + 2));
+        if (!r) r = dalloc(c, &F.iR2, (size_t)(N2 + 2) * (N3 + 2));
+        if (!r) r = dalloc(c, &F.S, (size_t)c->cx.h1p * N2 * N3);
+    };
+    on_ctx(c, alloc_fields);
+    if (c->fp32 && !r) r = dalloc(c, &c->stage, NP);
     if (r) { tcs_destroy(c); return r; }
+    auto &F = c->cx.f;
 
     // wavenumbers (module_solve_pressure.f90:93-129) and modal y coefficients (:599-609)
     const double PI = std::acos(-1.0), ddx = g.ph.L1 / (double)N1, ddz = g.ph.L3 / (double)N3;
@@ -382,8 +438,19 @@ int tcs_create(const tcs_config *cfg, tcs_ctx **out)
         for (int e = 0; e < n; e++) w[e] = make_double2(std::cos(2.0 * M_PI * (double)e / (double)n), -std::sin(2.0 * M_PI * (double)e / (double)n));
         return w;
     };
-    r = r ? r : upload_vec(c, twid(N1), &F.tw1);
-    r = r ? r : upload_vec(c, twid(N3), &F.tw3);
+    auto twid_f = [&](int n) {
+        const std::vector<double2> w = twid(n);
+        std::vector<float2> v(n);
+        for (int e = 0; e < n; e++) v[e] = make_float2((float)w[e].x, (float)w[e].y);
+        return v;
+    };
+    if (c->fp32) {
+        r = r ? r : upload_vec(c, twid_f(N1), &c->cf.f.tw1);
+        r = r ? r : upload_vec(c, twid_f(N3), &c->cf.f.tw3);
+    } else {
+        r = r ? r : upload_vec(c, twid(N1), &F.tw1);
+        r = r ? r : upload_vec(c, twid(N3), &F.tw3);
+    }
     {   // Pbc_a, Pbc_b (module_solve_pressure.f90:720-730)
         const int n2sub = N2 + 1, n2msub = N2;
         const double s1 = (dmx2[1] + dmx2[2]) * (dmx2[1] + dmx2[2]);
@@ -394,17 +461,28 @@ int tcs_create(const tcs_config *cfg, tcs_ctx **out)
         c->cx.wall_bt = dmx2[n2sub] * dmx2[n2sub] / (s2 - dmx2[n2sub] * dmx2[n2sub]);
     }
     c->cx.fp1 = fp1; c->cx.fp3 = fp3;
-    c->cx.tl_strided = 8;
-    c->cx.tl_contig = choose_tl(N1, true, 1, 8);
-    c->cx.tl_modal = choose_tl(N2, false, 2, 8);
+    const size_t rb1 = row_bytes(1, c->fp32);
+    c->cx.tl_contig = choose_tl(N1, true, rb1, 8);
+    c->cx.tl_modal = choose_tl(N2, false, row_bytes(2, false), 8);   // modal rows are FP64 in both forms
     {
-        const int tz = choose_tl(N3, true, 1, 8), ty = choose_tl(N2, false, 1, 8);
+        const int tz = choose_tl(N3, true, rb1, 8), ty = choose_tl(N2, false, rb1, 8);
         c->cx.tl_strided = tz < ty ? tz : ty;
     }
     // measured on B200 at 256^3: 4 lines per block beats 1, 2, 8 and 16 for both FFT kernels
     c->cx.fft_lines_x = N1 <= 256 ? 4 : (N1 <= 512 ? 2 : 1);
     c->cx.fft_lines_z = N3 <= 256 ? 4 : (N3 <= 512 ? 2 : 1);
     c->cx.probe = &c->probe;
+    sync_shapes(c);
+    {   // the FP32 context shares the grid, constants, scalars, tables and history
+        GridT<float> &gf = c->cf.g;
+        gf.N1 = g.N1; gf.N2 = g.N2; gf.N3 = g.N3; gf.P1 = g.P1; gf.P2 = g.P2; gf.NP = g.NP;
+        gf.d1 = g.d1; gf.d2 = g.d2; gf.d3 = g.d3;
+        gf.ph = phys_cast<float>(g.ph); gf.phd = g.ph;
+        gf.scal = g.scal;
+        FieldsT<float> &ff = c->cf.f;
+        ff.dxk2 = F.dxk2; ff.dzk = F.dzk; ff.fam = F.fam; ff.fap = F.fap;
+        ff.part = F.part; ff.hist = F.hist; ff.hist_cap = F.hist_cap;
+    }
 
     // initial fields: mpi_thermal_initial/boundary, mpi_momentum_initial/boundary,
     // mpi_pressure_initial, then ghost(T,U,V,W,P) (main.f90:92-109)
@@ -431,8 +509,15 @@ int tcs_create(const tcs_config *cfg, tcs_ctx **out)
     }
     host_ghost(T, N1, N2, N3);
     if (!r) {
-        cudaMemcpyAsync(F.T, T.data(), NP * sizeof(double), cudaMemcpyHostToDevice, c->stream);
-        cudaMemcpyAsync(F.Tn, T.data(), NP * sizeof(double), cudaMemcpyHostToDevice, c->stream);
+        if (c->fp32) {
+            const std::vector<float> Tf(T.begin(), T.end());
+            cudaMemcpyAsync(c->cf.f.T, Tf.data(), NP * sizeof(float), cudaMemcpyHostToDevice, c->stream);
+            cudaMemcpyAsync(c->cf.f.Tn, Tf.data(), NP * sizeof(float), cudaMemcpyHostToDevice, c->stream);
+            cudaStreamSynchronize(c->stream);   // Tf is a local
+        } else {
+            cudaMemcpyAsync(F.T, T.data(), NP * sizeof(double), cudaMemcpyHostToDevice, c->stream);
+            cudaMemcpyAsync(F.Tn, T.data(), NP * sizeof(double), cudaMemcpyHostToDevice, c->stream);
+        }
         double sc[S_NSCAL] = {0};
         sc[S_DT] = cfg->dtStart; sc[S_TIME] = cfg->tStart; sc[S_CFL] = cfg->MaxCFL;
         sc[S_FIXED_DT] = cfg->fixed_dt ? 1.0 : 0.0;
@@ -494,20 +579,39 @@ static int copy_field(tcs_ctx *c, int f, double *host, bool up, bool async)
     int r = flush_pending(c);
     if (r) return r;
     const size_t NP = (size_t)c->cx.g.NP;
-    const Grid &g = c->cx.g;
+    const GridT<double> &g = c->cx.g;
     if (f == TCS_F_MU || f == TCS_F_INVRHO) {
         if (up) return set_err(TCS_ERR_ARG, "Mu and invRho are derived from T");
         std::vector<double> t((size_t)(g.N2 + 2) * (g.N3 + 2));
-        CK(cudaMemcpyAsync(t.data(), f == TCS_F_MU ? c->cx.f.Mu2 : c->cx.f.iR2, t.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        if (c->fp32) {
+            std::vector<float> tf(t.size());
+            CK(cudaMemcpyAsync(tf.data(), f == TCS_F_MU ? c->cf.f.Mu2 : c->cf.f.iR2, tf.size() * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+            CK(cudaStreamSynchronize(c->stream));
+            for (size_t q = 0; q < t.size(); q++) t[q] = tf[q];
+        } else {
+            CK(cudaMemcpyAsync(t.data(), f == TCS_F_MU ? c->cx.f.Mu2 : c->cx.f.iR2, t.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        }
         CK(cudaStreamSynchronize(c->stream));
         for (int k = 0; k < g.N3 + 2; k++)
             for (int j = 0; j < g.N2 + 2; j++)
                 for (int i = 0; i < g.N1 + 2; i++) host[(size_t)i + (size_t)g.P1 * ((size_t)j + (size_t)g.P2 * k)] = t[j + (size_t)g.P2 * k];
         return TCS_OK;
     }
-    double *d = field_ptr(c, f);
+    void *d = field_ptr(c, f);
     if (!d) return set_err(TCS_ERR_ARG, "unknown field");
-    if (up) {
+    if (c->fp32) {   // FP64 host arrays pass through the FP64 staging buffer
+        float *df = (float *)d;
+        if (up) {
+            CK(cudaMemcpyAsync(c->stage, host, NP * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+            launch_convert_in<float>(c->stage, df, (long long)NP, c->stream);
+            if (f == TCS_F_T) launch_convert_in<float>(c->stage, c->cf.f.Tn, (long long)NP, c->stream);
+            c->ghost_ok &= ~(1u << f);
+        } else {
+            launch_convert<float>(df, c->stage, (long long)NP, c->stream);
+            CK(cudaMemcpyAsync(host, c->stage, NP * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        }
+        if ((r = take_launch_error())) return r;
+    } else if (up) {
         CK(cudaMemcpyAsync(d, host, NP * sizeof(double), cudaMemcpyHostToDevice, c->stream));
         if (f == TCS_F_T) CK(cudaMemcpyAsync(c->cx.f.Tn, host, NP * sizeof(double), cudaMemcpyHostToDevice, c->stream));
         c->ghost_ok &= ~(1u << f);
@@ -523,7 +627,9 @@ int tcs_download_field(tcs_ctx *c, int f, double *h) { return copy_field(c, f, h
 int tcs_upload_field_async(tcs_ctx *c, int f, const double *h) { return copy_field(c, f, (double *)h, true, true); }
 int tcs_download_field_async(tcs_ctx *c, int f, double *h) { return copy_field(c, f, h, false, true); }
 
-int tcs_field_device_ptr(tcs_ctx *c, int f, double **dev)
+int tcs_precision(const tcs_ctx *c) { return c ? c->cfg.precision : -1; }
+
+int tcs_field_device_ptr(tcs_ctx *c, int f, void **dev)
 {
     if (!c || !dev) return set_err(TCS_ERR_ARG, "null argument");
     int r = flush_pending(c);
@@ -559,7 +665,7 @@ int tcs_momentum_coeffi_clean(tcs_ctx *c) { ENTER(c); return TCS_OK; }
 static void ensure_ghosts(tcs_ctx *c, int f)
 {
     if (c->ghost_ok & (1u << f)) return;
-    launch_ghost(c->cx, field_ptr(c, f), c->stream);
+    on_ctx(c, [&](auto &x) { launch_ghost(x, field_ptr_t(x.f, f), c->stream); });
     c->ghost_ok |= (1u << f);
 }
 
@@ -582,8 +688,7 @@ int tcs_thermal_solver(tcs_ctx *c)
     int r = flush_pending(c);
     if (r) return r;
     ensure_ghosts(c, TCS_F_T); ensure_ghosts(c, TCS_F_U); ensure_ghosts(c, TCS_F_V); ensure_ghosts(c, TCS_F_W);
-    launch_thermal(c->cx, c->stream);
-    std::swap(c->cx.f.T, c->cx.f.Tn);
+    on_ctx(c, [&](auto &x) { launch_thermal(x, c->stream); swap_T(x); });
     return take_launch_error();
 }
 
@@ -593,7 +698,7 @@ int tcs_momentum_coeffi(tcs_ctx *c)
     int r = flush_pending(c);
     if (r) return r;
     ensure_ghosts(c, TCS_F_T);
-    launch_momentum_coeffi(c->cx, c->stream);
+    on_ctx(c, [&](auto &x) { launch_momentum_coeffi(x, c->stream); });
     return take_launch_error();
 }
 
@@ -603,7 +708,7 @@ int tcs_momentum_coeffi(tcs_ctx *c)
         ENTER(c);                                               \
         int r = flush_pending(c);                               \
         if (r) return r;                                        \
-        launcher(c->cx, c->stream);                             \
+        on_ctx(c, [&](auto &x) { launcher(x, c->stream); });    \
         if ((outfield) >= 0) c->ghost_ok |= (1u << (outfield)); \
         return take_launch_error();                             \
     }
@@ -618,7 +723,7 @@ int tcs_momentum_blockLdU(tcs_ctx *c)
     ENTER(c);
     int r = flush_pending(c);
     if (r) return r;
-    launch_blockld_u(c->cx, c->stream);
+    on_ctx(c, [&](auto &x) { launch_blockld_u(x, c->stream); });
     c->ghost_ok &= ~(1u << TCS_F_DU);   // the reference leaves dU's ghosts stale here
     return take_launch_error();
 }
@@ -638,12 +743,11 @@ int tcs_pressure_RHS(tcs_ctx *c)
     ENTER(c);
     ensure_ghosts(c, TCS_F_DPHAT);
     if (c->pending_pseudo) {
-        launch_pseudo_prhs_fftx(c->cx, c->stream, true);
-        std::swap(c->cx.f.U, c->cx.f.Un); std::swap(c->cx.f.V, c->cx.f.Vn); std::swap(c->cx.f.W, c->cx.f.Wn);
+        on_ctx(c, [&](auto &x) { launch_pseudo_prhs_fftx(x, c->stream, true); swap_UVW(x); });
         c->pending_pseudo = false;
     } else {
         ensure_ghosts(c, TCS_F_U); ensure_ghosts(c, TCS_F_V); ensure_ghosts(c, TCS_F_W);
-        launch_pseudo_prhs_fftx(c->cx, c->stream, false);
+        on_ctx(c, [&](auto &x) { launch_pseudo_prhs_fftx(x, c->stream, false); });
     }
     return take_launch_error();
 }
@@ -653,7 +757,7 @@ int tcs_pressure_Poisson_FFT2(tcs_ctx *c)
     ENTER(c);
     int r = flush_pending(c);
     if (r) return r;
-    launch_poisson_rest(c->cx, c->stream);
+    on_ctx(c, [&](auto &x) { launch_poisson_rest(x, c->stream); });
     c->ghost_ok |= (1u << TCS_F_DP);
     return take_launch_error();
 }
@@ -664,8 +768,7 @@ int tcs_pressure_Projection(tcs_ctx *c)
     int r = flush_pending(c);
     if (r) return r;
     ensure_ghosts(c, TCS_F_DPHAT);
-    launch_projection(c->cx, c->stream);
-    std::swap(c->cx.f.dPhat, c->cx.f.dPhatn); std::swap(c->cx.f.dP0, c->cx.f.dP0n);
+    on_ctx(c, [&](auto &x) { launch_projection(x, c->stream); swap_phat(x); });
     c->ghost_ok |= (1u << TCS_F_U) | (1u << TCS_F_V) | (1u << TCS_F_W) | (1u << TCS_F_P) | (1u << TCS_F_DPHAT);
     return take_launch_error();
 }
@@ -675,7 +778,7 @@ int tcs_post_div(tcs_ctx *c, double *maxDivU)
     ENTER(c);
     int r = flush_pending(c);
     if (r) return r;
-    launch_post(c->cx, c->stream, 1);
+    on_ctx(c, [&](auto &x) { launch_post(x, c->stream, 1); });
     if ((r = take_launch_error())) return r;
     double sc[S_NSCAL];
     CK(cudaMemcpyAsync(sc, c->cx.g.scal, sizeof(sc), cudaMemcpyDeviceToHost, c->stream));
@@ -695,12 +798,13 @@ int tcs_post_cfl(tcs_ctx *c, double *CFL, double *dt)
     return std::isfinite(sc[S_DT]) ? TCS_OK : set_err(TCS_ERR_NONFINITE, "dt is not finite");
 }
 
-static void launch_step(tcs_ctx *c)
+} // extern "C"
+
+template <class R>
+static void launch_step_t(Ctx<R> &cx, cudaStream_t s)
 {
-    Ctx &cx = c->cx;
-    cudaStream_t s = c->stream;
     launch_thermal(cx, s);
-    std::swap(cx.f.T, cx.f.Tn);
+    swap_T(cx);
     launch_momentum_coeffi(cx, s);
     launch_solve_du(cx, s);
     launch_solve_dv(cx, s);
@@ -708,12 +812,19 @@ static void launch_step(tcs_ctx *c)
     launch_blockld_v(cx, s);
     launch_blockld_u(cx, s);
     launch_pseudo_prhs_fftx(cx, s, true);
-    std::swap(cx.f.U, cx.f.Un); std::swap(cx.f.V, cx.f.Vn); std::swap(cx.f.W, cx.f.Wn);
+    swap_UVW(cx);
     launch_poisson_rest(cx, s);
     launch_projection(cx, s);
-    std::swap(cx.f.dPhat, cx.f.dPhatn); std::swap(cx.f.dP0, cx.f.dP0n);
+    swap_phat(cx);
     launch_post(cx, s, 1);
 }
+
+static void launch_step(tcs_ctx *c)
+{
+    on_ctx(c, [&](auto &x) { launch_step_t(x, c->stream); });
+}
+
+extern "C" {
 
 // Launch-shape knobs (lines per block of the line-solver families and of the
 // FFT kernels).  Values are validated against the shared-memory budget.
@@ -721,30 +832,32 @@ int tcs_set_tuning(tcs_ctx *c, int knob, int value)
 {
     ENTER(c);
     if (value < 1 || value > 64 || (value & (value - 1))) return set_err(TCS_ERR_ARG, "tuning value must be a power of two in 1..64");
-    Ctx &x = c->cx;
-    const Grid &g = x.g;
+    Ctx<double> &x = c->cx;
+    const GridT<double> &g = x.g;
+    const size_t rb1 = row_bytes(1, c->fp32), e = esize(c);
     switch (knob) {
     case TCS_TUNE_TL_STRIDED: {
         LinePlan a = make_line_plan(g.N3, true, value), b = make_line_plan(g.N2, false, value);
         const int LS = a.LS > b.LS ? a.LS : b.LS;
-        if ((size_t)3 * value * LS * 8 + 4096 * 4 > 200 * 1024) return set_err(TCS_ERR_ARG, "too many lines for shared memory");
+        if (rb1 * value * LS + 4096 * 4 > 200 * 1024) return set_err(TCS_ERR_ARG, "too many lines for shared memory");
         x.tl_strided = value; break; }
     case TCS_TUNE_TL_CONTIG: {
         LinePlan a = make_line_plan(g.N1, true, value);
-        if ((size_t)3 * value * a.LS * 8 + 4096 * 4 > 200 * 1024) return set_err(TCS_ERR_ARG, "too many lines for shared memory");
+        if (rb1 * value * a.LS + 4096 * 4 > 200 * 1024) return set_err(TCS_ERR_ARG, "too many lines for shared memory");
         x.tl_contig = value; break; }
     case TCS_TUNE_TL_MODAL: {
         LinePlan a = make_line_plan(g.N2, false, value);
-        if ((size_t)4 * value * a.LS * 8 + 4096 * 4 > 200 * 1024) return set_err(TCS_ERR_ARG, "too many lines for shared memory");
+        if (row_bytes(2, false) * value * a.LS + 4096 * 4 > 200 * 1024) return set_err(TCS_ERR_ARG, "too many lines for shared memory");
         x.tl_modal = value; break; }
     case TCS_TUNE_FFT_LINES_X:
-        if ((size_t)value * g.N1 * 40 > 200 * 1024) return set_err(TCS_ERR_ARG, "too many lines for shared memory");
+        if ((size_t)value * g.N1 * 5 * e > 200 * 1024) return set_err(TCS_ERR_ARG, "too many lines for shared memory");
         x.fft_lines_x = value; break;
     case TCS_TUNE_FFT_LINES_Z:
-        if ((size_t)value * g.N3 * 32 > 200 * 1024) return set_err(TCS_ERR_ARG, "too many lines for shared memory");
+        if ((size_t)value * g.N3 * 4 * e > 200 * 1024) return set_err(TCS_ERR_ARG, "too many lines for shared memory");
         x.fft_lines_z = value; break;
     default: return set_err(TCS_ERR_ARG, "unknown tuning knob");
     }
+    sync_shapes(c);
     for (auto &ge : c->graphs) cudaGraphExecDestroy(ge.exec);
     c->graphs.clear();
     return TCS_OK;
@@ -754,7 +867,7 @@ int tcs_get_tuning(tcs_ctx *c, int knob, int *value)
 {
     ENTER(c);
     if (!value) return set_err(TCS_ERR_ARG, "null argument");
-    const Ctx &x = c->cx;
+    const Ctx<double> &x = c->cx;
     switch (knob) {
     case TCS_TUNE_TL_STRIDED: *value = x.tl_strided; break;
     case TCS_TUNE_TL_CONTIG: *value = x.tl_contig; break;
@@ -794,7 +907,7 @@ int tcs_step(tcs_ctx *c, int nsteps, int *done)
             if ((r = take_launch_error())) return r;
             continue;
         }
-        const double *T0 = c->cx.f.T, *U0 = c->cx.f.U, *P0 = c->cx.f.dPhat;
+        const void *T0 = field_ptr(c, TCS_F_T), *U0 = field_ptr(c, TCS_F_U), *P0 = field_ptr(c, TCS_F_DPHAT);
         cudaGraphExec_t exec = nullptr;
         unsigned long long kernels_this = 0;
         for (auto &ge : c->graphs) if (ge.T == T0 && ge.U == U0 && ge.dPhat == P0) { exec = ge.exec; kernels_this = ge.kernels; break; }
@@ -813,9 +926,7 @@ int tcs_step(tcs_ctx *c, int nsteps, int *done)
             kernels_this = nk;
             // capture swapped the buffers already; the launch below performs that step
         } else {
-            std::swap(c->cx.f.T, c->cx.f.Tn);
-            std::swap(c->cx.f.U, c->cx.f.Un); std::swap(c->cx.f.V, c->cx.f.Vn); std::swap(c->cx.f.W, c->cx.f.Wn);
-            std::swap(c->cx.f.dPhat, c->cx.f.dPhatn); std::swap(c->cx.f.dP0, c->cx.f.dP0n);
+            on_ctx(c, [&](auto &x) { swap_T(x); swap_UVW(x); swap_phat(x); });
         }
         CK(cudaGraphLaunch(exec, c->stream));
         g_launches += kernels_this;
@@ -837,10 +948,12 @@ int tcs_snapshot(tcs_ctx *c)
     ENTER(c);
     int r = flush_pending(c);
     if (r) return r;
-    const size_t bytes = (size_t)c->cx.g.NP * sizeof(double);
+    const size_t bytes = (size_t)c->cx.g.NP * esize(c);
     const int fl[7] = {TCS_F_T, TCS_F_U, TCS_F_V, TCS_F_W, TCS_F_P, TCS_F_DPHAT, TCS_F_DP0};
     for (int q = 0; q < 7; q++) {
-        if (!c->snap[q] && (r = dalloc(c, &c->snap[q], (size_t)c->cx.g.NP))) return r;
+        unsigned char *sp = (unsigned char *)c->snap[q];
+        if (!sp && (r = dalloc(c, &sp, bytes))) return r;
+        c->snap[q] = sp;
         CK(cudaMemcpyAsync(c->snap[q], field_ptr(c, fl[q]), bytes, cudaMemcpyDeviceToDevice, c->stream));
     }
     CK(cudaMemcpyAsync(c->snap_scal, c->cx.g.scal, sizeof(c->snap_scal), cudaMemcpyDeviceToHost, c->stream));
@@ -855,7 +968,7 @@ int tcs_restore(tcs_ctx *c)
     if (!c->have_snap) return set_err(TCS_ERR_ARG, "no snapshot");
     int r = flush_pending(c);
     if (r) return r;
-    const size_t bytes = (size_t)c->cx.g.NP * sizeof(double);
+    const size_t bytes = (size_t)c->cx.g.NP * esize(c);
     const int fl[7] = {TCS_F_T, TCS_F_U, TCS_F_V, TCS_F_W, TCS_F_P, TCS_F_DPHAT, TCS_F_DP0};
     for (int q = 0; q < 7; q++)
         CK(cudaMemcpyAsync(field_ptr(c, fl[q]), c->snap[q], bytes, cudaMemcpyDeviceToDevice, c->stream));

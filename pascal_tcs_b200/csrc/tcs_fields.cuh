@@ -6,33 +6,35 @@
 
 namespace tcs {
 
-struct Fields {
+template <class R>
+struct FieldsT {
     // persistent fields (padded, i fastest)
-    double *T, *U, *V, *W, *P, *dPhat, *dP0;
+    R *T, *U, *V, *W, *P, *dPhat, *dP0;
     // second buffers of the fields that a kernel rewrites while other threads
     // still read the old values (T in the thermal y sweep, U/V/W in the fused
     // pseudo-update, dPhat/dP0 in the projection)
-    double *Tn, *Un, *Vn, *Wn, *dPhatn, *dP0n;
+    R *Tn, *Un, *Vn, *Wn, *dPhatn, *dP0n;
     // per-step increments and pressure correction
-    double *dU, *dV, *dW, *dP;
+    R *dU, *dV, *dW, *dP;
     // interior stage scratch (padded layout)
-    double *R;
+    R *scr;
     // 2-D (j,k) property tables: Mu and invRho of mpi_momentum_coeffi
-    double *Mu2, *iR2;
+    R *Mu2, *iR2;
     // Poisson spectral work array: (h1p, N2, N3) complex, kx fastest
-    double2 *S;
-    // modified wavenumbers and y coefficients of the modal solves
+    cplx_t<R> *S;
+    // modified wavenumbers and y coefficients of the modal solves (FP64 in both forms)
     const double *dxk2, *dzk, *fam, *fap;
     // FFT twiddles exp(-2 pi i e / n) for n = N1 and n = N3
-    const double2 *tw1, *tw3;
+    const cplx_t<R> *tw1, *tw3;
     // reduction scratch
     double *part;
-    double *hist;            // per-step diagnostics history (S_NSCAL doubles per step)
+    double *hist;            // per-step diagnostics history (7 doubles per step)
     int hist_cap;
 };
 
 // Skip all work once the divergence check has flagged a blow-up, so the
 // fields stay at the state of the step that blew up (main.f90:208-212).
-__device__ __forceinline__ bool blown(const Grid &g) { return g.scal[S_BLOWUP] != 0.0; }
+template <class R>
+__device__ __forceinline__ bool blown(const GridT<R> &g) { return g.scal[S_BLOWUP] != 0.0; }
 
 } // namespace tcs

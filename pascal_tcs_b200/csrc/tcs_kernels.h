@@ -28,9 +28,8 @@ struct FFTPlan {
 
 struct ProbeState;   // CUDA-event probes (tcs_capi.cu)
 
-struct Ctx {
-    Grid g;
-    Fields f;
+// Launch shapes shared by both forms.
+struct Shapes {
     int tl_strided, tl_contig, tl_modal;
     int fft_lines_x, fft_lines_z;
     FFTPlan fp1, fp3;
@@ -39,17 +38,30 @@ struct Ctx {
     ProbeState *probe;
 };
 
+template <class R>
+struct Ctx : Shapes {
+    GridT<R> g;
+    FieldsT<R> f;
+};
+
 LinePlan make_line_plan(int n, bool cyclic, int TL);
 bool make_fft_plan(int n, FFTPlan &fp);
-void probe_begin(const Ctx &cx, int kid, cudaStream_t s);
-void probe_end(const Ctx &cx, int kid, cudaStream_t s);
+void probe_begin(const Shapes &cx, int kid, cudaStream_t s);
+void probe_end(const Shapes &cx, int kid, cudaStream_t s);
 int record_launch_error(const char *what);
 int set_error(int code, const std::string &msg);
 
+// Dynamic shared memory of a line-solver launch.
 template <class Prob>
-inline void launch_lines(const Prob &p, const LinePlan &lp, dim3 grid, cudaStream_t s, int kid, const Ctx &cx)
+inline size_t line_smem(const LinePlan &lp)
 {
-    const size_t smem = (size_t)(2 + Prob::NRHS) * lp.TL * lp.LS * sizeof(double) + (size_t)lp.n * sizeof(int);
+    return (size_t)line_words<Prob>() * lp.TL * lp.LS * sizeof(typename Prob::Real) + (size_t)lp.n * sizeof(int);
+}
+
+template <class Prob>
+inline void launch_lines(const Prob &p, const LinePlan &lp, dim3 grid, cudaStream_t s, int kid, const Shapes &cx)
+{
+    const size_t smem = line_smem<Prob>(lp);
     static size_t configured = 0;
     if (smem > configured) {
         cudaFuncSetAttribute(line_solve_kernel<Prob>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -61,20 +73,22 @@ inline void launch_lines(const Prob &p, const LinePlan &lp, dim3 grid, cudaStrea
     record_launch_error(kernel_name(kid));
 }
 
-// Stage launchers (one per reference routine or fused group).
-void launch_thermal(const Ctx &cx, cudaStream_t s);
-void launch_momentum_coeffi(const Ctx &cx, cudaStream_t s);
-void launch_solve_du(const Ctx &cx, cudaStream_t s);
-void launch_solve_dv(const Ctx &cx, cudaStream_t s);
-void launch_solve_dw(const Ctx &cx, cudaStream_t s);
-void launch_blockld_v(const Ctx &cx, cudaStream_t s);
-void launch_blockld_u(const Ctx &cx, cudaStream_t s);
-void launch_pseudo_update(const Ctx &cx, cudaStream_t s);           // standalone (Un = U + dU, ...)
-void launch_pseudo_prhs_fftx(const Ctx &cx, cudaStream_t s, bool with_pseudo);
-void launch_poisson_rest(const Ctx &cx, cudaStream_t s);
-void launch_projection(const Ctx &cx, cudaStream_t s);
-void launch_post(const Ctx &cx, cudaStream_t s, int record_hist);
-void launch_ghost(const Ctx &cx, double *a, cudaStream_t s);
-void launch_set_fields_walls(const Ctx &cx, cudaStream_t s);
+// Stage launchers (one per reference routine or fused group), instantiated
+// for R = double and R = float.
+template <class R> void launch_thermal(const Ctx<R> &cx, cudaStream_t s);
+template <class R> void launch_momentum_coeffi(const Ctx<R> &cx, cudaStream_t s);
+template <class R> void launch_solve_du(const Ctx<R> &cx, cudaStream_t s);
+template <class R> void launch_solve_dv(const Ctx<R> &cx, cudaStream_t s);
+template <class R> void launch_solve_dw(const Ctx<R> &cx, cudaStream_t s);
+template <class R> void launch_blockld_v(const Ctx<R> &cx, cudaStream_t s);
+template <class R> void launch_blockld_u(const Ctx<R> &cx, cudaStream_t s);
+template <class R> void launch_pseudo_update(const Ctx<R> &cx, cudaStream_t s);   // standalone (Un = U + dU, ...)
+template <class R> void launch_pseudo_prhs_fftx(const Ctx<R> &cx, cudaStream_t s, bool with_pseudo);
+template <class R> void launch_poisson_rest(const Ctx<R> &cx, cudaStream_t s);
+template <class R> void launch_projection(const Ctx<R> &cx, cudaStream_t s);
+template <class R> void launch_post(const Ctx<R> &cx, cudaStream_t s, int record_hist);
+template <class R> void launch_ghost(const Ctx<R> &cx, R *a, cudaStream_t s);
+template <class R> void launch_convert(const R *src, double *dst, long long n, cudaStream_t s);   // field -> FP64 staging
+template <class R> void launch_convert_in(const double *src, R *dst, long long n, cudaStream_t s); // FP64 staging -> field
 
 } // namespace tcs

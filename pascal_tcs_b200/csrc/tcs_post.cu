@@ -2,7 +2,9 @@
 // (module_post.f90:100-158, 168-230) with the adaptive time step, the
 // blow-up test of main.f90:208-212, and the Nusselt / kinetic-energy series.
 // Two kernels: block partials in a fixed order, then one block that combines
-// them and updates dt, time and CFL on the device (deterministic).
+// them and updates dt, time and CFL on the device (deterministic).  Both forms
+// reduce in FP64 from their fields, and the per-thread sums are compensated
+// (Neumaier), so the diagnostics keep FP64 accuracy over 512^3 cells.
 #include "tcs_kernels.h"
 
 #include <math.h>
@@ -12,14 +14,24 @@ namespace tcs {
 enum { PT_DIV = 0, PT_CFL, PT_KE, PT_NUB, PT_NUT, PT_N };
 static const int POST_BLOCKS = 592;   // 4 x 148 SMs
 
-__global__ void __launch_bounds__(256) post_kernel(Grid g, Fields f)
+// s + e carries a sum and its running rounding error (Neumaier's variant of
+// Kahan summation).
+__device__ __forceinline__ void csum(double &s, double &e, double v)
+{
+    const double t = s + v;
+    e += (fabs(s) >= fabs(v)) ? (s - t) + v : (v - t) + s;
+    s = t;
+}
+
+template <class R>
+__global__ void __launch_bounds__(256) post_kernel(GridT<R> g, FieldsT<R> f)
 {
     __shared__ double red[PT_N][256];
     if (blown(g)) return;
     const long long n = (long long)g.N1 * g.N2 * g.N3;
-    double mdiv = -INFINITY, mcfl = -INFINITY, ke = 0.0, nub = 0.0, nut = 0.0;
-    const double *dx1 = g.m1.dx, *dx2 = g.m2.dx, *dx3 = g.m3.dx;
-    const double *rdx1 = g.m1.rdx, *rdx2 = g.m2.rdx, *rdx3 = g.m3.rdx;
+    double mdiv = -INFINITY, mcfl = -INFINITY, ke = 0.0, nub = 0.0, nut = 0.0, eke = 0.0, enb = 0.0, ent = 0.0;
+    const double *dx1 = g.d1.dx, *dx2 = g.d2.dx, *dx3 = g.d3.dx;
+    const double *rdx1 = g.d1.rdx, *rdx2 = g.d2.rdx, *rdx3 = g.d3.rdx;
     const long long sj = g.P1, sk = (long long)g.P1 * g.P2;
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
         const int i = 1 + (int)(t % g.N1);
@@ -27,15 +39,16 @@ __global__ void __launch_bounds__(256) post_kernel(Grid g, Fields f)
         const int j = 1 + (int)(q % g.N2), k = 1 + (int)(q / g.N2);
         const long long c = ix(g, i, j, k);
         const double Uc = ld(f.U + c), Vc = ld(f.V + c), Wc = ld(f.W + c);
-        const double Ux = ld(f.U + c + 1), Vy = ld(f.V + c + sj), Wz = ld(f.W + c + sk);
+        const double Ux = ld(f.U + c + 1), Vy = ld(f.V + c + sj), Wz = ld(f.W + c + sk);   // FP32 values are exact in FP64
         const double dv = (Ux - Uc) * rdx1[i] + (Vy - Vc) * rdx2[j] + (Wz - Wc) * rdx3[k];
         const double cf = (fabs(Ux + Uc) / 2.0) * rdx1[i] + (fabs(Vy + Vc) / 2.0) * rdx2[j] + (fabs(Wz + Wc) / 2.0) * rdx3[k];
         mdiv = fmax(mdiv, dv);
         mcfl = fmax(mcfl, cf);
-        ke += (Uc * Uc + Vc * Vc + Wc * Wc) * dx1[i] * dx2[j] * dx3[k];
-        if (j == 1) nub += -(ld(f.T + c) - g.ph.Tbt) / g.m2.dmx[1];
-        if (j == g.N2) nut += -(g.ph.Tup - ld(f.T + c)) / g.m2.dmx[g.N2 + 1];
+        csum(ke, eke, (Uc * Uc + Vc * Vc + Wc * Wc) * dx1[i] * dx2[j] * dx3[k]);
+        if (j == 1) csum(nub, enb, -((double)ld(f.T + c) - g.phd.Tbt) / g.d2.dmx[1]);
+        if (j == g.N2) csum(nut, ent, -(g.phd.Tup - (double)ld(f.T + c)) / g.d2.dmx[g.N2 + 1]);
     }
+    ke += eke; nub += enb; nut += ent;
     red[PT_DIV][threadIdx.x] = mdiv; red[PT_CFL][threadIdx.x] = mcfl;
     red[PT_KE][threadIdx.x] = ke; red[PT_NUB][threadIdx.x] = nub; red[PT_NUT][threadIdx.x] = nut;
     __syncthreads();
@@ -52,7 +65,8 @@ __global__ void __launch_bounds__(256) post_kernel(Grid g, Fields f)
     if (threadIdx.x < PT_N) f.part[blockIdx.x * PT_N + threadIdx.x] = red[threadIdx.x][0];
 }
 
-__global__ void __launch_bounds__(256) finalize_kernel(Grid g, Fields f, int nblocks, int record_hist)
+template <class R>
+__global__ void __launch_bounds__(256) finalize_kernel(GridT<R> g, FieldsT<R> f, int nblocks, int record_hist)
 {
     __shared__ double red[PT_N][256];
     if (blown(g)) return;
@@ -83,7 +97,7 @@ __global__ void __launch_bounds__(256) finalize_kernel(Grid g, Fields f, int nbl
     sc[S_MAXDIV] = maxdiv;
     sc[S_NUBOT] = red[PT_NUB][0] / cnt;
     sc[S_NUTOP] = red[PT_NUT][0] / cnt;
-    sc[S_KE] = 0.5 * red[PT_KE][0] / (g.ph.L1 * g.ph.L2 * g.ph.L3);
+    sc[S_KE] = 0.5 * red[PT_KE][0] / (g.phd.L1 * g.phd.L2 * g.phd.L3);
     if (maxdiv >= 1.0e-3 || maxdiv != maxdiv) {
         sc[S_BLOWUP] = sc[S_STEP] + 1.0;          // the step (1-based) that blew up
         return;
@@ -91,8 +105,8 @@ __global__ void __launch_bounds__(256) finalize_kernel(Grid g, Fields f, int nbl
     if (sc[S_FIXED_DT] != 0.0) {
         sc[S_CFL] = dt_used * mx;
     } else {
-        double nd = g.ph.MaxCFL / mx;              // +Inf for a resting fluid
-        if (nd > g.ph.dtMax) nd = g.ph.dtMax;
+        double nd = g.phd.MaxCFL / mx;              // +Inf for a resting fluid
+        if (nd > g.phd.dtMax) nd = g.phd.dtMax;
         sc[S_DT] = nd;
         sc[S_CFL] = nd * mx;
     }
@@ -106,7 +120,8 @@ __global__ void __launch_bounds__(256) finalize_kernel(Grid g, Fields f, int nbl
     sc[S_STEP] = step + 1;
 }
 
-void launch_post(const Ctx &cx, cudaStream_t s, int record_hist)
+template <class R>
+void launch_post(const Ctx<R> &cx, cudaStream_t s, int record_hist)
 {
     probe_begin(cx, K_POST, s);
     post_kernel<<<POST_BLOCKS, 256, 0, s>>>(cx.g, cx.f);
@@ -122,14 +137,16 @@ int post_partial_count() { return POST_BLOCKS * PT_N; }
 
 // Periodic ghost update of one padded field (module_mpi_subdomain.f90:758-791):
 // x faces first, then z faces including the x-ghost columns.
-__global__ void ghost_x_kernel(Grid g, double *a)
+template <class R>
+__global__ void ghost_x_kernel(GridT<R> g, R *a)
 {
     const int j = blockIdx.x * blockDim.x + threadIdx.x, k = blockIdx.y;
     if (j > g.N2 + 1) return;
     a[ix(g, 0, j, k)] = a[ix(g, g.N1, j, k)];
     a[ix(g, g.N1 + 1, j, k)] = a[ix(g, 1, j, k)];
 }
-__global__ void ghost_z_kernel(Grid g, double *a)
+template <class R>
+__global__ void ghost_z_kernel(GridT<R> g, R *a)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
     if (i > g.N1 + 1) return;
@@ -137,12 +154,49 @@ __global__ void ghost_z_kernel(Grid g, double *a)
     a[ix(g, i, j, g.N3 + 1)] = a[ix(g, i, j, 1)];
 }
 
-void launch_ghost(const Ctx &cx, double *a, cudaStream_t s)
+template <class R>
+void launch_ghost(const Ctx<R> &cx, R *a, cudaStream_t s)
 {
-    const Grid &g = cx.g;
+    const GridT<R> &g = cx.g;
     ghost_x_kernel<<<dim3((g.N2 + 2 + 127) / 128, g.N3 + 2), 128, 0, s>>>(g, a);
     ghost_z_kernel<<<dim3((g.N1 + 2 + 127) / 128, g.N2 + 2), 128, 0, s>>>(g, a);
     record_launch_error("ghost");
 }
+
+// Conversions between an FP32 field and an FP64 staging copy (the host API
+// moves FP64 arrays in both forms).
+template <class R>
+__global__ void convert_out_kernel(const R *src, double *dst, long long n)
+{
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) dst[t] = (double)src[t];
+}
+template <class R>
+__global__ void convert_in_kernel(const double *src, R *dst, long long n)
+{
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) dst[t] = (R)src[t];
+}
+
+template <class R>
+void launch_convert(const R *src, double *dst, long long n, cudaStream_t s)
+{
+    convert_out_kernel<R><<<4 * 148, 256, 0, s>>>(src, dst, n);
+    record_launch_error("convert_out");
+}
+template <class R>
+void launch_convert_in(const double *src, R *dst, long long n, cudaStream_t s)
+{
+    convert_in_kernel<R><<<4 * 148, 256, 0, s>>>(src, dst, n);
+    record_launch_error("convert_in");
+}
+
+// the two forms
+template void launch_post<double>(const Ctx<double> &, cudaStream_t, int);
+template void launch_post<float>(const Ctx<float> &, cudaStream_t, int);
+template void launch_ghost<double>(const Ctx<double> &, double *, cudaStream_t);
+template void launch_ghost<float>(const Ctx<float> &, float *, cudaStream_t);
+template void launch_convert<double>(const double *, double *, long long, cudaStream_t);
+template void launch_convert<float>(const float *, double *, long long, cudaStream_t);
+template void launch_convert_in<double>(const double *, double *, long long, cudaStream_t);
+template void launch_convert_in<float>(const double *, float *, long long, cudaStream_t);
 
 } // namespace tcs

@@ -14,139 +14,153 @@
 //   ifftx       c2r along x, /N1/N3, minus mean, periodic ghosts  S -> dP
 //   dp_wall     wall extrapolation of dP (:719-736)
 //   projection  U,V,W,P,dPhat,dP0 update (+ghosts, P walls)
+//
+// In the FP32-mixed form the FFTs run in FP32, while the right-hand side
+// (divergence and the dPhat correction), the modal solves, the mean, the
+// scaling, the wall extrapolations and the projection compute in FP64 from
+// the FP32 fields and round once when they store.
 #include "tcs_kernels.h"
 
 namespace tcs {
 
 #define IR(jj, kk) ld(f.iR2 + ix2(g, (jj), (kk)))
 
-__device__ __forceinline__ double2 cmul(double2 a, double2 b)
-{
-    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
-}
-__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
-__device__ __forceinline__ double2 cscale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
-// multiply by sign * i
-template <int SIGN>
-__device__ __forceinline__ double2 cmuli(double2 a) { return SIGN > 0 ? make_double2(-a.y, a.x) : make_double2(a.y, -a.x); }
+template <class C> struct CReal;
+template <> struct CReal<double2> { using T = double; };
+template <> struct CReal<float2> { using T = float; };
 
-// R-point DFTs y_q = sum_r v_r exp(SIGN 2 pi i r q / R), from the definition.
-template <int R, int SIGN> struct Bfly;
-template <int SIGN> struct Bfly<2, SIGN> {
-    __device__ static void run(double2 *v) { const double2 a = v[0], b = v[1]; v[0] = cadd(a, b); v[1] = csub(a, b); }
+template <class C> __device__ __forceinline__ C cmk(typename CReal<C>::T x, typename CReal<C>::T y) { C c; c.x = x; c.y = y; return c; }
+template <class C> __device__ __forceinline__ C cmul(C a, C b) { return cmk<C>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+template <class C> __device__ __forceinline__ C cadd(C a, C b) { return cmk<C>(a.x + b.x, a.y + b.y); }
+template <class C> __device__ __forceinline__ C csub(C a, C b) { return cmk<C>(a.x - b.x, a.y - b.y); }
+template <class C> __device__ __forceinline__ C cscale(C a, typename CReal<C>::T s) { return cmk<C>(a.x * s, a.y * s); }
+// multiply by sign * i
+template <int SIGN, class C>
+__device__ __forceinline__ C cmuli(C a) { return SIGN > 0 ? cmk<C>(-a.y, a.x) : cmk<C>(a.y, -a.x); }
+
+// RX-point DFTs y_q = sum_r v_r exp(SIGN 2 pi i r q / RX), from the definition.
+template <int RX, int SIGN, class C> struct Bfly;
+template <int SIGN, class C> struct Bfly<2, SIGN, C> {
+    __device__ static void run(C *v) { const C a = v[0], b = v[1]; v[0] = cadd(a, b); v[1] = csub(a, b); }
 };
-template <int SIGN> struct Bfly<4, SIGN> {
-    __device__ static void run(double2 *v)
+template <int SIGN, class C> struct Bfly<4, SIGN, C> {
+    __device__ static void run(C *v)
     {
-        const double2 a = cadd(v[0], v[2]), b = csub(v[0], v[2]), c = cadd(v[1], v[3]);
-        const double2 d = cmuli<SIGN>(csub(v[1], v[3]));
+        const C a = cadd(v[0], v[2]), b = csub(v[0], v[2]), c = cadd(v[1], v[3]);
+        const C d = cmuli<SIGN>(csub(v[1], v[3]));
         v[0] = cadd(a, c); v[2] = csub(a, c); v[1] = cadd(b, d); v[3] = csub(b, d);
     }
 };
-template <int SIGN> struct Bfly<3, SIGN> {
-    __device__ static void run(double2 *v)
+template <int SIGN, class C> struct Bfly<3, SIGN, C> {
+    __device__ static void run(C *v)
     {
-        const double S3 = 0.86602540378443864676;   // sin(2 pi / 3)
-        const double2 t1 = cadd(v[1], v[2]), t2 = csub(v[1], v[2]);
-        const double2 m = csub(v[0], cscale(t1, 0.5));
-        const double2 r = cmuli<SIGN>(cscale(t2, S3));
+        using T = typename CReal<C>::T;
+        const T S3 = T(0.86602540378443864676);   // sin(2 pi / 3)
+        const C t1 = cadd(v[1], v[2]), t2 = csub(v[1], v[2]);
+        const C m = csub(v[0], cscale(t1, T(0.5)));
+        const C r = cmuli<SIGN>(cscale(t2, S3));
         v[0] = cadd(v[0], t1); v[1] = cadd(m, r); v[2] = csub(m, r);
     }
 };
-template <int SIGN> struct Bfly<5, SIGN> {
-    __device__ static void run(double2 *v)
+template <int SIGN, class C> struct Bfly<5, SIGN, C> {
+    __device__ static void run(C *v)
     {
-        const double C1 = 0.30901699437494742410, C2 = -0.80901699437494742410;   // cos(2pi/5), cos(4pi/5)
-        const double S1 = 0.95105651629515357212, S2 = 0.58778525229247312917;    // sin(2pi/5), sin(4pi/5)
-        const double2 t1 = cadd(v[1], v[4]), t2 = cadd(v[2], v[3]), t3 = csub(v[1], v[4]), t4 = csub(v[2], v[3]);
-        const double2 a1 = cadd(v[0], cadd(cscale(t1, C1), cscale(t2, C2)));
-        const double2 a2 = cadd(v[0], cadd(cscale(t1, C2), cscale(t2, C1)));
-        const double2 b1 = cmuli<SIGN>(cadd(cscale(t3, S1), cscale(t4, S2)));
-        const double2 b2 = cmuli<SIGN>(csub(cscale(t3, S2), cscale(t4, S1)));
+        using T = typename CReal<C>::T;
+        const T C1 = T(0.30901699437494742410), C2 = T(-0.80901699437494742410);   // cos(2pi/5), cos(4pi/5)
+        const T S1 = T(0.95105651629515357212), S2 = T(0.58778525229247312917);    // sin(2pi/5), sin(4pi/5)
+        const C t1 = cadd(v[1], v[4]), t2 = cadd(v[2], v[3]), t3 = csub(v[1], v[4]), t4 = csub(v[2], v[3]);
+        const C a1 = cadd(v[0], cadd(cscale(t1, C1), cscale(t2, C2)));
+        const C a2 = cadd(v[0], cadd(cscale(t1, C2), cscale(t2, C1)));
+        const C b1 = cmuli<SIGN>(cadd(cscale(t3, S1), cscale(t4, S2)));
+        const C b2 = cmuli<SIGN>(csub(cscale(t3, S2), cscale(t4, S1)));
         v[0] = cadd(v[0], cadd(t1, t2));
         v[1] = cadd(a1, b1); v[4] = csub(a1, b1); v[2] = cadd(a2, b2); v[3] = csub(a2, b2);
     }
 };
 
-// One Stockham pass of radix R over nl lines (line stride ldl) in shared memory.
-template <int R, int SIGN>
-__device__ __forceinline__ void fft_pass(const double2 *src, double2 *dst, int nl, int ldl, int n, int Ns, const double2 *tw)
+// One Stockham pass of radix RX over nl lines (line stride ldl) in shared memory.
+template <int RX, int SIGN, class C>
+__device__ __forceinline__ void fft_pass(const C *src, C *dst, int nl, int ldl, int n, int Ns, const C *tw)
 {
-    const int nb = n / R, ts = n / (Ns * R);
+    const int nb = n / RX, ts = n / (Ns * RX);
     for (int t = threadIdx.x; t < nl * nb; t += blockDim.x) {
         const int l = t / nb, jb = t - l * nb;
-        const double2 *s = src + l * ldl;
-        double2 *d = dst + l * ldl;
+        const C *s = src + l * ldl;
+        C *d = dst + l * ldl;
         const int kk = jb % Ns;
-        double2 v[R];
+        C v[RX];
 #pragma unroll
-        for (int r = 0; r < R; r++) v[r] = s[jb + r * nb];
+        for (int r = 0; r < RX; r++) v[r] = s[jb + r * nb];
         if (kk) {
 #pragma unroll
-            for (int r = 1; r < R; r++) {
-                double2 w = __ldg(tw + r * kk * ts);
+            for (int r = 1; r < RX; r++) {
+                C w = __ldg(tw + r * kk * ts);
                 if (SIGN > 0) w.y = -w.y;
                 v[r] = cmul(v[r], w);
             }
         }
-        Bfly<R, SIGN>::run(v);
-        const int o = (jb / Ns) * Ns * R + kk;
+        Bfly<RX, SIGN, C>::run(v);
+        const int o = (jb / Ns) * Ns * RX + kk;
 #pragma unroll
-        for (int r = 0; r < R; r++) d[o + r * Ns] = v[r];
+        for (int r = 0; r < RX; r++) d[o + r * Ns] = v[r];
     }
 }
 
 // Unnormalised FFT of nl lines held in buf0; buf1 is scratch.  Returns the
 // buffer that holds the natural-order result.
-template <int SIGN>
-__device__ double2 *block_fft(double2 *buf0, double2 *buf1, int nl, int ldl, const FFTPlan &fp, const double2 *tw)
+template <int SIGN, class C>
+__device__ C *block_fft(C *buf0, C *buf1, int nl, int ldl, const FFTPlan &fp, const C *tw)
 {
-    double2 *src = buf0, *dst = buf1;
+    C *src = buf0, *dst = buf1;
     int Ns = 1;
     for (int ps = 0; ps < fp.npass; ps++) {
-        const int R = fp.radix[ps];
-        switch (R) {
+        const int RX = fp.radix[ps];
+        switch (RX) {
         case 2: fft_pass<2, SIGN>(src, dst, nl, ldl, fp.n, Ns, tw); break;
         case 3: fft_pass<3, SIGN>(src, dst, nl, ldl, fp.n, Ns, tw); break;
         case 4: fft_pass<4, SIGN>(src, dst, nl, ldl, fp.n, Ns, tw); break;
         default: fft_pass<5, SIGN>(src, dst, nl, ldl, fp.n, Ns, tw); break;
         }
         __syncthreads();
-        double2 *t = src; src = dst; dst = t;
-        Ns *= R;
+        C *t = src; src = dst; dst = t;
+        Ns *= RX;
     }
     return src;
 }
 
-__device__ __forceinline__ long long sidx(const Grid &g, int h1p, int kx, int j, int kz)
+template <class R>
+__device__ __forceinline__ long long sidx(const GridT<R> &g, int h1p, int kx, int j, int kz)
 {
     return (long long)kx + (long long)h1p * ((long long)(j - 1) + (long long)g.N2 * (long long)kz);
 }
 
 // ---------------------------------------------------------------------------
 // pseudo-update (:178-208) + ghost(U,V,W) + mpi_pressure_RHS (:182-229) +
-// forward r2c FFT along x.  Block: NL lines (j..j+NL-1, k).
+// forward r2c FFT along x.  Block: NL lines (j..j+NL-1, k).  The updated
+// velocities are formed in the field type (they are what is stored); the
+// right-hand side is evaluated in FP64 from them.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) prhs_fftx_kernel(Grid g, Fields f, FFTPlan fp, int NL, int h1p, int with_pseudo)
+template <class R>
+__global__ void __launch_bounds__(256) prhs_fftx_kernel(GridT<R> g, FieldsT<R> f, FFTPlan fp, int NL, int h1p, int with_pseudo)
 {
-    extern __shared__ double2 smz[];
+    using C = cplx_t<R>;
+    extern __shared__ __align__(16) unsigned char smraw[];
     if (blown(g)) return;
     const int N1 = g.N1, j0 = 1 + blockIdx.x * NL, k = 1 + blockIdx.y;
-    double2 *b0 = smz, *b1 = smz + NL * N1;
-    double *su = (double *)(b1 + NL * N1);       // NL x N1 new U along the line
-    const double *dx1 = g.m1.dx, *dx2 = g.m2.dx, *dx3 = g.m3.dx;
-    const double *rdx1 = g.m1.rdx, *rdx2 = g.m2.rdx, *rdx3 = g.m3.rdx;
-    const double *rdmx1 = g.m1.rdmx, *rdmx2 = g.m2.rdmx, *rdmx3 = g.m3.rdmx;
+    C *b0 = reinterpret_cast<C *>(smraw), *b1 = b0 + NL * N1;
+    R *su = reinterpret_cast<R *>(b1 + NL * N1);       // NL x N1 new U along the line
+    const double *dx1 = g.d1.dx, *dx2 = g.d2.dx, *dx3 = g.d3.dx;
+    const double *rdx1 = g.d1.rdx, *rdx2 = g.d2.rdx, *rdx3 = g.d3.rdx;
+    const double *rdmx1 = g.d1.rdmx, *rdmx2 = g.d2.rdmx, *rdmx3 = g.d3.rdmx;
     const long long sj = g.P1, sk = (long long)g.P1 * g.P2;
     for (int t = threadIdx.x; t < NL * N1; t += blockDim.x) {
         const int l = t / N1, i = t - l * N1 + 1, j = j0 + l;
         if (j > g.N2) continue;
         const long long c = ix(g, i, j, k);
-        double un;
+        R un;
         if (with_pseudo) {
             un = f.U[c] + f.dU[c];
-            const double vmask = (j == 1) ? 0.0 : 1.0;
+            const R vmask = (j == 1) ? R(0) : R(1);
             store_periodic(g, f.Un, i, j, k, un);
             store_periodic(g, f.Vn, i, j, k, f.V[c] + f.dV[c] * vmask);
             store_periodic(g, f.Wn, i, j, k, f.W[c] + f.dW[c]);
@@ -157,45 +171,45 @@ __global__ void __launch_bounds__(256) prhs_fftx_kernel(Grid g, Fields f, FFTPla
     }
     __syncthreads();
     const double dt = g.scal[S_DT], rdt = 1.0 / dt;
-    const Phys &p = g.ph;
+    const Phys &p = g.phd;
     for (int t = threadIdx.x; t < NL * N1; t += blockDim.x) {
         const int l = t / N1, i = t - l * N1 + 1, j = j0 + l;
-        if (j > g.N2) { b0[t] = make_double2(0.0, 0.0); continue; }
+        if (j > g.N2) { b0[t] = mkc<R>(R(0), R(0)); continue; }
         const int im = i - 1, ip = i + 1, jm = j - 1, jp = j + 1, km = k - 1, kp = k + 1;
         const long long c = ix(g, i, j, k);
         const double jvm = (j == 1) ? 0.0 : 1.0, jvp = (j == g.N2) ? 0.0 : 1.0;
         const double Uc = su[l * N1 + (i - 1)], Uxp = su[l * N1 + (i == N1 ? 0 : i)];
-        double Vc, Vyp, Wc, Wzp;
+        R Vc, Vyp, Wc, Wzp;
         const long long ckp = (k == g.N3) ? ix(g, i, j, 1) : c + sk;
         if (with_pseudo) {
-            Vc = f.V[c] + f.dV[c] * jvm;
+            Vc = f.V[c] + f.dV[c] * R(jvm);
             Vyp = (j < g.N2) ? f.V[c + sj] + f.dV[c + sj] : f.V[c + sj];
             Wc = f.W[c] + f.dW[c];
             Wzp = f.W[ckp] + f.dW[ckp];
         } else {
             Vc = f.V[c]; Vyp = f.V[c + sj]; Wc = f.W[c]; Wzp = f.W[ckp];
         }
-        const double DivUm = (Uxp - Uc) * rdx1[i] + (jvp * Vyp - jvm * Vc) * rdx2[j] + (Wzp - Wc) * rdx3[k];
+        const double DivUm = (Uxp - Uc) * rdx1[i] + (jvp * (double)Vyp - jvm * (double)Vc) * rdx2[j] + ((double)Wzp - (double)Wc) * rdx3[k];
         const double cbc = (1.0 - jvm) * p.Vbt * rdx2[j] - (1.0 - jvp) * p.Vup * rdx2[j];
-        const double *dPh = f.dPhat;
+        const R *dPh = f.dPhat;
         const double Pc = ld(dPh + c);
-        const double ddpdx1 = (Pc - ld(dPh + c - 1)) * rdmx1[i], ddpdx2 = (ld(dPh + c + 1) - Pc) * rdmx1[ip];
-        const double ddpdy3 = (Pc - ld(dPh + c - sj)) * rdmx2[j], ddpdy4 = (ld(dPh + c + sj) - Pc) * rdmx2[jp];
-        const double ddpdz5 = (Pc - ld(dPh + c - sk)) * rdmx3[k], ddpdz6 = (ld(dPh + c + sk) - Pc) * rdmx3[kp];
+        const double ddpdx1 = (Pc - (double)ld(dPh + c - 1)) * rdmx1[i], ddpdx2 = ((double)ld(dPh + c + 1) - Pc) * rdmx1[ip];
+        const double ddpdy3 = (Pc - (double)ld(dPh + c - sj)) * rdmx2[j], ddpdy4 = ((double)ld(dPh + c + sj) - Pc) * rdmx2[jp];
+        const double ddpdz5 = (Pc - (double)ld(dPh + c - sk)) * rdmx3[k], ddpdz6 = ((double)ld(dPh + c + sk) - Pc) * rdmx3[kp];
         const double iRjk = IR(j, k);
         const double iR1 = 0.5 * rdmx1[i] * (dx1[im] * iRjk + dx1[i] * iRjk);
         const double iR2_ = 0.5 * rdmx1[ip] * (dx1[ip] * iRjk + dx1[i] * iRjk);
-        const double iR3 = 0.5 * rdmx2[j] * (dx2[jm] * iRjk + dx2[j] * IR(jm, k));
-        const double iR4 = 0.5 * rdmx2[jp] * (dx2[jp] * iRjk + dx2[j] * IR(jp, k));
-        const double iR5 = 0.5 * rdmx3[k] * (dx3[km] * iRjk + dx3[k] * IR(j, km));
-        const double iR6 = 0.5 * rdmx3[kp] * (dx3[kp] * iRjk + dx3[k] * IR(j, kp));
+        const double iR3 = 0.5 * rdmx2[j] * (dx2[jm] * iRjk + dx2[j] * (double)IR(jm, k));
+        const double iR4 = 0.5 * rdmx2[jp] * (dx2[jp] * iRjk + dx2[j] * (double)IR(jp, k));
+        const double iR5 = 0.5 * rdmx3[k] * (dx3[km] * iRjk + dx3[k] * (double)IR(j, km));
+        const double iR6 = 0.5 * rdmx3[kp] * (dx3[kp] * iRjk + dx3[k] * (double)IR(j, kp));
         const double Extra = ((1.0 - iR2_) * ddpdx2 - (1.0 - iR1) * ddpdx1) * rdx1[i]
                            + ((1.0 - iR4) * ddpdy4 - (1.0 - iR3) * ddpdy3) * rdx2[j]
                            + ((1.0 - iR6) * ddpdz6 - (1.0 - iR5) * ddpdz5) * rdx3[k];
-        b0[t] = make_double2((DivUm - cbc) * rdt / p.Cmp + Extra, 0.0);
+        b0[t] = mkc<R>(R((DivUm - cbc) * rdt / p.Cmp + Extra), R(0));
     }
     __syncthreads();
-    const double2 *res = block_fft<-1>(b0, b1, NL, N1, fp, f.tw1);
+    const C *res = block_fft<-1>(b0, b1, NL, N1, fp, f.tw1);
     for (int t = threadIdx.x; t < NL * h1p; t += blockDim.x) {
         const int l = t / h1p, kx = t - l * h1p, j = j0 + l;
         if (j > g.N2) continue;
@@ -204,20 +218,21 @@ __global__ void __launch_bounds__(256) prhs_fftx_kernel(Grid g, Fields f, FFTPla
 }
 
 // c2c along z for NL consecutive kx at fixed j.
-template <int SIGN>
-__global__ void __launch_bounds__(256) fftz_kernel(Grid g, Fields f, FFTPlan fp, int NL, int h1p)
+template <int SIGN, class R>
+__global__ void __launch_bounds__(256) fftz_kernel(GridT<R> g, FieldsT<R> f, FFTPlan fp, int NL, int h1p)
 {
-    extern __shared__ double2 smz[];
+    using C = cplx_t<R>;
+    extern __shared__ __align__(16) unsigned char smraw[];
     if (blown(g)) return;
     const int N3 = g.N3, kx0 = blockIdx.x * NL, j = 1 + blockIdx.y;
     const int nl = min(NL, h1p - kx0);
-    double2 *b0 = smz, *b1 = smz + NL * N3;
+    C *b0 = reinterpret_cast<C *>(smraw), *b1 = b0 + NL * N3;
     for (int t = threadIdx.x; t < nl * N3; t += blockDim.x) {
         const int kz = t / nl, l = t - kz * nl;
         b0[l * N3 + kz] = f.S[sidx(g, h1p, kx0 + l, j, kz)];
     }
     __syncthreads();
-    const double2 *res = block_fft<SIGN>(b0, b1, nl, N3, fp, f.tw3);
+    const C *res = block_fft<SIGN>(b0, b1, nl, N3, fp, f.tw3);
     for (int t = threadIdx.x; t < nl * N3; t += blockDim.x) {
         const int kz = t / nl, l = t - kz * nl;
         f.S[sidx(g, h1p, kx0 + l, j, kz)] = res[l * N3 + kz];
@@ -226,22 +241,26 @@ __global__ void __launch_bounds__(256) fftz_kernel(Grid g, Fields f, FFTPlan fp,
 
 // Modal y solves (:597-652): one tridiagonal system per (kx, kz), real and
 // imaginary parts share the matrix.  Mode (0,0) is pinned at j=1; the
-// imaginary parts of (0,0) and (0,N3/2) are zeroed after the solve.
+// imaginary parts of (0,0) and (0,N3/2) are zeroed after the solve.  The
+// rows are FP64 in both forms: the zero and lowest wavenumbers are nearly
+// singular, and the FP32 form reads and writes its FP32 spectrum around them.
+template <class R>
 struct Modal {
+    using Real = double;
     static constexpr int NRHS = 2;
     static constexpr bool CONTIG = false;
-    Grid g; Fields f; int TL; int h1p;
+    GridT<R> g; FieldsT<R> f; int TL; int h1p;
     __device__ bool skip() const { return blown(g); }
     struct State { double dt; };
     __device__ State prepare() const { return State{g.scal[S_DT]}; }
     __device__ int lk(int l) const { return blockIdx.x * TL + l; }
     __device__ bool line_ok(int l) const { return lk(l) < h1p; }
-    __device__ Coef<2> build(int l, int r, const State &st) const
+    __device__ Coef<double, 2> build(int l, int r, const State &st) const
     {
         const int kx = lk(l), kz = blockIdx.y, j = r + 1;
         const double am = f.fam[j], ap = f.fap[j];
-        Coef<2> cf;
-        const double2 s = f.S[sidx(g, h1p, kx, j, kz)];
+        Coef<double, 2> cf;
+        const cplx_t<R> s = f.S[sidx(g, h1p, kx, j, kz)];
         if (kx == 0 && kz == 0 && j == 1) {
             cf.a = 0.0; cf.b = 1.0; cf.c = 0.0; cf.d[0] = 0.0; cf.d[1] = s.y;
         } else {
@@ -255,18 +274,19 @@ struct Modal {
     {
         const int kx = lk(l), kz = blockIdx.y, j = r + 1;
         const bool zi = (kx == 0) && (kz == 0 || kz == g.N3 / 2);
-        f.S[sidx(g, h1p, kx, j, kz)] = make_double2(x[0], zi ? 0.0 : x[1]);
+        f.S[sidx(g, h1p, kx, j, kz)] = mkc<R>(R(x[0]), zi ? R(0) : R(x[1]));
     }
 };
 
 // Unweighted mean of the solution (:703-710): the (i,k) sum of the inverse
 // transform of one j-plane is the real part of its (0,0) coefficient.
-__global__ void mean_kernel(Grid g, Fields f, int h1p)
+template <class R>
+__global__ void mean_kernel(GridT<R> g, FieldsT<R> f, int h1p)
 {
     __shared__ double red[256];
     if (blown(g)) return;
     double s = 0.0;
-    for (int j = 1 + threadIdx.x; j <= g.N2; j += blockDim.x) s += f.S[sidx(g, h1p, 0, j, 0)].x;
+    for (int j = 1 + threadIdx.x; j <= g.N2; j += blockDim.x) s += (double)f.S[sidx(g, h1p, 0, j, 0)].x;
     red[threadIdx.x] = s;
     __syncthreads();
     for (int w = blockDim.x / 2; w > 0; w >>= 1) {
@@ -278,174 +298,194 @@ __global__ void mean_kernel(Grid g, Fields f, int h1p)
 
 // c2r along x (:681-683) with the scaling (:694-700), the mean removal
 // (:712-714) and the periodic ghosts of ghost(dP) (main.f90:189).
-__global__ void __launch_bounds__(256) ifftx_kernel(Grid g, Fields f, FFTPlan fp, int NL, int h1p)
+template <class R>
+__global__ void __launch_bounds__(256) ifftx_kernel(GridT<R> g, FieldsT<R> f, FFTPlan fp, int NL, int h1p)
 {
-    extern __shared__ double2 smz[];
+    using C = cplx_t<R>;
+    extern __shared__ __align__(16) unsigned char smraw[];
     if (blown(g)) return;
     const int N1 = g.N1, j0 = 1 + blockIdx.x * NL, k = 1 + blockIdx.y;
-    double2 *b0 = smz, *b1 = smz + NL * N1;
+    C *b0 = reinterpret_cast<C *>(smraw), *b1 = b0 + NL * N1;
     for (int t = threadIdx.x; t < NL * N1; t += blockDim.x) {
         const int l = t / N1, kx = t - l * N1, j = j0 + l;
-        double2 v = make_double2(0.0, 0.0);
+        C v = mkc<R>(R(0), R(0));
         if (j <= g.N2) {
             if (kx < h1p) {
                 v = f.S[sidx(g, h1p, kx, j, k - 1)];
-                if (kx == 0 || 2 * kx == N1) v.y = 0.0;   // c2r ignores these imaginary parts
+                if (kx == 0 || 2 * kx == N1) v.y = R(0);   // c2r ignores these imaginary parts
             } else {
-                const double2 w = f.S[sidx(g, h1p, N1 - kx, j, k - 1)];
-                v = make_double2(w.x, -w.y);
+                const C w = f.S[sidx(g, h1p, N1 - kx, j, k - 1)];
+                v = mkc<R>(w.x, -w.y);
             }
         }
         b0[t] = v;
     }
     __syncthreads();
-    const double2 *res = block_fft<1>(b0, b1, NL, N1, fp, f.tw1);
+    const C *res = block_fft<1>(b0, b1, NL, N1, fp, f.tw1);
     const double aver = g.scal[S_AVER];
     for (int t = threadIdx.x; t < NL * N1; t += blockDim.x) {
         const int l = t / N1, i = t - l * N1 + 1, j = j0 + l;
         if (j > g.N2) continue;
-        const double v = res[t].x / (double)N1 / (double)g.N3 - aver;
-        store_periodic(g, f.dP, i, j, k, v);
+        const double v = (double)res[t].x / (double)N1 / (double)g.N3 - aver;
+        store_periodic(g, f.dP, i, j, k, R(v));
     }
 }
 
 // dP wall extrapolation (:719-736) on every (i,k) including ghost columns,
 // which is what the extrapolation followed by ghost(dP) produces.
-__global__ void dp_wall_kernel(Grid g, Fields f, double ab, double bb, double at, double bt)
+template <class R>
+__global__ void dp_wall_kernel(GridT<R> g, FieldsT<R> f, double ab, double bb, double at, double bt)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x, k = blockIdx.y;
     if (i > g.N1 + 1 || blown(g)) return;
-    double *dP = f.dP;
-    dP[ix(g, i, 0, k)] = ab * dP[ix(g, i, 1, k)] - bb * dP[ix(g, i, 2, k)];
-    dP[ix(g, i, g.N2 + 1, k)] = at * dP[ix(g, i, g.N2, k)] - bt * dP[ix(g, i, g.N2 - 1, k)];
+    R *dP = f.dP;
+    dP[ix(g, i, 0, k)] = R(ab * (double)dP[ix(g, i, 1, k)] - bb * (double)dP[ix(g, i, 2, k)]);
+    dP[ix(g, i, g.N2 + 1, k)] = R(at * (double)dP[ix(g, i, g.N2, k)] - bt * (double)dP[ix(g, i, g.N2 - 1, k)]);
 }
 
 // ---------------------------------------------------------------------------
 // mpi_pressure_Projection (:756-874) + ghost(U,V,W,P,dPhat), one thread per
-// cell.  The reference sweeps k, then j = 2..N2, then j = 1, with i
-// innermost, updating dPhat in place, so the pressure-correction term of a
-// cell reads the NEW dPhat of its x-lower neighbour (i >= 2), of its y-lower
-// neighbour (j >= 3) and of its z-lower neighbour (k >= 2), and the old value
-// otherwise.  New values are recomputed from the old ones with the same
-// arithmetic (dP0n = (dPhat + dP0)/2, dPhatn = 2 dP - dP0n) and written to
-// the second buffers.  The P wall rows (:853-869) follow in p_wall_kernel.
+// cell, in FP64 arithmetic in both forms.  The reference sweeps k, then
+// j = 2..N2, then j = 1, with i innermost, updating dPhat in place, so the
+// pressure-correction term of a cell reads the NEW dPhat of its x-lower
+// neighbour (i >= 2), of its y-lower neighbour (j >= 3) and of its z-lower
+// neighbour (k >= 2), and the old value otherwise.  New values are
+// recomputed from the old ones with the same arithmetic
+// (dP0n = (dPhat + dP0)/2, dPhatn = 2 dP - dP0n) and written to the second
+// buffers.  The P wall rows (:853-869) follow in p_wall_kernel.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ double new_phat(const Fields &f, long long n)
+template <class R>
+__device__ __forceinline__ double new_phat(const FieldsT<R> &f, long long n)
 {
-    const double dp0n = (ld(f.dPhat + n) + ld(f.dP0 + n)) / 2.0;
-    return 2.0 * ld(f.dP + n) - dp0n;
+    // the FP32 form rounds dP0n to the stored type first, as the neighbour itself does
+    const R dp0n = R(((double)ld(f.dPhat + n) + (double)ld(f.dP0 + n)) / 2.0);
+    return (double)R(2.0 * (double)ld(f.dP + n) - (double)dp0n);
 }
 
-__global__ void __launch_bounds__(256) projection_kernel(Grid g, Fields f)
+template <class R>
+__global__ void __launch_bounds__(256) projection_kernel(GridT<R> g, FieldsT<R> f)
 {
     const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x, j = 1 + blockIdx.y, k = 1 + blockIdx.z;
     if (i > g.N1 || blown(g)) return;
     const int im = i - 1, jm = j - 1, km = k - 1;
-    const double *dx1 = g.m1.dx, *dx2 = g.m2.dx, *dx3 = g.m3.dx;
-    const double *rdmx1 = g.m1.rdmx, *rdmx2 = g.m2.rdmx, *rdmx3 = g.m3.rdmx;
+    const double *dx1 = g.d1.dx, *dx2 = g.d2.dx, *dx3 = g.d3.dx;
+    const double *rdmx1 = g.d1.rdmx, *rdmx2 = g.d2.rdmx, *rdmx3 = g.d3.rdmx;
     const long long c = ix(g, i, j, k), sj = g.P1, sk = (long long)g.P1 * g.P2;
-    const double dtc = g.scal[S_DT] * g.ph.Cmp;
+    const double dtc = g.scal[S_DT] * g.phd.Cmp;
     const double dPc = ld(f.dP + c), ph = ld(f.dPhat + c), p0 = ld(f.dP0 + c);
-    const double dp0n = (ph + p0) / 2.0;
-    const double phn = 2.0 * dPc - dp0n;
+    const R dp0n = R((ph + p0) / 2.0);
+    const R phn = R(2.0 * dPc - (double)dp0n);
     const double iRjk = IR(j, k);
-    const double Xim = (i >= 2) ? new_phat(f, c - 1) : ld(f.dPhat + c - 1);
+    const double Xim = (i >= 2) ? new_phat(f, c - 1) : (double)ld(f.dPhat + c - 1);
     double invRhoc = 0.5 * rdmx1[i] * (dx1[i] * iRjk + dx1[im] * iRjk);
-    const double un = f.U[c] - dtc * ((dPc - ld(f.dP + c - 1)) * rdmx1[i] + (invRhoc - 1.0) * (ph - Xim) * rdmx1[i]);
+    const double un = (double)f.U[c] - dtc * ((dPc - (double)ld(f.dP + c - 1)) * rdmx1[i] + (invRhoc - 1.0) * (ph - Xim) * rdmx1[i]);
     double vn = f.V[c];
     if (j >= 2) {   // the lower wall plane keeps V: dble(2 - j_indexS) = 0
-        const double Xjm = (j >= 3) ? new_phat(f, c - sj) : ld(f.dPhat + c - sj);
-        invRhoc = 0.5 * rdmx2[j] * (dx2[j] * IR(jm, k) + dx2[jm] * iRjk);
-        vn = vn - dtc * ((dPc - ld(f.dP + c - sj)) * rdmx2[j] + (invRhoc - 1.0) * (ph - Xjm) * rdmx2[j]);
+        const double Xjm = (j >= 3) ? new_phat(f, c - sj) : (double)ld(f.dPhat + c - sj);
+        invRhoc = 0.5 * rdmx2[j] * (dx2[j] * (double)IR(jm, k) + dx2[jm] * iRjk);
+        vn = vn - dtc * ((dPc - (double)ld(f.dP + c - sj)) * rdmx2[j] + (invRhoc - 1.0) * (ph - Xjm) * rdmx2[j]);
     }
-    const double Xkm = (k >= 2) ? new_phat(f, c - sk) : ld(f.dPhat + c - sk);
-    invRhoc = 0.5 * rdmx3[k] * (dx3[k] * IR(j, km) + dx3[km] * iRjk);
-    const double wn = f.W[c] - dtc * ((dPc - ld(f.dP + c - sk)) * rdmx3[k] + (invRhoc - 1.0) * (ph - Xkm) * rdmx3[k]);
-    store_periodic(g, f.U, i, j, k, un);
-    store_periodic(g, f.V, i, j, k, vn);
-    store_periodic(g, f.W, i, j, k, wn);
-    store_periodic(g, f.P, i, j, k, f.P[c] + dPc);
+    const double Xkm = (k >= 2) ? new_phat(f, c - sk) : (double)ld(f.dPhat + c - sk);
+    invRhoc = 0.5 * rdmx3[k] * (dx3[k] * (double)IR(j, km) + dx3[km] * iRjk);
+    const double wn = (double)f.W[c] - dtc * ((dPc - (double)ld(f.dP + c - sk)) * rdmx3[k] + (invRhoc - 1.0) * (ph - Xkm) * rdmx3[k]);
+    store_periodic(g, f.U, i, j, k, R(un));
+    store_periodic(g, f.V, i, j, k, R(vn));
+    store_periodic(g, f.W, i, j, k, R(wn));
+    store_periodic(g, f.P, i, j, k, R((double)f.P[c] + dPc));
     store_periodic(g, f.dPhatn, i, j, k, phn);
     f.dP0n[c] = dp0n;
 }
 
 // P(i,0,k) = Pbc_a P(i,1,k) - Pbc_b P(i,2,k) and the top-wall counterpart
 // (:853-869), then ghost(P).
-__global__ void p_wall_kernel(Grid g, Fields f, double ab, double bb, double at, double bt)
+template <class R>
+__global__ void p_wall_kernel(GridT<R> g, FieldsT<R> f, double ab, double bb, double at, double bt)
 {
     const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x, k = 1 + blockIdx.y;
     if (i > g.N1 || blown(g)) return;
-    const double *P = f.P;
-    store_periodic(g, f.P, i, 0, k, ab * P[ix(g, i, 1, k)] - bb * P[ix(g, i, 2, k)]);
-    store_periodic(g, f.P, i, g.N2 + 1, k, at * P[ix(g, i, g.N2, k)] - bt * P[ix(g, i, g.N2 - 1, k)]);
+    const R *P = f.P;
+    store_periodic(g, f.P, i, 0, k, R(ab * (double)P[ix(g, i, 1, k)] - bb * (double)P[ix(g, i, 2, k)]));
+    store_periodic(g, f.P, i, g.N2 + 1, k, R(at * (double)P[ix(g, i, g.N2, k)] - bt * (double)P[ix(g, i, g.N2 - 1, k)]));
 }
 
-static size_t fftx_smem(const Ctx &cx) { return (size_t)cx.fft_lines_x * cx.g.N1 * (2 * sizeof(double2) + sizeof(double)); }
+template <class R>
+static size_t fftx_smem(const Ctx<R> &cx) { return (size_t)cx.fft_lines_x * cx.g.N1 * (2 * sizeof(cplx_t<R>) + sizeof(R)); }
 
-void launch_pseudo_prhs_fftx(const Ctx &cx, cudaStream_t s, bool with_pseudo)
+template <class R>
+void launch_pseudo_prhs_fftx(const Ctx<R> &cx, cudaStream_t s, bool with_pseudo)
 {
-    const Grid &g = cx.g;
+    const GridT<R> &g = cx.g;
     const int NL = cx.fft_lines_x;
     const size_t sm = fftx_smem(cx);
     static size_t conf = 0;
-    if (sm > conf) { cudaFuncSetAttribute(prhs_fftx_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm); conf = sm; }
+    if (sm > conf) { cudaFuncSetAttribute(prhs_fftx_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm); conf = sm; }
     probe_begin(cx, K_PRHS_FFTX, s);
-    prhs_fftx_kernel<<<dim3((g.N2 + NL - 1) / NL, g.N3), 256, sm, s>>>(g, cx.f, cx.fp1, NL, cx.h1p, with_pseudo ? 1 : 0);
+    prhs_fftx_kernel<R><<<dim3((g.N2 + NL - 1) / NL, g.N3), 256, sm, s>>>(g, cx.f, cx.fp1, NL, cx.h1p, with_pseudo ? 1 : 0);
     probe_end(cx, K_PRHS_FFTX, s);
     record_launch_error("prhs_fftx");
 }
 
-void launch_poisson_rest(const Ctx &cx, cudaStream_t s)
+template <class R>
+void launch_poisson_rest(const Ctx<R> &cx, cudaStream_t s)
 {
-    const Grid &g = cx.g;
+    const GridT<R> &g = cx.g;
     const int h1p = cx.h1p, NLz = cx.fft_lines_z, NLx = cx.fft_lines_x;
-    const size_t smz = (size_t)NLz * g.N3 * 2 * sizeof(double2);
-    const size_t smx = (size_t)NLx * g.N1 * 2 * sizeof(double2);
+    const size_t smz = (size_t)NLz * g.N3 * 2 * sizeof(cplx_t<R>);
+    const size_t smx = (size_t)NLx * g.N1 * 2 * sizeof(cplx_t<R>);
     static size_t cz = 0, cx2 = 0;
     if (smz > cz) {
-        cudaFuncSetAttribute(fftz_kernel<-1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smz);
-        cudaFuncSetAttribute(fftz_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smz);
+        cudaFuncSetAttribute(fftz_kernel<-1, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smz);
+        cudaFuncSetAttribute(fftz_kernel<1, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smz);
         cz = smz;
     }
-    if (smx > cx2) { cudaFuncSetAttribute(ifftx_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx); cx2 = smx; }
+    if (smx > cx2) { cudaFuncSetAttribute(ifftx_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx); cx2 = smx; }
     const dim3 gz((h1p + NLz - 1) / NLz, g.N2);
     probe_begin(cx, K_FFTZ_FWD, s);
-    fftz_kernel<-1><<<gz, 256, smz, s>>>(g, cx.f, cx.fp3, NLz, h1p);
+    fftz_kernel<-1, R><<<gz, 256, smz, s>>>(g, cx.f, cx.fp3, NLz, h1p);
     probe_end(cx, K_FFTZ_FWD, s);
     record_launch_error("fftz_fwd");
     LinePlan pm = make_line_plan(g.N2, false, cx.tl_modal);
-    launch_lines(Modal{g, cx.f, pm.TL, h1p}, pm, dim3((h1p + pm.TL - 1) / pm.TL, g.N3), s, K_MODAL, cx);
+    launch_lines(Modal<R>{g, cx.f, pm.TL, h1p}, pm, dim3((h1p + pm.TL - 1) / pm.TL, g.N3), s, K_MODAL, cx);
     probe_begin(cx, K_MEAN, s);
-    mean_kernel<<<1, 256, 0, s>>>(g, cx.f, h1p);
+    mean_kernel<R><<<1, 256, 0, s>>>(g, cx.f, h1p);
     probe_end(cx, K_MEAN, s);
     record_launch_error("mean");
     probe_begin(cx, K_FFTZ_INV, s);
-    fftz_kernel<1><<<gz, 256, smz, s>>>(g, cx.f, cx.fp3, NLz, h1p);
+    fftz_kernel<1, R><<<gz, 256, smz, s>>>(g, cx.f, cx.fp3, NLz, h1p);
     probe_end(cx, K_FFTZ_INV, s);
     record_launch_error("fftz_inv");
     probe_begin(cx, K_IFFTX, s);
-    ifftx_kernel<<<dim3((g.N2 + NLx - 1) / NLx, g.N3), 256, smx, s>>>(g, cx.f, cx.fp1, NLx, h1p);
+    ifftx_kernel<R><<<dim3((g.N2 + NLx - 1) / NLx, g.N3), 256, smx, s>>>(g, cx.f, cx.fp1, NLx, h1p);
     probe_end(cx, K_IFFTX, s);
     record_launch_error("ifftx");
     probe_begin(cx, K_DP_WALL, s);
-    dp_wall_kernel<<<dim3((g.N1 + 2 + 127) / 128, g.N3 + 2), 128, 0, s>>>(g, cx.f, cx.wall_ab, cx.wall_bb, cx.wall_at, cx.wall_bt);
+    dp_wall_kernel<R><<<dim3((g.N1 + 2 + 127) / 128, g.N3 + 2), 128, 0, s>>>(g, cx.f, cx.wall_ab, cx.wall_bb, cx.wall_at, cx.wall_bt);
     probe_end(cx, K_DP_WALL, s);
     record_launch_error("dp_wall");
 }
 
-void launch_projection(const Ctx &cx, cudaStream_t s)
+template <class R>
+void launch_projection(const Ctx<R> &cx, cudaStream_t s)
 {
-    const Grid &g = cx.g;
+    const GridT<R> &g = cx.g;
     probe_begin(cx, K_PROJECT, s);
-    projection_kernel<<<dim3((g.N1 + 255) / 256, g.N2, g.N3), 256, 0, s>>>(g, cx.f);
+    projection_kernel<R><<<dim3((g.N1 + 255) / 256, g.N2, g.N3), 256, 0, s>>>(g, cx.f);
     probe_end(cx, K_PROJECT, s);
     record_launch_error("projection");
     probe_begin(cx, K_P_WALL, s);
-    p_wall_kernel<<<dim3((g.N1 + 127) / 128, g.N3), 128, 0, s>>>(g, cx.f, cx.wall_ab, cx.wall_bb, cx.wall_at, cx.wall_bt);
+    p_wall_kernel<R><<<dim3((g.N1 + 127) / 128, g.N3), 128, 0, s>>>(g, cx.f, cx.wall_ab, cx.wall_bb, cx.wall_at, cx.wall_bt);
     probe_end(cx, K_P_WALL, s);
     record_launch_error("p_wall");
 }
 
 #undef IR
+
+// the two forms
+template void launch_pseudo_prhs_fftx<double>(const Ctx<double> &, cudaStream_t, bool);
+template void launch_pseudo_prhs_fftx<float>(const Ctx<float> &, cudaStream_t, bool);
+template void launch_poisson_rest<double>(const Ctx<double> &, cudaStream_t);
+template void launch_poisson_rest<float>(const Ctx<float> &, cudaStream_t);
+template void launch_projection<double>(const Ctx<double> &, cudaStream_t);
+template void launch_projection<float>(const Ctx<float> &, cudaStream_t);
 
 } // namespace tcs

@@ -13,213 +13,224 @@
 
 namespace tcs {
 
+template <class R>
 struct ThermalZ {
+    using Real = R;
     static constexpr int NRHS = 1;
     static constexpr bool CONTIG = false;
-    Grid g; Fields f; int TL;
+    GridT<R> g; FieldsT<R> f; int TL;
     __device__ bool skip() const { return blown(g); }
-    struct State { double dt; };
-    __device__ State prepare() const { return State{g.scal[S_DT]}; }
+    struct State { R dt; };
+    __device__ State prepare() const { return State{R(g.scal[S_DT])}; }
     __device__ int li(int l) const { return 1 + blockIdx.x * TL + l; }
     __device__ bool line_ok(int l) const { return li(l) <= g.N1; }
-    __device__ Coef<1> build(int l, int r, const State &st) const
+    __device__ Coef<R, 1> build(int l, int r, const State &st) const
     {
         const int i = li(l), j = 1 + blockIdx.y, k = r + 1;
         const int im = i - 1, ip = i + 1, jm = j - 1, jp = j + 1, km = k - 1, kp = k + 1;
-        const Phys &p = g.ph;
-        const double *dx1 = g.m1.dx, *dx2 = g.m2.dx, *dx3 = g.m3.dx;
-        const double *rdx1 = g.m1.rdx, *rdx2 = g.m2.rdx, *rdx3 = g.m3.rdx;
-        const double *rdmx1 = g.m1.rdmx, *rdmx2 = g.m2.rdmx, *rdmx3 = g.m3.rdmx;
+        const PhysT<R> &p = g.ph;
+        const R *dx1 = g.m1.dx, *dx2 = g.m2.dx, *dx3 = g.m3.dx;
+        const R *rdx1 = g.m1.rdx, *rdx2 = g.m2.rdx, *rdx3 = g.m3.rdx;
+        const R *rdmx1 = g.m1.rdmx, *rdmx2 = g.m2.rdmx, *rdmx3 = g.m3.rdmx;
         const long long c = ix(g, i, j, k), sj = g.P1, sk = (long long)g.P1 * g.P2;
-        const double *T = f.T;
-        const double Tc = ld(T + c), Txm = ld(T + c - 1), Txp = ld(T + c + 1);
-        const double Tym = ld(T + c - sj), Typ = ld(T + c + sj), Tzm = ld(T + c - sk), Tzp = ld(T + c + sk);
-        double Kc, dKc, Kxm, dKxm, Kxp, dKxp, Kym, dKym, Kyp, dKyp, Kzm, dKzm, Kzp, dKzp, irc, dirc;
+        const R *T = f.T;
+        const R Tc = ld(T + c), Txm = ld(T + c - 1), Txp = ld(T + c + 1);
+        const R Tym = ld(T + c - sj), Typ = ld(T + c + sj), Tzm = ld(T + c - sk), Tzp = ld(T + c + sk);
+        R Kc, dKc, Kxm, dKxm, Kxp, dKxp, Kym, dKym, Kyp, dKyp, Kzm, dKzm, Kzp, dKzp, irc, dirc;
         kpp_eval(p, Tc, Kc, dKc); kpp_eval(p, Txm, Kxm, dKxm); kpp_eval(p, Txp, Kxp, dKxp);
         kpp_eval(p, Tym, Kym, dKym); kpp_eval(p, Typ, Kyp, dKyp); kpp_eval(p, Tzm, Kzm, dKzm); kpp_eval(p, Tzp, Kzp, dKzp);
         rhocp_eval(p, Tc, irc, dirc);
-        const double jem = (j == 1) ? 0.0 : 1.0, jep = (j == g.N2) ? 0.0 : 1.0;   // jC_BC(jm), jC_BC(jp)
-        const double Uc = ld(f.U + c), Uxp = ld(f.U + c + 1), Vc = ld(f.V + c), Vyp = ld(f.V + c + sj);
-        const double Wc = ld(f.W + c), Wzp = ld(f.W + c + sk);
-        const double h = 0.5 * p.Ct * irc, dh = 0.5 * p.Ct * dirc;
-        const double e1 = (dx1[i] * Txm + dx1[im] * Tc) * (0.5 * rdmx1[i]);
-        const double e2 = (dx1[ip] * Tc + dx1[i] * Txp) * (0.5 * rdmx1[ip]);
-        const double e3 = (dx2[j] * Tym + dx2[jm] * Tc) * (0.5 * rdmx2[j]);
-        const double e4 = (dx2[jp] * Tc + dx2[j] * Typ) * (0.5 * rdmx2[jp]);
-        const double e5 = (dx3[k] * Tzm + dx3[km] * Tc) * (0.5 * rdmx3[k]);
-        const double e6 = (dx3[kp] * Tc + dx3[k] * Tzp) * (0.5 * rdmx3[kp]);
-        const double dedx1 = (Tc - Txm) * rdmx1[i], dedx2 = (Txp - Tc) * rdmx1[ip];
-        const double dedy3 = (Tc - Tym) * rdmx2[j], dedy4 = (Typ - Tc) * rdmx2[jp];
-        const double dedz5 = (Tc - Tzm) * rdmx3[k], dedz6 = (Tzp - Tc) * rdmx3[kp];
-        double rhs = -0.5 * ((Uc * dedx1 + Uxp * dedx2) * 0.5 + (Vc * dedy3 + Vyp * dedy4) * 0.5 + (Wc * dedz5 + Wzp * dedz6) * 0.5);
-        const double kPP1 = 0.5 * rdmx1[i] * (dx1[i] * Kxm + dx1[im] * Kc), kPP2 = 0.5 * rdmx1[ip] * (dx1[ip] * Kc + dx1[i] * Kxp);
-        const double kPP3 = 0.5 * rdmx2[j] * (dx2[j] * Kym + dx2[jm] * Kc), kPP4 = 0.5 * rdmx2[jp] * (dx2[jp] * Kc + dx2[j] * Kyp);
-        const double kPP5 = 0.5 * rdmx3[k] * (dx3[k] * Kzm + dx3[km] * Kc), kPP6 = 0.5 * rdmx3[kp] * (dx3[kp] * Kc + dx3[k] * Kzp);
-        const double dkPP1 = 0.5 * rdmx1[i] * (dx1[i] * dKxm + dx1[im] * dKc), dkPP2 = 0.5 * rdmx1[ip] * (dx1[ip] * dKc + dx1[i] * dKxp);
-        const double dkPP3 = 0.5 * rdmx2[j] * (dx2[j] * dKym + dx2[jm] * dKc), dkPP4 = 0.5 * rdmx2[jp] * (dx2[jp] * dKc + dx2[j] * dKyp);
-        const double dkPP5 = 0.5 * rdmx3[k] * (dx3[k] * dKzm + dx3[km] * dKc), dkPP6 = 0.5 * rdmx3[kp] * (dx3[kp] * dKc + dx3[k] * dKzp);
-        const double ve1 = (kPP2 * dedx2 - kPP1 * dedx1 - e2 * dkPP2 * dedx2 + e1 * dkPP1 * dedx1) * rdx1[i];
-        const double ve2 = (kPP4 * dedy4 - kPP3 * dedy3 - e4 * dkPP4 * dedy4 + e3 * dkPP3 * dedy3) * rdx2[j];
-        const double ve3 = (kPP6 * dedz6 - kPP5 * dedz5 - e6 * dkPP6 * dedz6 + e5 * dkPP5 * dedz5) * rdx3[k];
-        const double dv = (kPP2 * dedx2 - kPP1 * dedx1) * rdx1[i] + (kPP4 * dedy4 - kPP3 * dedy3) * rdx2[j] + (kPP6 * dedz6 - kPP5 * dedz5) * rdx3[k];
+        const R jem = (j == 1) ? R(0.0) : R(1.0), jep = (j == g.N2) ? R(0.0) : R(1.0);   // jC_BC(jm), jC_BC(jp)
+        const R Uc = ld(f.U + c), Uxp = ld(f.U + c + 1), Vc = ld(f.V + c), Vyp = ld(f.V + c + sj);
+        const R Wc = ld(f.W + c), Wzp = ld(f.W + c + sk);
+        const R h = R(0.5) * p.Ct * irc, dh = R(0.5) * p.Ct * dirc;
+        const R e1 = (dx1[i] * Txm + dx1[im] * Tc) * (R(0.5) * rdmx1[i]);
+        const R e2 = (dx1[ip] * Tc + dx1[i] * Txp) * (R(0.5) * rdmx1[ip]);
+        const R e3 = (dx2[j] * Tym + dx2[jm] * Tc) * (R(0.5) * rdmx2[j]);
+        const R e4 = (dx2[jp] * Tc + dx2[j] * Typ) * (R(0.5) * rdmx2[jp]);
+        const R e5 = (dx3[k] * Tzm + dx3[km] * Tc) * (R(0.5) * rdmx3[k]);
+        const R e6 = (dx3[kp] * Tc + dx3[k] * Tzp) * (R(0.5) * rdmx3[kp]);
+        const R dedx1 = (Tc - Txm) * rdmx1[i], dedx2 = (Txp - Tc) * rdmx1[ip];
+        const R dedy3 = (Tc - Tym) * rdmx2[j], dedy4 = (Typ - Tc) * rdmx2[jp];
+        const R dedz5 = (Tc - Tzm) * rdmx3[k], dedz6 = (Tzp - Tc) * rdmx3[kp];
+        R rhs = -R(0.5) * ((Uc * dedx1 + Uxp * dedx2) * R(0.5) + (Vc * dedy3 + Vyp * dedy4) * R(0.5) + (Wc * dedz5 + Wzp * dedz6) * R(0.5));
+        const R kPP1 = R(0.5) * rdmx1[i] * (dx1[i] * Kxm + dx1[im] * Kc), kPP2 = R(0.5) * rdmx1[ip] * (dx1[ip] * Kc + dx1[i] * Kxp);
+        const R kPP3 = R(0.5) * rdmx2[j] * (dx2[j] * Kym + dx2[jm] * Kc), kPP4 = R(0.5) * rdmx2[jp] * (dx2[jp] * Kc + dx2[j] * Kyp);
+        const R kPP5 = R(0.5) * rdmx3[k] * (dx3[k] * Kzm + dx3[km] * Kc), kPP6 = R(0.5) * rdmx3[kp] * (dx3[kp] * Kc + dx3[k] * Kzp);
+        const R dkPP1 = R(0.5) * rdmx1[i] * (dx1[i] * dKxm + dx1[im] * dKc), dkPP2 = R(0.5) * rdmx1[ip] * (dx1[ip] * dKc + dx1[i] * dKxp);
+        const R dkPP3 = R(0.5) * rdmx2[j] * (dx2[j] * dKym + dx2[jm] * dKc), dkPP4 = R(0.5) * rdmx2[jp] * (dx2[jp] * dKc + dx2[j] * dKyp);
+        const R dkPP5 = R(0.5) * rdmx3[k] * (dx3[k] * dKzm + dx3[km] * dKc), dkPP6 = R(0.5) * rdmx3[kp] * (dx3[kp] * dKc + dx3[k] * dKzp);
+        const R ve1 = (kPP2 * dedx2 - kPP1 * dedx1 - e2 * dkPP2 * dedx2 + e1 * dkPP1 * dedx1) * rdx1[i];
+        const R ve2 = (kPP4 * dedy4 - kPP3 * dedy3 - e4 * dkPP4 * dedy4 + e3 * dkPP3 * dedy3) * rdx2[j];
+        const R ve3 = (kPP6 * dedz6 - kPP5 * dedz5 - e6 * dkPP6 * dedz6 + e5 * dkPP5 * dedz5) * rdx3[k];
+        const R dv = (kPP2 * dedx2 - kPP1 * dedx1) * rdx1[i] + (kPP4 * dedy4 - kPP3 * dedy3) * rdx2[j] + (kPP6 * dedz6 - kPP5 * dedz5) * rdx3[k];
         rhs = rhs + h * (ve1 + ve2 + ve3) - dh * Tc * dv;
-        double ebc_up = -0.25 * Vyp * rdmx2[jp] * p.Tup;
-        double ebc_dn = 0.25 * Vc * rdmx2[j] * p.Tbt;
+        R ebc_up = -R(0.25) * Vyp * rdmx2[jp] * p.Tup;
+        R ebc_dn = R(0.25) * Vc * rdmx2[j] * p.Tbt;
         ebc_up = ebc_up + h * rdx2[j] * kPP4 * rdmx2[jp] * p.Tup + h * rdx2[j] * dkPP4 * dedy4 * p.Tup;
         ebc_dn = ebc_dn + h * rdx2[j] * kPP3 * rdmx2[j] * p.Tbt - h * rdx2[j] * dkPP3 * dedy3 * p.Tbt;
-        rhs = rhs + (1.0 - jem) * ebc_dn + (1.0 - jep) * ebc_up;
-        const double eACK = h * rdx3[k] * (kPP6 * rdmx3[kp] + kPP5 * rdmx3[k] - dx3[kp] * (0.5 * rdmx3[kp]) * dkPP6 * dedz6 + dx3[km] * (0.5 * rdmx3[k]) * dkPP5 * dedz5)
-                          + (-0.25 * Wzp * rdmx3[kp] + 0.25 * Wc * rdmx3[k]);
-        const double eAPK = -h * rdx3[k] * (kPP6 * rdmx3[kp] + dx3[k] * (0.5 * rdmx3[kp]) * dkPP6 * dedz6) + 0.25 * Wzp * rdmx3[kp];
-        const double eAMK = -h * rdx3[k] * (kPP5 * rdmx3[k] - dx3[k] * (0.5 * rdmx3[k]) * dkPP5 * dedz5) - 0.25 * Wc * rdmx3[k];
-        const double eACI = h * rdx1[i] * (kPP2 * rdmx1[ip] + kPP1 * rdmx1[i] - dx1[ip] * (0.5 * rdmx1[ip]) * dkPP2 * dedx2 + dx1[im] * (0.5 * rdmx1[i]) * dkPP1 * dedx1)
-                          + (0.25 * Uc * rdmx1[i] - 0.25 * Uxp * rdmx1[ip]);
-        const double eAPI = -h * rdx1[i] * (kPP2 * rdmx1[ip] + dx1[i] * (0.5 * rdmx1[ip]) * dkPP2 * dedx2) + 0.25 * Uxp * rdmx1[ip];
-        const double eAMI = -h * rdx1[i] * (kPP1 * rdmx1[i] - dx1[i] * (0.5 * rdmx1[i]) * dkPP1 * dedx1) - 0.25 * Uc * rdmx1[i];
-        const double eACJ = h * rdx2[j] * (kPP4 * rdmx2[jp] + kPP3 * rdmx2[j] - dx2[jp] * (0.5 * rdmx2[jp]) * dkPP4 * dedy4 * jep + dx2[jm] * (0.5 * rdmx2[j]) * dkPP3 * dedy3 * jem)
-                          + (0.25 * Vc * rdmx2[j] - 0.25 * Vyp * rdmx2[jp]);
-        const double eAPJ = (-h * rdx2[j] * (kPP4 * rdmx2[jp] + dx2[j] * (0.5 * rdmx2[jp]) * dkPP4 * dedy4) + 0.25 * Vyp * rdmx2[jp]) * jep;
-        const double eAMJ = (-h * rdx2[j] * (kPP3 * rdmx2[j] - dx2[j] * (0.5 * rdmx2[j]) * dkPP3 * dedy3) - 0.25 * Vc * rdmx2[j]) * jem;
+        rhs = rhs + (R(1.0) - jem) * ebc_dn + (R(1.0) - jep) * ebc_up;
+        const R eACK = h * rdx3[k] * (kPP6 * rdmx3[kp] + kPP5 * rdmx3[k] - dx3[kp] * (R(0.5) * rdmx3[kp]) * dkPP6 * dedz6 + dx3[km] * (R(0.5) * rdmx3[k]) * dkPP5 * dedz5)
+                          + (-R(0.25) * Wzp * rdmx3[kp] + R(0.25) * Wc * rdmx3[k]);
+        const R eAPK = -h * rdx3[k] * (kPP6 * rdmx3[kp] + dx3[k] * (R(0.5) * rdmx3[kp]) * dkPP6 * dedz6) + R(0.25) * Wzp * rdmx3[kp];
+        const R eAMK = -h * rdx3[k] * (kPP5 * rdmx3[k] - dx3[k] * (R(0.5) * rdmx3[k]) * dkPP5 * dedz5) - R(0.25) * Wc * rdmx3[k];
+        const R eACI = h * rdx1[i] * (kPP2 * rdmx1[ip] + kPP1 * rdmx1[i] - dx1[ip] * (R(0.5) * rdmx1[ip]) * dkPP2 * dedx2 + dx1[im] * (R(0.5) * rdmx1[i]) * dkPP1 * dedx1)
+                          + (R(0.25) * Uc * rdmx1[i] - R(0.25) * Uxp * rdmx1[ip]);
+        const R eAPI = -h * rdx1[i] * (kPP2 * rdmx1[ip] + dx1[i] * (R(0.5) * rdmx1[ip]) * dkPP2 * dedx2) + R(0.25) * Uxp * rdmx1[ip];
+        const R eAMI = -h * rdx1[i] * (kPP1 * rdmx1[i] - dx1[i] * (R(0.5) * rdmx1[i]) * dkPP1 * dedx1) - R(0.25) * Uc * rdmx1[i];
+        const R eACJ = h * rdx2[j] * (kPP4 * rdmx2[jp] + kPP3 * rdmx2[j] - dx2[jp] * (R(0.5) * rdmx2[jp]) * dkPP4 * dedy4 * jep + dx2[jm] * (R(0.5) * rdmx2[j]) * dkPP3 * dedy3 * jem)
+                          + (R(0.25) * Vc * rdmx2[j] - R(0.25) * Vyp * rdmx2[jp]);
+        const R eAPJ = (-h * rdx2[j] * (kPP4 * rdmx2[jp] + dx2[j] * (R(0.5) * rdmx2[jp]) * dkPP4 * dedy4) + R(0.25) * Vyp * rdmx2[jp]) * jep;
+        const R eAMJ = (-h * rdx2[j] * (kPP3 * rdmx2[j] - dx2[j] * (R(0.5) * rdmx2[j]) * dkPP3 * dedy3) - R(0.25) * Vc * rdmx2[j]) * jem;
         rhs = rhs - (eAPK * Tzp + eACK * Tc + eAMK * Tzm + eAPJ * Typ + eACJ * Tc + eAMJ * Tym
                      + eAPI * Txp + eACI * Tc + eAMI * Txm - dh * Tc * dv);
-        const double dt = st.dt;
-        Coef<1> cf;
-        cf.b = eACK * dt - 0.5 * dh * dv * dt + 1.0;
+        const R dt = st.dt;
+        Coef<R, 1> cf;
+        cf.b = eACK * dt - R(0.5) * dh * dv * dt + R(1.0);
         cf.c = eAPK * dt;
         cf.a = eAMK * dt;
         cf.d[0] = rhs * dt;
         return cf;
     }
-    __device__ void emit(int l, int r, const double *x, const State &st) const
+    __device__ void emit(int l, int r, const R *x, const State &st) const
     {
-        f.R[ix(g, li(l), 1 + blockIdx.y, r + 1)] = x[0];
+        f.scr[ix(g, li(l), 1 + blockIdx.y, r + 1)] = x[0];
     }
 };
 
 // Stage 2 (:388-429): jm, jp, km, kp keep the values of the last stage-1
 // iteration (N2-1, N2+1, N3-1, N3+1).
+template <class R>
 struct ThermalX {
+    using Real = R;
     static constexpr int NRHS = 1;
     static constexpr bool CONTIG = true;
-    Grid g; Fields f; int TL;
+    GridT<R> g; FieldsT<R> f; int TL;
     __device__ bool skip() const { return blown(g); }
-    struct State { double dt; };
-    __device__ State prepare() const { return State{g.scal[S_DT]}; }
+    struct State { R dt; };
+    __device__ State prepare() const { return State{R(g.scal[S_DT])}; }
     __device__ int lj(int l) const { return 1 + blockIdx.x * TL + l; }
     __device__ bool line_ok(int l) const { return lj(l) <= g.N2; }
-    __device__ Coef<1> build(int l, int r, const State &st) const
+    __device__ Coef<R, 1> build(int l, int r, const State &st) const
     {
         const int i = r + 1, j = lj(l), k = 1 + blockIdx.y;
         const int im = i - 1, ip = i + 1, jm = g.N2 - 1, jp = g.N2 + 1, km = g.N3 - 1, kp = g.N3 + 1;
-        const Phys &p = g.ph;
-        const double *dx1 = g.m1.dx, *dx2 = g.m2.dx, *dx3 = g.m3.dx;
-        const double *rdx1 = g.m1.rdx, *rdx2 = g.m2.rdx, *rdx3 = g.m3.rdx;
-        const double *rdmx1 = g.m1.rdmx, *rdmx2 = g.m2.rdmx, *rdmx3 = g.m3.rdmx;
+        const PhysT<R> &p = g.ph;
+        const R *dx1 = g.m1.dx, *dx2 = g.m2.dx, *dx3 = g.m3.dx;
+        const R *rdx1 = g.m1.rdx, *rdx2 = g.m2.rdx, *rdx3 = g.m3.rdx;
+        const R *rdmx1 = g.m1.rdmx, *rdmx2 = g.m2.rdmx, *rdmx3 = g.m3.rdmx;
         const long long c = ix(g, i, j, k);
-        const double *T = f.T;
-        const double Tc = ld(T + c), Txm = ld(T + c - 1), Txp = ld(T + c + 1);
-        const double Tjm = ld(T + ix(g, i, jm, k)), Tjp = ld(T + ix(g, i, jp, k));
-        const double Tkm = ld(T + ix(g, i, j, km)), Tkp = ld(T + ix(g, i, j, kp));
-        double Kc, dKc, Kxm, dKxm, Kxp, dKxp, irc, dirc;
+        const R *T = f.T;
+        const R Tc = ld(T + c), Txm = ld(T + c - 1), Txp = ld(T + c + 1);
+        const R Tjm = ld(T + ix(g, i, jm, k)), Tjp = ld(T + ix(g, i, jp, k));
+        const R Tkm = ld(T + ix(g, i, j, km)), Tkp = ld(T + ix(g, i, j, kp));
+        R Kc, dKc, Kxm, dKxm, Kxp, dKxp, irc, dirc;
         kpp_eval(p, Tc, Kc, dKc); kpp_eval(p, Txm, Kxm, dKxm); kpp_eval(p, Txp, Kxp, dKxp);
-        const double Kjm = kpp_only(p, Tjm), Kjp = kpp_only(p, Tjp), Kkm = kpp_only(p, Tkm), Kkp = kpp_only(p, Tkp);
+        const R Kjm = kpp_only(p, Tjm), Kjp = kpp_only(p, Tjp), Kkm = kpp_only(p, Tkm), Kkp = kpp_only(p, Tkp);
         rhocp_eval(p, Tc, irc, dirc);
-        const double h = 0.5 * p.Ct * irc;
-        const double kPP1 = 0.5 * rdmx1[i] * (dx1[i] * Kxm + dx1[im] * Kc), kPP2 = 0.5 * rdmx1[ip] * (dx1[ip] * Kc + dx1[i] * Kxp);
-        const double kPP3 = 0.5 * rdmx2[j] * (dx2[j] * Kjm + dx2[jm] * Kc), kPP4 = 0.5 * rdmx2[jp] * (dx2[jp] * Kc + dx2[j] * Kjp);
-        const double kPP5 = 0.5 * rdmx3[k] * (dx3[k] * Kkm + dx3[km] * Kc), kPP6 = 0.5 * rdmx3[kp] * (dx3[kp] * Kc + dx3[k] * Kkp);
-        const double dkPP1 = 0.5 * rdmx1[i] * (dx1[i] * dKxm + dx1[im] * dKc), dkPP2 = 0.5 * rdmx1[ip] * (dx1[ip] * dKc + dx1[i] * dKxp);
-        const double dedx1 = (Tc - Txm) * rdmx1[i], dedx2 = (Txp - Tc) * rdmx1[ip];
-        const double dedy3 = (Tc - Tjm) * rdmx2[j], dedy4 = (Tjp - Tc) * rdmx2[jp];
-        const double dedz5 = (Tc - Tkm) * rdmx3[k], dedz6 = (Tkp - Tc) * rdmx3[kp];
-        const double Uc = ld(f.U + c), Uxp = ld(f.U + c + 1);
-        const double eACI = h * rdx1[i] * (kPP2 * rdmx1[ip] + kPP1 * rdmx1[i] - dx1[ip] * (0.5 * rdmx1[ip]) * dkPP2 * dedx2 + dx1[im] * (0.5 * rdmx1[i]) * dkPP1 * dedx1)
-                          + (0.25 * Uc * rdmx1[i] - 0.25 * Uxp * rdmx1[ip])
-                          - 0.5 * h * ((kPP2 * dedx2 - kPP1 * dedx1) * rdx1[i] + (kPP4 * dedy4 - kPP3 * dedy3) * rdx2[j] + (kPP6 * dedz6 - kPP5 * dedz5) * rdx3[k]);
-        const double eAPI = -h * rdx1[i] * (kPP2 * rdmx1[ip] + dx1[i] * (0.5 * rdmx1[ip]) * dkPP2 * dedx2) + 0.25 * Uxp * rdmx1[ip];
-        const double eAMI = -h * rdx1[i] * (kPP1 * rdmx1[i] - dx1[i] * (0.5 * rdmx1[i]) * dkPP1 * dedx1) - 0.25 * Uc * rdmx1[i];
-        const double dt = st.dt;
-        Coef<1> cf;
-        cf.b = eACI * dt + 1.0;
+        const R h = R(0.5) * p.Ct * irc;
+        const R kPP1 = R(0.5) * rdmx1[i] * (dx1[i] * Kxm + dx1[im] * Kc), kPP2 = R(0.5) * rdmx1[ip] * (dx1[ip] * Kc + dx1[i] * Kxp);
+        const R kPP3 = R(0.5) * rdmx2[j] * (dx2[j] * Kjm + dx2[jm] * Kc), kPP4 = R(0.5) * rdmx2[jp] * (dx2[jp] * Kc + dx2[j] * Kjp);
+        const R kPP5 = R(0.5) * rdmx3[k] * (dx3[k] * Kkm + dx3[km] * Kc), kPP6 = R(0.5) * rdmx3[kp] * (dx3[kp] * Kc + dx3[k] * Kkp);
+        const R dkPP1 = R(0.5) * rdmx1[i] * (dx1[i] * dKxm + dx1[im] * dKc), dkPP2 = R(0.5) * rdmx1[ip] * (dx1[ip] * dKc + dx1[i] * dKxp);
+        const R dedx1 = (Tc - Txm) * rdmx1[i], dedx2 = (Txp - Tc) * rdmx1[ip];
+        const R dedy3 = (Tc - Tjm) * rdmx2[j], dedy4 = (Tjp - Tc) * rdmx2[jp];
+        const R dedz5 = (Tc - Tkm) * rdmx3[k], dedz6 = (Tkp - Tc) * rdmx3[kp];
+        const R Uc = ld(f.U + c), Uxp = ld(f.U + c + 1);
+        const R eACI = h * rdx1[i] * (kPP2 * rdmx1[ip] + kPP1 * rdmx1[i] - dx1[ip] * (R(0.5) * rdmx1[ip]) * dkPP2 * dedx2 + dx1[im] * (R(0.5) * rdmx1[i]) * dkPP1 * dedx1)
+                          + (R(0.25) * Uc * rdmx1[i] - R(0.25) * Uxp * rdmx1[ip])
+                          - R(0.5) * h * ((kPP2 * dedx2 - kPP1 * dedx1) * rdx1[i] + (kPP4 * dedy4 - kPP3 * dedy3) * rdx2[j] + (kPP6 * dedz6 - kPP5 * dedz5) * rdx3[k]);
+        const R eAPI = -h * rdx1[i] * (kPP2 * rdmx1[ip] + dx1[i] * (R(0.5) * rdmx1[ip]) * dkPP2 * dedx2) + R(0.25) * Uxp * rdmx1[ip];
+        const R eAMI = -h * rdx1[i] * (kPP1 * rdmx1[i] - dx1[i] * (R(0.5) * rdmx1[i]) * dkPP1 * dedx1) - R(0.25) * Uc * rdmx1[i];
+        const R dt = st.dt;
+        Coef<R, 1> cf;
+        cf.b = eACI * dt + R(1.0);
         cf.c = eAPI * dt;
         cf.a = eAMI * dt;
-        cf.d[0] = ld(f.R + c);
+        cf.d[0] = ld(f.scr + c);
         return cf;
     }
-    __device__ void emit(int l, int r, const double *x, const State &st) const
+    __device__ void emit(int l, int r, const R *x, const State &st) const
     {
-        f.R[ix(g, r + 1, lj(l), 1 + blockIdx.y)] = x[0];
+        f.scr[ix(g, r + 1, lj(l), 1 + blockIdx.y)] = x[0];
     }
 };
 
 // Stage 3 (:456-507): km, kp stale (N3-1, N3+1); T += solution (:518-524).
+template <class R>
 struct ThermalY {
+    using Real = R;
     static constexpr int NRHS = 1;
     static constexpr bool CONTIG = false;
-    Grid g; Fields f; int TL;
+    GridT<R> g; FieldsT<R> f; int TL;
     __device__ bool skip() const { return blown(g); }
-    struct State { double dt; };
-    __device__ State prepare() const { return State{g.scal[S_DT]}; }
+    struct State { R dt; };
+    __device__ State prepare() const { return State{R(g.scal[S_DT])}; }
     __device__ int li(int l) const { return 1 + blockIdx.x * TL + l; }
     __device__ bool line_ok(int l) const { return li(l) <= g.N1; }
-    __device__ Coef<1> build(int l, int r, const State &st) const
+    __device__ Coef<R, 1> build(int l, int r, const State &st) const
     {
         const int i = li(l), j = r + 1, k = 1 + blockIdx.y;
         const int im = i - 1, ip = i + 1, jm = j - 1, jp = j + 1, km = g.N3 - 1, kp = g.N3 + 1;
-        const Phys &p = g.ph;
-        const double *dx1 = g.m1.dx, *dx2 = g.m2.dx, *dx3 = g.m3.dx;
-        const double *rdx1 = g.m1.rdx, *rdx2 = g.m2.rdx, *rdx3 = g.m3.rdx;
-        const double *rdmx1 = g.m1.rdmx, *rdmx2 = g.m2.rdmx, *rdmx3 = g.m3.rdmx;
+        const PhysT<R> &p = g.ph;
+        const R *dx1 = g.m1.dx, *dx2 = g.m2.dx, *dx3 = g.m3.dx;
+        const R *rdx1 = g.m1.rdx, *rdx2 = g.m2.rdx, *rdx3 = g.m3.rdx;
+        const R *rdmx1 = g.m1.rdmx, *rdmx2 = g.m2.rdmx, *rdmx3 = g.m3.rdmx;
         const long long c = ix(g, i, j, k), sj = g.P1;
-        const double *T = f.T;
-        const double Tc = ld(T + c), Txm = ld(T + c - 1), Txp = ld(T + c + 1), Tym = ld(T + c - sj), Typ = ld(T + c + sj);
-        const double Tkm = ld(T + ix(g, i, j, km)), Tkp = ld(T + ix(g, i, j, kp));
-        double Kc, dKc, Kym, dKym, Kyp, dKyp, irc, dirc;
+        const R *T = f.T;
+        const R Tc = ld(T + c), Txm = ld(T + c - 1), Txp = ld(T + c + 1), Tym = ld(T + c - sj), Typ = ld(T + c + sj);
+        const R Tkm = ld(T + ix(g, i, j, km)), Tkp = ld(T + ix(g, i, j, kp));
+        R Kc, dKc, Kym, dKym, Kyp, dKyp, irc, dirc;
         kpp_eval(p, Tc, Kc, dKc); kpp_eval(p, Tym, Kym, dKym); kpp_eval(p, Typ, Kyp, dKyp);
-        const double Kxm = kpp_only(p, Txm), Kxp = kpp_only(p, Txp), Kkm = kpp_only(p, Tkm), Kkp = kpp_only(p, Tkp);
+        const R Kxm = kpp_only(p, Txm), Kxp = kpp_only(p, Txp), Kkm = kpp_only(p, Tkm), Kkp = kpp_only(p, Tkp);
         rhocp_eval(p, Tc, irc, dirc);
-        const double h = 0.5 * p.Ct * irc;
-        const double jem = (j == 1) ? 0.0 : 1.0, jep = (j == g.N2) ? 0.0 : 1.0;
-        const double KPP1 = 0.5 * rdmx1[i] * (dx1[i] * Kxm + dx1[im] * Kc), KPP2 = 0.5 * rdmx1[ip] * (dx1[ip] * Kc + dx1[i] * Kxp);
-        const double kPP3 = 0.5 * rdmx2[j] * (dx2[j] * Kym + dx2[jm] * Kc), kPP4 = 0.5 * rdmx2[jp] * (dx2[jp] * Kc + dx2[j] * Kyp);
-        const double KPP5 = 0.5 * rdmx3[k] * (dx3[k] * Kkm + dx3[km] * Kc), KPP6 = 0.5 * rdmx3[kp] * (dx3[kp] * Kc + dx3[k] * Kkp);
-        const double dkPP3 = 0.5 * rdmx2[j] * (dx2[j] * dKym + dx2[jm] * dKc), dkPP4 = 0.5 * rdmx2[jp] * (dx2[jp] * dKc + dx2[j] * dKyp);
-        const double dedx1 = (Tc - Txm) * rdmx1[i], dedx2 = (Txp - Tc) * rdmx1[ip];
-        const double dedy3 = (Tc - Tym) * rdmx2[j], dedy4 = (Typ - Tc) * rdmx2[jp];
-        const double dedz5 = (Tc - Tkm) * rdmx3[k], dedz6 = (Tkp - Tc) * rdmx3[kp];
-        const double Vc = ld(f.V + c), Vyp = ld(f.V + c + sj);
-        const double eACJ = h * rdx2[j] * (kPP4 * rdmx2[jp] + kPP3 * rdmx2[j] - dx2[jp] * (0.5 * rdmx2[jp]) * dkPP4 * dedy4 * jep + dx2[jm] * (0.5 * rdmx2[j]) * dkPP3 * dedy3 * jem)
-                          + (0.25 * Vc * rdmx2[j] - 0.25 * Vyp * rdmx2[jp])
-                          - 0.5 * h * ((KPP2 * dedx2 - KPP1 * dedx1) * rdx1[i] + (kPP4 * dedy4 - kPP3 * dedy3) * rdx2[j] + (KPP6 * dedz6 - KPP5 * dedz5) * rdx3[k]);
-        const double eAPJ = (-h * rdx2[j] * (kPP4 * rdmx2[jp] + dx2[j] * (0.5 * rdmx2[jp]) * dkPP4 * dedy4) + 0.25 * Vyp * rdmx2[jp]) * jep;
-        const double eAMJ = (-h * rdx2[j] * (kPP3 * rdmx2[j] - dx2[j] * (0.5 * rdmx2[j]) * dkPP3 * dedy3) - 0.25 * Vc * rdmx2[j]) * jem;
-        const double dt = st.dt;
-        Coef<1> cf;
-        cf.b = eACJ * dt + 1.0;
+        const R h = R(0.5) * p.Ct * irc;
+        const R jem = (j == 1) ? R(0.0) : R(1.0), jep = (j == g.N2) ? R(0.0) : R(1.0);
+        const R KPP1 = R(0.5) * rdmx1[i] * (dx1[i] * Kxm + dx1[im] * Kc), KPP2 = R(0.5) * rdmx1[ip] * (dx1[ip] * Kc + dx1[i] * Kxp);
+        const R kPP3 = R(0.5) * rdmx2[j] * (dx2[j] * Kym + dx2[jm] * Kc), kPP4 = R(0.5) * rdmx2[jp] * (dx2[jp] * Kc + dx2[j] * Kyp);
+        const R KPP5 = R(0.5) * rdmx3[k] * (dx3[k] * Kkm + dx3[km] * Kc), KPP6 = R(0.5) * rdmx3[kp] * (dx3[kp] * Kc + dx3[k] * Kkp);
+        const R dkPP3 = R(0.5) * rdmx2[j] * (dx2[j] * dKym + dx2[jm] * dKc), dkPP4 = R(0.5) * rdmx2[jp] * (dx2[jp] * dKc + dx2[j] * dKyp);
+        const R dedx1 = (Tc - Txm) * rdmx1[i], dedx2 = (Txp - Tc) * rdmx1[ip];
+        const R dedy3 = (Tc - Tym) * rdmx2[j], dedy4 = (Typ - Tc) * rdmx2[jp];
+        const R dedz5 = (Tc - Tkm) * rdmx3[k], dedz6 = (Tkp - Tc) * rdmx3[kp];
+        const R Vc = ld(f.V + c), Vyp = ld(f.V + c + sj);
+        const R eACJ = h * rdx2[j] * (kPP4 * rdmx2[jp] + kPP3 * rdmx2[j] - dx2[jp] * (R(0.5) * rdmx2[jp]) * dkPP4 * dedy4 * jep + dx2[jm] * (R(0.5) * rdmx2[j]) * dkPP3 * dedy3 * jem)
+                          + (R(0.25) * Vc * rdmx2[j] - R(0.25) * Vyp * rdmx2[jp])
+                          - R(0.5) * h * ((KPP2 * dedx2 - KPP1 * dedx1) * rdx1[i] + (kPP4 * dedy4 - kPP3 * dedy3) * rdx2[j] + (KPP6 * dedz6 - KPP5 * dedz5) * rdx3[k]);
+        const R eAPJ = (-h * rdx2[j] * (kPP4 * rdmx2[jp] + dx2[j] * (R(0.5) * rdmx2[jp]) * dkPP4 * dedy4) + R(0.25) * Vyp * rdmx2[jp]) * jep;
+        const R eAMJ = (-h * rdx2[j] * (kPP3 * rdmx2[j] - dx2[j] * (R(0.5) * rdmx2[j]) * dkPP3 * dedy3) - R(0.25) * Vc * rdmx2[j]) * jem;
+        const R dt = st.dt;
+        Coef<R, 1> cf;
+        cf.b = eACJ * dt + R(1.0);
         cf.c = eAPJ * dt;
         cf.a = eAMJ * dt;
-        cf.d[0] = ld(f.R + c);
+        cf.d[0] = ld(f.scr + c);
         return cf;
     }
-    __device__ void emit(int l, int r, const double *x, const State &st) const
+    __device__ void emit(int l, int r, const R *x, const State &st) const
     {
         const int i = li(l), j = r + 1, k = 1 + blockIdx.y;
         store_periodic(g, f.Tn, i, j, k, ld(f.T + ix(g, i, j, k)) + x[0]);
     }
 };
 
-void launch_thermal(const Ctx &cx, cudaStream_t s)
+template <class R>
+void launch_thermal(const Ctx<R> &cx, cudaStream_t s)
 {
-    const Grid &g = cx.g;
+    const GridT<R> &g = cx.g;
     LinePlan pz = make_line_plan(g.N3, true, cx.tl_strided);
     LinePlan px = make_line_plan(g.N1, true, cx.tl_contig);
     LinePlan py = make_line_plan(g.N2, false, cx.tl_strided);
-    ThermalZ z{g, cx.f, pz.TL};
+    ThermalZ<R> z{g, cx.f, pz.TL};
     launch_lines(z, pz, dim3((g.N1 + pz.TL - 1) / pz.TL, g.N2), s, K_THERMAL_Z, cx);
-    ThermalX xx{g, cx.f, px.TL};
+    ThermalX<R> xx{g, cx.f, px.TL};
     launch_lines(xx, px, dim3((g.N2 + px.TL - 1) / px.TL, g.N3), s, K_THERMAL_X, cx);
-    ThermalY y{g, cx.f, py.TL};
+    ThermalY<R> y{g, cx.f, py.TL};
     launch_lines(y, py, dim3((g.N1 + py.TL - 1) / py.TL, g.N3), s, K_THERMAL_Y, cx);
 }
+
+// the two forms
+template void launch_thermal<double>(const Ctx<double> &, cudaStream_t);
+template void launch_thermal<float>(const Ctx<float> &, cudaStream_t);
 
 } // namespace tcs

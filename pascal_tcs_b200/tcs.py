@@ -41,7 +41,7 @@ EXPORTS = [
     "tcs_tdma_plan_many_create", "tcs_tdma_plan_many_destroy", "tcs_tdma_many_solve",
     "tcs_tdma_many_solve_cycle", "tcs_tdma_many_solve_noalloc", "tcs_kernel_count", "tcs_launch_count", "tcs_kernel_name", "tcs_probe_enable",
     "tcs_probe_read", "tcs_probe_reset", "tcs_set_use_graph", "tcs_set_tuning", "tcs_get_tuning",
-    "tcs_last_error",
+    "tcs_last_error", "tcs_precision",
 ]
 
 
@@ -60,7 +60,12 @@ class TcsConfig(ctypes.Structure):
                 ("MaxCFL", ctypes.c_double), ("dtStart", ctypes.c_double), ("tStart", ctypes.c_double),
                 ("property_set", ctypes.c_int), ("fixed_dt", ctypes.c_int),
                 ("seed", ctypes.c_uint64), ("noise_amp", ctypes.c_double),
-                ("init_mode", ctypes.c_int), ("top_wall_mode", ctypes.c_int), ("device", ctypes.c_int)]
+                ("init_mode", ctypes.c_int), ("top_wall_mode", ctypes.c_int), ("device", ctypes.c_int),
+                ("precision", ctypes.c_int)]
+
+
+PREC_FP64 = 0          # the reference's arithmetic
+PREC_FP32_MIXED = 1    # FP32 fields/stencils/sweeps/FFTs, FP64 refinement, modal solves, projection, reductions
 
 
 def default_config(**kw) -> dict:
@@ -70,7 +75,7 @@ def default_config(**kw) -> dict:
              gamma1=3.0, gamma2=1.5, gamma3=3.0, aspect1=2.0, H=1.0, aspect3=2.0,
              Ra=1e5, Pr=0.71, DeltaT=10.0, MaxCFL=1.0, dtStart=1e-3, tStart=0.0,
              property_set=0, fixed_dt=1, seed=0, noise_amp=0.01, init_mode=0,
-             top_wall_mode=0, device=0)
+             top_wall_mode=0, device=0, precision=PREC_FP64)
     c.update(kw)
     return c
 
@@ -122,6 +127,7 @@ def load() -> ctypes.CDLL:
         "tcs_set_tuning": ([vp, ip, ip], ip),
         "tcs_get_tuning": ([vp, ip, ctypes.POINTER(ip)], ip),
         "tcs_last_error": ([], ctypes.c_char_p),
+        "tcs_precision": ([vp], ip),
     }
     for name in ("tcs_thermal_coeffi", "tcs_thermal_solver", "tcs_thermal_coeffi_clean",
                  "tcs_momentum_coeffi", "tcs_momentum_solvedU", "tcs_momentum_solvedV",
@@ -200,6 +206,11 @@ class Solver:
 
     def download_async(self, name: str, pinned_ptr: int) -> None:
         _check(load().tcs_download_field_async(self._h, FIELDS[name], pinned_ptr), f"download {name}")
+
+    @property
+    def precision(self) -> int:
+        """PREC_FP64 or PREC_FP32_MIXED; device buffers hold doubles or floats accordingly."""
+        return int(load().tcs_precision(self._h))
 
     def device_ptr(self, name: str) -> int:
         p = ctypes.c_void_p()

@@ -33,7 +33,7 @@ def tcs():
 
 def _pair(tcs, oracle_mod, **cfg):
     g = tcs.Solver(**cfg)
-    o = oracle_mod.Oracle(**{k: v for k, v in g.config.items() if k != "device"})
+    o = oracle_mod.Oracle(**{k: v for k, v in g.config.items() if k not in ("device", "precision")})
     return g, o
 
 

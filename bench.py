@@ -6,6 +6,8 @@ ADI, FFT pressure Poisson solve, projection, Div/CFL/Nu/KE) on one
 HBM-resident case.  Default workload: the 256^3 plain-FP64 case with
 temperature-dependent water properties (Ra = 1e8, Pr = 7, dt = 2e-4, tanh
 y-stretching gamma = 1.5, seeded conduction profile + 0.01 noise, seed 1).
+A plain-FP64 workload also times its FP32-mixed counterpart and states the
+mixed form's error against the FP64 form after the same steps.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME] [--impl ours|reference]
 
@@ -28,29 +30,36 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-WORKLOADS = {
-    # the plain FP64 256^3 water case the headline metric is quoted on
-    "rb256_water_fp64": dict(n1m=256, n2m=256, n3m=256, gamma2=1.5, property_set=1, Pr=7.0, Ra=1e8,
-                             DeltaT=10.0, dtStart=2e-4, fixed_dt=1, seed=1, noise_amp=0.01),
-    "rb64_const_fp64": dict(n1m=64, n2m=64, n3m=64, gamma2=1.5, property_set=0, Pr=0.71, Ra=1e5,
-                            dtStart=1e-3, fixed_dt=1, seed=0, noise_amp=0.01),
-    "rb512_water_fp64": dict(n1m=512, n2m=512, n3m=512, gamma2=2.0, property_set=1, Pr=7.0, Ra=1e9,
-                             DeltaT=10.0, dtStart=5e-5, fixed_dt=1, seed=2, noise_amp=0.01),
+_CASES = {
+    # the 256^3 water case the headline metric is quoted on
+    "rb256_water": dict(n1m=256, n2m=256, n3m=256, gamma2=1.5, property_set=1, Pr=7.0, Ra=1e8,
+                        DeltaT=10.0, dtStart=2e-4, fixed_dt=1, seed=1, noise_amp=0.01),
+    "rb64_const": dict(n1m=64, n2m=64, n3m=64, gamma2=1.5, property_set=0, Pr=0.71, Ra=1e5,
+                       dtStart=1e-3, fixed_dt=1, seed=0, noise_amp=0.01),
+    "rb512_water": dict(n1m=512, n2m=512, n3m=512, gamma2=2.0, property_set=1, Pr=7.0, Ra=1e9,
+                        DeltaT=10.0, dtStart=5e-5, fixed_dt=1, seed=2, noise_amp=0.01),
     # profiling size: inputs still larger than L2, about 1.3 GB on the device
-    "rb192_water_fp64": dict(n1m=192, n2m=192, n3m=192, gamma2=1.5, property_set=1, Pr=7.0, Ra=1e8,
-                             DeltaT=10.0, dtStart=2e-4, fixed_dt=1, seed=1, noise_amp=0.01),
+    "rb192_water": dict(n1m=192, n2m=192, n3m=192, gamma2=1.5, property_set=1, Pr=7.0, Ra=1e8,
+                        DeltaT=10.0, dtStart=2e-4, fixed_dt=1, seed=1, noise_amp=0.01),
 }
+# precision 0: plain FP64; 1: FP32-mixed
+WORKLOADS = {f"{k}_{form}": dict(v, precision=prec) for k, v in _CASES.items()
+             for form, prec in (("fp64", 0), ("mixed", 1))}
 # The water cases blow up after ~10 steps (256^3) in the reference algorithm itself (the
 # non-Boussinesq pressure term sees dPhat = 0 in the wall ghost row and dPhat grows
 # ~1.6x per step at the bottom wall; the oracle restatement and this library stop at
 # the same step).  Their timed steps therefore restart from the seeded initial state,
 # kept on the device, every RESET_EVERY steps; the restore copies are timed too.
-RESET_EVERY = {"rb256_water_fp64": 8, "rb512_water_fp64": 5, "rb192_water_fp64": 8}
+RESET_EVERY = {f"{k}_{form}": n for k, n in (("rb256_water", 8), ("rb512_water", 5), ("rb192_water", 8))
+               for form in ("fp64", "mixed")}
 
-# Compulsory-traffic model: FP64 arrays each kernel must stream once (reads +
+# Compulsory-traffic model: arrays each kernel must stream once (reads +
 # writes) per interior cell; properties and tridiagonal coefficients are
-# recomputed, 1-D metrics and ghosts ignored.  Whole step: 109 arrays = 872 B.
-STEP_ARRAYS_FP64 = 109
+# recomputed, 1-D metrics and ghosts ignored.  Whole step: 109 arrays, at
+# 8 B (872 B per cell-step) in the FP64 form and 4 B (436 B) in the FP32-mixed
+# form, whose every stored array is FP32 (its FP64 parts live in registers
+# and shared memory).
+STEP_ARRAYS = 109
 KERNEL_ARRAYS = {"thermal_z": 5, "thermal_x": 4, "thermal_y": 4,
                  "du_z": 6, "du_x": 4, "du_y": 4, "dv_z": 7, "dv_x": 4, "dv_y": 4,
                  "dw_z": 8, "dw_x": 4, "dw_y": 4, "blockld_v": 5, "blockld_u": 6,
@@ -58,19 +67,19 @@ KERNEL_ARRAYS = {"thermal_z": 5, "thermal_x": 4, "thermal_y": 4,
                  "projection": 14, "post": 4}
 
 
-def kernel_bytes(name: str, n1: int, n2: int, n3: int) -> float:
+def kernel_bytes(name: str, n1: int, n2: int, n3: int, esize: int = 8) -> float:
     cells = n1 * n2 * n3
     h1p = n1 // 2 + 1
-    spec = 16.0 * h1p * n2 * n3                       # one pass over the complex half-spectrum
+    spec = 2.0 * esize * h1p * n2 * n3                # one pass over the complex half-spectrum
     if name in ("fftz_fwd", "modal_tdma", "fftz_inv"):
         return 2 * spec
     if name == "ifftx":
-        return spec + 8.0 * cells
+        return spec + esize * cells
     if name == "prhs_fftx":
-        return 10 * 8.0 * cells + spec
+        return 10 * esize * cells + spec
     if name.startswith("dv_") or name == "blockld_v":
         cells = n1 * (n2 - 1) * n3
-    return KERNEL_ARRAYS[name] * 8.0 * cells
+    return KERNEL_ARRAYS[name] * esize * cells
 
 
 def measured_peaks():
@@ -191,7 +200,7 @@ def cpu_baseline(cfg: dict, target_s: float = 20.0, threads: int | None = None) 
     from oracle import oracle as O
     threads = threads or os.cpu_count() or 1
     O.set_threads(threads)
-    o = O.Oracle(**{k: v for k, v in cfg.items() if k != "device"})
+    o = O.Oracle(**{k: v for k, v in cfg.items() if k not in ("device", "precision")})
     t0 = time.perf_counter(); o.step(1); t1 = time.perf_counter()
     first = t1 - t0
     n = max(1, min(20, int(target_s / max(first, 1e-3))))
@@ -210,7 +219,7 @@ def run_reference(args, cfg, workload):
     from oracle import oracle as O
     threads = os.cpu_count() or 1
     O.set_threads(threads)
-    o = O.Oracle(**{k: v for k, v in cfg.items() if k != "device"})
+    o = O.Oracle(**{k: v for k, v in cfg.items() if k not in ("device", "precision")})
     if args.warmup:
         o.step(args.warmup)
     t0 = time.perf_counter()
@@ -232,30 +241,12 @@ def run_reference(args, cfg, workload):
     return 0
 
 
-def main():
-    ap = argparse.ArgumentParser()
-    ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
-    ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--workload", default="rb256_water_fp64", choices=sorted(WORKLOADS))
-    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-e2e", action="store_true")
-    args = ap.parse_args()
-    workload = args.workload
-    cfg = dict(WORKLOADS[workload])
-    if args.impl == "reference":
-        return run_reference(args, cfg, workload)
-
-    ws, rank, local = dist_setup(args.gpus)
-    import torch
-    import pascal_tcs_b200 as P
-
-    torch.cuda.set_device(local)
-    stream = torch.cuda.Stream()
-    cfg["device"] = local
+def device_run(P, torch, cfg: dict, workload: str, args, ws: int, local: int, stream):
+    """Warm-up, per-kernel probe, then K device-timed steps of one case.  Returns
+    the solver (left at its seeded snapshot) and the measurements."""
     n1, n2, n3 = cfg["n1m"], cfg["n2m"], cfg["n3m"]
     cells = n1 * n2 * n3
+    esize = 4 if cfg.get("precision", 0) else 8
     s = P.Solver(**cfg)
     s.set_stream(stream.cuda_stream)
     reset = RESET_EVERY.get(workload, 0)
@@ -299,23 +290,85 @@ def main():
         dist_barrier(ws)
         time.sleep(0.15)          # one more sample after the region
     launches = P.launch_count() - launches0
-    ms_local = e0.elapsed_time(e1)
-    ms = dist_max(ms_local, ws)
+    ms = dist_max(e0.elapsed_time(e1), ws)
     assert done == args.steps
-    value = ws * cells * args.steps / (ms * 1e-3)
     tk, nk = s.probe_read(top)
     s.probe([])
     peak, peak_kind = measured_peaks()
-    kb = kernel_bytes(top, n1, n2, n3)
+    kb = kernel_bytes(top, n1, n2, n3, esize)
     achieved = kb / (tk / nk * 1e-3) / 1e9 if nk else None
     roof = {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak if achieved else None, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
             "algorithmic_bytes_per_launch": kb, "launches": nk, "avg_launch_ms": tk / nk if nk else None,
             "traffic": profiled_traffic(top, workload)}
-    step_bytes = STEP_ARRAYS_FP64 * 8.0 * cells
-    whole = {"algorithmic_bytes_per_step": step_bytes, "achieved_gbs": step_bytes / (ms / args.steps * 1e-3) / 1e9}
+    step_bytes = STEP_ARRAYS * esize * cells
+    whole = {"algorithmic_bytes_per_step": step_bytes, "bytes_per_cell_step": STEP_ARRAYS * esize,
+             "achieved_gbs": step_bytes / (ms / args.steps * 1e-3) / 1e9}
     whole["frac_of_peak"] = whole["achieved_gbs"] / peak
     kernel_split = {k: round(v[0], 4) for k, v in sorted(per.items(), key=lambda kv: -kv[1][0]) if v[1]}
+    if reset:
+        s.restore()
+    return s, {"value": ws * cells * args.steps / (ms * 1e-3), "ms_per_step": ms / args.steps,
+               "launches": launches, "roofline": roof, "whole_step": whole,
+               "kernel_ms_one_step": kernel_split, "clocks": clk.summary(), "reset": reset}
+
+
+def rel_l2(a, b) -> float:
+    nb = float(np.linalg.norm(b))
+    d = float(np.linalg.norm(a - b))
+    return d / nb if nb > 0 else d
+
+
+def mixed_error(s64, s32, nsteps: int) -> dict:
+    """Both forms from the same seeded state for nsteps: relative L2 of the
+    interior fields, of the velocity vector and of the Nusselt / kinetic-energy
+    series."""
+    s64.restore(); s32.restore()
+    s64.step(nsteps); s32.step(nsteps)
+    out, du2, u2 = {}, 0.0, 0.0
+    for f in ("U", "V", "W", "T", "P"):
+        a, b = s32.get(f)[1:-1, 1:-1, 1:-1], s64.get(f)[1:-1, 1:-1, 1:-1]
+        out[f] = rel_l2(a, b)
+        if f in "UVW":
+            du2 += float(np.linalg.norm(a - b)) ** 2
+            u2 += float(np.linalg.norm(b)) ** 2
+    out["velocity"] = (du2 / u2) ** 0.5 if u2 > 0 else du2 ** 0.5
+    h64, h32 = s64.history(0, nsteps), s32.history(0, nsteps)
+    for col, n in ((4, "Nu_bot"), (5, "Nu_top"), (6, "KE")):
+        out[n] = rel_l2(h32[:, col], h64[:, col])
+    out["steps"] = nsteps
+    s64.restore(); s32.restore()
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--workload", default="rb256_water_fp64", choices=sorted(WORKLOADS))
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the FP32-mixed counterpart of an FP64 workload")
+    args = ap.parse_args()
+    workload = args.workload
+    cfg = dict(WORKLOADS[workload])
+    if args.impl == "reference":
+        return run_reference(args, cfg, workload)
+
+    ws, rank, local = dist_setup(args.gpus)
+    import torch
+    import pascal_tcs_b200 as P
+
+    torch.cuda.set_device(local)
+    stream = torch.cuda.Stream()
+    cfg["device"] = local
+    n1, n2, n3 = cfg["n1m"], cfg["n2m"], cfg["n3m"]
+    cells = n1 * n2 * n3
+    fp32 = bool(cfg.get("precision", 0))
+    s, m = device_run(P, torch, cfg, workload, args, ws, local, stream)
+    reset = m["reset"]
 
     # end to end through the C ABI with host buffers: fields uploaded from pinned
     # host memory, K steps driven one reference routine at a time (each step
@@ -344,8 +397,22 @@ def main():
         e2e = {"value": ws * cells * args.steps / el, "unit": "cell-steps/s",
                "h2d_bytes_per_step": 5 * nbytes / args.steps,
                "d2h_bytes_per_step": 5 * nbytes / args.steps + 2 * 11 * 8,
-               "what": "upload T,U,V,W,P from pinned host memory, K steps through the per-routine C-ABI "
-                       "entry points (maxDivU, CFL, dt read back every step), download T,U,V,W,P"}
+               "what": "upload T,U,V,W,P (FP64) from pinned host memory, K steps through the per-routine C-ABI "
+                       "entry points (maxDivU, CFL, dt read back every step), download T,U,V,W,P (FP64)"}
+
+    # the FP32-mixed counterpart of an FP64 workload, with its error against FP64
+    mixed = None
+    twin = workload.replace("_fp64", "_mixed")
+    if not fp32 and twin in WORKLOADS and not args.no_mixed:
+        cfg32 = dict(WORKLOADS[twin], device=local)
+        s32, m32 = device_run(P, torch, cfg32, twin, args, ws, local, stream)
+        nerr = reset if reset else 200
+        err = mixed_error(s, s32, nerr)
+        mixed = {"workload": twin, "value": m32["value"], "unit": "cell-steps/s", "ms_per_step": m32["ms_per_step"],
+                 "speedup_vs_fp64": m32["value"] / m["value"], "error_vs_fp64": err,
+                 "roofline": m32["roofline"], "whole_step": m32["whole_step"], "gpu_launches": m32["launches"],
+                 "kernel_ms_one_step": m32["kernel_ms_one_step"], "clocks": m32["clocks"]}
+        del s32
 
     base = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -353,20 +420,22 @@ def main():
         base.pop("seconds", None)
 
     if rank == 0:
-        line = {"metric": "cell-steps/s (FP64 plain, one 256^3 case per GPU)", "value": value,
+        form = "FP32-mixed" if fp32 else "FP64 plain"
+        line = {"metric": f"cell-steps/s ({form}, one {n1}x{n2}x{n3} case per GPU)", "value": m["value"],
                 "unit": "cell-steps/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
-                "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "f64",
+                "ms_per_step": m["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32+f64" if fp32 else "f64",
                 "data": "synthetic: seeded conduction profile + uniform noise 0.01, zero velocity",
-                "config": {"workload": workload, "grid": [n1, n2, n3], "properties": "water",
-                           "Ra": cfg["Ra"], "Pr": cfg["Pr"], "dt": cfg["dtStart"],
+                "config": {"workload": workload, "grid": [n1, n2, n3],
+                           "properties": "water" if cfg["property_set"] == 1 else "constant",
+                           "Ra": cfg["Ra"], "Pr": cfg["Pr"], "dt": cfg["dtStart"], "precision": form,
                            "parallelism": "replicas" if ws > 1 else "single",
-                           "l2": "inputs larger than L2 (each field %.0f MB)" % (8 * np.prod(s.shape) / 1e6),
+                           "l2": "inputs larger than L2 (each field %.0f MB)" % ((4 if fp32 else 8) * np.prod(s.shape) / 1e6),
                            "timing": "eager launches with one event-probed kernel; CUDA events on the solver stream",
                            "restart_every_steps": reset or None},
-                "gpu_launches": launches, "roofline": roof, "whole_step": whole,
-                "kernel_ms_one_step": kernel_split, "clocks": clk.summary(), "e2e": e2e,
-                "cpu_baseline": base}
+                "gpu_launches": m["launches"], "roofline": m["roofline"], "whole_step": m["whole_step"],
+                "kernel_ms_one_step": m["kernel_ms_one_step"], "clocks": m["clocks"], "e2e": e2e,
+                "fp32_mixed": mixed, "cpu_baseline": base}
         print(json.dumps(line))
     if ws > 1:
         import torch.distributed as dist

@@ -168,7 +168,7 @@ struct tcs_ctx {
     std::vector<GraphEntry> graphs;
     ProbeState probe;
     int partials = 0;
-    void *snap[7] = {};                  // on-device copy of T, U, V, W, P, dPhat, dP0
+    void *snap[10] = {};                 // on-device copy of T, U, V, W, P, dPhat, dP0 (+ U, V, W low words)
     double snap_scal[S_NSCAL] = {};
     bool have_snap = false;
 };
@@ -325,7 +325,21 @@ static void *field_ptr(tcs_ctx *c, int f)
 }
 
 template <class R> static void swap_T(Ctx<R> &x) { std::swap(x.f.T, x.f.Tn); }
-template <class R> static void swap_UVW(Ctx<R> &x) { std::swap(x.f.U, x.f.Un); std::swap(x.f.V, x.f.Vn); std::swap(x.f.W, x.f.Wn); }
+template <class R> static void swap_UVW(Ctx<R> &x)
+{
+    std::swap(x.f.U, x.f.Un); std::swap(x.f.V, x.f.Vn); std::swap(x.f.W, x.f.Wn);
+    std::swap(x.f.Ulo, x.f.Unlo); std::swap(x.f.Vlo, x.f.Vnlo); std::swap(x.f.Wlo, x.f.Wnlo);
+}
+
+// The low word of a velocity field (FP32 form), else null.
+template <class R>
+static R *lo_ptr_t(FieldsT<R> &F, int f)
+{
+    switch (f) {
+    case TCS_F_U: return F.Ulo; case TCS_F_V: return F.Vlo; case TCS_F_W: return F.Wlo;
+    default: return nullptr;
+    }
+}
 template <class R> static void swap_phat(Ctx<R> &x) { std::swap(x.f.dPhat, x.f.dPhatn); std::swap(x.f.dP0, x.f.dP0n); }
 
 static int flush_pending(tcs_ctx *c)
@@ -368,6 +382,7 @@ int tcs_create(const tcs_config *cfg, tcs_ctx **out)
     g.NP = (long long)(N1 + 2) * (N2 + 2) * (N3 + 2);
     set_properties(*cfg, g.ph);
     g.phd = g.ph;
+    g.kdeg2 = (g.ph.c13 == 0.0 && g.ph.c14 == 0.0 && g.ph.c15 == 0.0) ? 1 : 0;
     mesh_periodic(cfg->uniform1, g.ph.L1, cfg->gamma1, N1, c->hm[0], c->hm[1], c->hm[2]);
     mesh_wall(cfg->uniform2, g.ph.L2, cfg->gamma2, N2, c->hm[3], c->hm[4], c->hm[5]);
     mesh_periodic(cfg->uniform3, g.ph.L3, cfg->gamma3, N3, c->hm[6], c->hm[7], c->hm[8]);
@@ -409,6 +424,10 @@ int tcs_create(const tcs_config *cfg, tcs_ctx **out)
         if (!r) r = dalloc(c, &F.Mu2, (size_t)(N2 + 2) * (N3 + 2));
         if (!r) r = dalloc(c, &F.iR2, (size_t)(N2 + 2) * (N3 + 2));
         if (!r) r = dalloc(c, &F.S, (size_t)c->cx.h1p * N2 * N3);
+        if (HasLo<R>::on) {
+            R **lo[] = {&F.Ulo, &F.Vlo, &F.Wlo, &F.Unlo, &F.Vnlo, &F.Wnlo};
+            for (R **p : lo) if (!r) r = dalloc(c, p, NP);
+        }
     };
     on_ctx(c, alloc_fields);
     if (c->fp32 && !r) r = dalloc(c, &c->stage, NP);
@@ -438,19 +457,8 @@ int tcs_create(const tcs_config *cfg, tcs_ctx **out)
         for (int e = 0; e < n; e++) w[e] = make_double2(std::cos(2.0 * M_PI * (double)e / (double)n), -std::sin(2.0 * M_PI * (double)e / (double)n));
         return w;
     };
-    auto twid_f = [&](int n) {
-        const std::vector<double2> w = twid(n);
-        std::vector<float2> v(n);
-        for (int e = 0; e < n; e++) v[e] = make_float2((float)w[e].x, (float)w[e].y);
-        return v;
-    };
-    if (c->fp32) {
-        r = r ? r : upload_vec(c, twid_f(N1), &c->cf.f.tw1);
-        r = r ? r : upload_vec(c, twid_f(N3), &c->cf.f.tw3);
-    } else {
-        r = r ? r : upload_vec(c, twid(N1), &F.tw1);
-        r = r ? r : upload_vec(c, twid(N3), &F.tw3);
-    }
+    r = r ? r : upload_vec(c, twid(N1), &F.tw1);
+    r = r ? r : upload_vec(c, twid(N3), &F.tw3);
     {   // Pbc_a, Pbc_b (module_solve_pressure.f90:720-730)
         const int n2sub = N2 + 1, n2msub = N2;
         const double s1 = (dmx2[1] + dmx2[2]) * (dmx2[1] + dmx2[2]);
@@ -478,9 +486,10 @@ int tcs_create(const tcs_config *cfg, tcs_ctx **out)
         gf.N1 = g.N1; gf.N2 = g.N2; gf.N3 = g.N3; gf.P1 = g.P1; gf.P2 = g.P2; gf.NP = g.NP;
         gf.d1 = g.d1; gf.d2 = g.d2; gf.d3 = g.d3;
         gf.ph = phys_cast<float>(g.ph); gf.phd = g.ph;
-        gf.scal = g.scal;
+        gf.scal = g.scal; gf.kdeg2 = g.kdeg2;
         FieldsT<float> &ff = c->cf.f;
         ff.dxk2 = F.dxk2; ff.dzk = F.dzk; ff.fam = F.fam; ff.fap = F.fap;
+        ff.tw1 = F.tw1; ff.tw3 = F.tw3;
         ff.part = F.part; ff.hist = F.hist; ff.hist_cap = F.hist_cap;
     }
 
@@ -600,14 +609,16 @@ static int copy_field(tcs_ctx *c, int f, double *host, bool up, bool async)
     void *d = field_ptr(c, f);
     if (!d) return set_err(TCS_ERR_ARG, "unknown field");
     if (c->fp32) {   // FP64 host arrays pass through the FP64 staging buffer
-        float *df = (float *)d;
+        float *df = (float *)d, *lo = lo_ptr_t(c->cf.f, f);
         if (up) {
             CK(cudaMemcpyAsync(c->stage, host, NP * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-            launch_convert_in<float>(c->stage, df, (long long)NP, c->stream);
+            if (lo) launch_split(c->stage, df, lo, (long long)NP, c->stream);
+            else launch_convert_in<float>(c->stage, df, (long long)NP, c->stream);
             if (f == TCS_F_T) launch_convert_in<float>(c->stage, c->cf.f.Tn, (long long)NP, c->stream);
             c->ghost_ok &= ~(1u << f);
         } else {
-            launch_convert<float>(df, c->stage, (long long)NP, c->stream);
+            if (lo) launch_join(df, lo, c->stage, (long long)NP, c->stream);
+            else launch_convert<float>(df, c->stage, (long long)NP, c->stream);
             CK(cudaMemcpyAsync(host, c->stage, NP * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
         }
         if ((r = take_launch_error())) return r;
@@ -665,7 +676,10 @@ int tcs_momentum_coeffi_clean(tcs_ctx *c) { ENTER(c); return TCS_OK; }
 static void ensure_ghosts(tcs_ctx *c, int f)
 {
     if (c->ghost_ok & (1u << f)) return;
-    on_ctx(c, [&](auto &x) { launch_ghost(x, field_ptr_t(x.f, f), c->stream); });
+    on_ctx(c, [&](auto &x) {
+        launch_ghost(x, field_ptr_t(x.f, f), c->stream);
+        if (auto *lo = lo_ptr_t(x.f, f)) launch_ghost(x, lo, c->stream);
+    });
     c->ghost_ok |= (1u << f);
 }
 
@@ -850,10 +864,10 @@ int tcs_set_tuning(tcs_ctx *c, int knob, int value)
         if (row_bytes(2, false) * value * a.LS + 4096 * 4 > 200 * 1024) return set_err(TCS_ERR_ARG, "too many lines for shared memory");
         x.tl_modal = value; break; }
     case TCS_TUNE_FFT_LINES_X:
-        if ((size_t)value * g.N1 * 5 * e > 200 * 1024) return set_err(TCS_ERR_ARG, "too many lines for shared memory");
+        if ((size_t)value * g.N1 * (32 + e) > 200 * 1024) return set_err(TCS_ERR_ARG, "too many lines for shared memory");
         x.fft_lines_x = value; break;
     case TCS_TUNE_FFT_LINES_Z:
-        if ((size_t)value * g.N3 * 4 * e > 200 * 1024) return set_err(TCS_ERR_ARG, "too many lines for shared memory");
+        if ((size_t)value * g.N3 * 32 > 200 * 1024) return set_err(TCS_ERR_ARG, "too many lines for shared memory");
         x.fft_lines_z = value; break;
     default: return set_err(TCS_ERR_ARG, "unknown tuning knob");
     }
@@ -941,6 +955,17 @@ int tcs_step(tcs_ctx *c, int nsteps, int *done)
     return TCS_OK;
 }
 
+// The buffers a snapshot holds: T, U, V, W, P, dPhat, dP0 and, in the FP32
+// form, the low words of U, V, W.
+static int snap_buffers(tcs_ctx *c, void **b)
+{
+    const int fl[7] = {TCS_F_T, TCS_F_U, TCS_F_V, TCS_F_W, TCS_F_P, TCS_F_DPHAT, TCS_F_DP0};
+    for (int q = 0; q < 7; q++) b[q] = field_ptr(c, fl[q]);
+    if (!c->fp32) return 7;
+    b[7] = c->cf.f.Ulo; b[8] = c->cf.f.Vlo; b[9] = c->cf.f.Wlo;
+    return 10;
+}
+
 // On-device checkpoint of the state a time step reads (T, U, V, W, P, dPhat,
 // dP0 and the scalars): a restart that needs no host round trip.
 int tcs_snapshot(tcs_ctx *c)
@@ -949,12 +974,13 @@ int tcs_snapshot(tcs_ctx *c)
     int r = flush_pending(c);
     if (r) return r;
     const size_t bytes = (size_t)c->cx.g.NP * esize(c);
-    const int fl[7] = {TCS_F_T, TCS_F_U, TCS_F_V, TCS_F_W, TCS_F_P, TCS_F_DPHAT, TCS_F_DP0};
-    for (int q = 0; q < 7; q++) {
+    void *src[10];
+    const int n = snap_buffers(c, src);
+    for (int q = 0; q < n; q++) {
         unsigned char *sp = (unsigned char *)c->snap[q];
         if (!sp && (r = dalloc(c, &sp, bytes))) return r;
         c->snap[q] = sp;
-        CK(cudaMemcpyAsync(c->snap[q], field_ptr(c, fl[q]), bytes, cudaMemcpyDeviceToDevice, c->stream));
+        CK(cudaMemcpyAsync(c->snap[q], src[q], bytes, cudaMemcpyDeviceToDevice, c->stream));
     }
     CK(cudaMemcpyAsync(c->snap_scal, c->cx.g.scal, sizeof(c->snap_scal), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
@@ -969,9 +995,10 @@ int tcs_restore(tcs_ctx *c)
     int r = flush_pending(c);
     if (r) return r;
     const size_t bytes = (size_t)c->cx.g.NP * esize(c);
-    const int fl[7] = {TCS_F_T, TCS_F_U, TCS_F_V, TCS_F_W, TCS_F_P, TCS_F_DPHAT, TCS_F_DP0};
-    for (int q = 0; q < 7; q++)
-        CK(cudaMemcpyAsync(field_ptr(c, fl[q]), c->snap[q], bytes, cudaMemcpyDeviceToDevice, c->stream));
+    void *dst[10];
+    const int n = snap_buffers(c, dst);
+    for (int q = 0; q < n; q++)
+        CK(cudaMemcpyAsync(dst[q], c->snap[q], bytes, cudaMemcpyDeviceToDevice, c->stream));
     CK(cudaMemcpyAsync(c->cx.g.scal, c->snap_scal, sizeof(c->snap_scal), cudaMemcpyHostToDevice, c->stream));
     c->ghost_ok |= (1u << TCS_F_T) | (1u << TCS_F_U) | (1u << TCS_F_V) | (1u << TCS_F_W) | (1u << TCS_F_P) | (1u << TCS_F_DPHAT);
     return TCS_OK;

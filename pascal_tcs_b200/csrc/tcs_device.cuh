@@ -80,6 +80,7 @@ struct GridT {
     PhysT<R> ph;                // constants in the field type
     Phys phd;                   // FP64 constants
     double *scal;               // device scalars (S_*)
+    int kdeg2;                  // KPP has no terms above t^2 (c13 = c14 = c15 = 0: water, glycerol, constant)
 };
 using Grid = GridT<double>;
 
@@ -133,19 +134,27 @@ __device__ __forceinline__ void store_periodic(const GridT<R> &g, V *a, int i, i
 // (module_solve_thermal.f90:129-154), evaluated at the point where the
 // stencil needs them instead of being stored.
 // ---------------------------------------------------------------------------
-// Horner forms of KPP = c10 (1 + c11 t + ... + c15 t^5) / KPP0 and its derivative.
+// Horner forms of KPP = c10 (1 + c11 t + ... + c15 t^5) / KPP0 and its
+// derivative.  With d2 (c13 = c14 = c15 = 0) the zero leading terms are
+// skipped; in Horner form they only add exact zeros, so the values are the same.
 template <class R>
-__device__ __forceinline__ void kpp_eval(const PhysT<R> &p, R T, R &kpp, R &dkpp)
+__device__ __forceinline__ void kpp_eval(const PhysT<R> &p, bool d2, R T, R &kpp, R &dkpp)
 {
     const R t = p.DeltaT * T;
-    kpp = p.cK * (R(1) + t * (p.c11 + t * (p.c12 + t * (p.c13 + t * (p.c14 + t * p.c15)))));
-    dkpp = p.cK * (p.c11 + t * (p.k2 + t * (p.k3 + t * (p.k4 + t * p.k5))));
+    if (d2) {
+        kpp = p.cK * (R(1) + t * (p.c11 + t * p.c12));
+        dkpp = p.cK * (p.c11 + t * p.k2);
+    } else {
+        kpp = p.cK * (R(1) + t * (p.c11 + t * (p.c12 + t * (p.c13 + t * (p.c14 + t * p.c15)))));
+        dkpp = p.cK * (p.c11 + t * (p.k2 + t * (p.k3 + t * (p.k4 + t * p.k5))));
+    }
 }
 
 template <class R>
-__device__ __forceinline__ R kpp_only(const PhysT<R> &p, R T)
+__device__ __forceinline__ R kpp_only(const PhysT<R> &p, bool d2, R T)
 {
     const R t = p.DeltaT * T;
+    if (d2) return p.cK * (R(1) + t * (p.c11 + t * p.c12));
     return p.cK * (R(1) + t * (p.c11 + t * (p.c12 + t * (p.c13 + t * (p.c14 + t * p.c15)))));
 }
 
@@ -197,6 +206,12 @@ template <class R, int NR>
 struct Coef {
     R a, b, c, d[NR];
 };
+
+// Quotients of the line solver (correctly rounded in both forms: with the
+// hardware's approximate FP32 reciprocal the y-sweep of solvedV kept 6e-6
+// relative error after its refinement pass, against 5e-7 with this).
+template <class R>
+__device__ __forceinline__ R qdiv(R a, R b) { return a / b; }
 // Solve one line held in shared memory (normalised rows: b == 1).
 // A, C: coefficient rows; D: NR right-hand sides spaced by DS.
 template <class R, int NR>
@@ -218,7 +233,7 @@ __device__ __forceinline__ void warp_solve_line(R *A, R *C, R *D, int DS, const 
         for (int q = 0; q < NR; q++) dm1[q] = d[q * DS + 1];
         for (int r = 2; r < m; r++) {
             const R ar = a[r];
-            const R rr = R(1) / (R(1) - ar * cm1);
+            const R rr = qdiv(R(1), R(1) - ar * cm1);
 #pragma unroll
             for (int q = 0; q < NR; q++) { dm1[q] = rr * (d[q * DS + r] - ar * dm1[q]); d[q * DS + r] = dm1[q]; }
             cm1 = rr * c[r]; c[r] = cm1;
@@ -241,7 +256,7 @@ __device__ __forceinline__ void warp_solve_line(R *A, R *C, R *D, int DS, const 
             }
             // closure of row 0 with row 1 (pascal_tdma.f90:531-535)
             const R c0 = c[0];
-            const R rr = R(1) / (R(1) - ap1 * c0);
+            const R rr = qdiv(R(1), R(1) - ap1 * c0);
 #pragma unroll
             for (int q = 0; q < NR; q++) D0[q] = rr * (d[q * DS] - c0 * dp1[q]);
             A0 = rr * a[0];
@@ -274,31 +289,33 @@ __device__ __forceinline__ void warp_solve_line(R *A, R *C, R *D, int DS, const 
     if (!act) { al = R(0); be = R(1); ga = R(0);
 #pragma unroll
         for (int q = 0; q < NR; q++) de[q] = R(0); }
-    // parallel cyclic reduction across the P lanes
+    // parallel cyclic reduction across the P lanes; every lane forms the
+    // reciprocal of its own diagonal once per level and its neighbours read it
     for (int s = 1; s < P; s <<= 1) {
         int lo = lane - s, hi = lane + s;
         bool lo_ok = true, hi_ok = true;
         if (cyc) { lo = (lo + P) & (P - 1); hi = hi & (P - 1); }
         else { lo_ok = lo >= 0; hi_ok = hi < P; lo = lo_ok ? lo : lane; hi = hi_ok ? hi : lane; }
-        R alm = __shfl_sync(0xffffffffu, al, lo), bem = __shfl_sync(0xffffffffu, be, lo), gam = __shfl_sync(0xffffffffu, ga, lo);
-        R alp = __shfl_sync(0xffffffffu, al, hi), bep = __shfl_sync(0xffffffffu, be, hi), gap = __shfl_sync(0xffffffffu, ga, hi);
+        const R rbe = qdiv(R(1), be);
+        R alm = __shfl_sync(0xffffffffu, al, lo), rbm = __shfl_sync(0xffffffffu, rbe, lo), gam = __shfl_sync(0xffffffffu, ga, lo);
+        R alp = __shfl_sync(0xffffffffu, al, hi), rbp = __shfl_sync(0xffffffffu, rbe, hi), gap = __shfl_sync(0xffffffffu, ga, hi);
         R dem[NR], dep[NR];
 #pragma unroll
         for (int q = 0; q < NR; q++) { dem[q] = __shfl_sync(0xffffffffu, de[q], lo); dep[q] = __shfl_sync(0xffffffffu, de[q], hi); }
-        if (!lo_ok) { alm = R(0); bem = R(1); gam = R(0);
+        if (!lo_ok) { alm = R(0); rbm = R(1); gam = R(0);
 #pragma unroll
             for (int q = 0; q < NR; q++) dem[q] = R(0); }
-        if (!hi_ok) { alp = R(0); bep = R(1); gap = R(0);
+        if (!hi_ok) { alp = R(0); rbp = R(1); gap = R(0);
 #pragma unroll
             for (int q = 0; q < NR; q++) dep[q] = R(0); }
-        const R k1 = al / bem, k2 = ga / bep;
+        const R k1 = al * rbm, k2 = ga * rbp;
         const R nal = -k1 * alm, nga = -k2 * gap;
         const R nbe = be - k1 * gam - k2 * alp;
 #pragma unroll
         for (int q = 0; q < NR; q++) de[q] = de[q] - k1 * dem[q] - k2 * dep[q];
         al = nal; be = nbe; ga = nga;
     }
-    const R den = R(1) / (al + be + ga);
+    const R den = qdiv(R(1), al + be + ga);
     R z[NR], xl[NR];
     const int nxt = cyc ? ((lane + 1) & (P - 1)) : (lane + 1 < 32 ? lane + 1 : lane);
 #pragma unroll
@@ -321,7 +338,7 @@ __device__ __forceinline__ void warp_solve_line(R *A, R *C, R *D, int DS, const 
 
 // The kernel.  Prob supplies:
 //   using Real (row type: the field type, or double for FP64 solves of FP32 data);
-//   static constexpr int NRHS;  static constexpr bool CONTIG (rows contiguous in memory);
+//   static constexpr int NRHS, MINB (blocks per SM);  static constexpr bool CONTIG (rows contiguous in memory);
 //   struct State; __device__ State prepare()   -> per-block scalars (dt, stale values)
 //   __device__ bool skip(), line_ok(int l)
 //   __device__ Coef<Real, NRHS> build(int l, int r, const State &)
@@ -329,6 +346,19 @@ __device__ __forceinline__ void warp_solve_line(R *A, R *C, R *D, int DS, const 
 // TL (lines per block) is a power of two; blockDim.x is 256.
 template <class R>
 struct Refine { static constexpr bool on = std::is_same<R, float>::value; };
+
+// Blocks per SM a line-solver family is compiled for (each Prob's MINB; the
+// register budget is 65536 / (256 MINB), and fit_tl sizes the lines per block
+// to the matching shared-memory share).  Measured on B200 at 256^3: the FP64
+// z-sweep stencils need 128 registers and spill below that; the FP64 x and y
+// sweeps run fastest at 4 blocks (64 registers, no spills); the refined FP32
+// rows need 28 B each, so FP32 sweeps and the modal solves run best at 3.
+template <class R>
+struct LineOcc {
+    static constexpr int z = std::is_same<R, float>::value ? 3 : 2;
+    static constexpr int xy = std::is_same<R, float>::value ? 3 : 4;
+    static constexpr int modal = 3;
+};
 
 // Shared-memory words (of the row type) per row: A, C, D[NR]; refined rows
 // also keep the built rows A0, B0, C0, D0[NR].
@@ -339,7 +369,7 @@ __host__ __device__ constexpr int line_words()
 }
 
 template <class Prob>
-__global__ void __launch_bounds__(256, 2) line_solve_kernel(Prob prob, LinePlan lp)
+__global__ void __launch_bounds__(256, Prob::MINB) line_solve_kernel(Prob prob, LinePlan lp)
 {
     using R = typename Prob::Real;
     constexpr int NR = Prob::NRHS;
@@ -371,7 +401,7 @@ __global__ void __launch_bounds__(256, 2) line_solve_kernel(Prob prob, LinePlan 
 #pragma unroll
             for (int q = 0; q < NR; q++) cf.d[q] = R(0);
         }
-        const R rb = R(1) / cf.b;
+        const R rb = qdiv(R(1), cf.b);
         sA[pos] = cf.a * rb; sC[pos] = cf.c * rb;
 #pragma unroll
         for (int q = 0; q < NR; q++) sD[q * DS + pos] = cf.d[q] * rb;
@@ -389,34 +419,34 @@ __global__ void __launch_bounds__(256, 2) line_solve_kernel(Prob prob, LinePlan 
     }
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    for (int l = warp; l < TL; l += nw)
+    for (int l = warp; l < TL; l += nw) {
         warp_solve_line<R, NR>(sA + l * LS, sC + l * LS, sD + l * LS, DS, lp, lane);
-    __syncthreads();
-    if (REF) {
-        // FP64 residual of the first solution against the built rows; it
-        // replaces D0, and the normalised rows are restored for the second solve.
-        for (int t = threadIdx.x; t < TL * n; t += blockDim.x) {
-            const int l = t / n, r = t - l * n;
-            const int pos = l * LS + spos[r];
-            const int rm = r > 0 ? r - 1 : (lp.cyclic ? n - 1 : -1);
-            const int rp = r < n - 1 ? r + 1 : (lp.cyclic ? 0 : -1);
-            const int pm = l * LS + spos[rm >= 0 ? rm : r], pp = l * LS + spos[rp >= 0 ? rp : r];
-            const double a = (double)sA0[pos], b = (double)sB0[pos], c = (double)sC0[pos];
-            const R rb = R(1) / sB0[pos];
+        if (REF) {
+            // The warp refines its own line: FP64 residual of the first
+            // solution against the built rows (it replaces D0), the
+            // normalised rows restored, and one more solve for the correction.
+            __syncwarp();
+            for (int r = lane; r < n; r += 32) {
+                const int pos = l * LS + spos[r];
+                const int rm = r > 0 ? r - 1 : (lp.cyclic ? n - 1 : -1);
+                const int rp = r < n - 1 ? r + 1 : (lp.cyclic ? 0 : -1);
+                const int pm = l * LS + spos[rm >= 0 ? rm : r], pp = l * LS + spos[rp >= 0 ? rp : r];
+                const double a = (double)sA0[pos], b = (double)sB0[pos], c = (double)sC0[pos];
+                const R rb = qdiv(R(1), sB0[pos]);
 #pragma unroll
-            for (int q = 0; q < NR; q++) {
-                const double xm = rm >= 0 ? (double)sD[q * DS + pm] : 0.0;
-                const double xp = rp >= 0 ? (double)sD[q * DS + pp] : 0.0;
-                const double res = (double)sD0[q * DS + pos] - (a * xm + b * (double)sD[q * DS + pos] + c * xp);
-                sD0[q * DS + pos] = (R)res * rb;
+                for (int q = 0; q < NR; q++) {
+                    const double xm = rm >= 0 ? (double)sD[q * DS + pm] : 0.0;
+                    const double xp = rp >= 0 ? (double)sD[q * DS + pp] : 0.0;
+                    const double res = (double)sD0[q * DS + pos] - (a * xm + b * (double)sD[q * DS + pos] + c * xp);
+                    sD0[q * DS + pos] = (R)res * rb;
+                }
+                sA[pos] = sA0[pos] * rb; sC[pos] = sC0[pos] * rb;
             }
-            sA[pos] = sA0[pos] * rb; sC[pos] = sC0[pos] * rb;
-        }
-        __syncthreads();
-        for (int l = warp; l < TL; l += nw)
+            __syncwarp();
             warp_solve_line<R, NR>(sA + l * LS, sC + l * LS, sD0 + l * LS, DS, lp, lane);
-        __syncthreads();
+        }
     }
+    __syncthreads();
     auto out = [&](int l, int r) {
         if (!prob.line_ok(l)) return;
         const int pos = l * LS + spos[r];

@@ -14,6 +14,11 @@ struct FieldsT {
     // still read the old values (T in the thermal y sweep, U/V/W in the fused
     // pseudo-update, dPhat/dP0 in the projection)
     R *Tn, *Un, *Vn, *Wn, *dPhatn, *dP0n;
+    // FP32 form only: low words of the velocity (U = U + Ulo to FP64 accuracy)
+    // and of its second buffers.  The stencils read the FP32 high word; the
+    // pressure right-hand side, the projection and the diagnostics read both,
+    // so the storage rounding of the velocity never reaches the divergence.
+    R *Ulo, *Vlo, *Wlo, *Unlo, *Vnlo, *Wnlo;
     // per-step increments and pressure correction
     R *dU, *dV, *dW, *dP;
     // interior stage scratch (padded layout)
@@ -24,8 +29,8 @@ struct FieldsT {
     cplx_t<R> *S;
     // modified wavenumbers and y coefficients of the modal solves (FP64 in both forms)
     const double *dxk2, *dzk, *fam, *fap;
-    // FFT twiddles exp(-2 pi i e / n) for n = N1 and n = N3
-    const cplx_t<R> *tw1, *tw3;
+    // FFT twiddles exp(-2 pi i e / n) for n = N1 and n = N3 (FFT arithmetic is FP64 in both forms)
+    const double2 *tw1, *tw3;
     // reduction scratch
     double *part;
     double *hist;            // per-step diagnostics history (7 doubles per step)
@@ -36,5 +41,16 @@ struct FieldsT {
 // fields stay at the state of the step that blew up (main.f90:208-212).
 template <class R>
 __device__ __forceinline__ bool blown(const GridT<R> &g) { return g.scal[S_BLOWUP] != 0.0; }
+
+// The FP32 form keeps low words of the velocity.
+template <class R> struct HasLo { static constexpr bool on = std::is_same<R, float>::value; };
+
+// v = hi + lo in FP64, and its split back into an FP32 pair.
+__device__ __forceinline__ double join(float hi, float lo) { return (double)hi + (double)lo; }
+__device__ __forceinline__ void split(double v, float &hi, float &lo)
+{
+    hi = (float)v;
+    lo = (float)(v - (double)hi);
+}
 
 } // namespace tcs

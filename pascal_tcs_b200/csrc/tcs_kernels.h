@@ -58,6 +58,17 @@ inline size_t line_smem(const LinePlan &lp)
     return (size_t)line_words<Prob>() * lp.TL * lp.LS * sizeof(typename Prob::Real) + (size_t)lp.n * sizeof(int);
 }
 
+// Lines per block: the requested count, halved until MINB blocks fit in the
+// SM's shared memory (228 KB, 1 KB reserved per block).
+template <class Prob>
+inline int fit_tl(int n, bool cyclic, int want)
+{
+    const size_t budget = (size_t)228 * 1024 / Prob::MINB - 1024;
+    int tl = want;
+    while (tl > 1 && line_smem<Prob>(make_line_plan(n, cyclic, tl)) > budget) tl /= 2;
+    return tl;
+}
+
 template <class Prob>
 inline void launch_lines(const Prob &p, const LinePlan &lp, dim3 grid, cudaStream_t s, int kid, const Shapes &cx)
 {
@@ -90,5 +101,7 @@ template <class R> void launch_post(const Ctx<R> &cx, cudaStream_t s, int record
 template <class R> void launch_ghost(const Ctx<R> &cx, R *a, cudaStream_t s);
 template <class R> void launch_convert(const R *src, double *dst, long long n, cudaStream_t s);   // field -> FP64 staging
 template <class R> void launch_convert_in(const double *src, R *dst, long long n, cudaStream_t s); // FP64 staging -> field
+void launch_join(const float *hi, const float *lo, double *dst, long long n, cudaStream_t s);       // FP32 pair -> FP64 staging
+void launch_split(const double *src, float *hi, float *lo, long long n, cudaStream_t s);          // FP64 staging -> FP32 pair
 
 } // namespace tcs

@@ -48,6 +48,7 @@ template <class R>
 struct DUZ {
     using Real = R;
     static constexpr int NRHS = 1;
+    static constexpr int MINB = LineOcc<R>::z;
     static constexpr bool CONTIG = false;
     GridT<R> g; FieldsT<R> f; int TL;
     __device__ bool skip() const { return blown(g); }
@@ -133,6 +134,7 @@ template <class R>
 struct DUX {
     using Real = R;
     static constexpr int NRHS = 1;
+    static constexpr int MINB = LineOcc<R>::xy;
     static constexpr bool CONTIG = true;
     GridT<R> g; FieldsT<R> f; int TL;
     __device__ bool skip() const { return blown(g); }
@@ -167,6 +169,7 @@ template <class R>
 struct DUY {
     using Real = R;
     static constexpr int NRHS = 1;
+    static constexpr int MINB = LineOcc<R>::xy;
     static constexpr bool CONTIG = false;
     GridT<R> g; FieldsT<R> f; int TL;
     __device__ bool skip() const { return blown(g); }
@@ -212,6 +215,7 @@ template <class R>
 struct DVZ {
     using Real = R;
     static constexpr int NRHS = 1;
+    static constexpr int MINB = LineOcc<R>::z;
     static constexpr bool CONTIG = false;
     GridT<R> g; FieldsT<R> f; int TL;
     __device__ bool skip() const { return blown(g); }
@@ -309,6 +313,7 @@ template <class R>
 struct DVX {
     using Real = R;
     static constexpr int NRHS = 1;
+    static constexpr int MINB = LineOcc<R>::xy;
     static constexpr bool CONTIG = true;
     GridT<R> g; FieldsT<R> f; int TL;
     __device__ bool skip() const { return blown(g); }
@@ -348,6 +353,7 @@ template <class R>
 struct DVY {
     using Real = R;
     static constexpr int NRHS = 1;
+    static constexpr int MINB = LineOcc<R>::xy;
     static constexpr bool CONTIG = false;
     GridT<R> g; FieldsT<R> f; int TL;
     __device__ bool skip() const { return blown(g); }
@@ -387,6 +393,7 @@ template <class R>
 struct DWZ {
     using Real = R;
     static constexpr int NRHS = 1;
+    static constexpr int MINB = LineOcc<R>::z;
     static constexpr bool CONTIG = false;
     GridT<R> g; FieldsT<R> f; int TL;
     __device__ bool skip() const { return blown(g); }
@@ -494,6 +501,7 @@ template <class R>
 struct DWX {
     using Real = R;
     static constexpr int NRHS = 1;
+    static constexpr int MINB = LineOcc<R>::xy;
     static constexpr bool CONTIG = true;
     GridT<R> g; FieldsT<R> f; int TL;
     __device__ bool skip() const { return blown(g); }
@@ -534,6 +542,7 @@ template <class R>
 struct DWY {
     using Real = R;
     static constexpr int NRHS = 1;
+    static constexpr int MINB = LineOcc<R>::xy;
     static constexpr bool CONTIG = false;
     GridT<R> g; FieldsT<R> f; int TL;
     __device__ bool skip() const { return blown(g); }
@@ -576,8 +585,9 @@ template <class R>
 void launch_solve_du(const Ctx<R> &cx, cudaStream_t s)
 {
     const GridT<R> &g = cx.g;
-    LinePlan pz = make_line_plan(g.N3, true, cx.tl_strided), px = make_line_plan(g.N1, true, cx.tl_contig);
-    LinePlan py = make_line_plan(g.N2, false, cx.tl_strided);
+    LinePlan pz = make_line_plan(g.N3, true, fit_tl<DUZ<R>>(g.N3, true, cx.tl_strided));
+    LinePlan px = make_line_plan(g.N1, true, fit_tl<DUX<R>>(g.N1, true, cx.tl_contig));
+    LinePlan py = make_line_plan(g.N2, false, fit_tl<DUY<R>>(g.N2, false, cx.tl_strided));
     launch_lines(DUZ<R>{g, cx.f, pz.TL}, pz, dim3((g.N1 + pz.TL - 1) / pz.TL, g.N2), s, K_DU_Z, cx);
     launch_lines(DUX<R>{g, cx.f, px.TL}, px, dim3((g.N2 + px.TL - 1) / px.TL, g.N3), s, K_DU_X, cx);
     launch_lines(DUY<R>{g, cx.f, py.TL}, py, dim3((g.N1 + py.TL - 1) / py.TL, g.N3), s, K_DU_Y, cx);
@@ -587,8 +597,9 @@ template <class R>
 void launch_solve_dv(const Ctx<R> &cx, cudaStream_t s)
 {
     const GridT<R> &g = cx.g;
-    LinePlan pz = make_line_plan(g.N3, true, cx.tl_strided), px = make_line_plan(g.N1, true, cx.tl_contig);
-    LinePlan py = make_line_plan(g.N2 - 1, false, cx.tl_strided);
+    LinePlan pz = make_line_plan(g.N3, true, fit_tl<DVZ<R>>(g.N3, true, cx.tl_strided));
+    LinePlan px = make_line_plan(g.N1, true, fit_tl<DVX<R>>(g.N1, true, cx.tl_contig));
+    LinePlan py = make_line_plan(g.N2 - 1, false, fit_tl<DVY<R>>(g.N2 - 1, false, cx.tl_strided));
     launch_lines(DVZ<R>{g, cx.f, pz.TL}, pz, dim3((g.N1 + pz.TL - 1) / pz.TL, g.N2 - 1), s, K_DV_Z, cx);
     launch_lines(DVX<R>{g, cx.f, px.TL}, px, dim3((g.N2 - 1 + px.TL - 1) / px.TL, g.N3), s, K_DV_X, cx);
     launch_lines(DVY<R>{g, cx.f, py.TL}, py, dim3((g.N1 + py.TL - 1) / py.TL, g.N3), s, K_DV_Y, cx);
@@ -598,8 +609,9 @@ template <class R>
 void launch_solve_dw(const Ctx<R> &cx, cudaStream_t s)
 {
     const GridT<R> &g = cx.g;
-    LinePlan pz = make_line_plan(g.N3, true, cx.tl_strided), px = make_line_plan(g.N1, true, cx.tl_contig);
-    LinePlan py = make_line_plan(g.N2, false, cx.tl_strided);
+    LinePlan pz = make_line_plan(g.N3, true, fit_tl<DWZ<R>>(g.N3, true, cx.tl_strided));
+    LinePlan px = make_line_plan(g.N1, true, fit_tl<DWX<R>>(g.N1, true, cx.tl_contig));
+    LinePlan py = make_line_plan(g.N2, false, fit_tl<DWY<R>>(g.N2, false, cx.tl_strided));
     launch_lines(DWZ<R>{g, cx.f, pz.TL}, pz, dim3((g.N1 + pz.TL - 1) / pz.TL, g.N2), s, K_DW_Z, cx);
     launch_lines(DWX<R>{g, cx.f, px.TL}, px, dim3((g.N2 + px.TL - 1) / px.TL, g.N3), s, K_DW_X, cx);
     launch_lines(DWY<R>{g, cx.f, py.TL}, py, dim3((g.N1 + py.TL - 1) / py.TL, g.N3), s, K_DW_Y, cx);
@@ -703,9 +715,19 @@ __global__ void pseudo_update_kernel(GridT<R> g, FieldsT<R> f)
     if (i > g.N1 || blown(g)) return;
     const long long c = ix(g, i, j, k);
     const R vmask = (j == 1) ? R(0.0) : R(1.0);     // dble(2 - j_indexS) on the lower plane
-    store_periodic(g, f.Un, i, j, k, f.U[c] + f.dU[c]);
-    store_periodic(g, f.Vn, i, j, k, f.V[c] + f.dV[c] * vmask);
-    store_periodic(g, f.Wn, i, j, k, f.W[c] + f.dW[c]);
+    if constexpr (HasLo<R>::on) {                    // FP32 form: FP64 sums of the high/low pairs
+        float h, lo;
+        split(join(f.U[c], f.Ulo[c]) + (double)f.dU[c], h, lo);
+        store_periodic(g, f.Un, i, j, k, h); store_periodic(g, f.Unlo, i, j, k, lo);
+        split(join(f.V[c], f.Vlo[c]) + (double)f.dV[c] * (double)vmask, h, lo);
+        store_periodic(g, f.Vn, i, j, k, h); store_periodic(g, f.Vnlo, i, j, k, lo);
+        split(join(f.W[c], f.Wlo[c]) + (double)f.dW[c], h, lo);
+        store_periodic(g, f.Wn, i, j, k, h); store_periodic(g, f.Wnlo, i, j, k, lo);
+    } else {
+        store_periodic(g, f.Un, i, j, k, f.U[c] + f.dU[c]);
+        store_periodic(g, f.Vn, i, j, k, f.V[c] + f.dV[c] * vmask);
+        store_periodic(g, f.Wn, i, j, k, f.W[c] + f.dW[c]);
+    }
 }
 
 template <class R>

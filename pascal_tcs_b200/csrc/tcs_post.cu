@@ -38,8 +38,15 @@ __global__ void __launch_bounds__(256) post_kernel(GridT<R> g, FieldsT<R> f)
         const long long q = t / g.N1;
         const int j = 1 + (int)(q % g.N2), k = 1 + (int)(q / g.N2);
         const long long c = ix(g, i, j, k);
-        const double Uc = ld(f.U + c), Vc = ld(f.V + c), Wc = ld(f.W + c);
-        const double Ux = ld(f.U + c + 1), Vy = ld(f.V + c + sj), Wz = ld(f.W + c + sk);   // FP32 values are exact in FP64
+        double Uc, Vc, Wc, Ux, Vy, Wz;
+        if constexpr (HasLo<R>::on) {     // the FP32 form's velocity is its high + low pair
+            Uc = join(ld(f.U + c), ld(f.Ulo + c)); Vc = join(ld(f.V + c), ld(f.Vlo + c)); Wc = join(ld(f.W + c), ld(f.Wlo + c));
+            Ux = join(ld(f.U + c + 1), ld(f.Ulo + c + 1)); Vy = join(ld(f.V + c + sj), ld(f.Vlo + c + sj));
+            Wz = join(ld(f.W + c + sk), ld(f.Wlo + c + sk));
+        } else {
+            Uc = ld(f.U + c); Vc = ld(f.V + c); Wc = ld(f.W + c);
+            Ux = ld(f.U + c + 1); Vy = ld(f.V + c + sj); Wz = ld(f.W + c + sk);
+        }
         const double dv = (Ux - Uc) * rdx1[i] + (Vy - Vc) * rdx2[j] + (Wz - Wc) * rdx3[k];
         const double cf = (fabs(Ux + Uc) / 2.0) * rdx1[i] + (fabs(Vy + Vc) / 2.0) * rdx2[j] + (fabs(Wz + Wc) / 2.0) * rdx3[k];
         mdiv = fmax(mdiv, dv);
@@ -174,6 +181,31 @@ template <class R>
 __global__ void convert_in_kernel(const double *src, R *dst, long long n)
 {
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) dst[t] = (R)src[t];
+}
+
+// FP64 staging <-> FP32 high/low pair (the FP32 form's velocity).
+__global__ void join_kernel(const float *hi, const float *lo, double *dst, long long n)
+{
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) dst[t] = join(hi[t], lo[t]);
+}
+__global__ void split_kernel(const double *src, float *hi, float *lo, long long n)
+{
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        float h, l;
+        split(src[t], h, l);
+        hi[t] = h; lo[t] = l;
+    }
+}
+
+void launch_join(const float *hi, const float *lo, double *dst, long long n, cudaStream_t s)
+{
+    join_kernel<<<4 * 148, 256, 0, s>>>(hi, lo, dst, n);
+    record_launch_error("join");
+}
+void launch_split(const double *src, float *hi, float *lo, long long n, cudaStream_t s)
+{
+    split_kernel<<<4 * 148, 256, 0, s>>>(src, hi, lo, n);
+    record_launch_error("split");
 }
 
 template <class R>

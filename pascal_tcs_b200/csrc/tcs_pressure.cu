@@ -15,10 +15,17 @@
 //   dp_wall     wall extrapolation of dP (:719-736)
 //   projection  U,V,W,P,dPhat,dP0 update (+ghosts, P walls)
 //
-// In the FP32-mixed form the FFTs run in FP32, while the right-hand side
-// (divergence and the dPhat correction), the modal solves, the mean, the
-// scaling, the wall extrapolations and the projection compute in FP64 from
-// the FP32 fields and round once when they store.
+// In the FP32-mixed form the spectrum S is stored in FP32 but every FFT pass
+// computes in FP64 in shared memory, as do the right-hand side (divergence and
+// the dPhat correction), the modal solves, the mean, the scaling, the wall
+// extrapolations and the projection; each rounds once when it stores.  An
+// FP32 FFT has an absolute error of a few ulp of the line's norm in every
+// coefficient, and the Poisson solution is dominated by the lowest modes
+// (divided by the smallest eigenvalues) while its right-hand side is dominated
+// by grid-scale content: measured on the 64^3 case, an FP32 FFT left the
+// pressure correction dP with 2e-2 relative error per step.  Rounding each
+// FP64-computed coefficient to FP32 keeps every mode, small ones included,
+// at FP32 relative accuracy.
 #include "tcs_kernels.h"
 
 namespace tcs {
@@ -136,19 +143,21 @@ __device__ __forceinline__ long long sidx(const GridT<R> &g, int h1p, int kx, in
 
 // ---------------------------------------------------------------------------
 // pseudo-update (:178-208) + ghost(U,V,W) + mpi_pressure_RHS (:182-229) +
-// forward r2c FFT along x.  Block: NL lines (j..j+NL-1, k).  The updated
-// velocities are formed in the field type (they are what is stored); the
-// right-hand side is evaluated in FP64 from them.
+// forward r2c FFT along x.  Block: NL lines (j..j+NL-1, k).  The FP64 form
+// stores the updated velocities and evaluates the right-hand side from them.
+// The FP32 form forms them in FP64 from the velocity's high and low words,
+// stores them as such a pair, and evaluates the right-hand side from the FP64
+// values, so the divergence carries no storage rounding.
 // ---------------------------------------------------------------------------
 template <class R>
 __global__ void __launch_bounds__(256) prhs_fftx_kernel(GridT<R> g, FieldsT<R> f, FFTPlan fp, int NL, int h1p, int with_pseudo)
 {
-    using C = cplx_t<R>;
+    using C = double2;                                 // FFT arithmetic is FP64 in both forms
     extern __shared__ __align__(16) unsigned char smraw[];
     if (blown(g)) return;
     const int N1 = g.N1, j0 = 1 + blockIdx.x * NL, k = 1 + blockIdx.y;
     C *b0 = reinterpret_cast<C *>(smraw), *b1 = b0 + NL * N1;
-    R *su = reinterpret_cast<R *>(b1 + NL * N1);       // NL x N1 new U along the line
+    double *su = reinterpret_cast<double *>(b1 + NL * N1);   // NL x N1 new U along the line
     const double *dx1 = g.d1.dx, *dx2 = g.d2.dx, *dx3 = g.d3.dx;
     const double *rdx1 = g.d1.rdx, *rdx2 = g.d2.rdx, *rdx3 = g.d3.rdx;
     const double *rdmx1 = g.d1.rdmx, *rdmx2 = g.d2.rdmx, *rdmx3 = g.d3.rdmx;
@@ -157,13 +166,26 @@ __global__ void __launch_bounds__(256) prhs_fftx_kernel(GridT<R> g, FieldsT<R> f
         const int l = t / N1, i = t - l * N1 + 1, j = j0 + l;
         if (j > g.N2) continue;
         const long long c = ix(g, i, j, k);
-        R un;
-        if (with_pseudo) {
-            un = f.U[c] + f.dU[c];
+        double un;
+        if constexpr (HasLo<R>::on) {
+            un = join(f.U[c], f.Ulo[c]);
+            if (with_pseudo) {
+                const double vmask = (j == 1) ? 0.0 : 1.0;
+                un += (double)f.dU[c];
+                const double vn = join(f.V[c], f.Vlo[c]) + (double)f.dV[c] * vmask;
+                const double wn = join(f.W[c], f.Wlo[c]) + (double)f.dW[c];
+                float h, lo;
+                split(un, h, lo); store_periodic(g, f.Un, i, j, k, h); store_periodic(g, f.Unlo, i, j, k, lo);
+                split(vn, h, lo); store_periodic(g, f.Vn, i, j, k, h); store_periodic(g, f.Vnlo, i, j, k, lo);
+                split(wn, h, lo); store_periodic(g, f.Wn, i, j, k, h); store_periodic(g, f.Wnlo, i, j, k, lo);
+            }
+        } else if (with_pseudo) {
+            const R u = f.U[c] + f.dU[c];
             const R vmask = (j == 1) ? R(0) : R(1);
-            store_periodic(g, f.Un, i, j, k, un);
+            store_periodic(g, f.Un, i, j, k, u);
             store_periodic(g, f.Vn, i, j, k, f.V[c] + f.dV[c] * vmask);
             store_periodic(g, f.Wn, i, j, k, f.W[c] + f.dW[c]);
+            un = u;
         } else {
             un = f.U[c];
         }
@@ -174,14 +196,23 @@ __global__ void __launch_bounds__(256) prhs_fftx_kernel(GridT<R> g, FieldsT<R> f
     const Phys &p = g.phd;
     for (int t = threadIdx.x; t < NL * N1; t += blockDim.x) {
         const int l = t / N1, i = t - l * N1 + 1, j = j0 + l;
-        if (j > g.N2) { b0[t] = mkc<R>(R(0), R(0)); continue; }
+        if (j > g.N2) { b0[t] = make_double2(0.0, 0.0); continue; }
         const int im = i - 1, ip = i + 1, jm = j - 1, jp = j + 1, km = k - 1, kp = k + 1;
         const long long c = ix(g, i, j, k);
         const double jvm = (j == 1) ? 0.0 : 1.0, jvp = (j == g.N2) ? 0.0 : 1.0;
         const double Uc = su[l * N1 + (i - 1)], Uxp = su[l * N1 + (i == N1 ? 0 : i)];
-        R Vc, Vyp, Wc, Wzp;
+        double Vc, Vyp, Wc, Wzp;
         const long long ckp = (k == g.N3) ? ix(g, i, j, 1) : c + sk;
-        if (with_pseudo) {
+        if constexpr (HasLo<R>::on) {
+            Vc = join(f.V[c], f.Vlo[c]); Vyp = join(f.V[c + sj], f.Vlo[c + sj]);
+            Wc = join(f.W[c], f.Wlo[c]); Wzp = join(f.W[ckp], f.Wlo[ckp]);
+            if (with_pseudo) {
+                Vc += (double)f.dV[c] * jvm;
+                if (j < g.N2) Vyp += (double)f.dV[c + sj];
+                Wc += (double)f.dW[c];
+                Wzp += (double)f.dW[ckp];
+            }
+        } else if (with_pseudo) {
             Vc = f.V[c] + f.dV[c] * R(jvm);
             Vyp = (j < g.N2) ? f.V[c + sj] + f.dV[c + sj] : f.V[c + sj];
             Wc = f.W[c] + f.dW[c];
@@ -189,7 +220,7 @@ __global__ void __launch_bounds__(256) prhs_fftx_kernel(GridT<R> g, FieldsT<R> f
         } else {
             Vc = f.V[c]; Vyp = f.V[c + sj]; Wc = f.W[c]; Wzp = f.W[ckp];
         }
-        const double DivUm = (Uxp - Uc) * rdx1[i] + (jvp * (double)Vyp - jvm * (double)Vc) * rdx2[j] + ((double)Wzp - (double)Wc) * rdx3[k];
+        const double DivUm = (Uxp - Uc) * rdx1[i] + (jvp * Vyp - jvm * Vc) * rdx2[j] + (Wzp - Wc) * rdx3[k];
         const double cbc = (1.0 - jvm) * p.Vbt * rdx2[j] - (1.0 - jvp) * p.Vup * rdx2[j];
         const R *dPh = f.dPhat;
         const double Pc = ld(dPh + c);
@@ -206,14 +237,15 @@ __global__ void __launch_bounds__(256) prhs_fftx_kernel(GridT<R> g, FieldsT<R> f
         const double Extra = ((1.0 - iR2_) * ddpdx2 - (1.0 - iR1) * ddpdx1) * rdx1[i]
                            + ((1.0 - iR4) * ddpdy4 - (1.0 - iR3) * ddpdy3) * rdx2[j]
                            + ((1.0 - iR6) * ddpdz6 - (1.0 - iR5) * ddpdz5) * rdx3[k];
-        b0[t] = mkc<R>(R((DivUm - cbc) * rdt / p.Cmp + Extra), R(0));
+        b0[t] = make_double2((DivUm - cbc) * rdt / p.Cmp + Extra, 0.0);
     }
     __syncthreads();
     const C *res = block_fft<-1>(b0, b1, NL, N1, fp, f.tw1);
     for (int t = threadIdx.x; t < NL * h1p; t += blockDim.x) {
         const int l = t / h1p, kx = t - l * h1p, j = j0 + l;
         if (j > g.N2) continue;
-        f.S[sidx(g, h1p, kx, j, k - 1)] = res[l * N1 + kx];
+        const C v = res[l * N1 + kx];
+        f.S[sidx(g, h1p, kx, j, k - 1)] = mkc<R>(R(v.x), R(v.y));
     }
 }
 
@@ -221,7 +253,7 @@ __global__ void __launch_bounds__(256) prhs_fftx_kernel(GridT<R> g, FieldsT<R> f
 template <int SIGN, class R>
 __global__ void __launch_bounds__(256) fftz_kernel(GridT<R> g, FieldsT<R> f, FFTPlan fp, int NL, int h1p)
 {
-    using C = cplx_t<R>;
+    using C = double2;
     extern __shared__ __align__(16) unsigned char smraw[];
     if (blown(g)) return;
     const int N3 = g.N3, kx0 = blockIdx.x * NL, j = 1 + blockIdx.y;
@@ -229,13 +261,15 @@ __global__ void __launch_bounds__(256) fftz_kernel(GridT<R> g, FieldsT<R> f, FFT
     C *b0 = reinterpret_cast<C *>(smraw), *b1 = b0 + NL * N3;
     for (int t = threadIdx.x; t < nl * N3; t += blockDim.x) {
         const int kz = t / nl, l = t - kz * nl;
-        b0[l * N3 + kz] = f.S[sidx(g, h1p, kx0 + l, j, kz)];
+        const cplx_t<R> v = f.S[sidx(g, h1p, kx0 + l, j, kz)];
+        b0[l * N3 + kz] = make_double2(v.x, v.y);
     }
     __syncthreads();
     const C *res = block_fft<SIGN>(b0, b1, nl, N3, fp, f.tw3);
     for (int t = threadIdx.x; t < nl * N3; t += blockDim.x) {
         const int kz = t / nl, l = t - kz * nl;
-        f.S[sidx(g, h1p, kx0 + l, j, kz)] = res[l * N3 + kz];
+        const C v = res[l * N3 + kz];
+        f.S[sidx(g, h1p, kx0 + l, j, kz)] = mkc<R>(R(v.x), R(v.y));
     }
 }
 
@@ -248,6 +282,7 @@ template <class R>
 struct Modal {
     using Real = double;
     static constexpr int NRHS = 2;
+    static constexpr int MINB = LineOcc<R>::modal;
     static constexpr bool CONTIG = false;
     GridT<R> g; FieldsT<R> f; int TL; int h1p;
     __device__ bool skip() const { return blown(g); }
@@ -301,21 +336,22 @@ __global__ void mean_kernel(GridT<R> g, FieldsT<R> f, int h1p)
 template <class R>
 __global__ void __launch_bounds__(256) ifftx_kernel(GridT<R> g, FieldsT<R> f, FFTPlan fp, int NL, int h1p)
 {
-    using C = cplx_t<R>;
+    using C = double2;
     extern __shared__ __align__(16) unsigned char smraw[];
     if (blown(g)) return;
     const int N1 = g.N1, j0 = 1 + blockIdx.x * NL, k = 1 + blockIdx.y;
     C *b0 = reinterpret_cast<C *>(smraw), *b1 = b0 + NL * N1;
     for (int t = threadIdx.x; t < NL * N1; t += blockDim.x) {
         const int l = t / N1, kx = t - l * N1, j = j0 + l;
-        C v = mkc<R>(R(0), R(0));
+        C v = make_double2(0.0, 0.0);
         if (j <= g.N2) {
             if (kx < h1p) {
-                v = f.S[sidx(g, h1p, kx, j, k - 1)];
-                if (kx == 0 || 2 * kx == N1) v.y = R(0);   // c2r ignores these imaginary parts
+                const cplx_t<R> w = f.S[sidx(g, h1p, kx, j, k - 1)];
+                v = make_double2(w.x, w.y);
+                if (kx == 0 || 2 * kx == N1) v.y = 0.0;   // c2r ignores these imaginary parts
             } else {
-                const C w = f.S[sidx(g, h1p, N1 - kx, j, k - 1)];
-                v = mkc<R>(w.x, -w.y);
+                const cplx_t<R> w = f.S[sidx(g, h1p, N1 - kx, j, k - 1)];
+                v = make_double2(w.x, -w.y);
             }
         }
         b0[t] = v;
@@ -326,7 +362,7 @@ __global__ void __launch_bounds__(256) ifftx_kernel(GridT<R> g, FieldsT<R> f, FF
     for (int t = threadIdx.x; t < NL * N1; t += blockDim.x) {
         const int l = t / N1, i = t - l * N1 + 1, j = j0 + l;
         if (j > g.N2) continue;
-        const double v = (double)res[t].x / (double)N1 / (double)g.N3 - aver;
+        const double v = res[t].x / (double)N1 / (double)g.N3 - aver;
         store_periodic(g, f.dP, i, j, k, R(v));
     }
 }
@@ -378,8 +414,14 @@ __global__ void __launch_bounds__(256) projection_kernel(GridT<R> g, FieldsT<R> 
     const double iRjk = IR(j, k);
     const double Xim = (i >= 2) ? new_phat(f, c - 1) : (double)ld(f.dPhat + c - 1);
     double invRhoc = 0.5 * rdmx1[i] * (dx1[i] * iRjk + dx1[im] * iRjk);
-    const double un = (double)f.U[c] - dtc * ((dPc - (double)ld(f.dP + c - 1)) * rdmx1[i] + (invRhoc - 1.0) * (ph - Xim) * rdmx1[i]);
-    double vn = f.V[c];
+    double u0, v0, w0;       // the velocity after the pseudo-update (FP64 from the pair in the FP32 form)
+    if constexpr (HasLo<R>::on) {
+        u0 = join(f.U[c], f.Ulo[c]); v0 = join(f.V[c], f.Vlo[c]); w0 = join(f.W[c], f.Wlo[c]);
+    } else {
+        u0 = f.U[c]; v0 = f.V[c]; w0 = f.W[c];
+    }
+    const double un = u0 - dtc * ((dPc - (double)ld(f.dP + c - 1)) * rdmx1[i] + (invRhoc - 1.0) * (ph - Xim) * rdmx1[i]);
+    double vn = v0;
     if (j >= 2) {   // the lower wall plane keeps V: dble(2 - j_indexS) = 0
         const double Xjm = (j >= 3) ? new_phat(f, c - sj) : (double)ld(f.dPhat + c - sj);
         invRhoc = 0.5 * rdmx2[j] * (dx2[j] * (double)IR(jm, k) + dx2[jm] * iRjk);
@@ -387,10 +429,17 @@ __global__ void __launch_bounds__(256) projection_kernel(GridT<R> g, FieldsT<R> 
     }
     const double Xkm = (k >= 2) ? new_phat(f, c - sk) : (double)ld(f.dPhat + c - sk);
     invRhoc = 0.5 * rdmx3[k] * (dx3[k] * (double)IR(j, km) + dx3[km] * iRjk);
-    const double wn = (double)f.W[c] - dtc * ((dPc - (double)ld(f.dP + c - sk)) * rdmx3[k] + (invRhoc - 1.0) * (ph - Xkm) * rdmx3[k]);
-    store_periodic(g, f.U, i, j, k, R(un));
-    store_periodic(g, f.V, i, j, k, R(vn));
-    store_periodic(g, f.W, i, j, k, R(wn));
+    const double wn = w0 - dtc * ((dPc - (double)ld(f.dP + c - sk)) * rdmx3[k] + (invRhoc - 1.0) * (ph - Xkm) * rdmx3[k]);
+    if constexpr (HasLo<R>::on) {
+        float h, lo;
+        split(un, h, lo); store_periodic(g, f.U, i, j, k, h); store_periodic(g, f.Ulo, i, j, k, lo);
+        split(vn, h, lo); store_periodic(g, f.V, i, j, k, h); store_periodic(g, f.Vlo, i, j, k, lo);
+        split(wn, h, lo); store_periodic(g, f.W, i, j, k, h); store_periodic(g, f.Wlo, i, j, k, lo);
+    } else {
+        store_periodic(g, f.U, i, j, k, R(un));
+        store_periodic(g, f.V, i, j, k, R(vn));
+        store_periodic(g, f.W, i, j, k, R(wn));
+    }
     store_periodic(g, f.P, i, j, k, R((double)f.P[c] + dPc));
     store_periodic(g, f.dPhatn, i, j, k, phn);
     f.dP0n[c] = dp0n;
@@ -409,7 +458,7 @@ __global__ void p_wall_kernel(GridT<R> g, FieldsT<R> f, double ab, double bb, do
 }
 
 template <class R>
-static size_t fftx_smem(const Ctx<R> &cx) { return (size_t)cx.fft_lines_x * cx.g.N1 * (2 * sizeof(cplx_t<R>) + sizeof(R)); }
+static size_t fftx_smem(const Ctx<R> &cx) { return (size_t)cx.fft_lines_x * cx.g.N1 * (2 * sizeof(double2) + sizeof(double)); }
 
 template <class R>
 void launch_pseudo_prhs_fftx(const Ctx<R> &cx, cudaStream_t s, bool with_pseudo)
@@ -430,8 +479,8 @@ void launch_poisson_rest(const Ctx<R> &cx, cudaStream_t s)
 {
     const GridT<R> &g = cx.g;
     const int h1p = cx.h1p, NLz = cx.fft_lines_z, NLx = cx.fft_lines_x;
-    const size_t smz = (size_t)NLz * g.N3 * 2 * sizeof(cplx_t<R>);
-    const size_t smx = (size_t)NLx * g.N1 * 2 * sizeof(cplx_t<R>);
+    const size_t smz = (size_t)NLz * g.N3 * 2 * sizeof(double2);
+    const size_t smx = (size_t)NLx * g.N1 * 2 * sizeof(double2);
     static size_t cz = 0, cx2 = 0;
     if (smz > cz) {
         cudaFuncSetAttribute(fftz_kernel<-1, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smz);
@@ -444,7 +493,7 @@ void launch_poisson_rest(const Ctx<R> &cx, cudaStream_t s)
     fftz_kernel<-1, R><<<gz, 256, smz, s>>>(g, cx.f, cx.fp3, NLz, h1p);
     probe_end(cx, K_FFTZ_FWD, s);
     record_launch_error("fftz_fwd");
-    LinePlan pm = make_line_plan(g.N2, false, cx.tl_modal);
+    LinePlan pm = make_line_plan(g.N2, false, fit_tl<Modal<R>>(g.N2, false, cx.tl_modal));
     launch_lines(Modal<R>{g, cx.f, pm.TL, h1p}, pm, dim3((h1p + pm.TL - 1) / pm.TL, g.N3), s, K_MODAL, cx);
     probe_begin(cx, K_MEAN, s);
     mean_kernel<R><<<1, 256, 0, s>>>(g, cx.f, h1p);

@@ -17,6 +17,7 @@ template <class R>
 struct ThermalZ {
     using Real = R;
     static constexpr int NRHS = 1;
+    static constexpr int MINB = LineOcc<R>::z;
     static constexpr bool CONTIG = false;
     GridT<R> g; FieldsT<R> f; int TL;
     __device__ bool skip() const { return blown(g); }
@@ -29,6 +30,7 @@ struct ThermalZ {
         const int i = li(l), j = 1 + blockIdx.y, k = r + 1;
         const int im = i - 1, ip = i + 1, jm = j - 1, jp = j + 1, km = k - 1, kp = k + 1;
         const PhysT<R> &p = g.ph;
+        const bool d2 = g.kdeg2 != 0;
         const R *dx1 = g.m1.dx, *dx2 = g.m2.dx, *dx3 = g.m3.dx;
         const R *rdx1 = g.m1.rdx, *rdx2 = g.m2.rdx, *rdx3 = g.m3.rdx;
         const R *rdmx1 = g.m1.rdmx, *rdmx2 = g.m2.rdmx, *rdmx3 = g.m3.rdmx;
@@ -37,8 +39,8 @@ struct ThermalZ {
         const R Tc = ld(T + c), Txm = ld(T + c - 1), Txp = ld(T + c + 1);
         const R Tym = ld(T + c - sj), Typ = ld(T + c + sj), Tzm = ld(T + c - sk), Tzp = ld(T + c + sk);
         R Kc, dKc, Kxm, dKxm, Kxp, dKxp, Kym, dKym, Kyp, dKyp, Kzm, dKzm, Kzp, dKzp, irc, dirc;
-        kpp_eval(p, Tc, Kc, dKc); kpp_eval(p, Txm, Kxm, dKxm); kpp_eval(p, Txp, Kxp, dKxp);
-        kpp_eval(p, Tym, Kym, dKym); kpp_eval(p, Typ, Kyp, dKyp); kpp_eval(p, Tzm, Kzm, dKzm); kpp_eval(p, Tzp, Kzp, dKzp);
+        kpp_eval(p, d2, Tc, Kc, dKc); kpp_eval(p, d2, Txm, Kxm, dKxm); kpp_eval(p, d2, Txp, Kxp, dKxp);
+        kpp_eval(p, d2, Tym, Kym, dKym); kpp_eval(p, d2, Typ, Kyp, dKyp); kpp_eval(p, d2, Tzm, Kzm, dKzm); kpp_eval(p, d2, Tzp, Kzp, dKzp);
         rhocp_eval(p, Tc, irc, dirc);
         const R jem = (j == 1) ? R(0.0) : R(1.0), jep = (j == g.N2) ? R(0.0) : R(1.0);   // jC_BC(jm), jC_BC(jp)
         const R Uc = ld(f.U + c), Uxp = ld(f.U + c + 1), Vc = ld(f.V + c), Vyp = ld(f.V + c + sj);
@@ -104,6 +106,7 @@ template <class R>
 struct ThermalX {
     using Real = R;
     static constexpr int NRHS = 1;
+    static constexpr int MINB = LineOcc<R>::xy;
     static constexpr bool CONTIG = true;
     GridT<R> g; FieldsT<R> f; int TL;
     __device__ bool skip() const { return blown(g); }
@@ -116,6 +119,7 @@ struct ThermalX {
         const int i = r + 1, j = lj(l), k = 1 + blockIdx.y;
         const int im = i - 1, ip = i + 1, jm = g.N2 - 1, jp = g.N2 + 1, km = g.N3 - 1, kp = g.N3 + 1;
         const PhysT<R> &p = g.ph;
+        const bool d2 = g.kdeg2 != 0;
         const R *dx1 = g.m1.dx, *dx2 = g.m2.dx, *dx3 = g.m3.dx;
         const R *rdx1 = g.m1.rdx, *rdx2 = g.m2.rdx, *rdx3 = g.m3.rdx;
         const R *rdmx1 = g.m1.rdmx, *rdmx2 = g.m2.rdmx, *rdmx3 = g.m3.rdmx;
@@ -125,8 +129,8 @@ struct ThermalX {
         const R Tjm = ld(T + ix(g, i, jm, k)), Tjp = ld(T + ix(g, i, jp, k));
         const R Tkm = ld(T + ix(g, i, j, km)), Tkp = ld(T + ix(g, i, j, kp));
         R Kc, dKc, Kxm, dKxm, Kxp, dKxp, irc, dirc;
-        kpp_eval(p, Tc, Kc, dKc); kpp_eval(p, Txm, Kxm, dKxm); kpp_eval(p, Txp, Kxp, dKxp);
-        const R Kjm = kpp_only(p, Tjm), Kjp = kpp_only(p, Tjp), Kkm = kpp_only(p, Tkm), Kkp = kpp_only(p, Tkp);
+        kpp_eval(p, d2, Tc, Kc, dKc); kpp_eval(p, d2, Txm, Kxm, dKxm); kpp_eval(p, d2, Txp, Kxp, dKxp);
+        const R Kjm = kpp_only(p, d2, Tjm), Kjp = kpp_only(p, d2, Tjp), Kkm = kpp_only(p, d2, Tkm), Kkp = kpp_only(p, d2, Tkp);
         rhocp_eval(p, Tc, irc, dirc);
         const R h = R(0.5) * p.Ct * irc;
         const R kPP1 = R(0.5) * rdmx1[i] * (dx1[i] * Kxm + dx1[im] * Kc), kPP2 = R(0.5) * rdmx1[ip] * (dx1[ip] * Kc + dx1[i] * Kxp);
@@ -161,6 +165,7 @@ template <class R>
 struct ThermalY {
     using Real = R;
     static constexpr int NRHS = 1;
+    static constexpr int MINB = LineOcc<R>::xy;
     static constexpr bool CONTIG = false;
     GridT<R> g; FieldsT<R> f; int TL;
     __device__ bool skip() const { return blown(g); }
@@ -173,6 +178,7 @@ struct ThermalY {
         const int i = li(l), j = r + 1, k = 1 + blockIdx.y;
         const int im = i - 1, ip = i + 1, jm = j - 1, jp = j + 1, km = g.N3 - 1, kp = g.N3 + 1;
         const PhysT<R> &p = g.ph;
+        const bool d2 = g.kdeg2 != 0;
         const R *dx1 = g.m1.dx, *dx2 = g.m2.dx, *dx3 = g.m3.dx;
         const R *rdx1 = g.m1.rdx, *rdx2 = g.m2.rdx, *rdx3 = g.m3.rdx;
         const R *rdmx1 = g.m1.rdmx, *rdmx2 = g.m2.rdmx, *rdmx3 = g.m3.rdmx;
@@ -181,8 +187,8 @@ struct ThermalY {
         const R Tc = ld(T + c), Txm = ld(T + c - 1), Txp = ld(T + c + 1), Tym = ld(T + c - sj), Typ = ld(T + c + sj);
         const R Tkm = ld(T + ix(g, i, j, km)), Tkp = ld(T + ix(g, i, j, kp));
         R Kc, dKc, Kym, dKym, Kyp, dKyp, irc, dirc;
-        kpp_eval(p, Tc, Kc, dKc); kpp_eval(p, Tym, Kym, dKym); kpp_eval(p, Typ, Kyp, dKyp);
-        const R Kxm = kpp_only(p, Txm), Kxp = kpp_only(p, Txp), Kkm = kpp_only(p, Tkm), Kkp = kpp_only(p, Tkp);
+        kpp_eval(p, d2, Tc, Kc, dKc); kpp_eval(p, d2, Tym, Kym, dKym); kpp_eval(p, d2, Typ, Kyp, dKyp);
+        const R Kxm = kpp_only(p, d2, Txm), Kxp = kpp_only(p, d2, Txp), Kkm = kpp_only(p, d2, Tkm), Kkp = kpp_only(p, d2, Tkp);
         rhocp_eval(p, Tc, irc, dirc);
         const R h = R(0.5) * p.Ct * irc;
         const R jem = (j == 1) ? R(0.0) : R(1.0), jep = (j == g.N2) ? R(0.0) : R(1.0);
@@ -218,9 +224,9 @@ template <class R>
 void launch_thermal(const Ctx<R> &cx, cudaStream_t s)
 {
     const GridT<R> &g = cx.g;
-    LinePlan pz = make_line_plan(g.N3, true, cx.tl_strided);
-    LinePlan px = make_line_plan(g.N1, true, cx.tl_contig);
-    LinePlan py = make_line_plan(g.N2, false, cx.tl_strided);
+    LinePlan pz = make_line_plan(g.N3, true, fit_tl<ThermalZ<R>>(g.N3, true, cx.tl_strided));
+    LinePlan px = make_line_plan(g.N1, true, fit_tl<ThermalX<R>>(g.N1, true, cx.tl_contig));
+    LinePlan py = make_line_plan(g.N2, false, fit_tl<ThermalY<R>>(g.N2, false, cx.tl_strided));
     ThermalZ<R> z{g, cx.f, pz.TL};
     launch_lines(z, pz, dim3((g.N1 + pz.TL - 1) / pz.TL, g.N2), s, K_THERMAL_Z, cx);
     ThermalX<R> xx{g, cx.f, px.TL};

@@ -1,0 +1,195 @@
+"""The FP32-mixed form (tcs_config.precision = TCS_PREC_FP32_MIXED) against the
+CPU oracle and against the FP64 form, through the C ABI (needs a B200).
+
+The mixed form stores every field in FP32, so its results differ from the
+oracle's FP64 ones by rounding: the bars below are error bounds, stated per
+field and per diagnostic.
+  * one stage from identical inputs: <= STAGE_TOL relative L2 on every output,
+    the pressure correction dP included (measured 2e-8..1.5e-6, except 5.8e-6
+    for dV of the 64^3 case, whose stencils see the velocity rounded to FP32
+    while dV itself is two orders of magnitude below U);
+  * the 64^3 constant-property case after 100 steps and a water case after 40:
+    <= RUN_TOL on the velocity vector, U, T, the Nusselt and kinetic-energy
+    series (measured 3e-8..6e-7), and <= SMALL_TOL on the components V and W
+    and on P (measured 1e-5..2.4e-5: these start from zero and stay two to
+    three orders of magnitude below U, so the FP32 rounding of the momentum
+    increments is a larger relative error);
+  * determinism: graph and eager steps, the per-routine driver sequence and a
+    snapshot replay give bit-identical results.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+STAGE_TOL = 1e-5
+RUN_TOL = 1e-5
+SMALL_TOL = 1e-4
+MIXED = 1
+
+
+def rel_l2(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    nb = np.linalg.norm(b)
+    d = np.linalg.norm(a - b)
+    return d / nb if nb > 0 else d
+
+
+I = (slice(1, -1),) * 3
+
+
+@pytest.fixture(scope="module")
+def tcs():
+    import pascal_tcs_b200 as P
+    P.load()
+    return P
+
+
+def _oracle_cfg(g):
+    return {k: v for k, v in g.config.items() if k not in ("device", "precision")}
+
+
+CASES = [
+    dict(n1m=64, n2m=64, n3m=64, Ra=1e5, Pr=0.71, dtStart=1e-3, fixed_dt=1, seed=0, property_set=0),
+    dict(n1m=32, n2m=32, n3m=32, property_set=1, Pr=7.0, Ra=1e7, DeltaT=10.0, dtStart=2e-4, fixed_dt=1,
+         seed=1, top_wall_mode=1),
+]
+
+
+@pytest.mark.parametrize("case", range(len(CASES)))
+def test_mixed_each_stage_from_identical_inputs(tcs, oracle_mod, case):
+    # Evolve the oracle for a few steps so every field is non-trivial, hand the
+    # FP32-rounded state to both, then compare every stage's output; before each
+    # stage both sides are reset to the oracle's (rounded) inputs.
+    g = tcs.Solver(precision=MIXED, **CASES[case])
+    o = oracle_mod.Oracle(**_oracle_cfg(g))
+    o.step(20)
+    names = ["T", "U", "V", "W", "P", "dPhat", "dP0"]
+    for n in names:
+        g.set(n, o.get(n))
+    for n in names:
+        o.set(n, g.get(n))
+
+    def sync(fields):
+        for n in fields:
+            g.set(n, o.get(n))
+            o.set(n, g.get(n))
+
+    def check(fields, where):
+        for n in fields:
+            e = rel_l2(g.get(n)[I], o.get(n)[I])
+            print(f"case {case} {where:14s} {n:6s} rel L2 {e:.2e}")
+            assert e <= STAGE_TOL, f"{where} {n}: {e:.3e}"
+
+    g.thermal_solver(); o.stage("thermal"); o.stage("ghost_T")
+    check(["T"], "thermal"); sync(["T"])
+    g.momentum_coeffi(); o.stage("mom_coeffi")
+    g.momentum_solvedU(); o.stage("dU"); check(["dU"], "solvedU"); sync(["dU"])
+    g.momentum_solvedV(); o.stage("dV"); check(["dV"], "solvedV"); sync(["dV"])
+    g.momentum_solvedW(); o.stage("dW"); check(["dW"], "solvedW"); sync(["dW"])
+    g.momentum_blockLdV(); o.stage("blockLdV"); check(["dV"], "blockLdV"); sync(["dV"])
+    g.momentum_blockLdU(); o.stage("blockLdU"); check(["dU"], "blockLdU"); sync(["dU"])
+    g.momentum_pseudoupdateUVW(); g.pressure_RHS(); g.pressure_Poisson_FFT2()
+    o.stage("pseudo"); o.stage("prhs"); o.stage("poisson")
+    check(["U", "V", "W", "dP"], "poisson")
+    sync(["U", "V", "W", "dP"])
+    g.pressure_Projection(); o.stage("project")
+    check(["U", "V", "W", "P", "dPhat", "dP0"], "projection")
+
+
+def _run_vs_oracle(tcs, oracle_mod, steps, cfg):
+    g = tcs.Solver(precision=MIXED, **cfg)
+    o = oracle_mod.Oracle(**_oracle_cfg(g))
+    g.step(steps)
+    hd = o.step(steps)
+    hg = g.history(0, steps)
+    err = {n: rel_l2(g.get(n)[I], o.get(n)[I]) for n in ("U", "V", "W", "T", "P")}
+    du = sum(np.linalg.norm(g.get(n)[I] - o.get(n)[I]) ** 2 for n in "UVW")
+    uu = sum(np.linalg.norm(o.get(n)[I]) ** 2 for n in "UVW")
+    err["velocity"] = float(np.sqrt(du / uu))
+    for col, n in ((4, "Nu_bot"), (5, "Nu_top"), (6, "KE")):
+        err[n] = rel_l2(hg[:, col], hd[:, col])
+    print({k: f"{v:.2e}" for k, v in err.items()})
+    return err
+
+
+def test_mixed_64cube_100_steps_vs_oracle(tcs, oracle_mod):
+    err = _run_vs_oracle(tcs, oracle_mod, 100, CASES[0])
+    for k in ("velocity", "U", "T", "Nu_bot", "Nu_top", "KE"):
+        assert err[k] <= RUN_TOL, f"{k}: {err[k]:.3e}"
+    for k in ("V", "W", "P"):
+        assert err[k] <= SMALL_TOL, f"{k}: {err[k]:.3e}"
+
+
+def test_mixed_water_40_steps_vs_oracle(tcs, oracle_mod):
+    err = _run_vs_oracle(tcs, oracle_mod, 40, CASES[1])
+    for k in ("velocity", "U", "T", "Nu_bot", "Nu_top", "KE"):
+        assert err[k] <= RUN_TOL, f"{k}: {err[k]:.3e}"
+    for k in ("V", "W", "P"):
+        assert err[k] <= SMALL_TOL, f"{k}: {err[k]:.3e}"
+
+
+def test_mixed_storage(tcs):
+    # T is stored in FP32; the velocity as an FP32 high word plus an FP32 low word.
+    g = tcs.Solver(precision=MIXED, n1m=16, n2m=12, n3m=10)
+    assert g.precision == MIXED
+    rng = np.random.default_rng(3)
+    a = rng.standard_normal(g.shape)
+    g.set("T", a)
+    np.testing.assert_array_equal(g.get("T"), a.astype(np.float32).astype(np.float64))
+    g.set("U", a)
+    u = g.get("U")
+    assert np.max(np.abs(u - a)) <= 1e-13 * np.max(np.abs(a))
+    assert np.any(u != a.astype(np.float32).astype(np.float64))
+
+
+def test_mixed_graph_eager_driver_identical(tcs):
+    cfg = dict(n1m=32, n2m=16, n3m=24, property_set=1, Pr=7.0, Ra=1e6, dtStart=5e-4, precision=MIXED)
+    a, b, c = tcs.Solver(**cfg), tcs.Solver(**cfg), tcs.Solver(**cfg)
+    b.use_graph(False)
+    a.step(4); b.step(4)
+    for _ in range(4):
+        c.driver_step()
+    for n in ("T", "U", "V", "W", "P", "dPhat", "dP0"):
+        np.testing.assert_array_equal(a.get(n), b.get(n), err_msg=n)
+        np.testing.assert_array_equal(a.get(n), c.get(n), err_msg=n)
+    np.testing.assert_array_equal(a.history(0, 4), c.history(0, 4))
+
+
+def test_mixed_snapshot_restore_replays_identically(tcs):
+    g = tcs.Solver(n1m=24, n2m=16, n3m=20, property_set=1, Pr=7.0, Ra=1e6, dtStart=5e-4, precision=MIXED)
+    g.step(2)
+    g.snapshot()
+    g.step(3)
+    a = {n: g.get(n) for n in ("T", "U", "V", "W", "P", "dPhat")}
+    g.restore()
+    g.step(3)
+    for n, v in a.items():
+        np.testing.assert_array_equal(g.get(n), v, err_msg=n)
+
+
+def test_mixed_blowup_is_reported(tcs):
+    cfg = dict(n1m=16, n2m=16, n3m=16, property_set=1, Pr=7.0, Ra=1e6, dtStart=1e-3, precision=MIXED)
+    g = tcs.Solver(**cfg)
+    T = g.get("T")
+    T[1:-1, 1:-1, 1:-1] = np.random.default_rng(0).uniform(-5.0, 5.0, T[1:-1, 1:-1, 1:-1].shape)
+    g.set("T", T)
+    with pytest.raises(tcs.TcsError) as ei:
+        g.step(5)
+    assert ei.value.code == 4
+    assert g.scalars()["blowup"] >= 1.0
+
+
+def test_mixed_close_to_fp64_form(tcs):
+    # Both forms on the GPU from the same seeded state.
+    cfg = dict(n1m=48, n2m=40, n3m=36, property_set=1, Pr=7.0, Ra=1e7, DeltaT=10.0, dtStart=2e-4, seed=1)
+    a, b = tcs.Solver(precision=0, **cfg), tcs.Solver(precision=MIXED, **cfg)
+    a.step(10); b.step(10)
+    for n in ("U", "T"):
+        e = rel_l2(b.get(n)[I], a.get(n)[I])
+        print(n, f"{e:.2e}")
+        assert e <= RUN_TOL, (n, e)
+    ha, hb = a.history(0, 10), b.history(0, 10)
+    for col in (4, 5, 6):
+        assert rel_l2(hb[:, col], ha[:, col]) <= RUN_TOL

@@ -212,16 +212,28 @@ struct Coef {
 // relative error after its refinement pass, against 5e-7 with this).
 template <class R>
 __device__ __forceinline__ R qdiv(R a, R b) { return a / b; }
+// What a lane keeps from the elimination of its partition so that another
+// right-hand side can be solved with the same factors (the refinement pass).
+template <class R>
+struct LaneFactors {
+    R A0, C0, Am, Cm, rr0, c0, den;
+    R k1[5], k2[5];          // PCR multipliers per level (P <= 32: at most 5 levels)
+};
+
 // Solve one line held in shared memory (normalised rows: b == 1).
-// A, C: coefficient rows; D: NR right-hand sides spaced by DS.
-template <class R, int NR>
-__device__ __forceinline__ void warp_solve_line(R *A, R *C, R *D, int DS, const LinePlan &lp, int lane)
+// A, C: coefficient rows; D: NR right-hand sides spaced by DS.  With REC the
+// pivot reciprocals of rows 2.. are stored in F and the lane's remaining
+// factors in *lf, for warp_resolve_line.
+template <class R, int NR, bool REC = false>
+__device__ __forceinline__ void warp_solve_line(R *A, R *C, R *D, int DS, const LinePlan &lp, int lane,
+                                                R *F = nullptr, LaneFactors<R> *lf = nullptr)
 {
     const int P = lp.P;
     const bool act = lane < P;
     const int m = act ? lp.m0 + (lane < lp.rem ? 1 : 0) : 0;
     const int base = lane * lp.PS;
     R A0 = R(0), C0 = R(0), Am = R(0), Cm = R(0), D0[NR], Dm[NR];
+    R rr0 = R(0), c0 = R(0);
 #pragma unroll
     for (int q = 0; q < NR; q++) { D0[q] = R(0); Dm[q] = R(0); }
 
@@ -234,6 +246,7 @@ __device__ __forceinline__ void warp_solve_line(R *A, R *C, R *D, int DS, const 
         for (int r = 2; r < m; r++) {
             const R ar = a[r];
             const R rr = qdiv(R(1), R(1) - ar * cm1);
+            if (REC) F[base + r] = rr;
 #pragma unroll
             for (int q = 0; q < NR; q++) { dm1[q] = rr * (d[q * DS + r] - ar * dm1[q]); d[q * DS + r] = dm1[q]; }
             cm1 = rr * c[r]; c[r] = cm1;
@@ -255,12 +268,12 @@ __device__ __forceinline__ void warp_solve_line(R *A, R *C, R *D, int DS, const 
                 cp1 = -cr * cp1; c[r] = cp1;
             }
             // closure of row 0 with row 1 (pascal_tdma.f90:531-535)
-            const R c0 = c[0];
-            const R rr = qdiv(R(1), R(1) - ap1 * c0);
+            c0 = c[0];
+            rr0 = qdiv(R(1), R(1) - ap1 * c0);
 #pragma unroll
-            for (int q = 0; q < NR; q++) D0[q] = rr * (d[q * DS] - c0 * dp1[q]);
-            A0 = rr * a[0];
-            C0 = -rr * c0 * cp1;
+            for (int q = 0; q < NR; q++) D0[q] = rr0 * (d[q * DS] - c0 * dp1[q]);
+            A0 = rr0 * a[0];
+            C0 = -rr0 * c0 * cp1;
         } else {
             A0 = a[0]; C0 = c[0];
 #pragma unroll
@@ -291,7 +304,10 @@ __device__ __forceinline__ void warp_solve_line(R *A, R *C, R *D, int DS, const 
         for (int q = 0; q < NR; q++) de[q] = R(0); }
     // parallel cyclic reduction across the P lanes; every lane forms the
     // reciprocal of its own diagonal once per level and its neighbours read it
-    for (int s = 1; s < P; s <<= 1) {
+#pragma unroll
+    for (int lev = 0; lev < 5; lev++) {
+        const int s = 1 << lev;
+        if (s >= P) break;
         int lo = lane - s, hi = lane + s;
         bool lo_ok = true, hi_ok = true;
         if (cyc) { lo = (lo + P) & (P - 1); hi = hi & (P - 1); }
@@ -309,6 +325,7 @@ __device__ __forceinline__ void warp_solve_line(R *A, R *C, R *D, int DS, const 
 #pragma unroll
             for (int q = 0; q < NR; q++) dep[q] = R(0); }
         const R k1 = al * rbm, k2 = ga * rbp;
+        if (REC) { lf->k1[lev] = k1; lf->k2[lev] = k2; }
         const R nal = -k1 * alm, nga = -k2 * gap;
         const R nbe = be - k1 * gam - k2 * alp;
 #pragma unroll
@@ -316,6 +333,7 @@ __device__ __forceinline__ void warp_solve_line(R *A, R *C, R *D, int DS, const 
         al = nal; be = nbe; ga = nga;
     }
     const R den = qdiv(R(1), al + be + ga);
+    if (REC) { lf->A0 = A0; lf->C0 = C0; lf->Am = Am; lf->Cm = Cm; lf->rr0 = rr0; lf->c0 = c0; lf->den = den; }
     R z[NR], xl[NR];
     const int nxt = cyc ? ((lane + 1) & (P - 1)) : (lane + 1 < 32 ? lane + 1 : lane);
 #pragma unroll
@@ -326,6 +344,95 @@ __device__ __forceinline__ void warp_solve_line(R *A, R *C, R *D, int DS, const 
     }
     if (act) {
         R *a = A + base, *c = C + base, *d = D + base;
+#pragma unroll
+        for (int q = 0; q < NR; q++) { d[q * DS] = z[q]; d[q * DS + m - 1] = xl[q]; }
+        for (int r = 1; r < m - 1; r++) {
+            const R ar = a[r], cr = c[r];
+#pragma unroll
+            for (int q = 0; q < NR; q++) d[q * DS + r] = d[q * DS + r] - ar * z[q] - cr * xl[q];
+        }
+    }
+}
+
+// Solve the same line for another right-hand side D (in place) with the
+// factors of a recorded warp_solve_line: A, C hold its final eliminated rows,
+// A0n, C0n the normalised rows before elimination, F the pivot reciprocals.
+// The recurrences are the elimination's own, applied to D alone.
+template <class R, int NR>
+__device__ __forceinline__ void warp_resolve_line(const R *A, const R *C, R *D, int DS, const R *A0n, const R *C0n,
+                                                  const R *F, const LaneFactors<R> &lf, const LinePlan &lp, int lane)
+{
+    const int P = lp.P;
+    const bool act = lane < P;
+    const int m = act ? lp.m0 + (lane < lp.rem ? 1 : 0) : 0;
+    const int base = lane * lp.PS;
+    R D0[NR], Dm[NR];
+#pragma unroll
+    for (int q = 0; q < NR; q++) { D0[q] = R(0); Dm[q] = R(0); }
+    if (act) {
+        R *d = D + base;
+        const R *an = A0n + base, *cn = C0n + base, *f = F + base;
+        R dm1[NR];
+#pragma unroll
+        for (int q = 0; q < NR; q++) dm1[q] = d[q * DS + 1];
+        for (int r = 2; r < m; r++) {
+            const R rr = f[r], ar = an[r];
+#pragma unroll
+            for (int q = 0; q < NR; q++) { dm1[q] = rr * (d[q * DS + r] - ar * dm1[q]); d[q * DS + r] = dm1[q]; }
+        }
+#pragma unroll
+        for (int q = 0; q < NR; q++) Dm[q] = dm1[q];
+        if (m >= 3) {
+            R dp1[NR];
+#pragma unroll
+            for (int q = 0; q < NR; q++) dp1[q] = d[q * DS + m - 2];
+            for (int r = m - 3; r >= 1; r--) {
+                const R cr = r >= 2 ? f[r] * cn[r] : cn[r];    // the forward pass's c of row r
+#pragma unroll
+                for (int q = 0; q < NR; q++) { dp1[q] = d[q * DS + r] - cr * dp1[q]; d[q * DS + r] = dp1[q]; }
+            }
+#pragma unroll
+            for (int q = 0; q < NR; q++) D0[q] = lf.rr0 * (d[q * DS] - lf.c0 * dp1[q]);
+        } else {
+#pragma unroll
+            for (int q = 0; q < NR; q++) D0[q] = d[q * DS];
+        }
+    }
+    const bool cyc = lp.cyclic != 0;
+    const int prv = cyc ? ((lane - 1 + P) & (P - 1)) : (lane > 0 ? lane - 1 : 0);
+    R de[NR];
+#pragma unroll
+    for (int q = 0; q < NR; q++) {
+        const R Dmp = __shfl_sync(0xffffffffu, Dm[q], prv);
+        de[q] = act ? D0[q] - lf.A0 * Dmp - lf.C0 * Dm[q] : R(0);
+    }
+#pragma unroll
+    for (int lev = 0; lev < 5; lev++) {
+        const int s = 1 << lev;
+        if (s >= P) break;
+        int lo = lane - s, hi = lane + s;
+        bool lo_ok = true, hi_ok = true;
+        if (cyc) { lo = (lo + P) & (P - 1); hi = hi & (P - 1); }
+        else { lo_ok = lo >= 0; hi_ok = hi < P; lo = lo_ok ? lo : lane; hi = hi_ok ? hi : lane; }
+#pragma unroll
+        for (int q = 0; q < NR; q++) {
+            R dem = __shfl_sync(0xffffffffu, de[q], lo), dep = __shfl_sync(0xffffffffu, de[q], hi);
+            if (!lo_ok) dem = R(0);
+            if (!hi_ok) dep = R(0);
+            de[q] = de[q] - lf.k1[lev] * dem - lf.k2[lev] * dep;
+        }
+    }
+    R z[NR], xl[NR];
+    const int nxt = cyc ? ((lane + 1) & (P - 1)) : (lane + 1 < 32 ? lane + 1 : lane);
+#pragma unroll
+    for (int q = 0; q < NR; q++) {
+        z[q] = de[q] * lf.den;
+        const R zn = __shfl_sync(0xffffffffu, z[q], nxt);
+        xl[q] = Dm[q] - lf.Am * z[q] - lf.Cm * zn;
+    }
+    if (act) {
+        const R *a = A + base, *c = C + base;
+        R *d = D + base;
 #pragma unroll
         for (int q = 0; q < NR; q++) { d[q * DS] = z[q]; d[q * DS + m - 1] = xl[q]; }
         for (int r = 1; r < m - 1; r++) {
@@ -361,7 +468,8 @@ struct LineOcc {
 };
 
 // Shared-memory words (of the row type) per row: A, C, D[NR]; refined rows
-// also keep the built rows A0, B0, C0, D0[NR].
+// also keep the normalised rows as built (A0, C0, D0[NR]; D0 becomes the
+// residual) and the pivot reciprocals F of the first solve.
 template <class Prob>
 __host__ __device__ constexpr int line_words()
 {
@@ -382,7 +490,7 @@ __global__ void __launch_bounds__(256, Prob::MINB) line_solve_kernel(Prob prob, 
     const int lgTL = __ffs(TL) - 1;
     const int DS = TL * LS;
     R *sA = sm, *sC = sA + DS, *sD = sC + DS;
-    R *sA0 = sD + NR * DS, *sB0 = sA0 + DS, *sC0 = sB0 + DS, *sD0 = sC0 + DS;   // refined rows only
+    R *sA0 = sD + NR * DS, *sF = sA0 + DS, *sC0 = sF + DS, *sD0 = sC0 + DS;   // refined rows only
     int *spos = reinterpret_cast<int *>(sm + (size_t)line_words<Prob>() * DS);
     // row -> shared-memory position: partition p holds rows start_p .. start_p + m_p - 1
     if (threadIdx.x < lp.P) {
@@ -402,13 +510,14 @@ __global__ void __launch_bounds__(256, Prob::MINB) line_solve_kernel(Prob prob, 
             for (int q = 0; q < NR; q++) cf.d[q] = R(0);
         }
         const R rb = qdiv(R(1), cf.b);
-        sA[pos] = cf.a * rb; sC[pos] = cf.c * rb;
+        const R an = cf.a * rb, cn = cf.c * rb;
+        sA[pos] = an; sC[pos] = cn;
 #pragma unroll
         for (int q = 0; q < NR; q++) sD[q * DS + pos] = cf.d[q] * rb;
         if (REF) {
-            sA0[pos] = cf.a; sB0[pos] = cf.b; sC0[pos] = cf.c;
+            sA0[pos] = an; sC0[pos] = cn;
 #pragma unroll
-            for (int q = 0; q < NR; q++) sD0[q * DS + pos] = cf.d[q];
+            for (int q = 0; q < NR; q++) sD0[q * DS + pos] = sD[q * DS + pos];
         }
     };
     if (Prob::CONTIG) {
@@ -420,31 +529,33 @@ __global__ void __launch_bounds__(256, Prob::MINB) line_solve_kernel(Prob prob, 
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
     for (int l = warp; l < TL; l += nw) {
-        warp_solve_line<R, NR>(sA + l * LS, sC + l * LS, sD + l * LS, DS, lp, lane);
-        if (REF) {
-            // The warp refines its own line: FP64 residual of the first
-            // solution against the built rows (it replaces D0), the
-            // normalised rows restored, and one more solve for the correction.
-            __syncwarp();
-            for (int r = lane; r < n; r += 32) {
-                const int pos = l * LS + spos[r];
-                const int rm = r > 0 ? r - 1 : (lp.cyclic ? n - 1 : -1);
-                const int rp = r < n - 1 ? r + 1 : (lp.cyclic ? 0 : -1);
-                const int pm = l * LS + spos[rm >= 0 ? rm : r], pp = l * LS + spos[rp >= 0 ? rp : r];
-                const double a = (double)sA0[pos], b = (double)sB0[pos], c = (double)sC0[pos];
-                const R rb = qdiv(R(1), sB0[pos]);
-#pragma unroll
-                for (int q = 0; q < NR; q++) {
-                    const double xm = rm >= 0 ? (double)sD[q * DS + pm] : 0.0;
-                    const double xp = rp >= 0 ? (double)sD[q * DS + pp] : 0.0;
-                    const double res = (double)sD0[q * DS + pos] - (a * xm + b * (double)sD[q * DS + pos] + c * xp);
-                    sD0[q * DS + pos] = (R)res * rb;
-                }
-                sA[pos] = sA0[pos] * rb; sC[pos] = sC0[pos] * rb;
-            }
-            __syncwarp();
-            warp_solve_line<R, NR>(sA + l * LS, sC + l * LS, sD0 + l * LS, DS, lp, lane);
+        if (!REF) {
+            warp_solve_line<R, NR>(sA + l * LS, sC + l * LS, sD + l * LS, DS, lp, lane);
+            continue;
         }
+        // FP32 rows: solve recording the factors, form the residual of the
+        // solution against the rows as built in FP64 (it replaces D0), and
+        // solve for the correction with the recorded factors.
+        LaneFactors<R> lf;
+        warp_solve_line<R, NR, true>(sA + l * LS, sC + l * LS, sD + l * LS, DS, lp, lane, sF + l * LS, &lf);
+        __syncwarp();
+        for (int r = lane; r < n; r += 32) {
+            const int pos = l * LS + spos[r];
+            const int rm = r > 0 ? r - 1 : (lp.cyclic ? n - 1 : -1);
+            const int rp = r < n - 1 ? r + 1 : (lp.cyclic ? 0 : -1);
+            const int pm = l * LS + spos[rm >= 0 ? rm : r], pp = l * LS + spos[rp >= 0 ? rp : r];
+            const double a = (double)sA0[pos], c = (double)sC0[pos];
+#pragma unroll
+            for (int q = 0; q < NR; q++) {
+                const double xm = rm >= 0 ? (double)sD[q * DS + pm] : 0.0;
+                const double xp = rp >= 0 ? (double)sD[q * DS + pp] : 0.0;
+                const double res = (double)sD0[q * DS + pos] - (a * xm + (double)sD[q * DS + pos] + c * xp);
+                sD0[q * DS + pos] = (R)res;
+            }
+        }
+        __syncwarp();
+        warp_resolve_line<R, NR>(sA + l * LS, sC + l * LS, sD0 + l * LS, DS, sA0 + l * LS, sC0 + l * LS,
+                                 sF + l * LS, lf, lp, lane);
     }
     __syncthreads();
     auto out = [&](int l, int r) {

@@ -45,6 +45,43 @@ _CASES = {
 # precision 0: plain FP64; 1: FP32-mixed
 WORKLOADS = {f"{k}_{form}": dict(v, precision=prec) for k, v in _CASES.items()
              for form, prec in (("fp64", 0), ("mixed", 1))}
+# the batched ensemble: 48 independent cases advanced together on one GPU
+WORKLOADS.update({"ens48_fp64": dict(ensemble=48, precision=0), "ens48_mixed": dict(ensemble=48, precision=1)})
+
+
+def ensemble_cases(n: int, precision: int, seed: int = 2026) -> list[dict]:
+    """n seeded cases: every axis drawn from {64, 96, 128, 160, 192}, Ra
+    log-uniform in [1e5, 1e7], Pr = 7 with water properties or Pr = 0.71 with
+    constant properties, noise seed = case index, fixed dt 2e-4 (CFL-safe)."""
+    rng = np.random.default_rng(seed)
+    sizes = [64, 96, 128, 160, 192]
+    out = []
+    for i in range(n):
+        n1, n2, n3 = (int(rng.choice(sizes)) for _ in range(3))
+        ra = float(10.0 ** rng.uniform(5.0, 7.0))
+        water = bool(rng.integers(0, 2))
+        out.append(dict(n1m=n1, n2m=n2, n3m=n3, gamma2=1.5, property_set=1 if water else 0,
+                        Pr=7.0 if water else 0.71, Ra=ra, DeltaT=10.0, dtStart=2e-4, fixed_dt=1, seed=i,
+                        noise_amp=0.01, precision=precision))
+    return out
+
+
+def lpt_shard(cases: list[dict], ws: int, rank: int) -> list[dict]:
+    """Longest-processing-time bin packing of the cases over the ranks by cell count."""
+    load = [0] * ws
+    mine = []
+    order = sorted(range(len(cases)), key=lambda i: -cases[i]["n1m"] * cases[i]["n2m"] * cases[i]["n3m"])
+    for i in order:
+        r = min(range(ws), key=lambda q: load[q])
+        load[r] += cases[i]["n1m"] * cases[i]["n2m"] * cases[i]["n3m"]
+        if r == rank:
+            mine.append(cases[i])
+    return mine
+
+
+# Water cases restart from their seeded state every ENSEMBLE_RESET steps
+# (they blow up after ~20 steps in the reference algorithm).
+ENSEMBLE_RESET = 8
 # The water cases blow up after ~10 steps (256^3) in the reference algorithm itself (the
 # non-Boussinesq pressure term sees dPhat = 0 in the wall ghost row and dPhat grows
 # ~1.6x per step at the bottom wall; the oracle restatement and this library stop at
@@ -55,11 +92,18 @@ RESET_EVERY = {f"{k}_{form}": n for k, n in (("rb256_water", 8), ("rb512_water",
 
 # Compulsory-traffic model: arrays each kernel must stream once (reads +
 # writes) per interior cell; properties and tridiagonal coefficients are
-# recomputed, 1-D metrics and ghosts ignored.  Whole step: 109 arrays, at
-# 8 B (872 B per cell-step) in the FP64 form and 4 B (436 B) in the FP32-mixed
-# form, whose every stored array is FP32 (its FP64 parts live in registers
-# and shared memory).
+# recomputed, 1-D metrics and ghosts ignored.  Whole step: 109 arrays at 8 B
+# (872 B per cell-step) in the FP64 form.  The FP32-mixed form stores every
+# array in FP32 (its FP64 parts live in registers and shared memory) and adds
+# the velocity's low words: read and written by the pressure right-hand side
+# (6) and the projection (6), read by the diagnostics (3), so 124 arrays at
+# 4 B = 496 B per cell-step.
 STEP_ARRAYS = 109
+LO_ARRAYS = {"prhs_fftx": 6, "projection": 6, "post": 3}
+
+
+def step_bytes_per_cell(esize: int) -> int:
+    return STEP_ARRAYS * esize if esize == 8 else (STEP_ARRAYS + sum(LO_ARRAYS.values())) * esize
 KERNEL_ARRAYS = {"thermal_z": 5, "thermal_x": 4, "thermal_y": 4,
                  "du_z": 6, "du_x": 4, "du_y": 4, "dv_z": 7, "dv_x": 4, "dv_y": 4,
                  "dw_z": 8, "dw_x": 4, "dw_y": 4, "blockld_v": 5, "blockld_u": 6,
@@ -75,11 +119,12 @@ def kernel_bytes(name: str, n1: int, n2: int, n3: int, esize: int = 8) -> float:
         return 2 * spec
     if name == "ifftx":
         return spec + esize * cells
+    lo = LO_ARRAYS.get(name, 0) if esize == 4 else 0
     if name == "prhs_fftx":
-        return 10 * esize * cells + spec
+        return (10 + lo) * esize * cells + spec
     if name.startswith("dv_") or name == "blockld_v":
         cells = n1 * (n2 - 1) * n3
-    return KERNEL_ARRAYS[name] * esize * cells
+    return (KERNEL_ARRAYS[name] + lo) * esize * cells
 
 
 def measured_peaks():
@@ -212,6 +257,30 @@ def cpu_baseline(cfg: dict, target_s: float = 20.0, threads: int | None = None) 
             "seconds": t1 - t0}
 
 
+def run_reference_ensemble(args, cfg, workload, O, threads) -> int:
+    """The CPU restatement on a bounded sample of the ensemble: the first two
+    cases, each for K steps (one case at a time, as one MPI job would)."""
+    cases = ensemble_cases(cfg["ensemble"], cfg["precision"])[:2]
+    cells_steps, el = 0, 0.0
+    for c in cases:
+        o = O.Oracle(**{k: v for k, v in c.items() if k not in ("device", "precision")})
+        t0 = time.perf_counter()
+        o.step(args.steps)
+        el += time.perf_counter() - t0
+        cells_steps += c["n1m"] * c["n2m"] * c["n3m"] * args.steps
+    v = cells_steps / el
+    sample = f"{args.steps} steps of each of the first 2 of the {cfg['ensemble']} cases, one at a time"
+    line = {"impl": "reference", "metric": "cell-steps/s (batched ensemble)", "value": v, "unit": "cell-steps/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": None,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded conduction profiles + noise)",
+            "config": {"workload": workload, "cpu_threads": threads},
+            "cpu_baseline": {"value": v, "unit": "cell-steps/s", "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": v, "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
 def run_reference(args, cfg, workload):
     ws, rank, _ = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
     if rank != 0:
@@ -219,6 +288,8 @@ def run_reference(args, cfg, workload):
     from oracle import oracle as O
     threads = os.cpu_count() or 1
     O.set_threads(threads)
+    if "ensemble" in cfg:
+        return run_reference_ensemble(args, cfg, workload, O, threads)
     o = O.Oracle(**{k: v for k, v in cfg.items() if k not in ("device", "precision")})
     if args.warmup:
         o.step(args.warmup)
@@ -301,8 +372,8 @@ def device_run(P, torch, cfg: dict, workload: str, args, ws: int, local: int, st
             "frac": achieved / peak if achieved else None, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
             "algorithmic_bytes_per_launch": kb, "launches": nk, "avg_launch_ms": tk / nk if nk else None,
             "traffic": profiled_traffic(top, workload)}
-    step_bytes = STEP_ARRAYS * esize * cells
-    whole = {"algorithmic_bytes_per_step": step_bytes, "bytes_per_cell_step": STEP_ARRAYS * esize,
+    step_bytes = step_bytes_per_cell(esize) * cells
+    whole = {"algorithmic_bytes_per_step": step_bytes, "bytes_per_cell_step": step_bytes_per_cell(esize),
              "achieved_gbs": step_bytes / (ms / args.steps * 1e-3) / 1e9}
     whole["frac_of_peak"] = whole["achieved_gbs"] / peak
     kernel_split = {k: round(v[0], 4) for k, v in sorted(per.items(), key=lambda kv: -kv[1][0]) if v[1]}
@@ -341,6 +412,108 @@ def mixed_error(s64, s32, nsteps: int) -> dict:
     return out
 
 
+def run_ensemble(args, cfg: dict, workload: str) -> int:
+    """The batched ensemble: this rank's share of the cases (LPT by cell count)
+    advanced together by one CUDA graph per step, against the same cases
+    stepped one at a time."""
+    ws, rank, local = dist_setup(args.gpus)
+    import torch
+    import pascal_tcs_b200 as P
+
+    torch.cuda.set_device(local)
+    allcases = ensemble_cases(cfg["ensemble"], cfg["precision"])
+    cases = lpt_shard(allcases, ws, rank)
+    solvers = [P.Solver(device=local, **c) for c in cases]
+    for s in solvers:
+        s.snapshot()
+    ens = P.Ensemble(solvers)
+    cells = sum(c["n1m"] * c["n2m"] * c["n3m"] for c in cases)
+    reset = ENSEMBLE_RESET
+
+    def grouped(k: int):
+        done = 0
+        while done < k:
+            n = min(k - done, reset)
+            ens.step(n)
+            done += n
+            if n == reset:
+                for s in solvers:
+                    s.restore()
+
+    def one_at_a_time(k: int):
+        for s in solvers:
+            done = 0
+            while done < k:
+                n = min(k - done, reset)
+                s.step(n)
+                done += n
+                if n == reset:
+                    s.restore()
+
+    def timed(fn, k: int) -> float:
+        dist_barrier(ws)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        fn(k)
+        torch.cuda.synchronize()
+        e1.record()
+        torch.cuda.synchronize()
+        dist_barrier(ws)
+        return dist_max(e0.elapsed_time(e1), ws)
+
+    one_at_a_time(args.warmup)
+    for s in solvers:
+        s.restore()
+    grouped(args.warmup)
+    for s in solvers:
+        s.restore()
+    launches0 = P.launch_count()
+    with ClockSampler(local) as clk:
+        clk.wait_first()
+        ms = timed(grouped, args.steps)
+        time.sleep(0.15)
+    launches = P.launch_count() - launches0
+    for s in solvers:
+        s.restore()
+    ms_seq = timed(one_at_a_time, args.steps)
+    total_cells = sum(c["n1m"] * c["n2m"] * c["n3m"] for c in allcases)
+    value = total_cells * args.steps / (ms * 1e-3)
+    seq = total_cells * args.steps / (ms_seq * 1e-3)
+    esize = 4 if cfg["precision"] else 8
+    peak, peak_kind = measured_peaks()
+    step_bytes = step_bytes_per_cell(esize) * total_cells
+    achieved = step_bytes * args.steps / (ms * 1e-3) / 1e9
+    if rank == 0:
+        form = "FP32-mixed" if cfg["precision"] else "FP64 plain"
+        line = {"metric": f"cell-steps/s ({form}, batched ensemble of {len(allcases)} cases)", "value": value,
+                "unit": "cell-steps/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "strong" if ws > 1 else "weak",
+                "vs_baseline": None, "dtype": "f32+f64" if cfg["precision"] else "f64",
+                "data": "synthetic: seeded conduction profiles + uniform noise 0.01, zero velocity",
+                "config": {"workload": workload, "cases": len(allcases), "cases_on_rank0": len(cases),
+                           "grids": "each axis from {64,96,128,160,192}, seed 2026", "Ra": "log-uniform 1e5..1e7",
+                           "Pr": "7 (water) or 0.71 (constant)", "dt": 2e-4, "precision": form,
+                           "parallelism": f"LPT bin-packing of cases over {ws} GPU(s)" if ws > 1 else "single",
+                           "l2": "working set of %.1f GB, larger than L2" % (total_cells * esize * 24 / 1e9 / ws),
+                           "timing": "one CUDA graph per ensemble step; CUDA events around the region",
+                           "restart_every_steps": reset},
+                "gpu_launches": launches,
+                "roofline": {"bound": "hbm", "kernel": "whole ensemble step", "achieved": achieved, "peak": peak,
+                             "unit": "GB/s", "frac": achieved / peak,
+                             "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                             "algorithmic_bytes_per_step": step_bytes, "traffic": None},
+                "one_at_a_time": {"value": seq, "ms_per_step": ms_seq / args.steps},
+                "speedup_vs_one_at_a_time": value / seq,
+                "clocks": clk.summary(), "e2e": None, "cpu_baseline": None}
+        print(json.dumps(line))
+    del ens
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -356,6 +529,8 @@ def main():
     cfg = dict(WORKLOADS[workload])
     if args.impl == "reference":
         return run_reference(args, cfg, workload)
+    if "ensemble" in cfg:
+        return run_ensemble(args, cfg, workload)
 
     ws, rank, local = dist_setup(args.gpus)
     import torch

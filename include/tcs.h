@@ -152,6 +152,17 @@ int tcs_tdma_many_solve_noalloc(double *A, double *B, double *C, double *D, int 
 
 /* ---- measurement --------------------------------------------------------- */
 int tcs_kernel_count(void);
+/* Ensembles (no counterpart in the reference, which runs one case per MPI job):
+ * independent cases on one device advanced together.  Every tcs_ensemble_step
+ * replays one CUDA graph per step in which each case is its own branch, so the
+ * GPU runs the cases' kernels concurrently.  Cases keep their own state and
+ * entry points; tcs_ensemble_destroy does not destroy them.  Probes must be off. */
+typedef struct tcs_ensemble tcs_ensemble;
+int tcs_ensemble_create(tcs_ctx *const *cases, int n, tcs_ensemble **out);
+int tcs_ensemble_destroy(tcs_ensemble *ens);
+int tcs_ensemble_step(tcs_ensemble *ens, int nsteps, int *nblown);   /* *nblown: cases that have blown up */
+int tcs_ensemble_size(const tcs_ensemble *ens);
+
 unsigned long long tcs_launch_count(void);           /* kernels this library has launched so far */
 const char *tcs_kernel_name(int kernel_id);
 /* Record a CUDA event pair around every launch of the kernels in mask (bit =
@@ -161,10 +172,20 @@ int tcs_probe_enable(tcs_ctx *ctx, uint64_t mask);
 int tcs_probe_read(tcs_ctx *ctx, int kernel_id, double *total_ms, int *launches);
 int tcs_probe_reset(tcs_ctx *ctx);
 int tcs_set_use_graph(tcs_ctx *ctx, int on);
-/* launch-shape knobs: lines per thread block (powers of two) */
-enum { TCS_TUNE_TL_STRIDED = 0, TCS_TUNE_TL_CONTIG, TCS_TUNE_TL_MODAL, TCS_TUNE_FFT_LINES_X, TCS_TUNE_FFT_LINES_Z, TCS_TUNE_COUNT };
+/* launch-shape knobs (powers of two): lines per thread block of the strided
+ * (y, z), contiguous (x) and modal line solvers and of the x and z FFTs, and
+ * the most lanes (partitions) a tridiagonal line is split over */
+enum { TCS_TUNE_TL_STRIDED = 0, TCS_TUNE_TL_CONTIG, TCS_TUNE_TL_MODAL, TCS_TUNE_FFT_LINES_X, TCS_TUNE_FFT_LINES_Z,
+       TCS_TUNE_LANES, TCS_TUNE_COUNT };
 int tcs_set_tuning(tcs_ctx *ctx, int knob, int value);
 int tcs_get_tuning(tcs_ctx *ctx, int knob, int *value);
+/* Autotuner (no reference counterpart): coordinate descent over every knob,
+ * each candidate timed with CUDA events over trial_steps steps replayed from
+ * the same state, which is restored afterwards (through tcs_snapshot, whose
+ * earlier snapshot it replaces).  The winner is cached per (n1m, n2m, n3m,
+ * precision) for the process and appended to cache_path when given (NULL: no
+ * file); a cached shape is applied without timing and sets *from_cache. */
+int tcs_autotune(tcs_ctx *ctx, int trial_steps, const char *cache_path, int *from_cache);
 const char *tcs_last_error(void);
 
 #ifdef __cplusplus

@@ -9,7 +9,12 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <fstream>
+#include <map>
+#include <mutex>
+#include <sstream>
 #include <string>
+#include <tuple>
 #include <utility>
 #include <vector>
 
@@ -101,12 +106,13 @@ void probe_end(const Shapes &cx, int kid, cudaStream_t s)
 // ---------------------------------------------------------------------------
 // plans
 // ---------------------------------------------------------------------------
-LinePlan make_line_plan(int n, bool cyclic, int TL)
+LinePlan make_line_plan(int n, bool cyclic, int TL, int pmax)
 {
     LinePlan lp;
     int P;
-    if (cyclic) { P = 1; while (P * 2 <= 32 && n / (P * 2) >= 2) P *= 2; }
-    else { P = n / 2; if (P > 32) P = 32; if (P < 1) P = 1; }
+    if (pmax > 32) pmax = 32;
+    if (cyclic) { P = 1; while (P * 2 <= pmax && n / (P * 2) >= 2) P *= 2; }
+    else { P = n / 2; if (P > pmax) P = pmax; if (P < 1) P = 1; }
     lp.n = n; lp.P = P; lp.m0 = n / P; lp.rem = n % P;
     const int mmax = lp.m0 + (lp.rem > 0 ? 1 : 0);
     lp.PS = mmax | 1;
@@ -479,6 +485,7 @@ int tcs_create(const tcs_config *cfg, tcs_ctx **out)
     // measured on B200 at 256^3: 4 lines per block beats 1, 2, 8 and 16 for both FFT kernels
     c->cx.fft_lines_x = N1 <= 256 ? 4 : (N1 <= 512 ? 2 : 1);
     c->cx.fft_lines_z = N3 <= 256 ? 4 : (N3 <= 512 ? 2 : 1);
+    c->cx.lanes = 32;
     c->cx.probe = &c->probe;
     sync_shapes(c);
     {   // the FP32 context shares the grid, constants, scalars, tables and history
@@ -869,6 +876,9 @@ int tcs_set_tuning(tcs_ctx *c, int knob, int value)
     case TCS_TUNE_FFT_LINES_Z:
         if ((size_t)value * g.N3 * 32 > 200 * 1024) return set_err(TCS_ERR_ARG, "too many lines for shared memory");
         x.fft_lines_z = value; break;
+    case TCS_TUNE_LANES:
+        if (value < 2 || value > 32) return set_err(TCS_ERR_ARG, "lanes per line must be 2..32");
+        x.lanes = value; break;
     default: return set_err(TCS_ERR_ARG, "unknown tuning knob");
     }
     sync_shapes(c);
@@ -888,6 +898,7 @@ int tcs_get_tuning(tcs_ctx *c, int knob, int *value)
     case TCS_TUNE_TL_MODAL: *value = x.tl_modal; break;
     case TCS_TUNE_FFT_LINES_X: *value = x.fft_lines_x; break;
     case TCS_TUNE_FFT_LINES_Z: *value = x.fft_lines_z; break;
+    case TCS_TUNE_LANES: *value = x.lanes; break;
     default: return set_err(TCS_ERR_ARG, "unknown tuning knob");
     }
     return TCS_OK;
@@ -1138,3 +1149,242 @@ int tcs_tdma_many_solve_cycle(tcs_tdma_plan *p, double *A, double *B, double *C,
 }
 
 } // extern "C"
+
+// ---------------------------------------------------------------------------
+// Ensembles: many independent cases on one GPU advanced together.  One step
+// of every case is captured into a single CUDA graph, each case on its own
+// branch forked from a root stream, so one graph launch advances the whole
+// ensemble and the GPU runs the cases' kernels concurrently (small grids do
+// not fill 148 SMs on their own).  Graphs are cached per buffer state, as in
+// tcs_step.
+// ---------------------------------------------------------------------------
+struct tcs_ensemble {
+    std::vector<tcs_ctx *> cases;
+    int device = 0;
+    cudaStream_t root = nullptr;
+    cudaEvent_t fork = nullptr;
+    std::vector<cudaEvent_t> join;
+    struct Entry { std::vector<const void *> key; cudaGraphExec_t exec; unsigned long long kernels; };
+    std::vector<Entry> graphs;
+};
+
+static std::vector<const void *> ensemble_key(tcs_ensemble *e)
+{
+    std::vector<const void *> k;
+    for (tcs_ctx *c : e->cases) {
+        k.push_back(field_ptr(c, TCS_F_T));
+        k.push_back(field_ptr(c, TCS_F_U));
+        k.push_back(field_ptr(c, TCS_F_DPHAT));
+    }
+    return k;
+}
+
+extern "C" {
+
+int tcs_ensemble_create(tcs_ctx *const *cases, int n, tcs_ensemble **out)
+{
+    if (!cases || !out || n < 1) return set_err(TCS_ERR_ARG, "need at least one case");
+    *out = nullptr;
+    for (int i = 0; i < n; i++) {
+        if (!cases[i]) return set_err(TCS_ERR_ARG, "null case");
+        if (cases[i]->cfg.device != cases[0]->cfg.device) return set_err(TCS_ERR_ARG, "all cases must be on one device");
+        if (cases[i]->probe.mask) return set_err(TCS_ERR_ARG, "disable the probes of every case first");
+        for (int j = 0; j < i; j++)
+            if (cases[j] == cases[i] || cases[j]->stream == cases[i]->stream)
+                return set_err(TCS_ERR_ARG, "cases must be distinct and on distinct streams");
+    }
+    CK(cudaSetDevice(cases[0]->cfg.device));
+    tcs_ensemble *e = new tcs_ensemble();
+    e->cases.assign(cases, cases + n);
+    e->device = cases[0]->cfg.device;
+    bool ok = cudaStreamCreateWithFlags(&e->root, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming) == cudaSuccess;
+    e->join.assign(n, nullptr);
+    for (int i = 0; i < n && ok; i++) ok = cudaEventCreateWithFlags(&e->join[i], cudaEventDisableTiming) == cudaSuccess;
+    if (!ok) { tcs_ensemble_destroy(e); return set_err(TCS_ERR_CUDA, "ensemble streams/events"); }
+    *out = e;
+    return TCS_OK;
+}
+
+int tcs_ensemble_destroy(tcs_ensemble *e)
+{
+    if (!e) return TCS_ERR_ARG;
+    cudaSetDevice(e->device);
+    if (e->root) cudaStreamSynchronize(e->root);
+    for (auto &g : e->graphs) cudaGraphExecDestroy(g.exec);
+    for (cudaEvent_t ev : e->join) if (ev) cudaEventDestroy(ev);
+    if (e->fork) cudaEventDestroy(e->fork);
+    if (e->root) cudaStreamDestroy(e->root);
+    delete e;
+    return TCS_OK;
+}
+
+// nsteps whole steps of every case; *nblown receives how many cases have
+// blown up (their fields stay at the step that blew up, as in tcs_step).
+int tcs_ensemble_step(tcs_ensemble *e, int nsteps, int *nblown)
+{
+    if (!e || nsteps < 0) return set_err(TCS_ERR_ARG, "bad ensemble arguments");
+    CK(cudaSetDevice(e->device));
+    int r;
+    const int fl[] = {TCS_F_T, TCS_F_U, TCS_F_V, TCS_F_W, TCS_F_P, TCS_F_DPHAT};
+    for (tcs_ctx *c : e->cases) {
+        if ((r = flush_pending(c))) return r;
+        for (int f : fl) ensure_ghosts(c, f);
+        if ((r = take_launch_error())) return r;
+        CK(cudaStreamSynchronize(c->stream));
+    }
+    for (int s = 0; s < nsteps; s++) {
+        const std::vector<const void *> key = ensemble_key(e);
+        cudaGraphExec_t exec = nullptr;
+        unsigned long long kernels = 0;
+        for (auto &g : e->graphs) if (g.key == key) { exec = g.exec; kernels = g.kernels; break; }
+        if (!exec) {
+            cudaGraph_t gr;
+            const unsigned long long before = g_launches;
+            CK(cudaStreamBeginCapture(e->root, cudaStreamCaptureModeThreadLocal));
+            cudaEventRecord(e->fork, e->root);
+            for (size_t i = 0; i < e->cases.size(); i++) {
+                tcs_ctx *c = e->cases[i];
+                cudaStreamWaitEvent(c->stream, e->fork, 0);
+                launch_step(c);
+                cudaEventRecord(e->join[i], c->stream);
+                cudaStreamWaitEvent(e->root, e->join[i], 0);
+            }
+            const unsigned long long nk = g_launches - before;
+            g_launches = before;
+            cudaError_t ec = cudaStreamEndCapture(e->root, &gr);
+            if (ec != cudaSuccess || take_launch_error())
+                return set_err(TCS_ERR_CUDA, std::string("ensemble graph capture: ") + cudaGetErrorString(ec));
+            ec = cudaGraphInstantiate(&exec, gr, 0);
+            cudaGraphDestroy(gr);
+            if (ec != cudaSuccess) return set_err(TCS_ERR_CUDA, std::string("ensemble graph: ") + cudaGetErrorString(ec));
+            e->graphs.push_back({key, exec, nk});
+            kernels = nk;
+            // the capture swapped every case's buffers already
+        } else {
+            for (tcs_ctx *c : e->cases) on_ctx(c, [&](auto &x) { swap_T(x); swap_UVW(x); swap_phat(x); });
+        }
+        CK(cudaGraphLaunch(exec, e->root));
+        g_launches += kernels;
+    }
+    CK(cudaStreamSynchronize(e->root));
+    int blown = 0;
+    for (tcs_ctx *c : e->cases) {
+        double sc[S_NSCAL];
+        CK(cudaMemcpy(sc, c->cx.g.scal, sizeof(sc), cudaMemcpyDeviceToHost));
+        if (sc[S_BLOWUP] != 0.0) blown++;
+        c->ghost_ok |= (1u << TCS_F_T) | (1u << TCS_F_U) | (1u << TCS_F_V) | (1u << TCS_F_W) | (1u << TCS_F_P) |
+                       (1u << TCS_F_DPHAT) | (1u << TCS_F_DP);
+    }
+    if (nblown) *nblown = blown;
+    return TCS_OK;
+}
+
+int tcs_ensemble_size(const tcs_ensemble *e) { return e ? (int)e->cases.size() : 0; }
+
+} // extern "C"
+
+// ---------------------------------------------------------------------------
+// Autotuner: coordinate descent over the launch-shape knobs, each candidate
+// timed with CUDA events over a few graph-replayed steps from the same state.
+// Results are cached per (grid shape, precision) for the process and, when a
+// path is given, in a text file of lines "n1 n2 n3 precision k0 .. k5".
+// ---------------------------------------------------------------------------
+namespace {
+struct TuneKey {
+    int n1, n2, n3, prec;
+    bool operator<(const TuneKey &o) const
+    {
+        return std::tie(n1, n2, n3, prec) < std::tie(o.n1, o.n2, o.n3, o.prec);
+    }
+};
+std::mutex g_tune_mu;
+std::map<TuneKey, std::vector<int>> g_tune;
+std::map<std::string, bool> g_tune_files;
+
+void tune_load(const std::string &path)
+{
+    if (path.empty() || g_tune_files[path]) return;
+    g_tune_files[path] = true;
+    std::ifstream in(path);
+    std::string line;
+    while (std::getline(in, line)) {
+        std::istringstream ss(line);
+        TuneKey k;
+        std::vector<int> v(TCS_TUNE_COUNT);
+        if (!(ss >> k.n1 >> k.n2 >> k.n3 >> k.prec)) continue;
+        bool ok = true;
+        for (int &x : v) ok = ok && (bool)(ss >> x);
+        if (ok) g_tune[k] = v;
+    }
+}
+} // namespace
+
+static int tune_trial(tcs_ctx *c, int steps, float *ms)
+{
+    int r, done = 0;
+    cudaEvent_t e0, e1;
+    if ((r = tcs_restore(c))) return r;
+    if ((r = tcs_step(c, 1, &done)) && r != TCS_ERR_BLOWUP) return r;     // captures this shape's graph
+    if ((r = tcs_restore(c))) return r;
+    CK(cudaEventCreate(&e0)); CK(cudaEventCreate(&e1));
+    cudaEventRecord(e0, c->stream);
+    r = tcs_step(c, steps, &done);
+    cudaEventRecord(e1, c->stream);
+    cudaEventSynchronize(e1);
+    cudaEventElapsedTime(ms, e0, e1);
+    cudaEventDestroy(e0); cudaEventDestroy(e1);
+    return r == TCS_ERR_BLOWUP ? TCS_OK : r;
+}
+
+extern "C" int tcs_autotune(tcs_ctx *c, int trial_steps, const char *cache_path, int *from_cache)
+{
+    if (!c) return set_err(TCS_ERR_ARG, "null context");
+    if (trial_steps < 1) return set_err(TCS_ERR_ARG, "trial_steps must be >= 1");
+    cudaSetDevice(c->cfg.device);
+    if (from_cache) *from_cache = 0;
+    const TuneKey key{c->cfg.n1m, c->cfg.n2m, c->cfg.n3m, c->cfg.precision};
+    const std::string path = cache_path ? cache_path : "";
+    std::vector<int> best;
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        tune_load(path);
+        auto it = g_tune.find(key);
+        if (it != g_tune.end()) best = it->second;
+    }
+    int r;
+    if (!best.empty()) {
+        for (int k = 0; k < TCS_TUNE_COUNT; k++)
+            if ((r = tcs_set_tuning(c, k, best[k]))) return r;
+        if (from_cache) *from_cache = 1;
+        return TCS_OK;
+    }
+    if (c->probe.mask) return set_err(TCS_ERR_ARG, "disable the probes before tuning");
+    if ((r = tcs_snapshot(c))) return r;
+    best.resize(TCS_TUNE_COUNT);
+    for (int k = 0; k < TCS_TUNE_COUNT; k++) tcs_get_tuning(c, k, &best[k]);
+    float best_ms = 0.0f;
+    if ((r = tune_trial(c, trial_steps, &best_ms))) return r;
+    static const int cand[] = {1, 2, 4, 8, 16, 32};
+    for (int k = 0; k < TCS_TUNE_COUNT; k++) {
+        for (int v : cand) {
+            if (v == best[k]) continue;
+            if (tcs_set_tuning(c, k, v) != TCS_OK) continue;          // not valid for this shape
+            float ms = 0.0f;
+            if ((r = tune_trial(c, trial_steps, &ms))) return r;
+            if (ms < best_ms) { best_ms = ms; best[k] = v; }
+        }
+        if ((r = tcs_set_tuning(c, k, best[k]))) return r;
+    }
+    if ((r = tcs_restore(c))) return r;
+    CK(cudaStreamSynchronize(c->stream));
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune[key] = best;
+    if (!path.empty()) {
+        std::ofstream out(path, std::ios::app);
+        out << key.n1 << ' ' << key.n2 << ' ' << key.n3 << ' ' << key.prec;
+        for (int v : best) out << ' ' << v;
+        out << '\n';
+    }
+    return TCS_OK;
+}

@@ -32,6 +32,7 @@ struct ProbeState;   // CUDA-event probes (tcs_capi.cu)
 struct Shapes {
     int tl_strided, tl_contig, tl_modal;
     int fft_lines_x, fft_lines_z;
+    int lanes;                                   // at most this many partitions (lanes) per line
     FFTPlan fp1, fp3;
     int h1p;
     double wall_ab, wall_bb, wall_at, wall_bt;   // Pbc_a, Pbc_b of the two walls
@@ -44,7 +45,7 @@ struct Ctx : Shapes {
     FieldsT<R> f;
 };
 
-LinePlan make_line_plan(int n, bool cyclic, int TL);
+LinePlan make_line_plan(int n, bool cyclic, int TL, int pmax = 32);
 bool make_fft_plan(int n, FFTPlan &fp);
 void probe_begin(const Shapes &cx, int kid, cudaStream_t s);
 void probe_end(const Shapes &cx, int kid, cudaStream_t s);
@@ -61,11 +62,11 @@ inline size_t line_smem(const LinePlan &lp)
 // Lines per block: the requested count, halved until MINB blocks fit in the
 // SM's shared memory (228 KB, 1 KB reserved per block).
 template <class Prob>
-inline int fit_tl(int n, bool cyclic, int want)
+inline int fit_tl(int n, bool cyclic, int want, int pmax)
 {
     const size_t budget = (size_t)228 * 1024 / Prob::MINB - 1024;
     int tl = want;
-    while (tl > 1 && line_smem<Prob>(make_line_plan(n, cyclic, tl)) > budget) tl /= 2;
+    while (tl > 1 && line_smem<Prob>(make_line_plan(n, cyclic, tl, pmax)) > budget) tl /= 2;
     return tl;
 }
 

@@ -585,9 +585,9 @@ template <class R>
 void launch_solve_du(const Ctx<R> &cx, cudaStream_t s)
 {
     const GridT<R> &g = cx.g;
-    LinePlan pz = make_line_plan(g.N3, true, fit_tl<DUZ<R>>(g.N3, true, cx.tl_strided));
-    LinePlan px = make_line_plan(g.N1, true, fit_tl<DUX<R>>(g.N1, true, cx.tl_contig));
-    LinePlan py = make_line_plan(g.N2, false, fit_tl<DUY<R>>(g.N2, false, cx.tl_strided));
+    LinePlan pz = make_line_plan(g.N3, true, fit_tl<DUZ<R>>(g.N3, true, cx.tl_strided, cx.lanes), cx.lanes);
+    LinePlan px = make_line_plan(g.N1, true, fit_tl<DUX<R>>(g.N1, true, cx.tl_contig, cx.lanes), cx.lanes);
+    LinePlan py = make_line_plan(g.N2, false, fit_tl<DUY<R>>(g.N2, false, cx.tl_strided, cx.lanes), cx.lanes);
     launch_lines(DUZ<R>{g, cx.f, pz.TL}, pz, dim3((g.N1 + pz.TL - 1) / pz.TL, g.N2), s, K_DU_Z, cx);
     launch_lines(DUX<R>{g, cx.f, px.TL}, px, dim3((g.N2 + px.TL - 1) / px.TL, g.N3), s, K_DU_X, cx);
     launch_lines(DUY<R>{g, cx.f, py.TL}, py, dim3((g.N1 + py.TL - 1) / py.TL, g.N3), s, K_DU_Y, cx);
@@ -597,9 +597,9 @@ template <class R>
 void launch_solve_dv(const Ctx<R> &cx, cudaStream_t s)
 {
     const GridT<R> &g = cx.g;
-    LinePlan pz = make_line_plan(g.N3, true, fit_tl<DVZ<R>>(g.N3, true, cx.tl_strided));
-    LinePlan px = make_line_plan(g.N1, true, fit_tl<DVX<R>>(g.N1, true, cx.tl_contig));
-    LinePlan py = make_line_plan(g.N2 - 1, false, fit_tl<DVY<R>>(g.N2 - 1, false, cx.tl_strided));
+    LinePlan pz = make_line_plan(g.N3, true, fit_tl<DVZ<R>>(g.N3, true, cx.tl_strided, cx.lanes), cx.lanes);
+    LinePlan px = make_line_plan(g.N1, true, fit_tl<DVX<R>>(g.N1, true, cx.tl_contig, cx.lanes), cx.lanes);
+    LinePlan py = make_line_plan(g.N2 - 1, false, fit_tl<DVY<R>>(g.N2 - 1, false, cx.tl_strided, cx.lanes), cx.lanes);
     launch_lines(DVZ<R>{g, cx.f, pz.TL}, pz, dim3((g.N1 + pz.TL - 1) / pz.TL, g.N2 - 1), s, K_DV_Z, cx);
     launch_lines(DVX<R>{g, cx.f, px.TL}, px, dim3((g.N2 - 1 + px.TL - 1) / px.TL, g.N3), s, K_DV_X, cx);
     launch_lines(DVY<R>{g, cx.f, py.TL}, py, dim3((g.N1 + py.TL - 1) / py.TL, g.N3), s, K_DV_Y, cx);
@@ -609,9 +609,9 @@ template <class R>
 void launch_solve_dw(const Ctx<R> &cx, cudaStream_t s)
 {
     const GridT<R> &g = cx.g;
-    LinePlan pz = make_line_plan(g.N3, true, fit_tl<DWZ<R>>(g.N3, true, cx.tl_strided));
-    LinePlan px = make_line_plan(g.N1, true, fit_tl<DWX<R>>(g.N1, true, cx.tl_contig));
-    LinePlan py = make_line_plan(g.N2, false, fit_tl<DWY<R>>(g.N2, false, cx.tl_strided));
+    LinePlan pz = make_line_plan(g.N3, true, fit_tl<DWZ<R>>(g.N3, true, cx.tl_strided, cx.lanes), cx.lanes);
+    LinePlan px = make_line_plan(g.N1, true, fit_tl<DWX<R>>(g.N1, true, cx.tl_contig, cx.lanes), cx.lanes);
+    LinePlan py = make_line_plan(g.N2, false, fit_tl<DWY<R>>(g.N2, false, cx.tl_strided, cx.lanes), cx.lanes);
     launch_lines(DWZ<R>{g, cx.f, pz.TL}, pz, dim3((g.N1 + pz.TL - 1) / pz.TL, g.N2), s, K_DW_Z, cx);
     launch_lines(DWX<R>{g, cx.f, px.TL}, px, dim3((g.N2 + px.TL - 1) / px.TL, g.N3), s, K_DW_X, cx);
     launch_lines(DWY<R>{g, cx.f, py.TL}, py, dim3((g.N1 + py.TL - 1) / py.TL, g.N3), s, K_DW_Y, cx);

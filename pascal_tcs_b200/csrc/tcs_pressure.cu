@@ -493,7 +493,7 @@ void launch_poisson_rest(const Ctx<R> &cx, cudaStream_t s)
     fftz_kernel<-1, R><<<gz, 256, smz, s>>>(g, cx.f, cx.fp3, NLz, h1p);
     probe_end(cx, K_FFTZ_FWD, s);
     record_launch_error("fftz_fwd");
-    LinePlan pm = make_line_plan(g.N2, false, fit_tl<Modal<R>>(g.N2, false, cx.tl_modal));
+    LinePlan pm = make_line_plan(g.N2, false, fit_tl<Modal<R>>(g.N2, false, cx.tl_modal, cx.lanes), cx.lanes);
     launch_lines(Modal<R>{g, cx.f, pm.TL, h1p}, pm, dim3((h1p + pm.TL - 1) / pm.TL, g.N3), s, K_MODAL, cx);
     probe_begin(cx, K_MEAN, s);
     mean_kernel<R><<<1, 256, 0, s>>>(g, cx.f, h1p);

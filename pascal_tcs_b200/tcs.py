@@ -22,7 +22,7 @@ SCALARS = ["dt", "time", "CFL", "maxDivU", "Nu_bot", "Nu_top", "KE", "blowup",
            "aver", "step", "fixed_dt"]
 HISTORY = ["dt", "time", "maxDivU", "CFL", "Nu_bot", "Nu_top", "KE"]
 METRICS = ["x1", "dx1", "dmx1", "x2", "dx2", "dmx2", "x3", "dx3", "dmx3"]
-TUNING = ["tl_strided", "tl_contig", "tl_modal", "fft_lines_x", "fft_lines_z"]
+TUNING = ["tl_strided", "tl_contig", "tl_modal", "fft_lines_x", "fft_lines_z", "lanes"]
 ERRORS = {1: "bad argument", 2: "CUDA error", 3: "unsupported", 4: "BLOW UP",
           5: "out of device memory", 6: "non-finite scalar"}
 
@@ -41,7 +41,8 @@ EXPORTS = [
     "tcs_tdma_plan_many_create", "tcs_tdma_plan_many_destroy", "tcs_tdma_many_solve",
     "tcs_tdma_many_solve_cycle", "tcs_tdma_many_solve_noalloc", "tcs_kernel_count", "tcs_launch_count", "tcs_kernel_name", "tcs_probe_enable",
     "tcs_probe_read", "tcs_probe_reset", "tcs_set_use_graph", "tcs_set_tuning", "tcs_get_tuning",
-    "tcs_last_error", "tcs_precision",
+    "tcs_last_error", "tcs_precision", "tcs_ensemble_create", "tcs_ensemble_destroy", "tcs_ensemble_step",
+    "tcs_ensemble_size", "tcs_autotune",
 ]
 
 
@@ -128,6 +129,11 @@ def load() -> ctypes.CDLL:
         "tcs_get_tuning": ([vp, ip, ctypes.POINTER(ip)], ip),
         "tcs_last_error": ([], ctypes.c_char_p),
         "tcs_precision": ([vp], ip),
+        "tcs_ensemble_create": ([ctypes.POINTER(vp), ip, ctypes.POINTER(vp)], ip),
+        "tcs_ensemble_destroy": ([vp], ip),
+        "tcs_ensemble_step": ([vp, ip, ctypes.POINTER(ip)], ip),
+        "tcs_ensemble_size": ([vp], ip),
+        "tcs_autotune": ([vp, ip, ctypes.c_char_p, ctypes.POINTER(ip)], ip),
     }
     for name in ("tcs_thermal_coeffi", "tcs_thermal_solver", "tcs_thermal_coeffi_clean",
                  "tcs_momentum_coeffi", "tcs_momentum_solvedU", "tcs_momentum_solvedV",
@@ -326,6 +332,14 @@ class Solver:
     def set_tuning(self, knob: str, value: int) -> None:
         _check(load().tcs_set_tuning(self._h, TUNING.index(knob), int(value)), f"set_tuning {knob}")
 
+    def autotune(self, trial_steps: int = 3, cache_path: str | None = None) -> tuple[dict, bool]:
+        """Pick every launch-shape knob by timing (tcs_autotune); the case's state
+        is left as it was.  Returns the knobs and whether they came from the cache."""
+        hit = ctypes.c_int(0)
+        _check(load().tcs_autotune(self._h, int(trial_steps), cache_path.encode() if cache_path else None,
+                                   ctypes.byref(hit)), "autotune")
+        return self.tuning(), bool(hit.value)
+
     def tuning(self) -> dict:
         out = {}
         for i, k in enumerate(TUNING):
@@ -353,6 +367,37 @@ class Solver:
 
     def probe_reset(self) -> None:
         _check(load().tcs_probe_reset(self._h), "probe_reset")
+
+
+class Ensemble:
+    """Independent cases on one GPU advanced together: one CUDA-graph launch
+    per step runs every case's kernels concurrently (tcs_ensemble_*)."""
+
+    def __init__(self, solvers):
+        self.solvers = list(solvers)
+        arr = (ctypes.c_void_p * len(self.solvers))(*[s._h.value for s in self.solvers])
+        h = ctypes.c_void_p()
+        _check(load().tcs_ensemble_create(arr, len(self.solvers), ctypes.byref(h)), "tcs_ensemble_create")
+        self._h = h
+
+    def step(self, n: int = 1) -> int:
+        """n steps of every case; returns how many cases have blown up."""
+        blown = ctypes.c_int(0)
+        _check(load().tcs_ensemble_step(self._h, int(n), ctypes.byref(blown)), "tcs_ensemble_step")
+        for s in self.solvers:
+            s._since_restore += n
+        return blown.value
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.tcs_ensemble_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __len__(self):
+        return len(self.solvers)
 
 
 class TdmaPlan:

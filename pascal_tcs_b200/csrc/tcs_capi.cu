@@ -145,6 +145,14 @@ bool make_fft_plan(int n, FFTPlan &fp)
     while (m % 2 == 0 && fp.npass < 24) { fp.radix[fp.npass++] = 2; m /= 2; }
     while (m % 3 == 0 && fp.npass < 24) { fp.radix[fp.npass++] = 3; m /= 3; }
     while (m % 5 == 0 && fp.npass < 24) { fp.radix[fp.npass++] = 5; m /= 5; }
+    int Ns = 1;
+    for (int p = 0; p < fp.npass; p++) {
+        fp.dnb[p] = make_fastdiv((unsigned)(n / fp.radix[p]));
+        fp.dns[p] = make_fastdiv((unsigned)Ns);
+        Ns *= fp.radix[p];
+    }
+    fp.dn = make_fastdiv((unsigned)n);
+    fp.dh = make_fastdiv((unsigned)(n / 2 + 1));
     return m == 1;
 }
 

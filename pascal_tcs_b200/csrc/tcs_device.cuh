@@ -98,6 +98,26 @@ __host__ __device__ __forceinline__ cplx_t<R> mkc(R x, R y)
     return c;
 }
 
+// Division by a loop-invariant divisor d (1 <= d < 2^31) of x < 2^31 by a
+// multiply-high and a shift: m = ceil(2^(32+s) / d) - 2^32 with 2^s >= d
+// (Granlund and Montgomery, "Division by invariant integers using
+// multiplication", PLDI 1994).
+struct FastDiv {
+    unsigned d, m, s;
+    __device__ __forceinline__ unsigned div(unsigned x) const
+    {
+        return (unsigned)(((unsigned long long)__umulhi(x, m) + x) >> s);
+    }
+};
+inline FastDiv make_fastdiv(unsigned d)
+{
+    FastDiv f;
+    f.d = d; f.s = 0;
+    while ((1ull << f.s) < d) f.s++;
+    f.m = (unsigned)((((1ull << (32 + f.s)) + d - 1) / d) - (1ull << 32));
+    return f;
+}
+
 template <class R>
 __host__ __device__ __forceinline__ long long ix(const GridT<R> &g, int i, int j, int k)
 {

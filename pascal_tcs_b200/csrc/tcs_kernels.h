@@ -24,6 +24,8 @@ const char *kernel_name(int kid);
 struct FFTPlan {
     int n, npass;
     int radix[24];
+    FastDiv dnb[24], dns[24];   // per pass: n / radix and the span Ns
+    FastDiv dn, dh;             // n and n/2 + 1
 };
 
 struct ProbeState;   // CUDA-event probes (tcs_capi.cu)

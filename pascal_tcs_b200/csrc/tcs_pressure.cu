@@ -87,14 +87,15 @@ template <int SIGN, class C> struct Bfly<5, SIGN, C> {
 
 // One Stockham pass of radix RX over nl lines (line stride ldl) in shared memory.
 template <int RX, int SIGN, class C>
-__device__ __forceinline__ void fft_pass(const C *src, C *dst, int nl, int ldl, int n, int Ns, const C *tw)
+__device__ __forceinline__ void fft_pass(const C *src, C *dst, int nl, int ldl, int n, int Ns, const C *tw,
+                                         const FastDiv &dnb, const FastDiv &dns)
 {
     const int nb = n / RX, ts = n / (Ns * RX);
     for (int t = threadIdx.x; t < nl * nb; t += blockDim.x) {
-        const int l = t / nb, jb = t - l * nb;
+        const int l = (int)dnb.div(t), jb = t - l * nb;
         const C *s = src + l * ldl;
         C *d = dst + l * ldl;
-        const int kk = jb % Ns;
+        const int jq = (int)dns.div(jb), kk = jb - jq * Ns;
         C v[RX];
 #pragma unroll
         for (int r = 0; r < RX; r++) v[r] = s[jb + r * nb];
@@ -107,7 +108,7 @@ __device__ __forceinline__ void fft_pass(const C *src, C *dst, int nl, int ldl, 
             }
         }
         Bfly<RX, SIGN, C>::run(v);
-        const int o = (jb / Ns) * Ns * RX + kk;
+        const int o = jq * Ns * RX + kk;
 #pragma unroll
         for (int r = 0; r < RX; r++) d[o + r * Ns] = v[r];
     }
@@ -123,10 +124,10 @@ __device__ C *block_fft(C *buf0, C *buf1, int nl, int ldl, const FFTPlan &fp, co
     for (int ps = 0; ps < fp.npass; ps++) {
         const int RX = fp.radix[ps];
         switch (RX) {
-        case 2: fft_pass<2, SIGN>(src, dst, nl, ldl, fp.n, Ns, tw); break;
-        case 3: fft_pass<3, SIGN>(src, dst, nl, ldl, fp.n, Ns, tw); break;
-        case 4: fft_pass<4, SIGN>(src, dst, nl, ldl, fp.n, Ns, tw); break;
-        default: fft_pass<5, SIGN>(src, dst, nl, ldl, fp.n, Ns, tw); break;
+        case 2: fft_pass<2, SIGN>(src, dst, nl, ldl, fp.n, Ns, tw, fp.dnb[ps], fp.dns[ps]); break;
+        case 3: fft_pass<3, SIGN>(src, dst, nl, ldl, fp.n, Ns, tw, fp.dnb[ps], fp.dns[ps]); break;
+        case 4: fft_pass<4, SIGN>(src, dst, nl, ldl, fp.n, Ns, tw, fp.dnb[ps], fp.dns[ps]); break;
+        default: fft_pass<5, SIGN>(src, dst, nl, ldl, fp.n, Ns, tw, fp.dnb[ps], fp.dns[ps]); break;
         }
         __syncthreads();
         C *t = src; src = dst; dst = t;
@@ -162,32 +163,34 @@ __global__ void __launch_bounds__(256) prhs_fftx_kernel(GridT<R> g, FieldsT<R> f
     const double *rdx1 = g.d1.rdx, *rdx2 = g.d2.rdx, *rdx3 = g.d3.rdx;
     const double *rdmx1 = g.d1.rdmx, *rdmx2 = g.d2.rdmx, *rdmx3 = g.d3.rdmx;
     const long long sj = g.P1, sk = (long long)g.P1 * g.P2;
+    // U..dW are only read here and Un..Wnlo only written, so the reads take the
+    // read-only path and the next cell's loads need not wait for these stores.
     for (int t = threadIdx.x; t < NL * N1; t += blockDim.x) {
-        const int l = t / N1, i = t - l * N1 + 1, j = j0 + l;
+        const int l = (int)fp.dn.div(t), i = t - l * N1 + 1, j = j0 + l;
         if (j > g.N2) continue;
         const long long c = ix(g, i, j, k);
         double un;
         if constexpr (HasLo<R>::on) {
-            un = join(f.U[c], f.Ulo[c]);
+            un = join(ld(f.U + c), ld(f.Ulo + c));
             if (with_pseudo) {
                 const double vmask = (j == 1) ? 0.0 : 1.0;
-                un += (double)f.dU[c];
-                const double vn = join(f.V[c], f.Vlo[c]) + (double)f.dV[c] * vmask;
-                const double wn = join(f.W[c], f.Wlo[c]) + (double)f.dW[c];
+                un += (double)ld(f.dU + c);
+                const double vn = join(ld(f.V + c), ld(f.Vlo + c)) + (double)ld(f.dV + c) * vmask;
+                const double wn = join(ld(f.W + c), ld(f.Wlo + c)) + (double)ld(f.dW + c);
                 float h, lo;
                 split(un, h, lo); store_periodic(g, f.Un, i, j, k, h); store_periodic(g, f.Unlo, i, j, k, lo);
                 split(vn, h, lo); store_periodic(g, f.Vn, i, j, k, h); store_periodic(g, f.Vnlo, i, j, k, lo);
                 split(wn, h, lo); store_periodic(g, f.Wn, i, j, k, h); store_periodic(g, f.Wnlo, i, j, k, lo);
             }
         } else if (with_pseudo) {
-            const R u = f.U[c] + f.dU[c];
+            const R u = ld(f.U + c) + ld(f.dU + c);
             const R vmask = (j == 1) ? R(0) : R(1);
             store_periodic(g, f.Un, i, j, k, u);
-            store_periodic(g, f.Vn, i, j, k, f.V[c] + f.dV[c] * vmask);
-            store_periodic(g, f.Wn, i, j, k, f.W[c] + f.dW[c]);
+            store_periodic(g, f.Vn, i, j, k, ld(f.V + c) + ld(f.dV + c) * vmask);
+            store_periodic(g, f.Wn, i, j, k, ld(f.W + c) + ld(f.dW + c));
             un = u;
         } else {
-            un = f.U[c];
+            un = ld(f.U + c);
         }
         su[l * N1 + (i - 1)] = un;
     }
@@ -195,7 +198,7 @@ __global__ void __launch_bounds__(256) prhs_fftx_kernel(GridT<R> g, FieldsT<R> f
     const double dt = g.scal[S_DT], rdt = 1.0 / dt;
     const Phys &p = g.phd;
     for (int t = threadIdx.x; t < NL * N1; t += blockDim.x) {
-        const int l = t / N1, i = t - l * N1 + 1, j = j0 + l;
+        const int l = (int)fp.dn.div(t), i = t - l * N1 + 1, j = j0 + l;
         if (j > g.N2) { b0[t] = make_double2(0.0, 0.0); continue; }
         const int im = i - 1, ip = i + 1, jm = j - 1, jp = j + 1, km = k - 1, kp = k + 1;
         const long long c = ix(g, i, j, k);
@@ -204,21 +207,21 @@ __global__ void __launch_bounds__(256) prhs_fftx_kernel(GridT<R> g, FieldsT<R> f
         double Vc, Vyp, Wc, Wzp;
         const long long ckp = (k == g.N3) ? ix(g, i, j, 1) : c + sk;
         if constexpr (HasLo<R>::on) {
-            Vc = join(f.V[c], f.Vlo[c]); Vyp = join(f.V[c + sj], f.Vlo[c + sj]);
-            Wc = join(f.W[c], f.Wlo[c]); Wzp = join(f.W[ckp], f.Wlo[ckp]);
+            Vc = join(ld(f.V + c), ld(f.Vlo + c)); Vyp = join(ld(f.V + c + sj), ld(f.Vlo + c + sj));
+            Wc = join(ld(f.W + c), ld(f.Wlo + c)); Wzp = join(ld(f.W + ckp), ld(f.Wlo + ckp));
             if (with_pseudo) {
-                Vc += (double)f.dV[c] * jvm;
-                if (j < g.N2) Vyp += (double)f.dV[c + sj];
-                Wc += (double)f.dW[c];
-                Wzp += (double)f.dW[ckp];
+                Vc += (double)ld(f.dV + c) * jvm;
+                if (j < g.N2) Vyp += (double)ld(f.dV + c + sj);
+                Wc += (double)ld(f.dW + c);
+                Wzp += (double)ld(f.dW + ckp);
             }
         } else if (with_pseudo) {
-            Vc = f.V[c] + f.dV[c] * R(jvm);
-            Vyp = (j < g.N2) ? f.V[c + sj] + f.dV[c + sj] : f.V[c + sj];
-            Wc = f.W[c] + f.dW[c];
-            Wzp = f.W[ckp] + f.dW[ckp];
+            Vc = ld(f.V + c) + ld(f.dV + c) * R(jvm);
+            Vyp = (j < g.N2) ? ld(f.V + c + sj) + ld(f.dV + c + sj) : ld(f.V + c + sj);
+            Wc = ld(f.W + c) + ld(f.dW + c);
+            Wzp = ld(f.W + ckp) + ld(f.dW + ckp);
         } else {
-            Vc = f.V[c]; Vyp = f.V[c + sj]; Wc = f.W[c]; Wzp = f.W[ckp];
+            Vc = ld(f.V + c); Vyp = ld(f.V + c + sj); Wc = ld(f.W + c); Wzp = ld(f.W + ckp);
         }
         const double DivUm = (Uxp - Uc) * rdx1[i] + (jvp * Vyp - jvm * Vc) * rdx2[j] + (Wzp - Wc) * rdx3[k];
         const double cbc = (1.0 - jvm) * p.Vbt * rdx2[j] - (1.0 - jvp) * p.Vup * rdx2[j];
@@ -242,7 +245,7 @@ __global__ void __launch_bounds__(256) prhs_fftx_kernel(GridT<R> g, FieldsT<R> f
     __syncthreads();
     const C *res = block_fft<-1>(b0, b1, NL, N1, fp, f.tw1);
     for (int t = threadIdx.x; t < NL * h1p; t += blockDim.x) {
-        const int l = t / h1p, kx = t - l * h1p, j = j0 + l;
+        const int l = (int)fp.dh.div(t), kx = t - l * h1p, j = j0 + l;
         if (j > g.N2) continue;
         const C v = res[l * N1 + kx];
         f.S[sidx(g, h1p, kx, j, k - 1)] = mkc<R>(R(v.x), R(v.y));
@@ -257,17 +260,19 @@ __global__ void __launch_bounds__(256) fftz_kernel(GridT<R> g, FieldsT<R> f, FFT
     extern __shared__ __align__(16) unsigned char smraw[];
     if (blown(g)) return;
     const int N3 = g.N3, kx0 = blockIdx.x * NL, j = 1 + blockIdx.y;
-    const int nl = min(NL, h1p - kx0);
+    const int nl = min(NL, h1p - kx0), lgNL = __ffs(NL) - 1;     // NL is a power of two
     C *b0 = reinterpret_cast<C *>(smraw), *b1 = b0 + NL * N3;
-    for (int t = threadIdx.x; t < nl * N3; t += blockDim.x) {
-        const int kz = t / nl, l = t - kz * nl;
+    for (int t = threadIdx.x; t < NL * N3; t += blockDim.x) {
+        const int kz = t >> lgNL, l = t & (NL - 1);
+        if (l >= nl) continue;
         const cplx_t<R> v = f.S[sidx(g, h1p, kx0 + l, j, kz)];
         b0[l * N3 + kz] = make_double2(v.x, v.y);
     }
     __syncthreads();
     const C *res = block_fft<SIGN>(b0, b1, nl, N3, fp, f.tw3);
-    for (int t = threadIdx.x; t < nl * N3; t += blockDim.x) {
-        const int kz = t / nl, l = t - kz * nl;
+    for (int t = threadIdx.x; t < NL * N3; t += blockDim.x) {
+        const int kz = t >> lgNL, l = t & (NL - 1);
+        if (l >= nl) continue;
         const C v = res[l * N3 + kz];
         f.S[sidx(g, h1p, kx0 + l, j, kz)] = mkc<R>(R(v.x), R(v.y));
     }
@@ -342,7 +347,7 @@ __global__ void __launch_bounds__(256) ifftx_kernel(GridT<R> g, FieldsT<R> f, FF
     const int N1 = g.N1, j0 = 1 + blockIdx.x * NL, k = 1 + blockIdx.y;
     C *b0 = reinterpret_cast<C *>(smraw), *b1 = b0 + NL * N1;
     for (int t = threadIdx.x; t < NL * N1; t += blockDim.x) {
-        const int l = t / N1, kx = t - l * N1, j = j0 + l;
+        const int l = (int)fp.dn.div(t), kx = t - l * N1, j = j0 + l;
         C v = make_double2(0.0, 0.0);
         if (j <= g.N2) {
             if (kx < h1p) {
@@ -360,7 +365,7 @@ __global__ void __launch_bounds__(256) ifftx_kernel(GridT<R> g, FieldsT<R> f, FF
     const C *res = block_fft<1>(b0, b1, NL, N1, fp, f.tw1);
     const double aver = g.scal[S_AVER];
     for (int t = threadIdx.x; t < NL * N1; t += blockDim.x) {
-        const int l = t / N1, i = t - l * N1 + 1, j = j0 + l;
+        const int l = (int)fp.dn.div(t), i = t - l * N1 + 1, j = j0 + l;
         if (j > g.N2) continue;
         const double v = res[t].x / (double)N1 / (double)g.N3 - aver;
         store_periodic(g, f.dP, i, j, k, R(v));

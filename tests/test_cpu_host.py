@@ -75,3 +75,55 @@ def test_two_rank_max_over_ranks_gloo():
     got = dict(q.get(timeout=10) for _ in range(2))
     assert got == {0: 2.0, 1: 2.0}
     assert all(p.exitcode == 0 for p in ps)
+
+
+def test_ensemble_cases_and_lpt_sharding():
+    import bench
+    cases = bench.ensemble_cases(48, 0)
+    assert len(cases) == 48
+    assert all(c[a] in (64, 96, 128, 160, 192) for c in cases for a in ("n1m", "n2m", "n3m"))
+    assert all(1e5 <= c["Ra"] <= 1e7 for c in cases)
+    assert {c["property_set"] for c in cases} <= {0, 1} and [c["seed"] for c in cases] == list(range(48))
+    assert bench.ensemble_cases(48, 0) == cases                       # seeded
+    cells = lambda c: c["n1m"] * c["n2m"] * c["n3m"]
+    for ws in (1, 2, 3, 8):
+        shards = [bench.lpt_shard(cases, ws, r) for r in range(ws)]
+        assert sorted(c["seed"] for s in shards for c in s) == list(range(48))
+        loads = [sum(cells(c) for c in s) for s in shards]
+        assert max(loads) - min(loads) <= max(cells(c) for c in cases)    # LPT bound
+
+
+def _lpt_rank(rank, ws, port, out):
+    import torch.distributed as dist
+    import bench
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=ws)
+    mine = bench.lpt_shard(bench.ensemble_cases(48, 1), ws, rank)
+    import torch
+    t = torch.tensor([float(sum(c["n1m"] * c["n2m"] * c["n3m"] for c in mine)), float(len(mine))])
+    dist.all_reduce(t)
+    out[rank] = (t[0].item(), t[1].item())
+    dist.destroy_process_group()
+
+
+def test_lpt_sharding_two_gloo_ranks_cover_all_cases():
+    import multiprocessing as mp
+    import bench
+    ctx = mp.get_context("spawn")
+    with ctx.Manager() as man:
+        out = man.dict()
+        port = 29000 + os.getpid() % 1000
+        ps = [ctx.Process(target=_lpt_rank, args=(r, 2, port, out)) for r in range(2)]
+        for p in ps:
+            p.start()
+        for p in ps:
+            p.join(120)
+        assert all(p.exitcode == 0 for p in ps)
+        total = sum(c["n1m"] * c["n2m"] * c["n3m"] for c in bench.ensemble_cases(48, 1))
+        assert out[0] == out[1] == (float(total), 48.0)
+
+
+def test_tune_shape_parser():
+    from pascal_tcs_b200 import tune
+    assert tune.parse("256x128x64:1") == dict(n1m=256, n2m=128, n3m=64, precision=1)
+    assert tune.parse("64x64x64") == dict(n1m=64, n2m=64, n3m=64, precision=0)

@@ -245,8 +245,9 @@ struct LaneFactors {
 // pivot reciprocals of rows 2.. are stored in F and the lane's remaining
 // factors in *lf, for warp_resolve_line.
 template <class R, int NR, bool REC = false>
-__device__ __forceinline__ void warp_solve_line(R *A, R *C, R *D, int DS, const LinePlan &lp, int lane,
-                                                R *F = nullptr, LaneFactors<R> *lf = nullptr)
+__device__ __forceinline__ void warp_solve_line(R *__restrict__ A, R *__restrict__ C, R *__restrict__ D, int DS,
+                                                const LinePlan &lp, int lane,
+                                                R *__restrict__ F = nullptr, LaneFactors<R> *lf = nullptr)
 {
     const int P = lp.P;
     const bool act = lane < P;
@@ -374,13 +375,169 @@ __device__ __forceinline__ void warp_solve_line(R *A, R *C, R *D, int DS, const 
     }
 }
 
+// The same elimination with the lane's partition held in registers (at most
+// M rows; every loop is unrolled over M with the rows beyond m switched off),
+// so no shared-memory access sits on the elimination chains.  The rows are
+// read once and the solution (and, with REC, the eliminated rows and pivot
+// reciprocals the refinement replays) written once.
+template <class R, int NR, int M, bool REC = false>
+__device__ __forceinline__ void warp_solve_line_reg(R *__restrict__ A, R *__restrict__ C, R *__restrict__ D, int DS,
+                                                    const LinePlan &lp, int lane,
+                                                    R *__restrict__ F = nullptr, LaneFactors<R> *lf = nullptr)
+{
+    const int P = lp.P;
+    const bool act = lane < P;
+    const int m = act ? lp.m0 + (lane < lp.rem ? 1 : 0) : 0;
+    const int base = lane * lp.PS;
+    R a[M], c[M], d[NR][M];
+#pragma unroll
+    for (int r = 0; r < M; r++) {
+        const bool on = r < m;
+        a[r] = on ? A[base + r] : R(0);
+        c[r] = on ? C[base + r] : R(0);
+#pragma unroll
+        for (int q = 0; q < NR; q++) d[q][r] = on ? D[q * DS + base + r] : R(0);
+    }
+    // forward elimination (rows 0 and 1 are already normalised)
+#pragma unroll
+    for (int r = 2; r < M; r++) {
+        if (r < m) {
+            const R ar = a[r];
+            const R rr = qdiv(R(1), R(1) - ar * c[r - 1]);
+            if (REC) F[base + r] = rr;
+#pragma unroll
+            for (int q = 0; q < NR; q++) d[q][r] = rr * (d[q][r] - ar * d[q][r - 1]);
+            c[r] = rr * c[r];
+            a[r] = -rr * ar * a[r - 1];
+        }
+    }
+    R Am = R(0), Cm = R(0), Dm[NR];
+#pragma unroll
+    for (int q = 0; q < NR; q++) Dm[q] = R(0);
+#pragma unroll
+    for (int r = 1; r < M; r++)
+        if (r == m - 1) {
+            Am = a[r]; Cm = c[r];
+#pragma unroll
+            for (int q = 0; q < NR; q++) Dm[q] = d[q][r];
+        }
+    // backward elimination of the upper diagonal: rows m-3 .. 1
+#pragma unroll
+    for (int r = M - 3; r >= 1; r--) {
+        if (r <= m - 3) {
+            const R cr = c[r];
+#pragma unroll
+            for (int q = 0; q < NR; q++) d[q][r] = d[q][r] - cr * d[q][r + 1];
+            a[r] = a[r] - cr * a[r + 1];
+            c[r] = -cr * c[r + 1];
+        }
+    }
+    R A0 = R(0), C0 = R(0), D0[NR], rr0 = R(0), c0 = R(0);
+#pragma unroll
+    for (int q = 0; q < NR; q++) D0[q] = R(0);
+    if (act) {
+        if (m >= 3) {
+            // closure of row 0 with row 1 (pascal_tdma.f90:531-535)
+            c0 = c[0];
+            rr0 = qdiv(R(1), R(1) - a[1] * c0);
+#pragma unroll
+            for (int q = 0; q < NR; q++) D0[q] = rr0 * (d[q][0] - c0 * d[q][1]);
+            A0 = rr0 * a[0];
+            C0 = -rr0 * c0 * c[1];
+        } else {
+            A0 = a[0]; C0 = c[0];
+#pragma unroll
+            for (int q = 0; q < NR; q++) D0[q] = d[q][0];
+        }
+    }
+    const bool cyc = lp.cyclic != 0;
+    if (!cyc) {
+        if (lane == 0) A0 = R(0);
+        if (lane == P - 1) Cm = R(0);
+    }
+    const int prv = cyc ? ((lane - 1 + P) & (P - 1)) : (lane > 0 ? lane - 1 : 0);
+    const R Amp = __shfl_sync(0xffffffffu, Am, prv);
+    const R Cmp = __shfl_sync(0xffffffffu, Cm, prv);
+    R al = -A0 * Amp;
+    R be = R(1) - A0 * Cmp - C0 * Am;
+    R ga = -C0 * Cm;
+    R de[NR];
+#pragma unroll
+    for (int q = 0; q < NR; q++) {
+        const R Dmp = __shfl_sync(0xffffffffu, Dm[q], prv);
+        de[q] = D0[q] - A0 * Dmp - C0 * Dm[q];
+    }
+    if (!act) { al = R(0); be = R(1); ga = R(0);
+#pragma unroll
+        for (int q = 0; q < NR; q++) de[q] = R(0); }
+#pragma unroll
+    for (int lev = 0; lev < 5; lev++) {
+        const int s = 1 << lev;
+        if (s >= P) break;
+        int lo = lane - s, hi = lane + s;
+        bool lo_ok = true, hi_ok = true;
+        if (cyc) { lo = (lo + P) & (P - 1); hi = hi & (P - 1); }
+        else { lo_ok = lo >= 0; hi_ok = hi < P; lo = lo_ok ? lo : lane; hi = hi_ok ? hi : lane; }
+        const R rbe = qdiv(R(1), be);
+        R alm = __shfl_sync(0xffffffffu, al, lo), rbm = __shfl_sync(0xffffffffu, rbe, lo), gam = __shfl_sync(0xffffffffu, ga, lo);
+        R alp = __shfl_sync(0xffffffffu, al, hi), rbp = __shfl_sync(0xffffffffu, rbe, hi), gap = __shfl_sync(0xffffffffu, ga, hi);
+        R dem[NR], dep[NR];
+#pragma unroll
+        for (int q = 0; q < NR; q++) { dem[q] = __shfl_sync(0xffffffffu, de[q], lo); dep[q] = __shfl_sync(0xffffffffu, de[q], hi); }
+        if (!lo_ok) { alm = R(0); rbm = R(1); gam = R(0);
+#pragma unroll
+            for (int q = 0; q < NR; q++) dem[q] = R(0); }
+        if (!hi_ok) { alp = R(0); rbp = R(1); gap = R(0);
+#pragma unroll
+            for (int q = 0; q < NR; q++) dep[q] = R(0); }
+        const R k1 = al * rbm, k2 = ga * rbp;
+        if (REC) { lf->k1[lev] = k1; lf->k2[lev] = k2; }
+        const R nal = -k1 * alm, nga = -k2 * gap;
+        const R nbe = be - k1 * gam - k2 * alp;
+#pragma unroll
+        for (int q = 0; q < NR; q++) de[q] = de[q] - k1 * dem[q] - k2 * dep[q];
+        al = nal; be = nbe; ga = nga;
+    }
+    const R den = qdiv(R(1), al + be + ga);
+    if (REC) { lf->A0 = A0; lf->C0 = C0; lf->Am = Am; lf->Cm = Cm; lf->rr0 = rr0; lf->c0 = c0; lf->den = den; }
+    R z[NR], xl[NR];
+    const int nxt = cyc ? ((lane + 1) & (P - 1)) : (lane + 1 < 32 ? lane + 1 : lane);
+#pragma unroll
+    for (int q = 0; q < NR; q++) {
+        z[q] = de[q] * den;
+        const R zn = __shfl_sync(0xffffffffu, z[q], nxt);
+        xl[q] = Dm[q] - Am * z[q] - Cm * zn;
+    }
+#pragma unroll
+    for (int r = 0; r < M; r++) {
+        if (r < m) {
+#pragma unroll
+            for (int q = 0; q < NR; q++) {
+                const R x = (r == 0) ? z[q] : (r == m - 1 ? xl[q] : d[q][r] - a[r] * z[q] - c[r] * xl[q]);
+                D[q * DS + base + r] = x;
+            }
+            if (REC) { A[base + r] = a[r]; C[base + r] = c[r]; }
+        }
+    }
+}
+
+template <class R, int NR, int MREG, bool REC>
+__device__ __forceinline__ void solve_line(R *A, R *C, R *D, int DS, const LinePlan &lp, int lane, R *F, LaneFactors<R> *lf)
+{
+    if (MREG > 0 && lp.m0 + (lp.rem ? 1 : 0) <= MREG)
+        warp_solve_line_reg<R, NR, (MREG > 0 ? MREG : 1), REC>(A, C, D, DS, lp, lane, F, lf);
+    else
+        warp_solve_line<R, NR, REC>(A, C, D, DS, lp, lane, F, lf);
+}
+
 // Solve the same line for another right-hand side D (in place) with the
 // factors of a recorded warp_solve_line: A, C hold its final eliminated rows,
 // A0n, C0n the normalised rows before elimination, F the pivot reciprocals.
 // The recurrences are the elimination's own, applied to D alone.
 template <class R, int NR>
-__device__ __forceinline__ void warp_resolve_line(const R *A, const R *C, R *D, int DS, const R *A0n, const R *C0n,
-                                                  const R *F, const LaneFactors<R> &lf, const LinePlan &lp, int lane)
+__device__ __forceinline__ void warp_resolve_line(const R *__restrict__ A, const R *__restrict__ C, R *__restrict__ D, int DS,
+                                                  const R *__restrict__ A0n, const R *__restrict__ C0n,
+                                                  const R *__restrict__ F, const LaneFactors<R> &lf, const LinePlan &lp, int lane)
 {
     const int P = lp.P;
     const bool act = lane < P;
@@ -485,7 +642,19 @@ struct LineOcc {
     static constexpr int z = std::is_same<R, float>::value ? 3 : 2;
     static constexpr int xy = std::is_same<R, float>::value ? 3 : 4;
     static constexpr int modal = 3;
+    // rows per lane solved in registers (0: in shared memory), per family:
+    // wherever the registers allow it without spills (not the FP64 x/y sweeps
+    // at 64 registers, nor the two-right-hand-side modal solves at 80)
+    static constexpr int reg_z = 8;
+    static constexpr int reg_xy = std::is_same<R, float>::value ? 8 : 0;
+    static constexpr int reg_modal = 0;
 };
+
+// Solve a line with the register-resident elimination when the lane's
+// partition fits Prob::MREG rows, else in shared memory.
+template <class R, int NR, int MREG, bool REC = false>
+__device__ __forceinline__ void solve_line(R *A, R *C, R *D, int DS, const LinePlan &lp, int lane,
+                                           R *F = nullptr, LaneFactors<R> *lf = nullptr);
 
 // Shared-memory words (of the row type) per row: A, C, D[NR]; refined rows
 // also keep the normalised rows as built (A0, C0, D0[NR]; D0 becomes the
@@ -550,14 +719,14 @@ __global__ void __launch_bounds__(256, Prob::MINB) line_solve_kernel(Prob prob, 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
     for (int l = warp; l < TL; l += nw) {
         if (!REF) {
-            warp_solve_line<R, NR>(sA + l * LS, sC + l * LS, sD + l * LS, DS, lp, lane);
+            solve_line<R, NR, Prob::MREG>(sA + l * LS, sC + l * LS, sD + l * LS, DS, lp, lane);
             continue;
         }
         // FP32 rows: solve recording the factors, form the residual of the
         // solution against the rows as built in FP64 (it replaces D0), and
         // solve for the correction with the recorded factors.
         LaneFactors<R> lf;
-        warp_solve_line<R, NR, true>(sA + l * LS, sC + l * LS, sD + l * LS, DS, lp, lane, sF + l * LS, &lf);
+        solve_line<R, NR, Prob::MREG, true>(sA + l * LS, sC + l * LS, sD + l * LS, DS, lp, lane, sF + l * LS, &lf);
         __syncwarp();
         for (int r = lane; r < n; r += 32) {
             const int pos = l * LS + spos[r];

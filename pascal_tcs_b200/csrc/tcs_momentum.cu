@@ -49,6 +49,7 @@ struct DUZ {
     using Real = R;
     static constexpr int NRHS = 1;
     static constexpr int MINB = LineOcc<R>::z;
+    static constexpr int MREG = LineOcc<Real>::reg_z;
     static constexpr bool CONTIG = false;
     GridT<R> g; FieldsT<R> f; int TL;
     __device__ bool skip() const { return blown(g); }
@@ -135,6 +136,7 @@ struct DUX {
     using Real = R;
     static constexpr int NRHS = 1;
     static constexpr int MINB = LineOcc<R>::xy;
+    static constexpr int MREG = LineOcc<Real>::reg_xy;
     static constexpr bool CONTIG = true;
     GridT<R> g; FieldsT<R> f; int TL;
     __device__ bool skip() const { return blown(g); }
@@ -170,6 +172,7 @@ struct DUY {
     using Real = R;
     static constexpr int NRHS = 1;
     static constexpr int MINB = LineOcc<R>::xy;
+    static constexpr int MREG = LineOcc<Real>::reg_xy;
     static constexpr bool CONTIG = false;
     GridT<R> g; FieldsT<R> f; int TL;
     __device__ bool skip() const { return blown(g); }
@@ -216,6 +219,7 @@ struct DVZ {
     using Real = R;
     static constexpr int NRHS = 1;
     static constexpr int MINB = LineOcc<R>::z;
+    static constexpr int MREG = LineOcc<Real>::reg_z;
     static constexpr bool CONTIG = false;
     GridT<R> g; FieldsT<R> f; int TL;
     __device__ bool skip() const { return blown(g); }
@@ -314,6 +318,7 @@ struct DVX {
     using Real = R;
     static constexpr int NRHS = 1;
     static constexpr int MINB = LineOcc<R>::xy;
+    static constexpr int MREG = LineOcc<Real>::reg_xy;
     static constexpr bool CONTIG = true;
     GridT<R> g; FieldsT<R> f; int TL;
     __device__ bool skip() const { return blown(g); }
@@ -354,6 +359,7 @@ struct DVY {
     using Real = R;
     static constexpr int NRHS = 1;
     static constexpr int MINB = LineOcc<R>::xy;
+    static constexpr int MREG = LineOcc<Real>::reg_xy;
     static constexpr bool CONTIG = false;
     GridT<R> g; FieldsT<R> f; int TL;
     __device__ bool skip() const { return blown(g); }
@@ -394,6 +400,7 @@ struct DWZ {
     using Real = R;
     static constexpr int NRHS = 1;
     static constexpr int MINB = LineOcc<R>::z;
+    static constexpr int MREG = LineOcc<Real>::reg_z;
     static constexpr bool CONTIG = false;
     GridT<R> g; FieldsT<R> f; int TL;
     __device__ bool skip() const { return blown(g); }
@@ -502,6 +509,7 @@ struct DWX {
     using Real = R;
     static constexpr int NRHS = 1;
     static constexpr int MINB = LineOcc<R>::xy;
+    static constexpr int MREG = LineOcc<Real>::reg_xy;
     static constexpr bool CONTIG = true;
     GridT<R> g; FieldsT<R> f; int TL;
     __device__ bool skip() const { return blown(g); }
@@ -543,6 +551,7 @@ struct DWY {
     using Real = R;
     static constexpr int NRHS = 1;
     static constexpr int MINB = LineOcc<R>::xy;
+    static constexpr int MREG = LineOcc<Real>::reg_xy;
     static constexpr bool CONTIG = false;
     GridT<R> g; FieldsT<R> f; int TL;
     __device__ bool skip() const { return blown(g); }

@@ -28,15 +28,15 @@ __global__ void __launch_bounds__(256) post_kernel(GridT<R> g, FieldsT<R> f)
 {
     __shared__ double red[PT_N][256];
     if (blown(g)) return;
-    const int rows = g.N2 * g.N3;
+    const long long n = (long long)g.N1 * g.N2 * g.N3;
     double mdiv = -INFINITY, mcfl = -INFINITY, ke = 0.0, nub = 0.0, nut = 0.0, eke = 0.0, enb = 0.0, ent = 0.0;
     const double *dx1 = g.d1.dx, *dx2 = g.d2.dx, *dx3 = g.d3.dx;
     const double *rdx1 = g.d1.rdx, *rdx2 = g.d2.rdx, *rdx3 = g.d3.rdx;
     const long long sj = g.P1, sk = (long long)g.P1 * g.P2;
-    // blocks stride over the (j, k) rows, threads along i
-    for (int q = blockIdx.x; q < rows; q += gridDim.x)
-    for (int i = 1 + threadIdx.x; i <= g.N1; i += blockDim.x) {
-        const int k = 1 + q / g.N2, j = 1 + q - (k - 1) * g.N2;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const int i = 1 + (int)(t % g.N1);
+        const long long q = t / g.N1;
+        const int j = 1 + (int)(q % g.N2), k = 1 + (int)(q / g.N2);
         const long long c = ix(g, i, j, k);
         double Uc, Vc, Wc, Ux, Vy, Wz;
         if constexpr (HasLo<R>::on) {     // the FP32 form's velocity is its high + low pair

@@ -18,6 +18,7 @@ struct ThermalZ {
     using Real = R;
     static constexpr int NRHS = 1;
     static constexpr int MINB = LineOcc<R>::z;
+    static constexpr int MREG = LineOcc<Real>::reg_z;
     static constexpr bool CONTIG = false;
     GridT<R> g; FieldsT<R> f; int TL;
     __device__ bool skip() const { return blown(g); }
@@ -107,6 +108,7 @@ struct ThermalX {
     using Real = R;
     static constexpr int NRHS = 1;
     static constexpr int MINB = LineOcc<R>::xy;
+    static constexpr int MREG = LineOcc<Real>::reg_xy;
     static constexpr bool CONTIG = true;
     GridT<R> g; FieldsT<R> f; int TL;
     __device__ bool skip() const { return blown(g); }
@@ -166,6 +168,7 @@ struct ThermalY {
     using Real = R;
     static constexpr int NRHS = 1;
     static constexpr int MINB = LineOcc<R>::xy;
+    static constexpr int MREG = LineOcc<Real>::reg_xy;
     static constexpr bool CONTIG = false;
     GridT<R> g; FieldsT<R> f; int TL;
     __device__ bool skip() const { return blown(g); }

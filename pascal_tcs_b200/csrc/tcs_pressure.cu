@@ -157,8 +157,9 @@ __global__ void __launch_bounds__(256) prhs_fftx_kernel(GridT<R> g, FieldsT<R> f
     extern __shared__ __align__(16) unsigned char smraw[];
     if (blown(g)) return;
     const int N1 = g.N1, j0 = 1 + blockIdx.x * NL, k = 1 + blockIdx.y;
-    C *b0 = reinterpret_cast<C *>(smraw), *b1 = b0 + NL * N1;
-    double *su = reinterpret_cast<double *>(b1 + NL * N1);   // NL x N1 new U along the line
+    const int nfl = (NL + 1) >> 1;                     // packed complex FFT lines
+    C *b0 = reinterpret_cast<C *>(smraw), *b1 = b0 + nfl * N1;
+    double *su = reinterpret_cast<double *>(b1 + nfl * N1);  // NL x N1 new U along the line
     const double *dx1 = g.d1.dx, *dx2 = g.d2.dx, *dx3 = g.d3.dx;
     const double *rdx1 = g.d1.rdx, *rdx2 = g.d2.rdx, *rdx3 = g.d3.rdx;
     const double *rdmx1 = g.d1.rdmx, *rdmx2 = g.d2.rdmx, *rdmx3 = g.d3.rdmx;
@@ -199,7 +200,10 @@ __global__ void __launch_bounds__(256) prhs_fftx_kernel(GridT<R> g, FieldsT<R> f
     const Phys &p = g.phd;
     for (int t = threadIdx.x; t < NL * N1; t += blockDim.x) {
         const int l = (int)fp.dn.div(t), i = t - l * N1 + 1, j = j0 + l;
-        if (j > g.N2) { b0[t] = make_double2(0.0, 0.0); continue; }
+        // two real lines per complex FFT line: line l is the real (l even) or
+        // imaginary (l odd) part of packed line l/2
+        double *const slot = reinterpret_cast<double *>(b0) + 2 * ((l >> 1) * N1 + (i - 1)) + (l & 1);
+        if (j > g.N2) { *slot = 0.0; continue; }
         const int im = i - 1, ip = i + 1, jm = j - 1, jp = j + 1, km = k - 1, kp = k + 1;
         const long long c = ix(g, i, j, k);
         const double jvm = (j == 1) ? 0.0 : 1.0, jvp = (j == g.N2) ? 0.0 : 1.0;
@@ -240,14 +244,19 @@ __global__ void __launch_bounds__(256) prhs_fftx_kernel(GridT<R> g, FieldsT<R> f
         const double Extra = ((1.0 - iR2_) * ddpdx2 - (1.0 - iR1) * ddpdx1) * rdx1[i]
                            + ((1.0 - iR4) * ddpdy4 - (1.0 - iR3) * ddpdy3) * rdx2[j]
                            + ((1.0 - iR6) * ddpdz6 - (1.0 - iR5) * ddpdz5) * rdx3[k];
-        b0[t] = make_double2((DivUm - cbc) * rdt / p.Cmp + Extra, 0.0);
+        *slot = (DivUm - cbc) * rdt / p.Cmp + Extra;
     }
+    if (NL & 1)         // an odd line count leaves the last packed line without an imaginary part
+        for (int t = threadIdx.x; t < N1; t += blockDim.x) b0[(NL >> 1) * N1 + t].y = 0.0;
     __syncthreads();
-    const C *res = block_fft<-1>(b0, b1, NL, N1, fp, f.tw1);
+    const C *res = block_fft<-1>(b0, b1, nfl, N1, fp, f.tw1);
+    // Z = FFT(a + i b) of real a, b: A(k) = (Z(k) + conj Z(N-k)) / 2, B(k) = (Z(k) - conj Z(N-k)) / 2i
     for (int t = threadIdx.x; t < NL * h1p; t += blockDim.x) {
         const int l = (int)fp.dh.div(t), kx = t - l * h1p, j = j0 + l;
         if (j > g.N2) continue;
-        const C v = res[l * N1 + kx];
+        const C z = res[(l >> 1) * N1 + kx], zr = res[(l >> 1) * N1 + (kx == 0 ? 0 : N1 - kx)];
+        const C v = (l & 1) ? make_double2(0.5 * (z.y + zr.y), 0.5 * (zr.x - z.x))
+                            : make_double2(0.5 * (z.x + zr.x), 0.5 * (z.y - zr.y));
         f.S[sidx(g, h1p, kx, j, k - 1)] = mkc<R>(R(v.x), R(v.y));
     }
 }
@@ -346,11 +355,12 @@ __global__ void __launch_bounds__(256) ifftx_kernel(GridT<R> g, FieldsT<R> f, FF
     extern __shared__ __align__(16) unsigned char smraw[];
     if (blown(g)) return;
     const int N1 = g.N1, j0 = 1 + blockIdx.x * NL, k = 1 + blockIdx.y;
-    C *b0 = reinterpret_cast<C *>(smraw), *b1 = b0 + NL * N1;
-    for (int t = threadIdx.x; t < NL * N1; t += blockDim.x) {
-        const int l = (int)fp.dn.div(t), kx = t - l * N1, j = j0 + l;
+    C *b0 = reinterpret_cast<C *>(smraw), *b1 = b0 + ((NL + 1) >> 1) * N1;
+    // the Hermitian spectrum of line l at kx (zero for lines past the grid)
+    auto herm = [&](int l, int kx) -> C {
+        const int j = j0 + l;
         C v = make_double2(0.0, 0.0);
-        if (j <= g.N2) {
+        if (l < NL && j <= g.N2) {
             if (kx < h1p) {
                 const cplx_t<R> w = f.S[sidx(g, h1p, kx, j, k - 1)];
                 v = make_double2(w.x, w.y);
@@ -360,15 +370,23 @@ __global__ void __launch_bounds__(256) ifftx_kernel(GridT<R> g, FieldsT<R> f, FF
                 v = make_double2(w.x, -w.y);
             }
         }
-        b0[t] = v;
+        return v;
+    };
+    // two lines per complex inverse FFT: Z = A + i B gives a + i b with a, b real
+    const int nfl = (NL + 1) >> 1;
+    for (int t = threadIdx.x; t < nfl * N1; t += blockDim.x) {
+        const int p = (int)fp.dn.div(t), kx = t - p * N1;
+        const C a = herm(2 * p, kx), b = herm(2 * p + 1, kx);
+        b0[t] = make_double2(a.x - b.y, a.y + b.x);
     }
     __syncthreads();
-    const C *res = block_fft<1>(b0, b1, NL, N1, fp, f.tw1);
+    const C *res = block_fft<1>(b0, b1, nfl, N1, fp, f.tw1);
     const double aver = g.scal[S_AVER];
     for (int t = threadIdx.x; t < NL * N1; t += blockDim.x) {
         const int l = (int)fp.dn.div(t), i = t - l * N1 + 1, j = j0 + l;
         if (j > g.N2) continue;
-        const double v = res[t].x / (double)N1 / (double)g.N3 - aver;
+        const C z = res[(l >> 1) * N1 + (i - 1)];
+        const double v = ((l & 1) ? z.y : z.x) / (double)N1 / (double)g.N3 - aver;
         store_periodic(g, f.dP, i, j, k, R(v));
     }
 }
@@ -464,7 +482,11 @@ __global__ void p_wall_kernel(GridT<R> g, FieldsT<R> f, double ab, double bb, do
 }
 
 template <class R>
-static size_t fftx_smem(const Ctx<R> &cx) { return (size_t)cx.fft_lines_x * cx.g.N1 * (2 * sizeof(double2) + sizeof(double)); }
+static size_t fftx_smem(const Ctx<R> &cx)
+{
+    // two packed FFT buffers of (lines + 1) / 2 complex lines, and the new U of every line
+    return (size_t)((cx.fft_lines_x + 1) / 2) * cx.g.N1 * 2 * sizeof(double2) + (size_t)cx.fft_lines_x * cx.g.N1 * sizeof(double);
+}
 
 template <class R>
 void launch_pseudo_prhs_fftx(const Ctx<R> &cx, cudaStream_t s, bool with_pseudo)
@@ -486,7 +508,7 @@ void launch_poisson_rest(const Ctx<R> &cx, cudaStream_t s)
     const GridT<R> &g = cx.g;
     const int h1p = cx.h1p, NLz = cx.fft_lines_z, NLx = cx.fft_lines_x;
     const size_t smz = (size_t)NLz * g.N3 * 2 * sizeof(double2);
-    const size_t smx = (size_t)NLx * g.N1 * 2 * sizeof(double2);
+    const size_t smx = (size_t)((NLx + 1) / 2) * g.N1 * 2 * sizeof(double2);
     static size_t cz = 0, cx2 = 0;
     if (smz > cz) {
         cudaFuncSetAttribute(fftz_kernel<-1, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smz);

@@ -135,6 +135,14 @@ int tcs_tdma_plan_many_destroy(tcs_tdma_plan *plan);
 int tcs_tdma_many_solve(tcs_tdma_plan *plan, double *A, double *B, double *C, double *D, int n_sys, int n_row);
 /* pascal_tdma.f90:715 PaScaL_TDMA_many_solve_cycle(plan, A, B, C, D, n_sys, n_row) */
 int tcs_tdma_many_solve_cycle(tcs_tdma_plan *plan, double *A, double *B, double *C, double *D, int n_sys, int n_row);
+/* PaScaL_TDMA_plan_single_create/destroy, _single_solve(_cycle) (pascal_tdma.f90:139-175, 301-475) and
+ * _many_solve(_cycle)_nonblocking (:590-703, 818-930): on one rank the same kernel as the many solve */
+int tcs_tdma_plan_single_create(tcs_tdma_plan **plan, int myrank, int nprocs, int gather_rank);
+int tcs_tdma_plan_single_destroy(tcs_tdma_plan *plan);
+int tcs_tdma_single_solve(tcs_tdma_plan *plan, double *A, double *B, double *C, double *D, int n_row);
+int tcs_tdma_single_solve_cycle(tcs_tdma_plan *plan, double *A, double *B, double *C, double *D, int n_row);
+int tcs_tdma_many_solve_nonblocking(tcs_tdma_plan *plan, double *A, double *B, double *C, double *D, int n_sys, int n_row);
+int tcs_tdma_many_solve_cycle_nonblocking(tcs_tdma_plan *plan, double *A, double *B, double *C, double *D, int n_sys, int n_row);
 
 /* No counterpart in the reference.  The PaScaL_TDMA many-systems solve
  * (cyclic != 0: the _cycle form) for callers that cannot allocate device
@@ -152,6 +160,20 @@ int tcs_tdma_many_solve_noalloc(double *A, double *B, double *C, double *D, int 
 
 /* ---- measurement --------------------------------------------------------- */
 int tcs_kernel_count(void);
+/* Restart files and planes (module_post.f90): the continue files of
+ * :1264-1454 (cont_time.bin = time, dt; cont_U/V/W/P/T.bin = the n1m*n2m*n3m
+ * interior, i fastest, FP64) written and read by k-slabs straight from the
+ * device, plus cont_dPhat.bin and cont_dP0.bin so that a resumed run continues
+ * bit for bit (*with_pressure_history = 0 when those two are absent).  After a
+ * read the periodic ghosts are refreshed before the next stage.
+ * tcs_extract_plane copies one padded plane (axis 1: i = index over (j,k),
+ * 2: j = index over (i,k), 3: k = index over (i,j); first index fastest) of
+ * nfields fields into out, field after field: the instant-field planes of
+ * :270-361 without downloading whole fields. */
+int tcs_write_continue(tcs_ctx *ctx, const char *dir);
+int tcs_read_continue(tcs_ctx *ctx, const char *dir, int *with_pressure_history);
+int tcs_extract_plane(tcs_ctx *ctx, int axis, int index, int nfields, const int *fields, double *out);
+
 /* Ensembles (no counterpart in the reference, which runs one case per MPI job):
  * independent cases on one device advanced together.  Every tcs_ensemble_step
  * replays one CUDA graph per step in which each case is its own branch, so the

@@ -6,6 +6,7 @@
 #include "tcs_kernels.h"
 #include "tcs.h"
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -171,6 +172,8 @@ struct tcs_ctx {
     Ctx<double> cx;
     Ctx<float> cf;
     double *stage = nullptr;             // FP64 staging copy of one field (FP32 form)
+    double *io_dev = nullptr, *io_host = nullptr;   // file IO chunk: device staging and pinned host copy
+    size_t io_cap = 0;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     std::vector<double> hm[9];           // x1, dx1, dmx1, x2, dx2, dmx2, x3, dx3, dmx3
@@ -561,6 +564,7 @@ int tcs_destroy(tcs_ctx *c)
     if (c->stream) cudaStreamSynchronize(c->stream);
     for (auto &ge : c->graphs) cudaGraphExecDestroy(ge.exec);
     for (void *p : c->allocs) cudaFree(p);
+    if (c->io_host) cudaFreeHost(c->io_host);
     for (auto &v : c->probe.rec) for (auto &pr : v) { cudaEventDestroy(pr.first); cudaEventDestroy(pr.second); }
     for (cudaEvent_t e : c->probe.pool) cudaEventDestroy(e);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
@@ -1396,3 +1400,193 @@ extern "C" int tcs_autotune(tcs_ctx *c, int trial_steps, const char *cache_path,
     }
     return TCS_OK;
 }
+
+// ---------------------------------------------------------------------------
+// PaScaL_TDMA single-system and nonblocking entry points
+// (pascal_tdma.f90:139-175, 301-475, 590-703, 818-930).  On one rank the
+// single-system solve is the many-system solve with n_sys = 1 (tdma_single
+// and tdma_cycl_single of tdmas.f90:27-100 do the many versions' arithmetic
+// on the 2-row reduced system), and the nonblocking variants differ only in
+// their MPI calls, so all of them run the same kernel.
+// ---------------------------------------------------------------------------
+extern "C" {
+
+int tcs_tdma_plan_single_create(tcs_tdma_plan **plan, int myrank, int nprocs, int gather_rank)
+{
+    if (gather_rank != 0) return set_err(TCS_ERR_UNSUPPORTED, "one GPU holds the whole line: gather_rank must be 0");
+    return tcs_tdma_plan_many_create(plan, 1, myrank, nprocs);
+}
+
+int tcs_tdma_plan_single_destroy(tcs_tdma_plan *p) { return tcs_tdma_plan_many_destroy(p); }
+
+int tcs_tdma_single_solve(tcs_tdma_plan *p, double *A, double *B, double *C, double *D, int n_row)
+{
+    return tdma_solve(p, A, B, C, D, 1, n_row, 0);
+}
+
+int tcs_tdma_single_solve_cycle(tcs_tdma_plan *p, double *A, double *B, double *C, double *D, int n_row)
+{
+    return tdma_solve(p, A, B, C, D, 1, n_row, 1);
+}
+
+int tcs_tdma_many_solve_nonblocking(tcs_tdma_plan *p, double *A, double *B, double *C, double *D, int n_sys, int n_row)
+{
+    return tdma_solve(p, A, B, C, D, n_sys, n_row, 0);
+}
+
+int tcs_tdma_many_solve_cycle_nonblocking(tcs_tdma_plan *p, double *A, double *B, double *C, double *D, int n_sys, int n_row)
+{
+    return tdma_solve(p, A, B, C, D, n_sys, n_row, 1);
+}
+
+} // extern "C"
+
+// ---------------------------------------------------------------------------
+// Restart files and planes from the device.
+//
+// tcs_write_continue / tcs_read_continue write and read the reference's
+// continue files (module_post.f90:1264-1454: cont_time.bin = time, dt;
+// cont_U/V/W/P/T.bin = the n1m x n2m x n3m interior, i fastest, FP64) by
+// k-slabs through one device staging chunk and one pinned host chunk, and add
+// cont_dPhat.bin and cont_dP0.bin, which the reference does not save, so that
+// a resumed run continues bit for bit.  tcs_extract_plane copies one padded
+// plane of chosen fields to the host (the instant-field planes of
+// module_post.f90:270-361) without moving the rest of the field.
+// ---------------------------------------------------------------------------
+static int io_chunk(tcs_ctx *c, size_t n)
+{
+    if (n <= c->io_cap) return TCS_OK;
+    if (c->io_host) { cudaFreeHost(c->io_host); c->io_host = nullptr; }
+    int r = dalloc(c, &c->io_dev, n);
+    if (r) return r;
+    if (cudaMallocHost(&c->io_host, n * sizeof(double)) != cudaSuccess) return set_err(TCS_ERR_NOMEM, "pinned IO buffer");
+    c->io_cap = n;
+    return TCS_OK;
+}
+
+static const struct { int field; const char *name; } k_cont[] = {
+    {TCS_F_U, "cont_U.bin"}, {TCS_F_V, "cont_V.bin"}, {TCS_F_W, "cont_W.bin"}, {TCS_F_P, "cont_P.bin"},
+    {TCS_F_T, "cont_T.bin"}, {TCS_F_DPHAT, "cont_dPhat.bin"}, {TCS_F_DP0, "cont_dP0.bin"}};
+
+static std::string join_path(const char *dir, const char *name)
+{
+    std::string d = dir ? dir : "";
+    if (!d.empty() && d.back() != '/') d += '/';
+    return d + name;
+}
+
+extern "C" {
+
+int tcs_write_continue(tcs_ctx *c, const char *dir)
+{
+    ENTER(c);
+    int r = flush_pending(c);
+    if (r) return r;
+    const GridT<double> &g = c->cx.g;
+    const int ks = std::max(1, (int)((size_t)(4u << 20) / ((size_t)g.N1 * g.N2)));
+    if ((r = io_chunk(c, (size_t)g.N1 * g.N2 * ks))) return r;
+    double sc[S_NSCAL];
+    CK(cudaMemcpyAsync(sc, g.scal, sizeof(sc), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    {
+        FILE *fp = std::fopen(join_path(dir, "cont_time.bin").c_str(), "wb");
+        if (!fp) return set_err(TCS_ERR_ARG, "cannot open cont_time.bin for writing");
+        const double td[2] = {sc[S_TIME], sc[S_DT]};
+        const bool ok = std::fwrite(td, sizeof(double), 2, fp) == 2;
+        std::fclose(fp);
+        if (!ok) return set_err(TCS_ERR_ARG, "short write of cont_time.bin");
+    }
+    for (const auto &cf : k_cont) {
+        FILE *fp = std::fopen(join_path(dir, cf.name).c_str(), "wb");
+        if (!fp) return set_err(TCS_ERR_ARG, std::string("cannot open ") + cf.name + " for writing");
+        bool ok = true;
+        for (int k0 = 1; k0 <= g.N3 && ok; k0 += ks) {
+            const int nk = std::min(ks, g.N3 - k0 + 1);
+            const size_t n = (size_t)g.N1 * g.N2 * nk;
+            on_ctx(c, [&](auto &x) { launch_pack(x, field_ptr_t(x.f, cf.field), lo_ptr_t(x.f, cf.field), c->io_dev, k0, nk, c->stream); });
+            if ((r = take_launch_error())) { std::fclose(fp); return r; }
+            if (cudaMemcpyAsync(c->io_host, c->io_dev, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||
+                cudaStreamSynchronize(c->stream) != cudaSuccess) { std::fclose(fp); return set_err(TCS_ERR_CUDA, "continue-file copy"); }
+            ok = std::fwrite(c->io_host, sizeof(double), n, fp) == n;
+        }
+        std::fclose(fp);
+        if (!ok) return set_err(TCS_ERR_ARG, std::string("short write of ") + cf.name);
+    }
+    return TCS_OK;
+}
+
+int tcs_read_continue(tcs_ctx *c, const char *dir, int *with_pressure_history)
+{
+    ENTER(c);
+    int r = flush_pending(c);
+    if (r) return r;
+    const GridT<double> &g = c->cx.g;
+    const int ks = std::max(1, (int)((size_t)(4u << 20) / ((size_t)g.N1 * g.N2)));
+    if ((r = io_chunk(c, (size_t)g.N1 * g.N2 * ks))) return r;
+    double td[2];
+    {
+        FILE *fp = std::fopen(join_path(dir, "cont_time.bin").c_str(), "rb");
+        if (!fp) return set_err(TCS_ERR_ARG, "cannot open cont_time.bin");
+        const bool ok = std::fread(td, sizeof(double), 2, fp) == 2;
+        std::fclose(fp);
+        if (!ok) return set_err(TCS_ERR_ARG, "cont_time.bin is short");
+    }
+    int history = 1;
+    const size_t want = (size_t)g.N1 * g.N2 * g.N3;
+    for (const auto &cf : k_cont) {
+        FILE *fp = std::fopen(join_path(dir, cf.name).c_str(), "rb");
+        const bool optional = cf.field == TCS_F_DPHAT || cf.field == TCS_F_DP0;
+        if (!fp) {
+            if (optional) { history = 0; continue; }
+            return set_err(TCS_ERR_ARG, std::string("cannot open ") + cf.name);
+        }
+        std::fseek(fp, 0, SEEK_END);
+        const long sz = std::ftell(fp);
+        std::fseek(fp, 0, SEEK_SET);
+        if (sz != (long)(want * sizeof(double))) { std::fclose(fp); return set_err(TCS_ERR_ARG, std::string(cf.name) + " does not hold n1m*n2m*n3m doubles"); }
+        for (int k0 = 1; k0 <= g.N3; k0 += ks) {
+            const int nk = std::min(ks, g.N3 - k0 + 1);
+            const size_t n = (size_t)g.N1 * g.N2 * nk;
+            if (std::fread(c->io_host, sizeof(double), n, fp) != n) { std::fclose(fp); return set_err(TCS_ERR_ARG, std::string("short read of ") + cf.name); }
+            if (cudaMemcpyAsync(c->io_dev, c->io_host, n * sizeof(double), cudaMemcpyHostToDevice, c->stream) != cudaSuccess) {
+                std::fclose(fp); return set_err(TCS_ERR_CUDA, "continue-file copy");
+            }
+            on_ctx(c, [&](auto &x) {
+                auto *d2 = cf.field == TCS_F_T ? x.f.Tn : nullptr;
+                launch_unpack(x, c->io_dev, field_ptr_t(x.f, cf.field), d2, lo_ptr_t(x.f, cf.field), k0, nk, c->stream);
+            });
+            if ((r = take_launch_error())) { std::fclose(fp); return r; }
+            CK(cudaStreamSynchronize(c->stream));     // the pinned chunk is refilled next
+        }
+        std::fclose(fp);
+        c->ghost_ok &= ~(1u << cf.field);
+    }
+    CK(cudaMemcpyAsync(g.scal + S_TIME, &td[0], sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(g.scal + S_DT, &td[1], sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (with_pressure_history) *with_pressure_history = history;
+    return TCS_OK;
+}
+
+int tcs_extract_plane(tcs_ctx *c, int axis, int index, int nfields, const int *fields, double *out)
+{
+    ENTER(c);
+    if (axis < 1 || axis > 3 || nfields < 1 || !fields || !out) return set_err(TCS_ERR_ARG, "bad plane arguments");
+    const GridT<double> &g = c->cx.g;
+    const int P3 = g.N3 + 2, lim = axis == 1 ? g.P1 : (axis == 2 ? g.P2 : P3);
+    if (index < 0 || index >= lim) return set_err(TCS_ERR_ARG, "plane index outside the padded range");
+    int r = flush_pending(c);
+    if (r) return r;
+    const size_t n = (size_t)(axis == 1 ? g.P2 : g.P1) * (axis == 3 ? g.P2 : P3);
+    if ((r = io_chunk(c, n))) return r;
+    for (int q = 0; q < nfields; q++) {
+        if (fields[q] < 0 || fields[q] >= TCS_F_MU) return set_err(TCS_ERR_ARG, "unknown field");
+        on_ctx(c, [&](auto &x) { launch_plane(x, field_ptr_t(x.f, fields[q]), lo_ptr_t(x.f, fields[q]), c->io_dev, axis, index, c->stream); });
+        if ((r = take_launch_error())) return r;
+        CK(cudaMemcpyAsync(out + q * n, c->io_dev, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    return TCS_OK;
+}
+
+} // extern "C"

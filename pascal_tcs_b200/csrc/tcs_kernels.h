@@ -105,6 +105,9 @@ template <class R> void launch_ghost(const Ctx<R> &cx, R *a, cudaStream_t s);
 template <class R> void launch_convert(const R *src, double *dst, long long n, cudaStream_t s);   // field -> FP64 staging
 template <class R> void launch_convert_in(const double *src, R *dst, long long n, cudaStream_t s); // FP64 staging -> field
 void launch_join(const float *hi, const float *lo, double *dst, long long n, cudaStream_t s);       // FP32 pair -> FP64 staging
+template <class R> void launch_pack(const Ctx<R> &cx, const R *src, const R *lo, double *dst, int k0, int nk, cudaStream_t s);
+template <class R> void launch_unpack(const Ctx<R> &cx, const double *src, R *dst, R *dst2, R *lo, int k0, int nk, cudaStream_t s);
+template <class R> void launch_plane(const Ctx<R> &cx, const R *src, const R *lo, double *dst, int axis, int index, cudaStream_t s);
 void launch_split(const double *src, float *hi, float *lo, long long n, cudaStream_t s);          // FP64 staging -> FP32 pair
 
 } // namespace tcs

@@ -221,6 +221,73 @@ void launch_convert_in(const double *src, R *dst, long long n, cudaStream_t s)
     record_launch_error("convert_in");
 }
 
+// Interior k-slabs of a field to/from a packed FP64 array (i fastest), the
+// layout of the reference's continue files (module_post.f90:1264-1454); in the
+// FP32 form the velocity's low word is added on the way out and split off on
+// the way in.
+template <class R>
+__global__ void pack_kernel(GridT<R> g, const R *src, const R *lo, double *dst, int k0, int nk)
+{
+    const int n = g.N1 * g.N2 * nk;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        const int i = t % g.N1, q = t / g.N1, j = q % g.N2, k = q / g.N2;
+        const long long c = ix(g, 1 + i, 1 + j, k0 + k);
+        dst[t] = lo ? (double)src[c] + (double)lo[c] : (double)src[c];
+    }
+}
+template <class R>
+__global__ void unpack_kernel(GridT<R> g, const double *src, R *dst, R *dst2, R *lo, int k0, int nk)
+{
+    const int n = g.N1 * g.N2 * nk;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        const int i = t % g.N1, q = t / g.N1, j = q % g.N2, k = q / g.N2;
+        const long long c = ix(g, 1 + i, 1 + j, k0 + k);
+        const R h = (R)src[t];
+        dst[c] = h;
+        if (dst2) dst2[c] = h;
+        if (lo) lo[c] = (R)(src[t] - (double)h);
+    }
+}
+// One padded plane of a field: axis 1 (i = index) over (j, k), axis 2 over
+// (i, k), axis 3 over (i, j); the first of the two remaining indices fastest.
+template <class R>
+__global__ void plane_kernel(GridT<R> g, const R *src, const R *lo, double *dst, int axis, int index)
+{
+    const int P3 = g.N3 + 2;
+    const int na = axis == 1 ? g.P2 : g.P1, nb = axis == 3 ? g.P2 : P3;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < na * nb; t += gridDim.x * blockDim.x) {
+        const int a = t % na, b = t / na;
+        const long long c = axis == 1 ? ix(g, index, a, b) : (axis == 2 ? ix(g, a, index, b) : ix(g, a, b, index));
+        dst[t] = lo ? (double)src[c] + (double)lo[c] : (double)src[c];
+    }
+}
+
+template <class R>
+void launch_pack(const Ctx<R> &cx, const R *src, const R *lo, double *dst, int k0, int nk, cudaStream_t s)
+{
+    pack_kernel<R><<<4 * 148, 256, 0, s>>>(cx.g, src, lo, dst, k0, nk);
+    record_launch_error("pack");
+}
+template <class R>
+void launch_unpack(const Ctx<R> &cx, const double *src, R *dst, R *dst2, R *lo, int k0, int nk, cudaStream_t s)
+{
+    unpack_kernel<R><<<4 * 148, 256, 0, s>>>(cx.g, src, dst, dst2, lo, k0, nk);
+    record_launch_error("unpack");
+}
+template <class R>
+void launch_plane(const Ctx<R> &cx, const R *src, const R *lo, double *dst, int axis, int index, cudaStream_t s)
+{
+    plane_kernel<R><<<148, 256, 0, s>>>(cx.g, src, lo, dst, axis, index);
+    record_launch_error("plane");
+}
+
+template void launch_pack<double>(const Ctx<double> &, const double *, const double *, double *, int, int, cudaStream_t);
+template void launch_pack<float>(const Ctx<float> &, const float *, const float *, double *, int, int, cudaStream_t);
+template void launch_unpack<double>(const Ctx<double> &, const double *, double *, double *, double *, int, int, cudaStream_t);
+template void launch_unpack<float>(const Ctx<float> &, const double *, float *, float *, float *, int, int, cudaStream_t);
+template void launch_plane<double>(const Ctx<double> &, const double *, const double *, double *, int, int, cudaStream_t);
+template void launch_plane<float>(const Ctx<float> &, const float *, const float *, double *, int, int, cudaStream_t);
+
 // the two forms
 template void launch_post<double>(const Ctx<double> &, cudaStream_t, int);
 template void launch_post<float>(const Ctx<float> &, cudaStream_t, int);

@@ -42,7 +42,9 @@ EXPORTS = [
     "tcs_tdma_many_solve_cycle", "tcs_tdma_many_solve_noalloc", "tcs_kernel_count", "tcs_launch_count", "tcs_kernel_name", "tcs_probe_enable",
     "tcs_probe_read", "tcs_probe_reset", "tcs_set_use_graph", "tcs_set_tuning", "tcs_get_tuning",
     "tcs_last_error", "tcs_precision", "tcs_ensemble_create", "tcs_ensemble_destroy", "tcs_ensemble_step",
-    "tcs_ensemble_size", "tcs_autotune",
+    "tcs_ensemble_size", "tcs_autotune", "tcs_write_continue", "tcs_read_continue", "tcs_extract_plane",
+    "tcs_tdma_plan_single_create", "tcs_tdma_plan_single_destroy", "tcs_tdma_single_solve",
+    "tcs_tdma_single_solve_cycle", "tcs_tdma_many_solve_nonblocking", "tcs_tdma_many_solve_cycle_nonblocking",
 ]
 
 
@@ -134,6 +136,15 @@ def load() -> ctypes.CDLL:
         "tcs_ensemble_step": ([vp, ip, ctypes.POINTER(ip)], ip),
         "tcs_ensemble_size": ([vp], ip),
         "tcs_autotune": ([vp, ip, ctypes.c_char_p, ctypes.POINTER(ip)], ip),
+        "tcs_write_continue": ([vp, ctypes.c_char_p], ip),
+        "tcs_read_continue": ([vp, ctypes.c_char_p, ctypes.POINTER(ip)], ip),
+        "tcs_extract_plane": ([vp, ip, ip, ip, ctypes.POINTER(ip), dp], ip),
+        "tcs_tdma_plan_single_create": ([ctypes.POINTER(vp), ip, ip, ip], ip),
+        "tcs_tdma_plan_single_destroy": ([vp], ip),
+        "tcs_tdma_single_solve": ([vp, vp, vp, vp, vp, ip], ip),
+        "tcs_tdma_single_solve_cycle": ([vp, vp, vp, vp, vp, ip], ip),
+        "tcs_tdma_many_solve_nonblocking": ([vp, vp, vp, vp, vp, ip, ip], ip),
+        "tcs_tdma_many_solve_cycle_nonblocking": ([vp, vp, vp, vp, vp, ip, ip], ip),
     }
     for name in ("tcs_thermal_coeffi", "tcs_thermal_solver", "tcs_thermal_coeffi_clean",
                  "tcs_momentum_coeffi", "tcs_momentum_solvedU", "tcs_momentum_solvedV",
@@ -212,6 +223,26 @@ class Solver:
 
     def download_async(self, name: str, pinned_ptr: int) -> None:
         _check(load().tcs_download_field_async(self._h, FIELDS[name], pinned_ptr), f"download {name}")
+
+    def write_continue(self, directory: str) -> None:
+        """cont_time/U/V/W/P/T.bin (the reference's continue files) plus cont_dPhat/dP0.bin."""
+        _check(load().tcs_write_continue(self._h, directory.encode()), "write_continue")
+
+    def read_continue(self, directory: str) -> bool:
+        """Read continue files; True when dPhat and dP0 were there too."""
+        h = ctypes.c_int(0)
+        _check(load().tcs_read_continue(self._h, directory.encode(), ctypes.byref(h)), "read_continue")
+        return bool(h.value)
+
+    def plane(self, axis: int, index: int, fields=("U", "V", "W", "P", "T")) -> np.ndarray:
+        """Padded planes (axis 1: i=index, 2: j=index, 3: k=index) of the fields, shape (nfields, nb, na)."""
+        P3, P2, P1 = self.shape
+        na = P2 if axis == 1 else P1
+        nb = P2 if axis == 3 else P3
+        ids = (ctypes.c_int * len(fields))(*[FIELDS[f] for f in fields])
+        out = np.empty((len(fields), nb, na))
+        _check(load().tcs_extract_plane(self._h, int(axis), int(index), len(fields), ids, _dptr(out)), "extract_plane")
+        return out
 
     @property
     def precision(self) -> int:
@@ -433,6 +464,41 @@ class TdmaPlan:
 
     def many_solve_cycle(self, A, B, C, D, n_sys: int, n_row: int) -> None:
         self._solve("tcs_tdma_many_solve_cycle", A, B, C, D, n_sys, n_row)
+
+    def many_solve_nonblocking(self, A, B, C, D, n_sys: int, n_row: int) -> None:
+        self._solve("tcs_tdma_many_solve_nonblocking", A, B, C, D, n_sys, n_row)
+
+    def many_solve_cycle_nonblocking(self, A, B, C, D, n_sys: int, n_row: int) -> None:
+        self._solve("tcs_tdma_many_solve_cycle_nonblocking", A, B, C, D, n_sys, n_row)
+
+
+class TdmaPlanSingle(TdmaPlan):
+    """PaScaL_TDMA_plan_single_create / single_solve(_cycle) / destroy
+    (pascal_tdma.f90:139-175, 301-475): one system of n_row rows."""
+
+    def __init__(self, myrank: int = 0, nprocs: int = 1, gather_rank: int = 0):
+        h = ctypes.c_void_p()
+        _check(load().tcs_tdma_plan_single_create(ctypes.byref(h), int(myrank), int(nprocs), int(gather_rank)),
+               "PaScaL_TDMA_plan_single_create")
+        self._h, self.n_sys = h, 1
+
+    def destroy(self) -> None:
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.tcs_tdma_plan_single_destroy(self._h)
+            self._h = None
+
+    def _single(self, fn: str, A, B, C, D, n_row: int) -> None:
+        ptrs = []
+        for x in (A, B, C, D):
+            assert isinstance(x, np.ndarray) and x.dtype == np.float64 and x.flags["C_CONTIGUOUS"]
+            ptrs.append(x.ctypes.data)
+        _check(getattr(load(), fn)(self._h, *ptrs, int(n_row)), fn)
+
+    def single_solve(self, A, B, C, D, n_row: int) -> None:
+        self._single("tcs_tdma_single_solve", A, B, C, D, n_row)
+
+    def single_solve_cycle(self, A, B, C, D, n_row: int) -> None:
+        self._single("tcs_tdma_single_solve_cycle", A, B, C, D, n_row)
 
 
 # Largest n_sys * n_row accepted by tdma_many_solve_noalloc (TCS_TDMA_NOALLOC_MAX_ELEMS).

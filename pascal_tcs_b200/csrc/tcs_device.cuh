@@ -622,32 +622,43 @@ __device__ __forceinline__ void warp_resolve_line(const R *__restrict__ A, const
 
 // The kernel.  Prob supplies:
 //   using Real (row type: the field type, or double for FP64 solves of FP32 data);
-//   static constexpr int NRHS, MINB (blocks per SM);  static constexpr bool CONTIG (rows contiguous in memory);
+//   static constexpr int NRHS, NT (threads per block), MINB (blocks per SM), MREG (rows per lane in
+//   registers, 0: in shared memory);  static constexpr bool CONTIG (rows contiguous in memory);
 //   struct State; __device__ State prepare()   -> per-block scalars (dt, stale values)
 //   __device__ bool skip(), line_ok(int l)
 //   __device__ Coef<Real, NRHS> build(int l, int r, const State &)
 //   __device__ void emit(int l, int r, const Real *x, const State &)
-// TL (lines per block) is a power of two; blockDim.x is 256.
+// TL (lines per block) is a power of two; blockDim.x is Prob::NT (a multiple of 32).
 template <class R>
 struct Refine { static constexpr bool on = std::is_same<R, float>::value; };
 
 // Blocks per SM a line-solver family is compiled for (each Prob's MINB; the
-// register budget is 65536 / (256 MINB), and fit_tl sizes the lines per block
+// register budget is 65536 / (NT MINB), and fit_tl sizes the lines per block
 // to the matching shared-memory share).  Measured on B200 at 256^3: the FP64
 // z-sweep stencils need 128 registers and spill below that; the FP64 x and y
 // sweeps run fastest at 4 blocks (64 registers, no spills); the refined FP32
-// rows need 28 B each, so FP32 sweeps and the modal solves run best at 3.
+// rows need 28 B each, so the FP32 z and y sweeps and the modal solves run best
+// at 3 blocks of 256 threads and the FP32 x sweeps at 6 blocks of 128.
 template <class R>
 struct LineOcc {
-    static constexpr int z = std::is_same<R, float>::value ? 3 : 2;
-    static constexpr int xy = std::is_same<R, float>::value ? 3 : 4;
+    static constexpr bool f32 = std::is_same<R, float>::value;
+    static constexpr int z = f32 ? 3 : 2;
+    static constexpr int x = f32 ? 6 : 4;
+    static constexpr int y = f32 ? 3 : 4;
     static constexpr int modal = 3;
     // rows per lane solved in registers (0: in shared memory), per family:
     // wherever the registers allow it without spills (not the FP64 x/y sweeps
     // at 64 registers, nor the two-right-hand-side modal solves at 80)
     static constexpr int reg_z = 8;
-    static constexpr int reg_xy = std::is_same<R, float>::value ? 8 : 0;
+    static constexpr int reg_x = f32 ? 8 : 0;
+    static constexpr int reg_y = f32 ? 8 : 0;
     static constexpr int reg_modal = 0;
+    // threads per block, per family (the FP32 x sweeps run best as 128-thread
+    // blocks of 4 lines: the refined rows fill shared memory, and smaller
+    // blocks wait less at their barriers)
+    static constexpr int nt_z = 256, nt_x = f32 ? 128 : 256, nt_y = 256, nt_modal = 256;
+    // the x sweeps' wide shape, for lines too long to fit 4 per 128-thread block
+    static constexpr int xw = f32 ? 3 : 4, nt_xw = 256, reg_xw = reg_x;
 };
 
 // Solve a line with the register-resident elimination when the lane's
@@ -666,7 +677,7 @@ __host__ __device__ constexpr int line_words()
 }
 
 template <class Prob>
-__global__ void __launch_bounds__(256, Prob::MINB) line_solve_kernel(Prob prob, LinePlan lp)
+__global__ void __launch_bounds__(Prob::NT, Prob::MINB) line_solve_kernel(Prob prob, LinePlan lp)
 {
     using R = typename Prob::Real;
     constexpr int NR = Prob::NRHS;

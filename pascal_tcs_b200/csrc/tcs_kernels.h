@@ -82,9 +82,27 @@ inline void launch_lines(const Prob &p, const LinePlan &lp, dim3 grid, cudaStrea
         configured = smem;
     }
     probe_begin(cx, kid, s);
-    line_solve_kernel<Prob><<<grid, 256, smem, s>>>(p, lp);
+    line_solve_kernel<Prob><<<grid, Prob::NT, smem, s>>>(p, lp);
     probe_end(cx, kid, s);
     record_launch_error(kernel_name(kid));
+}
+
+// An x sweep: lines along i, one block row per (j-range, k).  FP32 runs the
+// 128-thread shape when at least 4 lines fit a block, else the wide shape.
+template <template <class, int> class X, class R>
+inline void launch_x(const Ctx<R> &cx, int nlines, cudaStream_t s, int kid)
+{
+    const GridT<R> &g = cx.g;
+    const int tl = fit_tl<X<R, 0>>(g.N1, true, cx.tl_contig, cx.lanes);
+    if constexpr (LineOcc<R>::f32) {
+        if (tl < 4) {
+            const LinePlan p = make_line_plan(g.N1, true, fit_tl<X<R, 1>>(g.N1, true, cx.tl_contig, cx.lanes), cx.lanes);
+            launch_lines(X<R, 1>{g, cx.f, p.TL}, p, dim3((nlines + p.TL - 1) / p.TL, g.N3), s, kid, cx);
+            return;
+        }
+    }
+    const LinePlan p = make_line_plan(g.N1, true, tl, cx.lanes);
+    launch_lines(X<R, 0>{g, cx.f, p.TL}, p, dim3((nlines + p.TL - 1) / p.TL, g.N3), s, kid, cx);
 }
 
 // Stage launchers (one per reference routine or fused group), instantiated

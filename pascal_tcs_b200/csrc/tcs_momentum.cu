@@ -50,6 +50,7 @@ struct DUZ {
     static constexpr int NRHS = 1;
     static constexpr int MINB = LineOcc<R>::z;
     static constexpr int MREG = LineOcc<Real>::reg_z;
+    static constexpr int NT = LineOcc<Real>::nt_z;
     static constexpr bool CONTIG = false;
     GridT<R> g; FieldsT<R> f; int TL;
     __device__ bool skip() const { return blown(g); }
@@ -131,12 +132,13 @@ struct DUZ {
     __device__ void emit(int l, int r, const R *x, const State &st) const { f.scr[ix(g, li(l), 1 + blockIdx.y, r + 1)] = x[0]; }
 };
 
-template <class R>
+template <class R, int WIDE = 0>
 struct DUX {
     using Real = R;
     static constexpr int NRHS = 1;
-    static constexpr int MINB = LineOcc<R>::xy;
-    static constexpr int MREG = LineOcc<Real>::reg_xy;
+    static constexpr int MINB = WIDE ? LineOcc<R>::xw : LineOcc<R>::x;
+    static constexpr int MREG = WIDE ? LineOcc<Real>::reg_xw : LineOcc<Real>::reg_x;
+    static constexpr int NT = WIDE ? LineOcc<Real>::nt_xw : LineOcc<Real>::nt_x;
     static constexpr bool CONTIG = true;
     GridT<R> g; FieldsT<R> f; int TL;
     __device__ bool skip() const { return blown(g); }
@@ -171,8 +173,9 @@ template <class R>
 struct DUY {
     using Real = R;
     static constexpr int NRHS = 1;
-    static constexpr int MINB = LineOcc<R>::xy;
-    static constexpr int MREG = LineOcc<Real>::reg_xy;
+    static constexpr int MINB = LineOcc<R>::y;
+    static constexpr int MREG = LineOcc<Real>::reg_y;
+    static constexpr int NT = LineOcc<Real>::nt_y;
     static constexpr bool CONTIG = false;
     GridT<R> g; FieldsT<R> f; int TL;
     __device__ bool skip() const { return blown(g); }
@@ -220,6 +223,7 @@ struct DVZ {
     static constexpr int NRHS = 1;
     static constexpr int MINB = LineOcc<R>::z;
     static constexpr int MREG = LineOcc<Real>::reg_z;
+    static constexpr int NT = LineOcc<Real>::nt_z;
     static constexpr bool CONTIG = false;
     GridT<R> g; FieldsT<R> f; int TL;
     __device__ bool skip() const { return blown(g); }
@@ -313,12 +317,13 @@ __device__ __forceinline__ void dv_stale_mu12(const GridT<R> &g, const FieldsT<R
     mu2 = R(0.5) * (dx1[ip] * mxy + dx1[i] * mxy) * rdmx1[ip];
 }
 
-template <class R>
+template <class R, int WIDE = 0>
 struct DVX {
     using Real = R;
     static constexpr int NRHS = 1;
-    static constexpr int MINB = LineOcc<R>::xy;
-    static constexpr int MREG = LineOcc<Real>::reg_xy;
+    static constexpr int MINB = WIDE ? LineOcc<R>::xw : LineOcc<R>::x;
+    static constexpr int MREG = WIDE ? LineOcc<Real>::reg_xw : LineOcc<Real>::reg_x;
+    static constexpr int NT = WIDE ? LineOcc<Real>::nt_xw : LineOcc<Real>::nt_x;
     static constexpr bool CONTIG = true;
     GridT<R> g; FieldsT<R> f; int TL;
     __device__ bool skip() const { return blown(g); }
@@ -358,8 +363,9 @@ template <class R>
 struct DVY {
     using Real = R;
     static constexpr int NRHS = 1;
-    static constexpr int MINB = LineOcc<R>::xy;
-    static constexpr int MREG = LineOcc<Real>::reg_xy;
+    static constexpr int MINB = LineOcc<R>::y;
+    static constexpr int MREG = LineOcc<Real>::reg_y;
+    static constexpr int NT = LineOcc<Real>::nt_y;
     static constexpr bool CONTIG = false;
     GridT<R> g; FieldsT<R> f; int TL;
     __device__ bool skip() const { return blown(g); }
@@ -401,6 +407,7 @@ struct DWZ {
     static constexpr int NRHS = 1;
     static constexpr int MINB = LineOcc<R>::z;
     static constexpr int MREG = LineOcc<Real>::reg_z;
+    static constexpr int NT = LineOcc<Real>::nt_z;
     static constexpr bool CONTIG = false;
     GridT<R> g; FieldsT<R> f; int TL;
     __device__ bool skip() const { return blown(g); }
@@ -504,12 +511,13 @@ __device__ __forceinline__ void dw_stale_mu(const GridT<R> &g, const FieldsT<R> 
     mu4 = R(0.5) * (dx2[jp] * mxz + dx2[j] * mub) * rdmx2[jp];
 }
 
-template <class R>
+template <class R, int WIDE = 0>
 struct DWX {
     using Real = R;
     static constexpr int NRHS = 1;
-    static constexpr int MINB = LineOcc<R>::xy;
-    static constexpr int MREG = LineOcc<Real>::reg_xy;
+    static constexpr int MINB = WIDE ? LineOcc<R>::xw : LineOcc<R>::x;
+    static constexpr int MREG = WIDE ? LineOcc<Real>::reg_xw : LineOcc<Real>::reg_x;
+    static constexpr int NT = WIDE ? LineOcc<Real>::nt_xw : LineOcc<Real>::nt_x;
     static constexpr bool CONTIG = true;
     GridT<R> g; FieldsT<R> f; int TL;
     __device__ bool skip() const { return blown(g); }
@@ -550,8 +558,9 @@ template <class R>
 struct DWY {
     using Real = R;
     static constexpr int NRHS = 1;
-    static constexpr int MINB = LineOcc<R>::xy;
-    static constexpr int MREG = LineOcc<Real>::reg_xy;
+    static constexpr int MINB = LineOcc<R>::y;
+    static constexpr int MREG = LineOcc<Real>::reg_y;
+    static constexpr int NT = LineOcc<Real>::nt_y;
     static constexpr bool CONTIG = false;
     GridT<R> g; FieldsT<R> f; int TL;
     __device__ bool skip() const { return blown(g); }
@@ -595,10 +604,9 @@ void launch_solve_du(const Ctx<R> &cx, cudaStream_t s)
 {
     const GridT<R> &g = cx.g;
     LinePlan pz = make_line_plan(g.N3, true, fit_tl<DUZ<R>>(g.N3, true, cx.tl_strided, cx.lanes), cx.lanes);
-    LinePlan px = make_line_plan(g.N1, true, fit_tl<DUX<R>>(g.N1, true, cx.tl_contig, cx.lanes), cx.lanes);
     LinePlan py = make_line_plan(g.N2, false, fit_tl<DUY<R>>(g.N2, false, cx.tl_strided, cx.lanes), cx.lanes);
     launch_lines(DUZ<R>{g, cx.f, pz.TL}, pz, dim3((g.N1 + pz.TL - 1) / pz.TL, g.N2), s, K_DU_Z, cx);
-    launch_lines(DUX<R>{g, cx.f, px.TL}, px, dim3((g.N2 + px.TL - 1) / px.TL, g.N3), s, K_DU_X, cx);
+    launch_x<DUX>(cx, g.N2, s, K_DU_X);
     launch_lines(DUY<R>{g, cx.f, py.TL}, py, dim3((g.N1 + py.TL - 1) / py.TL, g.N3), s, K_DU_Y, cx);
 }
 
@@ -607,10 +615,9 @@ void launch_solve_dv(const Ctx<R> &cx, cudaStream_t s)
 {
     const GridT<R> &g = cx.g;
     LinePlan pz = make_line_plan(g.N3, true, fit_tl<DVZ<R>>(g.N3, true, cx.tl_strided, cx.lanes), cx.lanes);
-    LinePlan px = make_line_plan(g.N1, true, fit_tl<DVX<R>>(g.N1, true, cx.tl_contig, cx.lanes), cx.lanes);
     LinePlan py = make_line_plan(g.N2 - 1, false, fit_tl<DVY<R>>(g.N2 - 1, false, cx.tl_strided, cx.lanes), cx.lanes);
     launch_lines(DVZ<R>{g, cx.f, pz.TL}, pz, dim3((g.N1 + pz.TL - 1) / pz.TL, g.N2 - 1), s, K_DV_Z, cx);
-    launch_lines(DVX<R>{g, cx.f, px.TL}, px, dim3((g.N2 - 1 + px.TL - 1) / px.TL, g.N3), s, K_DV_X, cx);
+    launch_x<DVX>(cx, g.N2 - 1, s, K_DV_X);
     launch_lines(DVY<R>{g, cx.f, py.TL}, py, dim3((g.N1 + py.TL - 1) / py.TL, g.N3), s, K_DV_Y, cx);
 }
 
@@ -619,10 +626,9 @@ void launch_solve_dw(const Ctx<R> &cx, cudaStream_t s)
 {
     const GridT<R> &g = cx.g;
     LinePlan pz = make_line_plan(g.N3, true, fit_tl<DWZ<R>>(g.N3, true, cx.tl_strided, cx.lanes), cx.lanes);
-    LinePlan px = make_line_plan(g.N1, true, fit_tl<DWX<R>>(g.N1, true, cx.tl_contig, cx.lanes), cx.lanes);
     LinePlan py = make_line_plan(g.N2, false, fit_tl<DWY<R>>(g.N2, false, cx.tl_strided, cx.lanes), cx.lanes);
     launch_lines(DWZ<R>{g, cx.f, pz.TL}, pz, dim3((g.N1 + pz.TL - 1) / pz.TL, g.N2), s, K_DW_Z, cx);
-    launch_lines(DWX<R>{g, cx.f, px.TL}, px, dim3((g.N2 + px.TL - 1) / px.TL, g.N3), s, K_DW_X, cx);
+    launch_x<DWX>(cx, g.N2, s, K_DW_X);
     launch_lines(DWY<R>{g, cx.f, py.TL}, py, dim3((g.N1 + py.TL - 1) / py.TL, g.N3), s, K_DW_Y, cx);
 }
 

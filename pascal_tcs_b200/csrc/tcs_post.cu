@@ -24,7 +24,7 @@ __device__ __forceinline__ void csum(double &s, double &e, double v)
 }
 
 template <class R>
-__global__ void __launch_bounds__(256) post_kernel(GridT<R> g, FieldsT<R> f)
+__global__ void __launch_bounds__(256) post_kernel(GridT<R> g, FieldsT<R> f, FastDiv dn1, FastDiv dn2)
 {
     __shared__ double red[PT_N][256];
     if (blown(g)) return;
@@ -34,9 +34,9 @@ __global__ void __launch_bounds__(256) post_kernel(GridT<R> g, FieldsT<R> f)
     const double *rdx1 = g.d1.rdx, *rdx2 = g.d2.rdx, *rdx3 = g.d3.rdx;
     const long long sj = g.P1, sk = (long long)g.P1 * g.P2;
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
-        const int i = 1 + (int)(t % g.N1);
-        const long long q = t / g.N1;
-        const int j = 1 + (int)(q % g.N2), k = 1 + (int)(q / g.N2);
+        const unsigned q = dn1.div((unsigned)t), r = dn2.div(q);     // n < 2^31: 32-bit multiply-shift division
+        const int i = 1 + (int)((unsigned)t - q * (unsigned)g.N1);
+        const int j = 1 + (int)(q - r * (unsigned)g.N2), k = 1 + (int)r;
         const long long c = ix(g, i, j, k);
         double Uc, Vc, Wc, Ux, Vy, Wz;
         if constexpr (HasLo<R>::on) {     // the FP32 form's velocity is its high + low pair
@@ -131,7 +131,7 @@ template <class R>
 void launch_post(const Ctx<R> &cx, cudaStream_t s, int record_hist)
 {
     probe_begin(cx, K_POST, s);
-    post_kernel<<<POST_BLOCKS, 256, 0, s>>>(cx.g, cx.f);
+    post_kernel<<<POST_BLOCKS, 256, 0, s>>>(cx.g, cx.f, make_fastdiv((unsigned)cx.g.N1), make_fastdiv((unsigned)cx.g.N2));
     probe_end(cx, K_POST, s);
     record_launch_error("post");
     probe_begin(cx, K_FINAL, s);

@@ -298,6 +298,7 @@ struct Modal {
     static constexpr int NRHS = 2;
     static constexpr int MINB = LineOcc<R>::modal;
     static constexpr int MREG = LineOcc<Real>::reg_modal;
+    static constexpr int NT = LineOcc<Real>::nt_modal;
     static constexpr bool CONTIG = false;
     GridT<R> g; FieldsT<R> f; int TL; int h1p;
     __device__ bool skip() const { return blown(g); }

@@ -19,6 +19,7 @@ struct ThermalZ {
     static constexpr int NRHS = 1;
     static constexpr int MINB = LineOcc<R>::z;
     static constexpr int MREG = LineOcc<Real>::reg_z;
+    static constexpr int NT = LineOcc<Real>::nt_z;
     static constexpr bool CONTIG = false;
     GridT<R> g; FieldsT<R> f; int TL;
     __device__ bool skip() const { return blown(g); }
@@ -103,12 +104,13 @@ struct ThermalZ {
 
 // Stage 2 (:388-429): jm, jp, km, kp keep the values of the last stage-1
 // iteration (N2-1, N2+1, N3-1, N3+1).
-template <class R>
+template <class R, int WIDE = 0>
 struct ThermalX {
     using Real = R;
     static constexpr int NRHS = 1;
-    static constexpr int MINB = LineOcc<R>::xy;
-    static constexpr int MREG = LineOcc<Real>::reg_xy;
+    static constexpr int MINB = WIDE ? LineOcc<R>::xw : LineOcc<R>::x;
+    static constexpr int MREG = WIDE ? LineOcc<Real>::reg_xw : LineOcc<Real>::reg_x;
+    static constexpr int NT = WIDE ? LineOcc<Real>::nt_xw : LineOcc<Real>::nt_x;
     static constexpr bool CONTIG = true;
     GridT<R> g; FieldsT<R> f; int TL;
     __device__ bool skip() const { return blown(g); }
@@ -167,8 +169,9 @@ template <class R>
 struct ThermalY {
     using Real = R;
     static constexpr int NRHS = 1;
-    static constexpr int MINB = LineOcc<R>::xy;
-    static constexpr int MREG = LineOcc<Real>::reg_xy;
+    static constexpr int MINB = LineOcc<R>::y;
+    static constexpr int MREG = LineOcc<Real>::reg_y;
+    static constexpr int NT = LineOcc<Real>::nt_y;
     static constexpr bool CONTIG = false;
     GridT<R> g; FieldsT<R> f; int TL;
     __device__ bool skip() const { return blown(g); }
@@ -228,12 +231,10 @@ void launch_thermal(const Ctx<R> &cx, cudaStream_t s)
 {
     const GridT<R> &g = cx.g;
     LinePlan pz = make_line_plan(g.N3, true, fit_tl<ThermalZ<R>>(g.N3, true, cx.tl_strided, cx.lanes), cx.lanes);
-    LinePlan px = make_line_plan(g.N1, true, fit_tl<ThermalX<R>>(g.N1, true, cx.tl_contig, cx.lanes), cx.lanes);
     LinePlan py = make_line_plan(g.N2, false, fit_tl<ThermalY<R>>(g.N2, false, cx.tl_strided, cx.lanes), cx.lanes);
     ThermalZ<R> z{g, cx.f, pz.TL};
     launch_lines(z, pz, dim3((g.N1 + pz.TL - 1) / pz.TL, g.N2), s, K_THERMAL_Z, cx);
-    ThermalX<R> xx{g, cx.f, px.TL};
-    launch_lines(xx, px, dim3((g.N2 + px.TL - 1) / px.TL, g.N3), s, K_THERMAL_X, cx);
+    launch_x<ThermalX>(cx, g.N2, s, K_THERMAL_X);
     ThermalY<R> y{g, cx.f, py.TL};
     launch_lines(y, py, dim3((g.N1 + py.TL - 1) / py.TL, g.N3), s, K_THERMAL_Y, cx);
 }

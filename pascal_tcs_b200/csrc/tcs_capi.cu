@@ -7,6 +7,7 @@
 #include "tcs.h"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -26,7 +27,7 @@ namespace tcs {
 // ---------------------------------------------------------------------------
 static thread_local std::string g_err;
 static thread_local int g_launch_err = 0;
-static unsigned long long g_launches = 0;   // kernels launched by this library (graph replays included)
+static std::atomic<unsigned long long> g_launches{0};   // kernels launched by this library (graph replays included)
 
 static int set_err(int code, const std::string &msg)
 {
@@ -1335,18 +1336,22 @@ void tune_load(const std::string &path)
 static int tune_trial(tcs_ctx *c, int steps, float *ms)
 {
     int r, done = 0;
-    cudaEvent_t e0, e1;
     if ((r = tcs_restore(c))) return r;
     if ((r = tcs_step(c, 1, &done)) && r != TCS_ERR_BLOWUP) return r;     // captures this shape's graph
     if ((r = tcs_restore(c))) return r;
-    CK(cudaEventCreate(&e0)); CK(cudaEventCreate(&e1));
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+        if (e0) cudaEventDestroy(e0);
+        return set_err(TCS_ERR_CUDA, "tuning events");
+    }
     cudaEventRecord(e0, c->stream);
     r = tcs_step(c, steps, &done);
     cudaEventRecord(e1, c->stream);
-    cudaEventSynchronize(e1);
-    cudaEventElapsedTime(ms, e0, e1);
-    cudaEventDestroy(e0); cudaEventDestroy(e1);
-    return r == TCS_ERR_BLOWUP ? TCS_OK : r;
+    const bool ok = cudaEventSynchronize(e1) == cudaSuccess && cudaEventElapsedTime(ms, e0, e1) == cudaSuccess;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (r == TCS_ERR_BLOWUP) r = TCS_OK;
+    return (r == TCS_OK && !ok) ? set_err(TCS_ERR_CUDA, "tuning trial timing") : r;
 }
 
 extern "C" int tcs_autotune(tcs_ctx *c, int trial_steps, const char *cache_path, int *from_cache)

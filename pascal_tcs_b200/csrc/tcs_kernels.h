@@ -72,15 +72,26 @@ inline int fit_tl(int n, bool cyclic, int want, int pmax)
     return tl;
 }
 
+// Opt a kernel in to smem bytes of dynamic shared memory on the current
+// device.  The attribute belongs to the function on each device, so the
+// largest size set so far is kept per device (cache: one entry per ordinal).
+inline void smem_opt_in(const void *fn, size_t smem, size_t *cache)
+{
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) dev = 0;
+    if (smem > cache[dev]) {
+        cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cache[dev] = smem;
+    }
+}
+
 template <class Prob>
 inline void launch_lines(const Prob &p, const LinePlan &lp, dim3 grid, cudaStream_t s, int kid, const Shapes &cx)
 {
     const size_t smem = line_smem<Prob>(lp);
-    static size_t configured = 0;
-    if (smem > configured) {
-        cudaFuncSetAttribute(line_solve_kernel<Prob>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        configured = smem;
-    }
+    static size_t configured[64] = {};
+    smem_opt_in((const void *)line_solve_kernel<Prob>, smem, configured);
     probe_begin(cx, kid, s);
     line_solve_kernel<Prob><<<grid, Prob::NT, smem, s>>>(p, lp);
     probe_end(cx, kid, s);

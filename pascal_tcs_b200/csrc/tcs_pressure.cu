@@ -495,8 +495,8 @@ void launch_pseudo_prhs_fftx(const Ctx<R> &cx, cudaStream_t s, bool with_pseudo)
     const GridT<R> &g = cx.g;
     const int NL = cx.fft_lines_x;
     const size_t sm = fftx_smem(cx);
-    static size_t conf = 0;
-    if (sm > conf) { cudaFuncSetAttribute(prhs_fftx_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm); conf = sm; }
+    static size_t conf[64] = {};
+    smem_opt_in((const void *)prhs_fftx_kernel<R>, sm, conf);
     probe_begin(cx, K_PRHS_FFTX, s);
     prhs_fftx_kernel<R><<<dim3((g.N2 + NL - 1) / NL, g.N3), 256, sm, s>>>(g, cx.f, cx.fp1, NL, cx.h1p, with_pseudo ? 1 : 0);
     probe_end(cx, K_PRHS_FFTX, s);
@@ -510,13 +510,10 @@ void launch_poisson_rest(const Ctx<R> &cx, cudaStream_t s)
     const int h1p = cx.h1p, NLz = cx.fft_lines_z, NLx = cx.fft_lines_x;
     const size_t smz = (size_t)NLz * g.N3 * 2 * sizeof(double2);
     const size_t smx = (size_t)((NLx + 1) / 2) * g.N1 * 2 * sizeof(double2);
-    static size_t cz = 0, cx2 = 0;
-    if (smz > cz) {
-        cudaFuncSetAttribute(fftz_kernel<-1, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smz);
-        cudaFuncSetAttribute(fftz_kernel<1, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smz);
-        cz = smz;
-    }
-    if (smx > cx2) { cudaFuncSetAttribute(ifftx_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx); cx2 = smx; }
+    static size_t cz1[64] = {}, cz2[64] = {}, cx2[64] = {};
+    smem_opt_in((const void *)fftz_kernel<-1, R>, smz, cz1);
+    smem_opt_in((const void *)fftz_kernel<1, R>, smz, cz2);
+    smem_opt_in((const void *)ifftx_kernel<R>, smx, cx2);
     const dim3 gz((h1p + NLz - 1) / NLz, g.N2);
     probe_begin(cx, K_FFTZ_FWD, s);
     fftz_kernel<-1, R><<<gz, 256, smz, s>>>(g, cx.f, cx.fp3, NLz, h1p);

@@ -472,6 +472,12 @@ def run_ensemble(args, cfg: dict, workload: str) -> int:
     one_at_a_time(args.warmup)
     for s in solvers:
         s.restore()
+    # the auto form selection's 8 measuring steps (real steps) are part of the warm-up
+    while ens.form()[0] < 0:
+        ens.step(1)
+    ens_form, tune_br, tune_bat = ens.form()
+    for s in solvers:
+        s.restore()
     grouped(args.warmup)
     for s in solvers:
         s.restore()
@@ -481,19 +487,31 @@ def run_ensemble(args, cfg: dict, workload: str) -> int:
         ms = timed(grouped, args.steps)
         time.sleep(0.15)
     launches = P.launch_count() - launches0
+    # the same ensemble in the other form
+    ens.set_batched(not ens_form)
+    for s in solvers:
+        s.restore()
+    grouped(args.warmup)
+    for s in solvers:
+        s.restore()
+    ms_other = timed(grouped, args.steps)
+    ens.set_batched(None)
+    ms_bat, ms_br = (ms, ms_other) if ens_form == 1 else (ms_other, ms)
     for s in solvers:
         s.restore()
     ms_seq = timed(one_at_a_time, args.steps)
     total_cells = sum(c["n1m"] * c["n2m"] * c["n3m"] for c in allcases)
     value = total_cells * args.steps / (ms * 1e-3)
     seq = total_cells * args.steps / (ms_seq * 1e-3)
+    br = total_cells * args.steps / (ms_br * 1e-3)
+    bat = total_cells * args.steps / (ms_bat * 1e-3)
     esize = 4 if cfg["precision"] else 8
     peak, peak_kind = measured_peaks()
     step_bytes = step_bytes_per_cell(esize) * total_cells
     achieved = step_bytes * args.steps / (ms * 1e-3) / 1e9
     if rank == 0:
         form = "FP32-mixed" if cfg["precision"] else "FP64 plain"
-        line = {"metric": f"cell-steps/s ({form}, batched ensemble of {len(allcases)} cases)", "value": value,
+        line = {"metric": f"cell-steps/s ({form}, ensemble of {len(allcases)} cases)", "value": value,
                 "unit": "cell-steps/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "strong" if ws > 1 else "weak",
                 "vs_baseline": None, "dtype": "f32+f64" if cfg["precision"] else "f64",
@@ -503,13 +521,17 @@ def run_ensemble(args, cfg: dict, workload: str) -> int:
                            "Pr": "7 (water) or 0.71 (constant)", "dt": 2e-4, "precision": form,
                            "parallelism": f"LPT bin-packing of cases over {ws} GPU(s)" if ws > 1 else "single",
                            "l2": "working set of %.1f GB, larger than L2" % (total_cells * esize * 24 / 1e9 / ws),
-                           "timing": "one CUDA graph per ensemble step; CUDA events around the region",
+                           "timing": "one CUDA graph per ensemble step, in the form the auto selection keeps; CUDA events around the region",
                            "restart_every_steps": reset},
                 "gpu_launches": launches,
                 "roofline": {"bound": "hbm", "kernel": "whole ensemble step", "achieved": achieved, "peak": peak,
                              "unit": "GB/s", "frac": achieved / peak,
                              "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
                              "algorithmic_bytes_per_step": step_bytes, "traffic": None},
+                "form": {"chosen": "batched" if ens_form == 1 else "one branch per case",
+                         "measured_ms_per_step": {"one_branch_per_case": tune_br, "batched": tune_bat}},
+                "batched": {"value": bat, "ms_per_step": ms_bat / args.steps},
+                "one_branch_per_case": {"value": br, "ms_per_step": ms_br / args.steps},
                 "one_at_a_time": {"value": seq, "ms_per_step": ms_seq / args.steps},
                 "speedup_vs_one_at_a_time": value / seq,
                 "clocks": clk.summary(), "e2e": None, "cpu_baseline": None}

@@ -176,14 +176,25 @@ int tcs_extract_plane(tcs_ctx *ctx, int axis, int index, int nfields, const int 
 
 /* Ensembles (no counterpart in the reference, which runs one case per MPI job):
  * independent cases on one device advanced together.  Every tcs_ensemble_step
- * replays one CUDA graph per step in which each case is its own branch, so the
- * GPU runs the cases' kernels concurrently.  Cases keep their own state and
- * entry points; tcs_ensemble_destroy does not destroy them.  Probes must be off. */
+ * replays one CUDA graph per step, in one of two forms:
+ *   batched (1): each line sweep (thermal, solvedU/V/W, the modal Poisson
+ *     solves) is ONE launch over all cases (up to a parameter block's worth of
+ *     cases per launch), a persistent grid whose blocks pull (case, block)
+ *     work items; the kernels between the sweeps run as one branch per case;
+ *   branch per case (0): every case's whole step is its own graph branch.
+ * Both give results bit-identical to stepping each case alone.  The default,
+ * auto (-1), runs the first 8 steps (real steps) 4 in each form, times the
+ * last 2 of each and keeps the faster form; tcs_ensemble_form reports the
+ * form in use (-1 while still measuring) and the measured ms per step of each.
+ * Cases keep their own state and entry points; tcs_ensemble_destroy does not
+ * destroy them.  Probes must be off. */
 typedef struct tcs_ensemble tcs_ensemble;
 int tcs_ensemble_create(tcs_ctx *const *cases, int n, tcs_ensemble **out);
 int tcs_ensemble_destroy(tcs_ensemble *ens);
 int tcs_ensemble_step(tcs_ensemble *ens, int nsteps, int *nblown);   /* *nblown: cases that have blown up */
 int tcs_ensemble_size(const tcs_ensemble *ens);
+int tcs_ensemble_set_batched(tcs_ensemble *ens, int mode);             /* 1, 0 or -1 (auto, the default) */
+int tcs_ensemble_form(const tcs_ensemble *ens, int *form, float *ms_branches, float *ms_batched);
 
 unsigned long long tcs_launch_count(void);           /* kernels this library has launched so far */
 const char *tcs_kernel_name(int kernel_id);

@@ -1175,11 +1175,142 @@ struct tcs_ensemble {
     std::vector<tcs_ctx *> cases;
     int device = 0;
     cudaStream_t root = nullptr;
-    cudaEvent_t fork = nullptr;
-    std::vector<cudaEvent_t> join;
-    struct Entry { std::vector<const void *> key; cudaGraphExec_t exec; unsigned long long kernels; };
+    cudaEvent_t fork = nullptr, fork2 = nullptr;
+    std::vector<cudaEvent_t> join, join2;
+    // the form of a step: 1 = batched (a line sweep is one multi-case launch),
+    // 0 = one graph branch per case, -1 = auto (measure both, keep the faster)
+    int mode = -1;
+    int chosen = -1;          // auto: the form picked, -1 while measuring
+    int tune_step = 0;        // auto: steps of the measurement taken so far (of 8)
+    float tune_ms[2] = {-1.f, -1.f};
+    cudaEvent_t tev[2][2] = {};
+    struct Entry {
+        std::vector<const void *> key;
+        bool batched;
+        cudaGraphExec_t exec;
+        unsigned long long kernels;
+        void *arena;
+    };
     std::vector<Entry> graphs;
 };
+
+static void ensemble_drop_graphs(tcs_ensemble *e)
+{
+    for (auto &g : e->graphs) {
+        cudaGraphExecDestroy(g.exec);
+        if (g.arena) cudaFree(g.arena);
+    }
+    e->graphs.clear();
+}
+
+// One step of every case in the batched form.  The line sweeps (thermal,
+// solvedU/V/W, the modal Poisson solves) run as one line_solve_multi launch
+// per sweep on the root stream; the kernels between them run as one branch
+// per case (forked from and joined back to the root).  In planning mode
+// nothing is launched: the multi-case launches append their work lists to
+// the arena and the host-side buffer swaps are applied as the step makes them.
+static void ensemble_sequence(tcs_ensemble *e, MultiArena &A)
+{
+    const bool plan = A.planning;
+    std::vector<Ctx<double> *> d;
+    std::vector<Ctx<float> *> f;
+    for (tcs_ctx *c : e->cases) {
+        if (c->fp32) f.push_back(&c->cf);
+        else d.push_back(&c->cx);
+    }
+    auto branches = [&](auto &&body) {
+        if (!plan) cudaEventRecord(e->fork, e->root);
+        for (size_t i = 0; i < e->cases.size(); i++) {
+            tcs_ctx *c = e->cases[i];
+            if (!plan) cudaStreamWaitEvent(c->stream, e->fork, 0);
+            on_ctx(c, [&](auto &x) { body(x, c->stream); });
+            if (!plan) {
+                cudaEventRecord(e->join[i], c->stream);
+                cudaStreamWaitEvent(e->root, e->join[i], 0);
+            }
+        }
+    };
+    launch_thermal_multi(d, A, e->root);
+    launch_thermal_multi(f, A, e->root);
+    branches([&](auto &x, cudaStream_t s) {
+        swap_T(x);
+        if (!plan) launch_momentum_coeffi(x, s);
+    });
+    launch_momentum_multi(d, A, e->root);
+    launch_momentum_multi(f, A, e->root);
+    branches([&](auto &x, cudaStream_t s) {
+        if (!plan) {
+            launch_blockld_v(x, s);
+            launch_blockld_u(x, s);
+            launch_pseudo_prhs_fftx(x, s, true);
+        }
+        swap_UVW(x);
+        if (!plan) launch_poisson_fwd(x, s);
+    });
+    launch_modal_multi(d, A, e->root);
+    launch_modal_multi(f, A, e->root);
+    branches([&](auto &x, cudaStream_t s) {
+        if (!plan) {
+            launch_poisson_back(x, s);
+            launch_projection(x, s);
+        }
+        swap_phat(x);
+        if (!plan) launch_post(x, s, 1);
+    });
+}
+
+// Capture one step of every case into a graph (the buffers swap as the step
+// swaps them).  Batched: plan the multi-case launches, put the buffer state
+// back, upload the work lists once, then capture; the graph keeps the upload.
+static int ensemble_capture(tcs_ensemble *e, bool batched, cudaGraphExec_t *exec, unsigned long long *nk, void **arena)
+{
+    *exec = nullptr;
+    *arena = nullptr;
+    MultiArena A;
+    if (batched) {
+        ensemble_sequence(e, A);
+        for (tcs_ctx *c : e->cases) on_ctx(c, [&](auto &x) { swap_T(x); swap_UVW(x); swap_phat(x); });
+        CK(cudaMalloc(&A.dev, std::max<size_t>(A.host.size(), 16)));
+        *arena = A.dev;
+        CK(cudaMemcpy(A.dev, A.host.data(), A.host.size(), cudaMemcpyHostToDevice));
+        A.planning = false;
+        A.cursor = 0;
+        // a stage's later launches run on the case streams (idle while the root runs a stage)
+        A.fork = e->fork2;
+        for (size_t i = 0; i < e->cases.size(); i++) {
+            A.aux.push_back(e->cases[i]->stream);
+            A.join.push_back(e->join2[i]);
+        }
+    }
+    cudaGraph_t gr;
+    const unsigned long long before = g_launches;
+    CK(cudaStreamBeginCapture(e->root, cudaStreamCaptureModeThreadLocal));
+    if (batched) {
+        ensemble_sequence(e, A);
+    } else {
+        cudaEventRecord(e->fork, e->root);
+        for (size_t i = 0; i < e->cases.size(); i++) {
+            tcs_ctx *c = e->cases[i];
+            cudaStreamWaitEvent(c->stream, e->fork, 0);
+            launch_step(c);
+            cudaEventRecord(e->join[i], c->stream);
+            cudaStreamWaitEvent(e->root, e->join[i], 0);
+        }
+    }
+    *nk = g_launches - before;
+    g_launches = before;
+    cudaError_t ec = cudaStreamEndCapture(e->root, &gr);
+    if (ec != cudaSuccess || take_launch_error())
+        return set_err(TCS_ERR_CUDA, std::string("ensemble graph capture: ") + cudaGetErrorString(ec));
+    if (batched && A.cursor != A.host.size()) {
+        cudaGraphDestroy(gr);
+        return set_err(TCS_ERR_CUDA, "ensemble work lists do not match the captured step");
+    }
+    ec = cudaGraphInstantiate(exec, gr, 0);
+    cudaGraphDestroy(gr);
+    if (ec != cudaSuccess) return set_err(TCS_ERR_CUDA, std::string("ensemble graph: ") + cudaGetErrorString(ec));
+    return TCS_OK;
+}
 
 static std::vector<const void *> ensemble_key(tcs_ensemble *e)
 {
@@ -1211,9 +1342,15 @@ int tcs_ensemble_create(tcs_ctx *const *cases, int n, tcs_ensemble **out)
     e->cases.assign(cases, cases + n);
     e->device = cases[0]->cfg.device;
     bool ok = cudaStreamCreateWithFlags(&e->root, cudaStreamNonBlocking) == cudaSuccess &&
-              cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming) == cudaSuccess;
+              cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming) == cudaSuccess &&
+              cudaEventCreateWithFlags(&e->fork2, cudaEventDisableTiming) == cudaSuccess;
+    for (int f = 0; f < 2 && ok; f++)
+        for (int q = 0; q < 2 && ok; q++) ok = cudaEventCreate(&e->tev[f][q]) == cudaSuccess;
     e->join.assign(n, nullptr);
-    for (int i = 0; i < n && ok; i++) ok = cudaEventCreateWithFlags(&e->join[i], cudaEventDisableTiming) == cudaSuccess;
+    e->join2.assign(n, nullptr);
+    for (int i = 0; i < n && ok; i++)
+        ok = cudaEventCreateWithFlags(&e->join[i], cudaEventDisableTiming) == cudaSuccess &&
+             cudaEventCreateWithFlags(&e->join2[i], cudaEventDisableTiming) == cudaSuccess;
     if (!ok) { tcs_ensemble_destroy(e); return set_err(TCS_ERR_CUDA, "ensemble streams/events"); }
     *out = e;
     return TCS_OK;
@@ -1224,9 +1361,13 @@ int tcs_ensemble_destroy(tcs_ensemble *e)
     if (!e) return TCS_ERR_ARG;
     cudaSetDevice(e->device);
     if (e->root) cudaStreamSynchronize(e->root);
-    for (auto &g : e->graphs) cudaGraphExecDestroy(g.exec);
+    ensemble_drop_graphs(e);
     for (cudaEvent_t ev : e->join) if (ev) cudaEventDestroy(ev);
+    for (cudaEvent_t ev : e->join2) if (ev) cudaEventDestroy(ev);
     if (e->fork) cudaEventDestroy(e->fork);
+    if (e->fork2) cudaEventDestroy(e->fork2);
+    for (auto &tf : e->tev)
+        for (cudaEvent_t ev : tf) if (ev) cudaEventDestroy(ev);
     if (e->root) cudaStreamDestroy(e->root);
     delete e;
     return TCS_OK;
@@ -1247,38 +1388,44 @@ int tcs_ensemble_step(tcs_ensemble *e, int nsteps, int *nblown)
         CK(cudaStreamSynchronize(c->stream));
     }
     for (int s = 0; s < nsteps; s++) {
+        // auto: steps 0-3 run one branch per case, 4-7 batched; steps 2-3 and 6-7 are timed
+        bool form;
+        int tstep = -1;
+        if (e->mode >= 0) form = e->mode == 1;
+        else if (e->chosen >= 0) form = e->chosen == 1;
+        else {
+            tstep = e->tune_step;
+            form = tstep >= 4;
+        }
         const std::vector<const void *> key = ensemble_key(e);
         cudaGraphExec_t exec = nullptr;
         unsigned long long kernels = 0;
-        for (auto &g : e->graphs) if (g.key == key) { exec = g.exec; kernels = g.kernels; break; }
+        for (auto &g : e->graphs)
+            if (g.key == key && g.batched == form) { exec = g.exec; kernels = g.kernels; break; }
         if (!exec) {
-            cudaGraph_t gr;
-            const unsigned long long before = g_launches;
-            CK(cudaStreamBeginCapture(e->root, cudaStreamCaptureModeThreadLocal));
-            cudaEventRecord(e->fork, e->root);
-            for (size_t i = 0; i < e->cases.size(); i++) {
-                tcs_ctx *c = e->cases[i];
-                cudaStreamWaitEvent(c->stream, e->fork, 0);
-                launch_step(c);
-                cudaEventRecord(e->join[i], c->stream);
-                cudaStreamWaitEvent(e->root, e->join[i], 0);
+            void *arena = nullptr;
+            const int rc = ensemble_capture(e, form, &exec, &kernels, &arena);
+            if (rc) {
+                if (arena) cudaFree(arena);
+                return rc;
             }
-            const unsigned long long nk = g_launches - before;
-            g_launches = before;
-            cudaError_t ec = cudaStreamEndCapture(e->root, &gr);
-            if (ec != cudaSuccess || take_launch_error())
-                return set_err(TCS_ERR_CUDA, std::string("ensemble graph capture: ") + cudaGetErrorString(ec));
-            ec = cudaGraphInstantiate(&exec, gr, 0);
-            cudaGraphDestroy(gr);
-            if (ec != cudaSuccess) return set_err(TCS_ERR_CUDA, std::string("ensemble graph: ") + cudaGetErrorString(ec));
-            e->graphs.push_back({key, exec, nk});
-            kernels = nk;
+            e->graphs.push_back({key, form, exec, kernels, arena});
             // the capture swapped every case's buffers already
         } else {
             for (tcs_ctx *c : e->cases) on_ctx(c, [&](auto &x) { swap_T(x); swap_UVW(x); swap_phat(x); });
         }
+        if (tstep >= 0 && (tstep & 3) == 2) CK(cudaEventRecord(e->tev[form][0], e->root));
         CK(cudaGraphLaunch(exec, e->root));
         g_launches += kernels;
+        if (tstep >= 0 && (tstep & 3) == 3) CK(cudaEventRecord(e->tev[form][1], e->root));
+        if (tstep >= 0 && ++e->tune_step == 8) {
+            CK(cudaStreamSynchronize(e->root));
+            for (int f = 0; f < 2; f++) {
+                CK(cudaEventElapsedTime(&e->tune_ms[f], e->tev[f][0], e->tev[f][1]));
+                e->tune_ms[f] *= 0.5f;
+            }
+            e->chosen = e->tune_ms[1] < e->tune_ms[0] ? 1 : 0;
+        }
     }
     CK(cudaStreamSynchronize(e->root));
     int blown = 0;
@@ -1295,6 +1442,21 @@ int tcs_ensemble_step(tcs_ensemble *e, int nsteps, int *nblown)
 
 int tcs_ensemble_size(const tcs_ensemble *e) { return e ? (int)e->cases.size() : 0; }
 
+int tcs_ensemble_set_batched(tcs_ensemble *e, int mode)
+{
+    if (!e || mode < -1 || mode > 1) return set_err(TCS_ERR_ARG, "mode must be 1 (batched), 0 (branch per case) or -1 (auto)");
+    e->mode = mode;
+    return TCS_OK;
+}
+
+int tcs_ensemble_form(const tcs_ensemble *e, int *form, float *ms_branches, float *ms_batched)
+{
+    if (!e) return set_err(TCS_ERR_ARG, "null ensemble");
+    if (form) *form = e->mode >= 0 ? e->mode : e->chosen;
+    if (ms_branches) *ms_branches = e->tune_ms[0];
+    if (ms_batched) *ms_batched = e->tune_ms[1];
+    return TCS_OK;
+}
 } // extern "C"
 
 // ---------------------------------------------------------------------------

@@ -667,6 +667,14 @@ template <class R, int NR, int MREG, bool REC = false>
 __device__ __forceinline__ void solve_line(R *A, R *C, R *D, int DS, const LinePlan &lp, int lane,
                                            R *F = nullptr, LaneFactors<R> *lf = nullptr);
 
+// The block a line problem works on, read through vbx<ITEM>() / vby<ITEM>():
+// blockIdx in a one-case launch (ITEM = 0), the work item's block in a
+// multi-case launch (ITEM = 1, line_solve_multi).  The problem structs carry
+// ITEM as a template parameter, so one-case launches keep reading blockIdx.
+static __shared__ int2 s_vblk;
+template <int ITEM> __device__ __forceinline__ int vbx() { return ITEM ? s_vblk.x : (int)blockIdx.x; }
+template <int ITEM> __device__ __forceinline__ int vby() { return ITEM ? s_vblk.y : (int)blockIdx.y; }
+
 // Shared-memory words (of the row type) per row: A, C, D[NR]; refined rows
 // also keep the normalised rows as built (A0, C0, D0[NR]; D0 becomes the
 // residual) and the pivot reciprocals F of the first solve.
@@ -677,7 +685,7 @@ __host__ __device__ constexpr int line_words()
 }
 
 template <class Prob>
-__global__ void __launch_bounds__(Prob::NT, Prob::MINB) line_solve_kernel(Prob prob, LinePlan lp)
+__device__ __forceinline__ void line_block(const Prob &prob, const LinePlan &lp)
 {
     using R = typename Prob::Real;
     constexpr int NR = Prob::NRHS;
@@ -771,6 +779,71 @@ __global__ void __launch_bounds__(Prob::NT, Prob::MINB) line_solve_kernel(Prob p
             for (int r = threadIdx.x; r < n; r += blockDim.x) out(l, r);
     } else {
         for (int t = threadIdx.x; t < TL * n; t += blockDim.x) out(t & (TL - 1), t >> lgTL);
+    }
+}
+
+template <class Prob>
+__global__ void __launch_bounds__(Prob::NT, Prob::MINB) line_solve_kernel(Prob prob, LinePlan lp)
+{
+    line_block(prob, lp);
+}
+
+// The parameters of a multi-case line launch: the problems and plans of up to
+// K cases, held in the kernel-parameter space (32 KB) so that, as in
+// line_solve_kernel, the kernel reads their members as constant operands (a
+// copy in global or shared memory costs registers and spills in the FP64
+// sweeps).  Case c owns the work items start[c] .. start[c+1]-1, block
+// (bx, by) being item start[c] + by * gx[c] + bx.
+template <class Prob>
+struct MultiParams {
+    static constexpr int K = (int)((32000 - 64) / (sizeof(Prob) + sizeof(LinePlan) + 2 * sizeof(int)));
+    static_assert(K >= 1, "a problem struct must fit the kernel-parameter space");
+    Prob p[K];
+    LinePlan lp[K];
+    int start[K + 1];
+    int gx[K];
+    int nitems;
+    int *ctr;   // [0] next item, [1] blocks done
+};
+
+// Many cases in one launch: a persistent grid whose blocks pull work items
+// (case, bx, by) from a counter and run the same block body as
+// line_solve_kernel on them.  Each block claims its next item while it works
+// on the current one, so the counter's round trip stays off the critical
+// path.  The last block to finish sets the counter back to 0, so the next
+// launch (or graph replay) starts again from item 0.
+template <class Prob>
+__global__ void __launch_bounds__(Prob::NT, Prob::MINB) line_solve_multi(const __grid_constant__ MultiParams<Prob> mp)
+{
+    __shared__ int s_case;
+    int nxt = 0;   // thread 0: the item claimed next
+    if (threadIdx.x == 0) nxt = atomicAdd(mp.ctr, 1);
+    for (;;) {
+        if (threadIdx.x == 0) {
+            const int it = nxt;
+            int c = -1;
+            if (it < mp.nitems) {
+                c = 0;
+                while (it >= mp.start[c + 1]) c++;
+                const int r = it - mp.start[c], by = r / mp.gx[c];
+                s_vblk = make_int2(r - by * mp.gx[c], by);
+                nxt = atomicAdd(mp.ctr, 1);
+            }
+            s_case = c;
+        }
+        __syncthreads();
+        const int c = s_case;
+        if (c < 0) break;
+        const LinePlan lp = mp.lp[c];   // a local copy keeps the solver's row arrays in registers
+        line_block(mp.p[c], lp);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(mp.ctr + 1, 1) == (int)gridDim.x - 1) {
+            atomicExch(mp.ctr, 0);
+            atomicExch(mp.ctr + 1, 0);
+        }
     }
 }
 

@@ -6,7 +6,10 @@
 
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <algorithm>
+#include <cstring>
 #include <string>
+#include <vector>
 
 namespace tcs {
 
@@ -62,11 +65,12 @@ inline size_t line_smem(const LinePlan &lp)
 }
 
 // Lines per block: the requested count, halved until MINB blocks fit in the
-// SM's shared memory (228 KB, 1 KB reserved per block).
+// SM's shared memory (228 KB, 1 KB reserved per block);
+// extra: static shared memory the kernel adds per block.
 template <class Prob>
-inline int fit_tl(int n, bool cyclic, int want, int pmax)
+inline int fit_tl(int n, bool cyclic, int want, int pmax, size_t extra = 0)
 {
-    const size_t budget = (size_t)228 * 1024 / Prob::MINB - 1024;
+    const size_t budget = (size_t)228 * 1024 / Prob::MINB - 1024 - extra;
     int tl = want;
     while (tl > 1 && line_smem<Prob>(make_line_plan(n, cyclic, tl, pmax)) > budget) tl /= 2;
     return tl;
@@ -98,22 +102,145 @@ inline void launch_lines(const Prob &p, const LinePlan &lp, dim3 grid, cudaStrea
     record_launch_error(kernel_name(kid));
 }
 
+// ---------------------------------------------------------------------------
+// Ensemble launches: one line stage of many cases as line_solve_multi
+// launches of up to MultiParams::K cases each.  An ensemble builds each
+// step's launches twice in the same order: in planning mode every launch
+// reserves its item counter in the arena, then (after one upload of the
+// arena) in launch mode each launch takes its counter's device address.
+// The launches of one stage run concurrently on the aux streams (forked from
+// and joined back to the stage's stream).
+// ---------------------------------------------------------------------------
+struct MultiArena {
+    std::vector<unsigned char> host;
+    unsigned char *dev = nullptr;
+    size_t cursor = 0;
+    bool planning = true;
+    std::vector<cudaStream_t> aux;       // streams for a stage's second and later launches
+    std::vector<cudaEvent_t> join;       // one per aux stream
+    cudaEvent_t fork = nullptr;
+    int *counter()
+    {
+        const size_t off = (cursor + 15) & ~(size_t)15;
+        cursor = off + 16;
+        if (planning) {
+            host.resize(cursor, 0);
+            return nullptr;
+        }
+        return (int *)(dev + off);
+    }
+};
+
+// One case's share of a multi-case line stage: the line length, cyclicity,
+// requested lines per block, and the block grid (lines / TL rounded up, gy).
+struct StageShape {
+    int n;
+    bool cyclic;
+    int want, lines, gy;
+};
+
+template <class Prob>
+inline void launch_lines_multi(MultiParams<Prob> &mp, int ncase, cudaStream_t s, const char *what)
+{
+    size_t smem = 0;
+    for (int c = 0; c < ncase; c++) smem = std::max(smem, line_smem<Prob>(mp.lp[c]));
+    static size_t conf[64] = {};
+    smem_opt_in((const void *)line_solve_multi<Prob>, smem, conf);
+    int dev = 0, sms = 148, occ = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, line_solve_multi<Prob>, Prob::NT, smem);
+    const int grid = (int)std::min<long long>(mp.nitems, (long long)std::max(occ, 1) * sms);
+    line_solve_multi<Prob><<<grid, Prob::NT, smem, s>>>(mp);
+    record_launch_error(what);
+}
+
+// A line stage for a group of same-precision cases: per case the same plan
+// and block grid as its one-case launch; the cases with the longest blocks
+// first (so the blocks that pull the last items finish close together),
+// MultiParams::K cases per launch.
+template <class P, class R, class Shape, class Make>
+inline void multi_stage(const std::vector<Ctx<R> *> &cs, MultiArena &A, cudaStream_t s, const char *what, Shape shape,
+                        Make make)
+{
+    struct Entry { P prob; LinePlan lp; int gx, gy; long long cost; };
+    std::vector<Entry> es;
+    for (const Ctx<R> *xp : cs) {
+        const Ctx<R> &x = *xp;
+        const StageShape sh = shape(x);
+        const LinePlan lp = make_line_plan(sh.n, sh.cyclic, fit_tl<P>(sh.n, sh.cyclic, sh.want, x.lanes, 64), x.lanes);
+        es.push_back({make(x, lp.TL), lp, (sh.lines + lp.TL - 1) / lp.TL, sh.gy, (long long)sh.n * lp.TL});
+    }
+    std::stable_sort(es.begin(), es.end(), [](const Entry &a, const Entry &b) { return a.cost > b.cost; });
+    constexpr int K = MultiParams<P>::K;
+    const int nl = (int)((es.size() + K - 1) / K);
+    const bool fan = !A.planning && nl > 1 && (int)A.aux.size() >= nl - 1;
+    if (fan) cudaEventRecord(A.fork, s);
+    for (int l = 0; l < nl; l++) {
+        const size_t c0 = (size_t)l * K;
+        const int nc = (int)std::min<size_t>(K, es.size() - c0);
+        int *ctr = A.counter();
+        if (A.planning) continue;
+        MultiParams<P> mp;
+        mp.start[0] = 0;
+        for (int c = 0; c < nc; c++) {
+            const Entry &e = es[c0 + c];
+            mp.p[c] = e.prob;
+            mp.lp[c] = e.lp;
+            mp.gx[c] = e.gx;
+            mp.start[c + 1] = mp.start[c] + e.gx * e.gy;
+        }
+        mp.nitems = mp.start[nc];
+        mp.ctr = ctr;
+        cudaStream_t ls = s;
+        if (fan && l > 0) {
+            ls = A.aux[l - 1];
+            cudaStreamWaitEvent(ls, A.fork, 0);
+        }
+        launch_lines_multi(mp, nc, ls, what);
+        if (fan && l > 0) {
+            cudaEventRecord(A.join[l - 1], ls);
+            cudaStreamWaitEvent(s, A.join[l - 1], 0);
+        }
+    }
+}
+
+// Whether a case runs its x sweeps in the wide shape (the rule of launch_x).
+template <template <class, int, int> class X, class R>
+inline bool x_is_wide(const Ctx<R> &cx)
+{
+    if constexpr (LineOcc<R>::f32) return fit_tl<X<R, 0, 0>>(cx.g.N1, true, cx.tl_contig, cx.lanes) < 4;
+    return false;
+}
+
+// A multi-case x sweep: the cases split by shape, one launch per shape.
+template <template <class, int, int> class X, class R, class Lines>
+inline void multi_x(const std::vector<Ctx<R> *> &cs, MultiArena &A, cudaStream_t s, const char *what, Lines lines)
+{
+    std::vector<Ctx<R> *> narrow, wide;
+    for (Ctx<R> *c : cs) (x_is_wide<X>(*c) ? wide : narrow).push_back(c);
+    auto shape = [&](const Ctx<R> &x) { return StageShape{x.g.N1, true, x.tl_contig, lines(x), x.g.N3}; };
+    multi_stage<X<R, 0, 1>>(narrow, A, s, what, shape, [](const Ctx<R> &x, int tl) { return X<R, 0, 1>{x.g, x.f, tl}; });
+    if constexpr (LineOcc<R>::f32)
+        multi_stage<X<R, 1, 1>>(wide, A, s, what, shape, [](const Ctx<R> &x, int tl) { return X<R, 1, 1>{x.g, x.f, tl}; });
+}
+
 // An x sweep: lines along i, one block row per (j-range, k).  FP32 runs the
 // 128-thread shape when at least 4 lines fit a block, else the wide shape.
-template <template <class, int> class X, class R>
+template <template <class, int, int> class X, class R>
 inline void launch_x(const Ctx<R> &cx, int nlines, cudaStream_t s, int kid)
 {
     const GridT<R> &g = cx.g;
-    const int tl = fit_tl<X<R, 0>>(g.N1, true, cx.tl_contig, cx.lanes);
+    const int tl = fit_tl<X<R, 0, 0>>(g.N1, true, cx.tl_contig, cx.lanes);
     if constexpr (LineOcc<R>::f32) {
         if (tl < 4) {
-            const LinePlan p = make_line_plan(g.N1, true, fit_tl<X<R, 1>>(g.N1, true, cx.tl_contig, cx.lanes), cx.lanes);
-            launch_lines(X<R, 1>{g, cx.f, p.TL}, p, dim3((nlines + p.TL - 1) / p.TL, g.N3), s, kid, cx);
+            const LinePlan p = make_line_plan(g.N1, true, fit_tl<X<R, 1, 0>>(g.N1, true, cx.tl_contig, cx.lanes), cx.lanes);
+            launch_lines(X<R, 1, 0>{g, cx.f, p.TL}, p, dim3((nlines + p.TL - 1) / p.TL, g.N3), s, kid, cx);
             return;
         }
     }
     const LinePlan p = make_line_plan(g.N1, true, tl, cx.lanes);
-    launch_lines(X<R, 0>{g, cx.f, p.TL}, p, dim3((nlines + p.TL - 1) / p.TL, g.N3), s, kid, cx);
+    launch_lines(X<R, 0, 0>{g, cx.f, p.TL}, p, dim3((nlines + p.TL - 1) / p.TL, g.N3), s, kid, cx);
 }
 
 // Stage launchers (one per reference routine or fused group), instantiated
@@ -128,9 +255,16 @@ template <class R> void launch_blockld_u(const Ctx<R> &cx, cudaStream_t s);
 template <class R> void launch_pseudo_update(const Ctx<R> &cx, cudaStream_t s);   // standalone (Un = U + dU, ...)
 template <class R> void launch_pseudo_prhs_fftx(const Ctx<R> &cx, cudaStream_t s, bool with_pseudo);
 template <class R> void launch_poisson_rest(const Ctx<R> &cx, cudaStream_t s);
+template <class R> void launch_modal(const Ctx<R> &cx, cudaStream_t s);
+template <class R> void launch_poisson_fwd(const Ctx<R> &cx, cudaStream_t s);   // z FFTs (forward)
+template <class R> void launch_poisson_back(const Ctx<R> &cx, cudaStream_t s);  // mean, z and x inverse FFTs, dP walls
 template <class R> void launch_projection(const Ctx<R> &cx, cudaStream_t s);
 template <class R> void launch_post(const Ctx<R> &cx, cudaStream_t s, int record_hist);
 template <class R> void launch_ghost(const Ctx<R> &cx, R *a, cudaStream_t s);
+// the line stages of a step for a group of same-precision cases, one launch per stage
+template <class R> void launch_thermal_multi(const std::vector<Ctx<R> *> &cs, MultiArena &A, cudaStream_t s);
+template <class R> void launch_momentum_multi(const std::vector<Ctx<R> *> &cs, MultiArena &A, cudaStream_t s);
+template <class R> void launch_modal_multi(const std::vector<Ctx<R> *> &cs, MultiArena &A, cudaStream_t s);
 template <class R> void launch_convert(const R *src, double *dst, long long n, cudaStream_t s);   // field -> FP64 staging
 template <class R> void launch_convert_in(const double *src, R *dst, long long n, cudaStream_t s); // FP64 staging -> field
 void launch_join(const float *hi, const float *lo, double *dst, long long n, cudaStream_t s);       // FP32 pair -> FP64 staging

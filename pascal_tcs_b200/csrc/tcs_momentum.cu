@@ -44,7 +44,7 @@ void launch_momentum_coeffi(const Ctx<R> &cx, cudaStream_t s)
 // ---------------------------------------------------------------------------
 // solvedU (:225-563)
 // ---------------------------------------------------------------------------
-template <class R>
+template <class R, int ITEM = 0>
 struct DUZ {
     using Real = R;
     static constexpr int NRHS = 1;
@@ -56,11 +56,11 @@ struct DUZ {
     __device__ bool skip() const { return blown(g); }
     struct State { R dt; };
     __device__ State prepare() const { return State{R(g.scal[S_DT])}; }
-    __device__ int li(int l) const { return 1 + blockIdx.x * TL + l; }
+    __device__ int li(int l) const { return 1 + vbx<ITEM>() * TL + l; }
     __device__ bool line_ok(int l) const { return li(l) <= g.N1; }
     __device__ Coef<R, 1> build(int l, int r, const State &st) const
     {
-        const int i = li(l), j = 1 + blockIdx.y, k = r + 1;
+        const int i = li(l), j = 1 + vby<ITEM>(), k = r + 1;
         const int im = i - 1, ip = i + 1, jm = j - 1, jp = j + 1, km = k - 1, kp = k + 1;
         const PhysT<R> &p = g.ph;
         const R *dx1 = g.m1.dx, *dx2 = g.m2.dx, *dx3 = g.m3.dx;
@@ -129,10 +129,10 @@ struct DUZ {
         cf.b = mACK * dt + R(1.0); cf.c = mAPK * dt; cf.a = mAMK * dt; cf.d[0] = rhs * dt;
         return cf;
     }
-    __device__ void emit(int l, int r, const R *x, const State &st) const { f.scr[ix(g, li(l), 1 + blockIdx.y, r + 1)] = x[0]; }
+    __device__ void emit(int l, int r, const R *x, const State &st) const { f.scr[ix(g, li(l), 1 + vby<ITEM>(), r + 1)] = x[0]; }
 };
 
-template <class R, int WIDE = 0>
+template <class R, int WIDE = 0, int ITEM = 0>
 struct DUX {
     using Real = R;
     static constexpr int NRHS = 1;
@@ -144,11 +144,11 @@ struct DUX {
     __device__ bool skip() const { return blown(g); }
     struct State { R dt; };
     __device__ State prepare() const { return State{R(g.scal[S_DT])}; }
-    __device__ int lj(int l) const { return 1 + blockIdx.x * TL + l; }
+    __device__ int lj(int l) const { return 1 + vbx<ITEM>() * TL + l; }
     __device__ bool line_ok(int l) const { return lj(l) <= g.N2; }
     __device__ Coef<R, 1> build(int l, int r, const State &st) const
     {
-        const int i = r + 1, j = lj(l), k = 1 + blockIdx.y, im = i - 1;
+        const int i = r + 1, j = lj(l), k = 1 + vby<ITEM>(), im = i - 1;
         const PhysT<R> &p = g.ph;
         const R *dx1 = g.m1.dx, *rdx1 = g.m1.rdx, *rdmx1 = g.m1.rdmx;
         const long long c = ix(g, i, j, k);
@@ -166,10 +166,10 @@ struct DUX {
         cf.b = mACI * dt + R(1.0); cf.c = mAPI * dt; cf.a = mAMI * dt; cf.d[0] = ld(f.scr + c);
         return cf;
     }
-    __device__ void emit(int l, int r, const R *x, const State &st) const { f.scr[ix(g, r + 1, lj(l), 1 + blockIdx.y)] = x[0]; }
+    __device__ void emit(int l, int r, const R *x, const State &st) const { f.scr[ix(g, r + 1, lj(l), 1 + vby<ITEM>())] = x[0]; }
 };
 
-template <class R>
+template <class R, int ITEM = 0>
 struct DUY {
     using Real = R;
     static constexpr int NRHS = 1;
@@ -181,11 +181,11 @@ struct DUY {
     __device__ bool skip() const { return blown(g); }
     struct State { R dt; };
     __device__ State prepare() const { return State{R(g.scal[S_DT])}; }
-    __device__ int li(int l) const { return 1 + blockIdx.x * TL + l; }
+    __device__ int li(int l) const { return 1 + vbx<ITEM>() * TL + l; }
     __device__ bool line_ok(int l) const { return li(l) <= g.N1; }
     __device__ Coef<R, 1> build(int l, int r, const State &st) const
     {
-        const int i = li(l), j = r + 1, k = 1 + blockIdx.y, im = i - 1, jm = j - 1, jp = j + 1;
+        const int i = li(l), j = r + 1, k = 1 + vby<ITEM>(), im = i - 1, jm = j - 1, jp = j + 1;
         const PhysT<R> &p = g.ph;
         const R *dx1 = g.m1.dx, *dx2 = g.m2.dx;
         const R *rdx2 = g.m2.rdx, *rdmx1 = g.m1.rdmx, *rdmx2 = g.m2.rdmx;
@@ -209,7 +209,7 @@ struct DUY {
         cf.b = mACJ * dt + R(1.0); cf.c = mAPJ * dt; cf.a = mAMJ * dt; cf.d[0] = ld(f.scr + c);
         return cf;
     }
-    __device__ void emit(int l, int r, const R *x, const State &st) const { store_periodic(g, f.dU, li(l), r + 1, 1 + blockIdx.y, x[0]); }
+    __device__ void emit(int l, int r, const R *x, const State &st) const { store_periodic(g, f.dU, li(l), r + 1, 1 + vby<ITEM>(), x[0]); }
 };
 
 // ---------------------------------------------------------------------------
@@ -217,7 +217,7 @@ struct DUY {
 // by the last stage-1 iteration (i=N1, j=N2, k=N3); the y stage scales the
 // upper coefficient by jvp = jS_BC(j-1) and the lower one by jvm = jS_BC(j+1).
 // ---------------------------------------------------------------------------
-template <class R>
+template <class R, int ITEM = 0>
 struct DVZ {
     using Real = R;
     static constexpr int NRHS = 1;
@@ -229,11 +229,11 @@ struct DVZ {
     __device__ bool skip() const { return blown(g); }
     struct State { R dt; };
     __device__ State prepare() const { return State{R(g.scal[S_DT])}; }
-    __device__ int li(int l) const { return 1 + blockIdx.x * TL + l; }
+    __device__ int li(int l) const { return 1 + vbx<ITEM>() * TL + l; }
     __device__ bool line_ok(int l) const { return li(l) <= g.N1; }
     __device__ Coef<R, 1> build(int l, int r, const State &st) const
     {
-        const int i = li(l), j = 2 + blockIdx.y, k = r + 1;
+        const int i = li(l), j = 2 + vby<ITEM>(), k = r + 1;
         const int im = i - 1, ip = i + 1, jm = j - 1, jp = j + 1, km = k - 1, kp = k + 1;
         const PhysT<R> &p = g.ph;
         const R *dx1 = g.m1.dx, *dx2 = g.m2.dx, *dx3 = g.m3.dx;
@@ -303,7 +303,7 @@ struct DVZ {
         cf.b = mACK * dt + R(1.0); cf.c = mAPK * dt; cf.a = mAMK * dt; cf.d[0] = rhs * dt;
         return cf;
     }
-    __device__ void emit(int l, int r, const R *x, const State &st) const { f.scr[ix(g, li(l), 2 + blockIdx.y, r + 1)] = x[0]; }
+    __device__ void emit(int l, int r, const R *x, const State &st) const { f.scr[ix(g, li(l), 2 + vby<ITEM>(), r + 1)] = x[0]; }
 };
 
 // mu1, mu2 of solvedV's last stage-1 iteration (i = N1, j = N2, k = N3).
@@ -317,7 +317,7 @@ __device__ __forceinline__ void dv_stale_mu12(const GridT<R> &g, const FieldsT<R
     mu2 = R(0.5) * (dx1[ip] * mxy + dx1[i] * mxy) * rdmx1[ip];
 }
 
-template <class R, int WIDE = 0>
+template <class R, int WIDE = 0, int ITEM = 0>
 struct DVX {
     using Real = R;
     static constexpr int NRHS = 1;
@@ -335,11 +335,11 @@ struct DVX {
         dv_stale_mu12(g, f, s.mu1, s.mu2);
         return s;
     }
-    __device__ int lj(int l) const { return 2 + blockIdx.x * TL + l; }
+    __device__ int lj(int l) const { return 2 + vbx<ITEM>() * TL + l; }
     __device__ bool line_ok(int l) const { return lj(l) <= g.N2; }
     __device__ Coef<R, 1> build(int l, int r, const State &st) const
     {
-        const int i = r + 1, j = lj(l), k = 1 + blockIdx.y, ip = i + 1, jm = j - 1;
+        const int i = r + 1, j = lj(l), k = 1 + vby<ITEM>(), ip = i + 1, jm = j - 1;
         const PhysT<R> &p = g.ph;
         const R *dx2 = g.m2.dx, *rdx1 = g.m1.rdx, *rdmx1 = g.m1.rdmx, *rdmx2 = g.m2.rdmx;
         const long long c = ix(g, i, j, k), sj = g.P1;
@@ -356,10 +356,10 @@ struct DVX {
         cf.b = mACI * dt + R(1.0); cf.c = mAPI * dt; cf.a = mAMI * dt; cf.d[0] = ld(f.scr + c);
         return cf;
     }
-    __device__ void emit(int l, int r, const R *x, const State &st) const { f.scr[ix(g, r + 1, lj(l), 1 + blockIdx.y)] = x[0]; }
+    __device__ void emit(int l, int r, const R *x, const State &st) const { f.scr[ix(g, r + 1, lj(l), 1 + vby<ITEM>())] = x[0]; }
 };
 
-template <class R>
+template <class R, int ITEM = 0>
 struct DVY {
     using Real = R;
     static constexpr int NRHS = 1;
@@ -371,11 +371,11 @@ struct DVY {
     __device__ bool skip() const { return blown(g); }
     struct State { R dt; };
     __device__ State prepare() const { return State{R(g.scal[S_DT])}; }
-    __device__ int li(int l) const { return 1 + blockIdx.x * TL + l; }
+    __device__ int li(int l) const { return 1 + vbx<ITEM>() * TL + l; }
     __device__ bool line_ok(int l) const { return li(l) <= g.N1; }
     __device__ Coef<R, 1> build(int l, int r, const State &st) const
     {
-        const int i = li(l), j = r + 2, k = 1 + blockIdx.y, jm = j - 1, jp = j + 1;
+        const int i = li(l), j = r + 2, k = 1 + vby<ITEM>(), jm = j - 1, jp = j + 1;
         const PhysT<R> &p = g.ph;
         const R *dx2 = g.m2.dx, *rdx2 = g.m2.rdx, *rdmx2 = g.m2.rdmx;
         const long long c = ix(g, i, j, k), sj = g.P1;
@@ -394,14 +394,14 @@ struct DVY {
         cf.b = mACJ * dt + R(1.0); cf.c = mAPJ * dt; cf.a = mAMJ * dt; cf.d[0] = ld(f.scr + c);
         return cf;
     }
-    __device__ void emit(int l, int r, const R *x, const State &st) const { store_periodic(g, f.dV, li(l), r + 2, 1 + blockIdx.y, x[0]); }
+    __device__ void emit(int l, int r, const R *x, const State &st) const { store_periodic(g, f.dV, li(l), r + 2, 1 + vby<ITEM>(), x[0]); }
 };
 
 // ---------------------------------------------------------------------------
 // solvedW (:930-1272).  Stage 2 uses stale mu1, mu2 and stage 3 stale mu3,
 // mu4 (last stage-1 iteration) and a stale km = N3-1 (last stage-2 iteration).
 // ---------------------------------------------------------------------------
-template <class R>
+template <class R, int ITEM = 0>
 struct DWZ {
     using Real = R;
     static constexpr int NRHS = 1;
@@ -413,11 +413,11 @@ struct DWZ {
     __device__ bool skip() const { return blown(g); }
     struct State { R dt; };
     __device__ State prepare() const { return State{R(g.scal[S_DT])}; }
-    __device__ int li(int l) const { return 1 + blockIdx.x * TL + l; }
+    __device__ int li(int l) const { return 1 + vbx<ITEM>() * TL + l; }
     __device__ bool line_ok(int l) const { return li(l) <= g.N1; }
     __device__ Coef<R, 1> build(int l, int r, const State &st) const
     {
-        const int i = li(l), j = 1 + blockIdx.y, k = r + 1;
+        const int i = li(l), j = 1 + vby<ITEM>(), k = r + 1;
         const int im = i - 1, ip = i + 1, jm = j - 1, jp = j + 1, km = k - 1, kp = k + 1;
         const PhysT<R> &p = g.ph;
         const R *dx1 = g.m1.dx, *dx2 = g.m2.dx, *dx3 = g.m3.dx;
@@ -492,7 +492,7 @@ struct DWZ {
         cf.b = mACK * dt + R(1.0); cf.c = mAPK * dt; cf.a = mAMK * dt; cf.d[0] = rhs * dt;
         return cf;
     }
-    __device__ void emit(int l, int r, const R *x, const State &st) const { f.scr[ix(g, li(l), 1 + blockIdx.y, r + 1)] = x[0]; }
+    __device__ void emit(int l, int r, const R *x, const State &st) const { f.scr[ix(g, li(l), 1 + vby<ITEM>(), r + 1)] = x[0]; }
 };
 
 // mu1..mu4 of solvedW's last stage-1 iteration (i = N1, j = N2, k = N3).
@@ -511,7 +511,7 @@ __device__ __forceinline__ void dw_stale_mu(const GridT<R> &g, const FieldsT<R> 
     mu4 = R(0.5) * (dx2[jp] * mxz + dx2[j] * mub) * rdmx2[jp];
 }
 
-template <class R, int WIDE = 0>
+template <class R, int WIDE = 0, int ITEM = 0>
 struct DWX {
     using Real = R;
     static constexpr int NRHS = 1;
@@ -529,11 +529,11 @@ struct DWX {
         dw_stale_mu(g, f, s.mu1, s.mu2, s.mu3, s.mu4);
         return s;
     }
-    __device__ int lj(int l) const { return 1 + blockIdx.x * TL + l; }
+    __device__ int lj(int l) const { return 1 + vbx<ITEM>() * TL + l; }
     __device__ bool line_ok(int l) const { return lj(l) <= g.N2; }
     __device__ Coef<R, 1> build(int l, int r, const State &st) const
     {
-        const int i = r + 1, j = lj(l), k = 1 + blockIdx.y, ip = i + 1, km = k - 1;
+        const int i = r + 1, j = lj(l), k = 1 + vby<ITEM>(), ip = i + 1, km = k - 1;
         const PhysT<R> &p = g.ph;
         const R *dx3 = g.m3.dx, *rdx1 = g.m1.rdx, *rdmx1 = g.m1.rdmx, *rdmx3 = g.m3.rdmx;
         const long long c = ix(g, i, j, k), sk = (long long)g.P1 * g.P2;
@@ -551,10 +551,10 @@ struct DWX {
         cf.b = mACI * dt + R(1.0); cf.c = mAPI * dt; cf.a = mAMI * dt; cf.d[0] = ld(f.scr + c);
         return cf;
     }
-    __device__ void emit(int l, int r, const R *x, const State &st) const { f.scr[ix(g, r + 1, lj(l), 1 + blockIdx.y)] = x[0]; }
+    __device__ void emit(int l, int r, const R *x, const State &st) const { f.scr[ix(g, r + 1, lj(l), 1 + vby<ITEM>())] = x[0]; }
 };
 
-template <class R>
+template <class R, int ITEM = 0>
 struct DWY {
     using Real = R;
     static constexpr int NRHS = 1;
@@ -572,11 +572,11 @@ struct DWY {
         dw_stale_mu(g, f, s.mu1, s.mu2, s.mu3, s.mu4);
         return s;
     }
-    __device__ int li(int l) const { return 1 + blockIdx.x * TL + l; }
+    __device__ int li(int l) const { return 1 + vbx<ITEM>() * TL + l; }
     __device__ bool line_ok(int l) const { return li(l) <= g.N1; }
     __device__ Coef<R, 1> build(int l, int r, const State &st) const
     {
-        const int i = li(l), j = r + 1, k = 1 + blockIdx.y, jp = j + 1, km = g.N3 - 1;
+        const int i = li(l), j = r + 1, k = 1 + vby<ITEM>(), jp = j + 1, km = g.N3 - 1;
         const PhysT<R> &p = g.ph;
         const R *dx3 = g.m3.dx, *rdx2 = g.m2.rdx, *rdmx2 = g.m2.rdmx, *rdmx3 = g.m3.rdmx;
         const long long c = ix(g, i, j, k), sj = g.P1;
@@ -596,7 +596,7 @@ struct DWY {
         cf.b = mACJ * dt + R(1.0); cf.c = mAPJ * dt; cf.a = mAMJ * dt; cf.d[0] = ld(f.scr + c);
         return cf;
     }
-    __device__ void emit(int l, int r, const R *x, const State &st) const { store_periodic(g, f.dW, li(l), r + 1, 1 + blockIdx.y, x[0]); }
+    __device__ void emit(int l, int r, const R *x, const State &st) const { store_periodic(g, f.dW, li(l), r + 1, 1 + vby<ITEM>(), x[0]); }
 };
 
 template <class R>
@@ -759,6 +759,30 @@ void launch_pseudo_update(const Ctx<R> &cx, cudaStream_t s)
 #undef IR
 
 // the two forms
+// The nine sweeps of solvedU, solvedV and solvedW for many cases, one launch per sweep.
+template <class R>
+void launch_momentum_multi(const std::vector<Ctx<R> *> &cs, MultiArena &A, cudaStream_t s)
+{
+    auto z = [](int ny) {
+        return [ny](const Ctx<R> &x) { return StageShape{x.g.N3, true, x.tl_strided, x.g.N1, x.g.N2 - ny}; };
+    };
+    auto y = [](int ny) {
+        return [ny](const Ctx<R> &x) { return StageShape{x.g.N2 - ny, false, x.tl_strided, x.g.N1, x.g.N3}; };
+    };
+    auto lines = [](int ny) { return [ny](const Ctx<R> &x) { return x.g.N2 - ny; }; };
+    multi_stage<DUZ<R, 1>>(cs, A, s, "du_z", z(0), [](const Ctx<R> &x, int tl) { return DUZ<R, 1>{x.g, x.f, tl}; });
+    multi_x<DUX>(cs, A, s, "du_x", lines(0));
+    multi_stage<DUY<R, 1>>(cs, A, s, "du_y", y(0), [](const Ctx<R> &x, int tl) { return DUY<R, 1>{x.g, x.f, tl}; });
+    multi_stage<DVZ<R, 1>>(cs, A, s, "dv_z", z(1), [](const Ctx<R> &x, int tl) { return DVZ<R, 1>{x.g, x.f, tl}; });
+    multi_x<DVX>(cs, A, s, "dv_x", lines(1));
+    multi_stage<DVY<R, 1>>(cs, A, s, "dv_y", y(1), [](const Ctx<R> &x, int tl) { return DVY<R, 1>{x.g, x.f, tl}; });
+    multi_stage<DWZ<R, 1>>(cs, A, s, "dw_z", z(0), [](const Ctx<R> &x, int tl) { return DWZ<R, 1>{x.g, x.f, tl}; });
+    multi_x<DWX>(cs, A, s, "dw_x", lines(0));
+    multi_stage<DWY<R, 1>>(cs, A, s, "dw_y", y(0), [](const Ctx<R> &x, int tl) { return DWY<R, 1>{x.g, x.f, tl}; });
+}
+
+template void launch_momentum_multi<double>(const std::vector<Ctx<double> *> &, MultiArena &, cudaStream_t);
+template void launch_momentum_multi<float>(const std::vector<Ctx<float> *> &, MultiArena &, cudaStream_t);
 template void launch_momentum_coeffi<double>(const Ctx<double> &, cudaStream_t);
 template void launch_momentum_coeffi<float>(const Ctx<float> &, cudaStream_t);
 template void launch_solve_du<double>(const Ctx<double> &, cudaStream_t);

@@ -292,7 +292,7 @@ __global__ void __launch_bounds__(256) fftz_kernel(GridT<R> g, FieldsT<R> f, FFT
 // imaginary parts of (0,0) and (0,N3/2) are zeroed after the solve.  The
 // rows are FP64 in both forms: the zero and lowest wavenumbers are nearly
 // singular, and the FP32 form reads and writes its FP32 spectrum around them.
-template <class R>
+template <class R, int ITEM = 0>
 struct Modal {
     using Real = double;
     static constexpr int NRHS = 2;
@@ -304,11 +304,11 @@ struct Modal {
     __device__ bool skip() const { return blown(g); }
     struct State { double dt; };
     __device__ State prepare() const { return State{g.scal[S_DT]}; }
-    __device__ int lk(int l) const { return blockIdx.x * TL + l; }
+    __device__ int lk(int l) const { return vbx<ITEM>() * TL + l; }
     __device__ bool line_ok(int l) const { return lk(l) < h1p; }
     __device__ Coef<double, 2> build(int l, int r, const State &st) const
     {
-        const int kx = lk(l), kz = blockIdx.y, j = r + 1;
+        const int kx = lk(l), kz = vby<ITEM>(), j = r + 1;
         const double am = f.fam[j], ap = f.fap[j];
         Coef<double, 2> cf;
         const cplx_t<R> s = f.S[sidx(g, h1p, kx, j, kz)];
@@ -323,7 +323,7 @@ struct Modal {
     }
     __device__ void emit(int l, int r, const double *x, const State &st) const
     {
-        const int kx = lk(l), kz = blockIdx.y, j = r + 1;
+        const int kx = lk(l), kz = vby<ITEM>(), j = r + 1;
         const bool zi = (kx == 0) && (kz == 0 || kz == g.N3 / 2);
         f.S[sidx(g, h1p, kx, j, kz)] = mkc<R>(R(x[0]), zi ? R(0) : R(x[1]));
     }
@@ -503,30 +503,46 @@ void launch_pseudo_prhs_fftx(const Ctx<R> &cx, cudaStream_t s, bool with_pseudo)
     record_launch_error("prhs_fftx");
 }
 
+// The Poisson solve after the right-hand side, in three parts so that an
+// ensemble can run the modal solves of all its cases in one launch.
 template <class R>
-void launch_poisson_rest(const Ctx<R> &cx, cudaStream_t s)
+void launch_poisson_fwd(const Ctx<R> &cx, cudaStream_t s)
+{
+    const GridT<R> &g = cx.g;
+    const int h1p = cx.h1p, NLz = cx.fft_lines_z;
+    const size_t smz = (size_t)NLz * g.N3 * 2 * sizeof(double2);
+    static size_t cz1[64] = {};
+    smem_opt_in((const void *)fftz_kernel<-1, R>, smz, cz1);
+    probe_begin(cx, K_FFTZ_FWD, s);
+    fftz_kernel<-1, R><<<dim3((h1p + NLz - 1) / NLz, g.N2), 256, smz, s>>>(g, cx.f, cx.fp3, NLz, h1p);
+    probe_end(cx, K_FFTZ_FWD, s);
+    record_launch_error("fftz_fwd");
+}
+
+template <class R>
+void launch_modal(const Ctx<R> &cx, cudaStream_t s)
+{
+    const GridT<R> &g = cx.g;
+    LinePlan pm = make_line_plan(g.N2, false, fit_tl<Modal<R>>(g.N2, false, cx.tl_modal, cx.lanes), cx.lanes);
+    launch_lines(Modal<R>{g, cx.f, pm.TL, cx.h1p}, pm, dim3((cx.h1p + pm.TL - 1) / pm.TL, g.N3), s, K_MODAL, cx);
+}
+
+template <class R>
+void launch_poisson_back(const Ctx<R> &cx, cudaStream_t s)
 {
     const GridT<R> &g = cx.g;
     const int h1p = cx.h1p, NLz = cx.fft_lines_z, NLx = cx.fft_lines_x;
     const size_t smz = (size_t)NLz * g.N3 * 2 * sizeof(double2);
     const size_t smx = (size_t)((NLx + 1) / 2) * g.N1 * 2 * sizeof(double2);
-    static size_t cz1[64] = {}, cz2[64] = {}, cx2[64] = {};
-    smem_opt_in((const void *)fftz_kernel<-1, R>, smz, cz1);
+    static size_t cz2[64] = {}, cx2[64] = {};
     smem_opt_in((const void *)fftz_kernel<1, R>, smz, cz2);
     smem_opt_in((const void *)ifftx_kernel<R>, smx, cx2);
-    const dim3 gz((h1p + NLz - 1) / NLz, g.N2);
-    probe_begin(cx, K_FFTZ_FWD, s);
-    fftz_kernel<-1, R><<<gz, 256, smz, s>>>(g, cx.f, cx.fp3, NLz, h1p);
-    probe_end(cx, K_FFTZ_FWD, s);
-    record_launch_error("fftz_fwd");
-    LinePlan pm = make_line_plan(g.N2, false, fit_tl<Modal<R>>(g.N2, false, cx.tl_modal, cx.lanes), cx.lanes);
-    launch_lines(Modal<R>{g, cx.f, pm.TL, h1p}, pm, dim3((h1p + pm.TL - 1) / pm.TL, g.N3), s, K_MODAL, cx);
     probe_begin(cx, K_MEAN, s);
     mean_kernel<R><<<1, 256, 0, s>>>(g, cx.f, h1p);
     probe_end(cx, K_MEAN, s);
     record_launch_error("mean");
     probe_begin(cx, K_FFTZ_INV, s);
-    fftz_kernel<1, R><<<gz, 256, smz, s>>>(g, cx.f, cx.fp3, NLz, h1p);
+    fftz_kernel<1, R><<<dim3((h1p + NLz - 1) / NLz, g.N2), 256, smz, s>>>(g, cx.f, cx.fp3, NLz, h1p);
     probe_end(cx, K_FFTZ_INV, s);
     record_launch_error("fftz_inv");
     probe_begin(cx, K_IFFTX, s);
@@ -537,6 +553,14 @@ void launch_poisson_rest(const Ctx<R> &cx, cudaStream_t s)
     dp_wall_kernel<R><<<dim3((g.N1 + 2 + 127) / 128, g.N3 + 2), 128, 0, s>>>(g, cx.f, cx.wall_ab, cx.wall_bb, cx.wall_at, cx.wall_bt);
     probe_end(cx, K_DP_WALL, s);
     record_launch_error("dp_wall");
+}
+
+template <class R>
+void launch_poisson_rest(const Ctx<R> &cx, cudaStream_t s)
+{
+    launch_poisson_fwd(cx, s);
+    launch_modal(cx, s);
+    launch_poisson_back(cx, s);
 }
 
 template <class R>
@@ -556,10 +580,27 @@ void launch_projection(const Ctx<R> &cx, cudaStream_t s)
 #undef IR
 
 // the two forms
+// The modal solves of many cases in one launch.
+template <class R>
+void launch_modal_multi(const std::vector<Ctx<R> *> &cs, MultiArena &A, cudaStream_t s)
+{
+    multi_stage<Modal<R, 1>>(cs, A, s, "modal",
+        [](const Ctx<R> &x) { return StageShape{x.g.N2, false, x.tl_modal, x.h1p, x.g.N3}; },
+        [](const Ctx<R> &x, int tl) { return Modal<R, 1>{x.g, x.f, tl, x.h1p}; });
+}
+
+template void launch_modal_multi<double>(const std::vector<Ctx<double> *> &, MultiArena &, cudaStream_t);
+template void launch_modal_multi<float>(const std::vector<Ctx<float> *> &, MultiArena &, cudaStream_t);
+template void launch_modal<double>(const Ctx<double> &, cudaStream_t);
+template void launch_modal<float>(const Ctx<float> &, cudaStream_t);
 template void launch_pseudo_prhs_fftx<double>(const Ctx<double> &, cudaStream_t, bool);
 template void launch_pseudo_prhs_fftx<float>(const Ctx<float> &, cudaStream_t, bool);
 template void launch_poisson_rest<double>(const Ctx<double> &, cudaStream_t);
 template void launch_poisson_rest<float>(const Ctx<float> &, cudaStream_t);
+template void launch_poisson_fwd<double>(const Ctx<double> &, cudaStream_t);
+template void launch_poisson_fwd<float>(const Ctx<float> &, cudaStream_t);
+template void launch_poisson_back<double>(const Ctx<double> &, cudaStream_t);
+template void launch_poisson_back<float>(const Ctx<float> &, cudaStream_t);
 template void launch_projection<double>(const Ctx<double> &, cudaStream_t);
 template void launch_projection<float>(const Ctx<float> &, cudaStream_t);
 

@@ -13,7 +13,7 @@
 
 namespace tcs {
 
-template <class R>
+template <class R, int ITEM = 0>
 struct ThermalZ {
     using Real = R;
     static constexpr int NRHS = 1;
@@ -25,11 +25,11 @@ struct ThermalZ {
     __device__ bool skip() const { return blown(g); }
     struct State { R dt; };
     __device__ State prepare() const { return State{R(g.scal[S_DT])}; }
-    __device__ int li(int l) const { return 1 + blockIdx.x * TL + l; }
+    __device__ int li(int l) const { return 1 + vbx<ITEM>() * TL + l; }
     __device__ bool line_ok(int l) const { return li(l) <= g.N1; }
     __device__ Coef<R, 1> build(int l, int r, const State &st) const
     {
-        const int i = li(l), j = 1 + blockIdx.y, k = r + 1;
+        const int i = li(l), j = 1 + vby<ITEM>(), k = r + 1;
         const int im = i - 1, ip = i + 1, jm = j - 1, jp = j + 1, km = k - 1, kp = k + 1;
         const PhysT<R> &p = g.ph;
         const bool d2 = g.kdeg2 != 0;
@@ -98,13 +98,13 @@ struct ThermalZ {
     }
     __device__ void emit(int l, int r, const R *x, const State &st) const
     {
-        f.scr[ix(g, li(l), 1 + blockIdx.y, r + 1)] = x[0];
+        f.scr[ix(g, li(l), 1 + vby<ITEM>(), r + 1)] = x[0];
     }
 };
 
 // Stage 2 (:388-429): jm, jp, km, kp keep the values of the last stage-1
 // iteration (N2-1, N2+1, N3-1, N3+1).
-template <class R, int WIDE = 0>
+template <class R, int WIDE = 0, int ITEM = 0>
 struct ThermalX {
     using Real = R;
     static constexpr int NRHS = 1;
@@ -116,11 +116,11 @@ struct ThermalX {
     __device__ bool skip() const { return blown(g); }
     struct State { R dt; };
     __device__ State prepare() const { return State{R(g.scal[S_DT])}; }
-    __device__ int lj(int l) const { return 1 + blockIdx.x * TL + l; }
+    __device__ int lj(int l) const { return 1 + vbx<ITEM>() * TL + l; }
     __device__ bool line_ok(int l) const { return lj(l) <= g.N2; }
     __device__ Coef<R, 1> build(int l, int r, const State &st) const
     {
-        const int i = r + 1, j = lj(l), k = 1 + blockIdx.y;
+        const int i = r + 1, j = lj(l), k = 1 + vby<ITEM>();
         const int im = i - 1, ip = i + 1, jm = g.N2 - 1, jp = g.N2 + 1, km = g.N3 - 1, kp = g.N3 + 1;
         const PhysT<R> &p = g.ph;
         const bool d2 = g.kdeg2 != 0;
@@ -160,12 +160,12 @@ struct ThermalX {
     }
     __device__ void emit(int l, int r, const R *x, const State &st) const
     {
-        f.scr[ix(g, r + 1, lj(l), 1 + blockIdx.y)] = x[0];
+        f.scr[ix(g, r + 1, lj(l), 1 + vby<ITEM>())] = x[0];
     }
 };
 
 // Stage 3 (:456-507): km, kp stale (N3-1, N3+1); T += solution (:518-524).
-template <class R>
+template <class R, int ITEM = 0>
 struct ThermalY {
     using Real = R;
     static constexpr int NRHS = 1;
@@ -177,11 +177,11 @@ struct ThermalY {
     __device__ bool skip() const { return blown(g); }
     struct State { R dt; };
     __device__ State prepare() const { return State{R(g.scal[S_DT])}; }
-    __device__ int li(int l) const { return 1 + blockIdx.x * TL + l; }
+    __device__ int li(int l) const { return 1 + vbx<ITEM>() * TL + l; }
     __device__ bool line_ok(int l) const { return li(l) <= g.N1; }
     __device__ Coef<R, 1> build(int l, int r, const State &st) const
     {
-        const int i = li(l), j = r + 1, k = 1 + blockIdx.y;
+        const int i = li(l), j = r + 1, k = 1 + vby<ITEM>();
         const int im = i - 1, ip = i + 1, jm = j - 1, jp = j + 1, km = g.N3 - 1, kp = g.N3 + 1;
         const PhysT<R> &p = g.ph;
         const bool d2 = g.kdeg2 != 0;
@@ -221,7 +221,7 @@ struct ThermalY {
     }
     __device__ void emit(int l, int r, const R *x, const State &st) const
     {
-        const int i = li(l), j = r + 1, k = 1 + blockIdx.y;
+        const int i = li(l), j = r + 1, k = 1 + vby<ITEM>();
         store_periodic(g, f.Tn, i, j, k, ld(f.T + ix(g, i, j, k)) + x[0]);
     }
 };
@@ -239,8 +239,23 @@ void launch_thermal(const Ctx<R> &cx, cudaStream_t s)
     launch_lines(y, py, dim3((g.N1 + py.TL - 1) / py.TL, g.N3), s, K_THERMAL_Y, cx);
 }
 
+// The same three sweeps for many cases, one launch per sweep.
+template <class R>
+void launch_thermal_multi(const std::vector<Ctx<R> *> &cs, MultiArena &A, cudaStream_t s)
+{
+    multi_stage<ThermalZ<R, 1>>(cs, A, s, "thermal_z",
+        [](const Ctx<R> &x) { return StageShape{x.g.N3, true, x.tl_strided, x.g.N1, x.g.N2}; },
+        [](const Ctx<R> &x, int tl) { return ThermalZ<R, 1>{x.g, x.f, tl}; });
+    multi_x<ThermalX>(cs, A, s, "thermal_x", [](const Ctx<R> &x) { return x.g.N2; });
+    multi_stage<ThermalY<R, 1>>(cs, A, s, "thermal_y",
+        [](const Ctx<R> &x) { return StageShape{x.g.N2, false, x.tl_strided, x.g.N1, x.g.N3}; },
+        [](const Ctx<R> &x, int tl) { return ThermalY<R, 1>{x.g, x.f, tl}; });
+}
+
 // the two forms
 template void launch_thermal<double>(const Ctx<double> &, cudaStream_t);
 template void launch_thermal<float>(const Ctx<float> &, cudaStream_t);
+template void launch_thermal_multi<double>(const std::vector<Ctx<double> *> &, MultiArena &, cudaStream_t);
+template void launch_thermal_multi<float>(const std::vector<Ctx<float> *> &, MultiArena &, cudaStream_t);
 
 } // namespace tcs

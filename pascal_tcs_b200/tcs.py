@@ -42,7 +42,7 @@ EXPORTS = [
     "tcs_tdma_many_solve_cycle", "tcs_tdma_many_solve_noalloc", "tcs_kernel_count", "tcs_launch_count", "tcs_kernel_name", "tcs_probe_enable",
     "tcs_probe_read", "tcs_probe_reset", "tcs_set_use_graph", "tcs_set_tuning", "tcs_get_tuning",
     "tcs_last_error", "tcs_precision", "tcs_ensemble_create", "tcs_ensemble_destroy", "tcs_ensemble_step",
-    "tcs_ensemble_size", "tcs_autotune", "tcs_write_continue", "tcs_read_continue", "tcs_extract_plane",
+    "tcs_ensemble_size", "tcs_ensemble_set_batched", "tcs_ensemble_form", "tcs_autotune", "tcs_write_continue", "tcs_read_continue", "tcs_extract_plane",
     "tcs_tdma_plan_single_create", "tcs_tdma_plan_single_destroy", "tcs_tdma_single_solve",
     "tcs_tdma_single_solve_cycle", "tcs_tdma_many_solve_nonblocking", "tcs_tdma_many_solve_cycle_nonblocking",
 ]
@@ -135,6 +135,8 @@ def load() -> ctypes.CDLL:
         "tcs_ensemble_destroy": ([vp], ip),
         "tcs_ensemble_step": ([vp, ip, ctypes.POINTER(ip)], ip),
         "tcs_ensemble_size": ([vp], ip),
+        "tcs_ensemble_set_batched": ([vp, ip], ip),
+        "tcs_ensemble_form": ([vp, ctypes.POINTER(ip), ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)], ip),
         "tcs_autotune": ([vp, ip, ctypes.c_char_p, ctypes.POINTER(ip)], ip),
         "tcs_write_continue": ([vp, ctypes.c_char_p], ip),
         "tcs_read_continue": ([vp, ctypes.c_char_p, ctypes.POINTER(ip)], ip),
@@ -401,15 +403,30 @@ class Solver:
 
 
 class Ensemble:
-    """Independent cases on one GPU advanced together: one CUDA-graph launch
-    per step runs every case's kernels concurrently (tcs_ensemble_*)."""
+    """Independent cases on one GPU advanced together by one CUDA-graph launch
+    per step (tcs_ensemble_*).  batched: True = each line sweep is one launch
+    over all cases (blocks pull (case, block) work items); False = every
+    case's step is its own graph branch; None (default) = auto: the first 8
+    steps measure both forms, then the faster one is kept."""
 
-    def __init__(self, solvers):
+    def __init__(self, solvers, batched=None):
         self.solvers = list(solvers)
         arr = (ctypes.c_void_p * len(self.solvers))(*[s._h.value for s in self.solvers])
         h = ctypes.c_void_p()
         _check(load().tcs_ensemble_create(arr, len(self.solvers), ctypes.byref(h)), "tcs_ensemble_create")
         self._h = h
+        self.set_batched(batched)
+
+    def set_batched(self, on) -> None:
+        mode = -1 if on is None else (1 if on else 0)
+        _check(load().tcs_ensemble_set_batched(self._h, mode), "tcs_ensemble_set_batched")
+
+    def form(self):
+        """(form in use: 1 batched, 0 branch per case, -1 still measuring;
+        measured ms per step of the branch and batched forms, -1 if not measured)."""
+        f, a, b = ctypes.c_int(0), ctypes.c_float(0), ctypes.c_float(0)
+        _check(load().tcs_ensemble_form(self._h, ctypes.byref(f), ctypes.byref(a), ctypes.byref(b)), "tcs_ensemble_form")
+        return f.value, a.value, b.value
 
     def step(self, n: int = 1) -> int:
         """n steps of every case; returns how many cases have blown up."""

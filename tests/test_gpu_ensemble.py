@@ -1,6 +1,8 @@
 """Ensembles (tcs_ensemble_*): independent cases of uneven sizes, properties
 and precisions advanced together by one CUDA graph per step must give, case
-by case, exactly what each case gives when stepped alone (needs a B200)."""
+by case, exactly what each case gives when stepped alone, in both forms (the
+batched one: one multi-case launch per line sweep; one branch per case) and
+in the auto mode that measures both (needs a B200)."""
 import numpy as np
 import pytest
 
@@ -21,12 +23,14 @@ def tcs():
     return P
 
 
-def test_ensemble_matches_cases_stepped_alone(tcs):
+@pytest.mark.parametrize("batched", [True, False, None])
+def test_ensemble_matches_cases_stepped_alone(tcs, batched):
+    # None (auto) runs both forms within these 5 steps
     alone = [tcs.Solver(**c) for c in CASES]
     grouped = [tcs.Solver(**c) for c in CASES]
     for s in alone:
         s.step(5)
-    ens = tcs.Ensemble(grouped)
+    ens = tcs.Ensemble(grouped, batched=batched)
     assert len(ens) == len(CASES)
     assert ens.step(3) == 0
     assert ens.step(2) == 0          # the second graph state, then a cached one
@@ -53,3 +57,55 @@ def test_ensemble_rejects_repeated_case(tcs):
     s = tcs.Solver(**CASES[0])
     with pytest.raises(tcs.TcsError):
         tcs.Ensemble([s, s])
+
+
+def test_batched_ensemble_more_cases_than_one_launch_holds(tcs):
+    # 24 FP64 cases: more than one multi-case launch's parameter block holds,
+    # so every sweep is split over several launches; two sizes, so the items
+    # of the longer lines come first.
+    cfgs = [dict(n1m=16, n2m=12 + 4 * (i % 2), n3m=(10, 12, 16)[i % 3], property_set=1, Pr=7.0, Ra=1e6,
+                 dtStart=5e-4, seed=10 + i) for i in range(24)]
+    alone = [tcs.Solver(**c) for c in cfgs]
+    grouped = [tcs.Solver(**c) for c in cfgs]
+    for s in alone:
+        s.step(3)
+    ens = tcs.Ensemble(grouped)
+    assert ens.step(3) == 0
+    for a, b in zip(alone, grouped):
+        for n in ("T", "U", "V", "W", "P"):
+            np.testing.assert_array_equal(a.get(n), b.get(n), err_msg=n)
+
+
+def test_ensemble_switch_between_forms(tcs):
+    alone = [tcs.Solver(**c) for c in CASES[:2]]
+    grouped = [tcs.Solver(**c) for c in CASES[:2]]
+    for s in alone:
+        s.step(4)
+    ens = tcs.Ensemble(grouped, batched=True)
+    ens.step(1)
+    assert ens.form()[0] == 1
+    ens.set_batched(False)
+    ens.step(2)
+    assert ens.form()[0] == 0
+    ens.set_batched(True)
+    ens.step(1)
+    for a, b in zip(alone, grouped):
+        for n in ("T", "U", "W", "P", "dPhat"):
+            np.testing.assert_array_equal(a.get(n), b.get(n), err_msg=n)
+
+
+def test_ensemble_auto_picks_a_form(tcs):
+    alone = [tcs.Solver(**c) for c in CASES]
+    grouped = [tcs.Solver(**c) for c in CASES]
+    for s in alone:
+        s.step(10)
+    ens = tcs.Ensemble(grouped)
+    ens.step(7)
+    assert ens.form()[0] == -1                       # still measuring
+    ens.step(3)
+    form, ms_br, ms_bat = ens.form()
+    assert form in (0, 1) and ms_br > 0 and ms_bat > 0
+    assert form == (1 if ms_bat < ms_br else 0)
+    for a, b in zip(alone, grouped):
+        for n in ("T", "U", "V", "W", "P"):
+            np.testing.assert_array_equal(a.get(n), b.get(n), err_msg=n)

@@ -148,6 +148,17 @@ def profiled_traffic(kernel: str, workload: str):
     return d.get(workload, {}).get(kernel)
 
 
+def profiled_fp64_flop_per_cell(kernel: str):
+    """FP64 FLOP per cell of an FP64 line kernel (DFMA = 2) from the committed
+    ncu instruction counts (profiles/fp64_flops.json), or None."""
+    p = os.path.join(ROOT, "profiles", "fp64_flops.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        d = json.load(f)
+    return d.get(kernel, {}).get("fp64_flop_per_cell")
+
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled every 100 ms."""
 
@@ -379,6 +390,17 @@ def device_run(P, torch, cfg: dict, workload: str, args, ws: int, local: int, st
             "frac": achieved / peak if achieved else None, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
             "algorithmic_bytes_per_launch": kb, "launches": nk, "avg_launch_ms": tk / nk if nk else None,
             "traffic": profiled_traffic(top, workload)}
+    fpc = profiled_fp64_flop_per_cell(top) if esize == 8 else None
+    if fpc and nk:
+        # the line kernels' stencil builds and eliminations are FP64 arithmetic above the
+        # FP64 ridge point: their second roof is the FP64 pipe, measured live on this GPU
+        peak64 = P.measure_fp64_peak(local)
+        kcells = n1 * (n2 - 1) * n3 if top.startswith("dv_") else cells
+        ach64 = fpc * kcells / (tk / nk * 1e-3) / 1e12
+        roof["fp64_pipe"] = {"achieved_tflops": ach64, "peak_tflops": peak64, "frac": ach64 / peak64,
+                             "flop_per_cell": fpc,
+                             "flop_source": "ncu FP64 instruction counts, DFMA = 2 (profiles/fp64_flops.json)",
+                             "peak_source": "measured (tcs_measure_fp64_peak: FP64 FMA chains on every SM)"}
     step_bytes = step_bytes_per_cell(esize) * cells
     whole = {"algorithmic_bytes_per_step": step_bytes, "bytes_per_cell_step": step_bytes_per_cell(esize),
              "achieved_gbs": step_bytes / (ms / args.steps * 1e-3) / 1e9}

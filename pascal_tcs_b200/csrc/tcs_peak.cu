@@ -1,0 +1,62 @@
+// tcs_peak.cu -- the FP64 arithmetic peak of the device, measured: the
+// denominator of the FP64-pipe roofline of the line-solver kernels, whose
+// stencil builds and eliminations are FP64 arithmetic at 8-9 FLOP per byte
+// of compulsory HBM traffic (above the B200's FP64 ridge point, so these
+// kernels are bound by the FP64 pipe, not by HBM).
+#include "tcs_kernels.h"
+#include "tcs.h"
+
+namespace tcs {
+
+// Eight independent FMA chains per thread, ITERS steps each: 16 * ITERS FP64
+// FLOP per thread.  x -> x * a + b with |a| < 1 stays bounded.
+constexpr int PEAK_ITERS = 2048;
+
+__global__ void __launch_bounds__(256) fp64_fma_kernel(double a, double b, double *out)
+{
+    double x[8];
+#pragma unroll
+    for (int q = 0; q < 8; q++) x[q] = 1e-3 * (threadIdx.x + q);
+    for (int it = 0; it < PEAK_ITERS; it++) {
+#pragma unroll
+        for (int q = 0; q < 8; q++) x[q] = fma(x[q], a, b);
+    }
+    double s = 0.0;
+#pragma unroll
+    for (int q = 0; q < 8; q++) s += x[q];
+    if (s == 12345.678) out[0] = s;   // keeps the chains live; never true for these inputs
+}
+
+} // namespace tcs
+
+extern "C" int tcs_measure_fp64_peak(int device, double *tflops)
+{
+    using namespace tcs;
+    if (!tflops) return TCS_ERR_ARG;
+    *tflops = 0.0;
+    if (cudaSetDevice(device) != cudaSuccess) return TCS_ERR_CUDA;
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    double *out = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaStream_t s = nullptr;
+    bool ok = cudaMalloc(&out, sizeof(double)) == cudaSuccess && cudaEventCreate(&e0) == cudaSuccess &&
+              cudaEventCreate(&e1) == cudaSuccess && cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) == cudaSuccess;
+    const int grid = sms * 8, block = 256;
+    float best = 0.f;
+    for (int rep = 0; ok && rep < 6; rep++) {
+        cudaEventRecord(e0, s);
+        fp64_fma_kernel<<<grid, block, 0, s>>>(0.999999, 1e-7, out);
+        cudaEventRecord(e1, s);
+        ok = record_launch_error("fp64_fma") == 0 && cudaEventSynchronize(e1) == cudaSuccess;
+        float ms = 0.f;
+        if (ok) cudaEventElapsedTime(&ms, e0, e1);
+        if (ok && rep > 0 && (best == 0.f || ms < best)) best = ms;   // the first launch warms up
+    }
+    if (ok && best > 0.f) *tflops = (double)grid * block * 16.0 * PEAK_ITERS / (best * 1e-3) / 1e12;
+    if (s) cudaStreamDestroy(s);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (out) cudaFree(out);
+    return ok ? TCS_OK : TCS_ERR_CUDA;
+}

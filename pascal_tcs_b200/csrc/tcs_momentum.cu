@@ -636,10 +636,8 @@ void launch_solve_dw(const Ctx<R> &cx, cudaStream_t s)
 // blockLdV (:1278-1356): dV -= dt*M23 dW, j = 2..N2, then ghost(dV).
 // ---------------------------------------------------------------------------
 template <class R>
-__global__ void blockld_v_kernel(GridT<R> g, FieldsT<R> f)
+__device__ __forceinline__ R blockld_v_value(const GridT<R> &g, const FieldsT<R> &f, int i, int j, int k)
 {
-    const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x, j = 2 + blockIdx.y, k = 1 + blockIdx.z;
-    if (i > g.N1 || blown(g)) return;
     const int jm = j - 1, km = k - 1, kp = k + 1;
     const R *dx2 = g.m2.dx, *dx3 = g.m3.dx, *rdx3 = g.m3.rdx, *rdmx2 = g.m2.rdmx, *rdmx3 = g.m3.rdmx;
     const long long c = ix(g, i, j, k), sj = g.P1, sk = (long long)g.P1 * g.P2;
@@ -656,8 +654,21 @@ __global__ void blockld_v_kernel(GridT<R> g, FieldsT<R> f)
     const R mu5 = R(0.5) * (dx3[km] * muc + dx3[k] * mua) * rdmx3[k];
     const R mu6 = R(0.5) * (dx3[kp] * muc + dx3[k] * mub) * rdmx3[kp];
     const R dt = g.scal[S_DT];
-    const R v = f.dV[c] - dt * (R(0.25) * (dwm5 * dvdz5 + dwm6 * dvdz6) - R(0.5) * g.ph.Cmu * invRhoc * rdx3[k] * (mu6 * ddwdy6 - mu5 * ddwdy5));
-    store_periodic(g, f.dV, i, j, k, v);
+    return f.dV[c] - dt * (R(0.25) * (dwm5 * dvdz5 + dwm6 * dvdz6) - R(0.5) * g.ph.Cmu * invRhoc * rdx3[k] * (mu6 * ddwdy6 - mu5 * ddwdy5));
+}
+
+// KZ planes per thread: every input of the KZ cells is loaded before the first store
+template <class R, int KZ>
+__global__ void blockld_v_kernel(GridT<R> g, FieldsT<R> f)
+{
+    const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x, j = 2 + blockIdx.y, k0 = 1 + KZ * blockIdx.z;
+    if (i > g.N1 || blown(g)) return;
+    R v[KZ];
+#pragma unroll
+    for (int q = 0; q < KZ; q++) v[q] = k0 + q <= g.N3 ? blockld_v_value(g, f, i, j, k0 + q) : R(0);
+#pragma unroll
+    for (int q = 0; q < KZ; q++)
+        if (k0 + q <= g.N3) store_periodic(g, f.dV, i, j, k0 + q, v[q]);
 }
 
 template <class R>
@@ -665,7 +676,7 @@ void launch_blockld_v(const Ctx<R> &cx, cudaStream_t s)
 {
     const GridT<R> &g = cx.g;
     probe_begin(cx, K_BLOCKLDV, s);
-    blockld_v_kernel<<<dim3((g.N1 + 127) / 128, g.N2 - 1, g.N3), 128, 0, s>>>(g, cx.f);
+    blockld_v_kernel<R, 2><<<dim3((g.N1 + 127) / 128, g.N2 - 1, (g.N3 + 1) / 2), 128, 0, s>>>(g, cx.f);
     probe_end(cx, K_BLOCKLDV, s);
     record_launch_error("blockld_v");
 }
@@ -673,10 +684,8 @@ void launch_blockld_v(const Ctx<R> &cx, cudaStream_t s)
 // blockLdU (:1362-1460): dU -= dt*(M12 dV + M13 dW), j = 1..N2 (no ghost
 // update follows in the driver; only interior dU is read afterwards).
 template <class R>
-__global__ void blockld_u_kernel(GridT<R> g, FieldsT<R> f)
+__device__ __forceinline__ R blockld_u_value(const GridT<R> &g, const FieldsT<R> &f, int i, int j, int k)
 {
-    const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x, j = 1 + blockIdx.y, k = 1 + blockIdx.z;
-    if (i > g.N1 || blown(g)) return;
     const int im = i - 1, jm = j - 1, jp = j + 1, km = k - 1, kp = k + 1;
     const R *dx1 = g.m1.dx, *dx2 = g.m2.dx, *dx3 = g.m3.dx, *rdx2 = g.m2.rdx, *rdx3 = g.m3.rdx;
     const R *rdmx1 = g.m1.rdmx, *rdmx2 = g.m2.rdmx, *rdmx3 = g.m3.rdmx;
@@ -705,9 +714,24 @@ __global__ void blockld_u_kernel(GridT<R> g, FieldsT<R> f)
     const R mu5 = R(0.5) * (dx3[km] * muc + dx3[k] * mua) * rdmx3[k];
     const R mu6 = R(0.5) * (dx3[kp] * muc + dx3[k] * mub) * rdmx3[kp];
     const R dt = g.scal[S_DT], Cmu = g.ph.Cmu;
-    f.dU[c] = f.dU[c]
+    return f.dU[c]
         - dt * (R(0.25) * (dvm4 * dudy4 + dvm3 * dudy3) - R(0.5) * Cmu * invRhoc * rdx2[j] * (mu4 * dvmdx4 - mu3 * dvmdx3))
         - dt * (R(0.25) * (dwm6 * dudz6 + dwm5 * dudz5) - R(0.5) * Cmu * invRhoc * rdx3[k] * (mu6 * dwmdx6 - mu5 * dwmdx5));
+}
+
+// KZ planes per thread: every input of the KZ cells is loaded before the first store
+template <class R, int KZ>
+__global__ void blockld_u_kernel(GridT<R> g, FieldsT<R> f)
+{
+    const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x, j = 1 + blockIdx.y, k0 = 1 + KZ * blockIdx.z;
+    if (i > g.N1 || blown(g)) return;
+    R v[KZ];
+#pragma unroll
+    for (int q = 0; q < KZ; q++) v[q] = k0 + q <= g.N3 ? blockld_u_value(g, f, i, j, k0 + q) : R(0);
+    const long long sk = (long long)g.P1 * g.P2;
+#pragma unroll
+    for (int q = 0; q < KZ; q++)
+        if (k0 + q <= g.N3) f.dU[ix(g, i, j, k0) + q * sk] = v[q];
 }
 
 template <class R>
@@ -715,7 +739,7 @@ void launch_blockld_u(const Ctx<R> &cx, cudaStream_t s)
 {
     const GridT<R> &g = cx.g;
     probe_begin(cx, K_BLOCKLDU, s);
-    blockld_u_kernel<<<dim3((g.N1 + 127) / 128, g.N2, g.N3), 128, 0, s>>>(g, cx.f);
+    blockld_u_kernel<R, 2><<<dim3((g.N1 + 127) / 128, g.N2, (g.N3 + 1) / 2), 128, 0, s>>>(g, cx.f);
     probe_end(cx, K_BLOCKLDU, s);
     record_launch_error("blockld_u");
 }

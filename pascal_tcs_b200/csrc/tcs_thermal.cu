@@ -27,6 +27,17 @@ struct ThermalZ {
     __device__ State prepare() const { return State{R(g.scal[S_DT])}; }
     __device__ int li(int l) const { return 1 + vbx<ITEM>() * TL + l; }
     __device__ bool line_ok(int l) const { return li(l) <= g.N1; }
+    // The right-hand side of :236-361 is the explicit operator minus the three
+    // implicit operators applied to T.  Expanded, per direction d with faces
+    // -/+ (kPP the face conductivity, ded the face gradient, u the face
+    // velocity), the dK/dT products (e dkPP ded) of the explicit operator and
+    // of the implicit one cancel, and so do the two dh Tc dv terms, leaving
+    //   2 h rdx_d (kPP+ ded+ - kPP- ded-) - (u- ded- + u+ ded+) / 2.
+    // This build evaluates that reduced form (the same value in exact
+    // arithmetic, about half the arithmetic), except for the y direction on the
+    // two wall-adjacent planes (j = 1, N2), where the jC_BC masks and the wall
+    // terms keep the reference's full expression.  The z rows (am, ac, ap) are
+    // the reference's, dK/dT terms included.
     __device__ Coef<R, 1> build(int l, int r, const State &st) const
     {
         const int i = li(l), j = 1 + vby<ITEM>(), k = r + 1;
@@ -40,54 +51,55 @@ struct ThermalZ {
         const R *T = f.T;
         const R Tc = ld(T + c), Txm = ld(T + c - 1), Txp = ld(T + c + 1);
         const R Tym = ld(T + c - sj), Typ = ld(T + c + sj), Tzm = ld(T + c - sk), Tzp = ld(T + c + sk);
-        R Kc, dKc, Kxm, dKxm, Kxp, dKxp, Kym, dKym, Kyp, dKyp, Kzm, dKzm, Kzp, dKzp, irc, dirc;
-        kpp_eval(p, d2, Tc, Kc, dKc); kpp_eval(p, d2, Txm, Kxm, dKxm); kpp_eval(p, d2, Txp, Kxp, dKxp);
-        kpp_eval(p, d2, Tym, Kym, dKym); kpp_eval(p, d2, Typ, Kyp, dKyp); kpp_eval(p, d2, Tzm, Kzm, dKzm); kpp_eval(p, d2, Tzp, Kzp, dKzp);
+        R Kc, dKc, Kzm, dKzm, Kzp, dKzp, irc, dirc;
+        kpp_eval(p, d2, Tc, Kc, dKc); kpp_eval(p, d2, Tzm, Kzm, dKzm); kpp_eval(p, d2, Tzp, Kzp, dKzp);
+        const R Kxm = kpp_only(p, d2, Txm), Kxp = kpp_only(p, d2, Txp);
         rhocp_eval(p, Tc, irc, dirc);
-        const R jem = (j == 1) ? R(0.0) : R(1.0), jep = (j == g.N2) ? R(0.0) : R(1.0);   // jC_BC(jm), jC_BC(jp)
+        const bool wall = j == 1 || j == g.N2;
         const R Uc = ld(f.U + c), Uxp = ld(f.U + c + 1), Vc = ld(f.V + c), Vyp = ld(f.V + c + sj);
         const R Wc = ld(f.W + c), Wzp = ld(f.W + c + sk);
         const R h = R(0.5) * p.Ct * irc, dh = R(0.5) * p.Ct * dirc;
-        const R e1 = (dx1[i] * Txm + dx1[im] * Tc) * (R(0.5) * rdmx1[i]);
-        const R e2 = (dx1[ip] * Tc + dx1[i] * Txp) * (R(0.5) * rdmx1[ip]);
-        const R e3 = (dx2[j] * Tym + dx2[jm] * Tc) * (R(0.5) * rdmx2[j]);
-        const R e4 = (dx2[jp] * Tc + dx2[j] * Typ) * (R(0.5) * rdmx2[jp]);
-        const R e5 = (dx3[k] * Tzm + dx3[km] * Tc) * (R(0.5) * rdmx3[k]);
-        const R e6 = (dx3[kp] * Tc + dx3[k] * Tzp) * (R(0.5) * rdmx3[kp]);
         const R dedx1 = (Tc - Txm) * rdmx1[i], dedx2 = (Txp - Tc) * rdmx1[ip];
         const R dedy3 = (Tc - Tym) * rdmx2[j], dedy4 = (Typ - Tc) * rdmx2[jp];
         const R dedz5 = (Tc - Tzm) * rdmx3[k], dedz6 = (Tzp - Tc) * rdmx3[kp];
-        R rhs = -R(0.5) * ((Uc * dedx1 + Uxp * dedx2) * R(0.5) + (Vc * dedy3 + Vyp * dedy4) * R(0.5) + (Wc * dedz5 + Wzp * dedz6) * R(0.5));
         const R kPP1 = R(0.5) * rdmx1[i] * (dx1[i] * Kxm + dx1[im] * Kc), kPP2 = R(0.5) * rdmx1[ip] * (dx1[ip] * Kc + dx1[i] * Kxp);
-        const R kPP3 = R(0.5) * rdmx2[j] * (dx2[j] * Kym + dx2[jm] * Kc), kPP4 = R(0.5) * rdmx2[jp] * (dx2[jp] * Kc + dx2[j] * Kyp);
         const R kPP5 = R(0.5) * rdmx3[k] * (dx3[k] * Kzm + dx3[km] * Kc), kPP6 = R(0.5) * rdmx3[kp] * (dx3[kp] * Kc + dx3[k] * Kzp);
-        const R dkPP1 = R(0.5) * rdmx1[i] * (dx1[i] * dKxm + dx1[im] * dKc), dkPP2 = R(0.5) * rdmx1[ip] * (dx1[ip] * dKc + dx1[i] * dKxp);
-        const R dkPP3 = R(0.5) * rdmx2[j] * (dx2[j] * dKym + dx2[jm] * dKc), dkPP4 = R(0.5) * rdmx2[jp] * (dx2[jp] * dKc + dx2[j] * dKyp);
         const R dkPP5 = R(0.5) * rdmx3[k] * (dx3[k] * dKzm + dx3[km] * dKc), dkPP6 = R(0.5) * rdmx3[kp] * (dx3[kp] * dKc + dx3[k] * dKzp);
-        const R ve1 = (kPP2 * dedx2 - kPP1 * dedx1 - e2 * dkPP2 * dedx2 + e1 * dkPP1 * dedx1) * rdx1[i];
-        const R ve2 = (kPP4 * dedy4 - kPP3 * dedy3 - e4 * dkPP4 * dedy4 + e3 * dkPP3 * dedy3) * rdx2[j];
-        const R ve3 = (kPP6 * dedz6 - kPP5 * dedz5 - e6 * dkPP6 * dedz6 + e5 * dkPP5 * dedz5) * rdx3[k];
-        const R dv = (kPP2 * dedx2 - kPP1 * dedx1) * rdx1[i] + (kPP4 * dedy4 - kPP3 * dedy3) * rdx2[j] + (kPP6 * dedz6 - kPP5 * dedz5) * rdx3[k];
-        rhs = rhs + h * (ve1 + ve2 + ve3) - dh * Tc * dv;
-        R ebc_up = -R(0.25) * Vyp * rdmx2[jp] * p.Tup;
-        R ebc_dn = R(0.25) * Vc * rdmx2[j] * p.Tbt;
-        ebc_up = ebc_up + h * rdx2[j] * kPP4 * rdmx2[jp] * p.Tup + h * rdx2[j] * dkPP4 * dedy4 * p.Tup;
-        ebc_dn = ebc_dn + h * rdx2[j] * kPP3 * rdmx2[j] * p.Tbt - h * rdx2[j] * dkPP3 * dedy3 * p.Tbt;
-        rhs = rhs + (R(1.0) - jem) * ebc_dn + (R(1.0) - jep) * ebc_up;
+        const R fx = kPP2 * dedx2 - kPP1 * dedx1, fz = kPP6 * dedz6 - kPP5 * dedz5;
+        R rhs = R(2) * h * (fx * rdx1[i] + fz * rdx3[k]) - R(0.5) * (Uc * dedx1 + Uxp * dedx2) - R(0.5) * (Wc * dedz5 + Wzp * dedz6);
+        R fy;
+        if (!wall) {
+            const R Kym = kpp_only(p, d2, Tym), Kyp = kpp_only(p, d2, Typ);
+            const R kPP3 = R(0.5) * rdmx2[j] * (dx2[j] * Kym + dx2[jm] * Kc), kPP4 = R(0.5) * rdmx2[jp] * (dx2[jp] * Kc + dx2[j] * Kyp);
+            fy = kPP4 * dedy4 - kPP3 * dedy3;
+            rhs = rhs + R(2) * h * fy * rdx2[j] - R(0.5) * (Vc * dedy3 + Vyp * dedy4);
+        } else {
+            // the reference's y terms: convection, h ve2, the wall terms, minus the implicit y operator on T
+            R Kym, dKym, Kyp, dKyp;
+            kpp_eval(p, d2, Tym, Kym, dKym); kpp_eval(p, d2, Typ, Kyp, dKyp);
+            const R jem = (j == 1) ? R(0.0) : R(1.0), jep = (j == g.N2) ? R(0.0) : R(1.0);   // jC_BC(jm), jC_BC(jp)
+            const R e3 = (dx2[j] * Tym + dx2[jm] * Tc) * (R(0.5) * rdmx2[j]);
+            const R e4 = (dx2[jp] * Tc + dx2[j] * Typ) * (R(0.5) * rdmx2[jp]);
+            const R kPP3 = R(0.5) * rdmx2[j] * (dx2[j] * Kym + dx2[jm] * Kc), kPP4 = R(0.5) * rdmx2[jp] * (dx2[jp] * Kc + dx2[j] * Kyp);
+            const R dkPP3 = R(0.5) * rdmx2[j] * (dx2[j] * dKym + dx2[jm] * dKc), dkPP4 = R(0.5) * rdmx2[jp] * (dx2[jp] * dKc + dx2[j] * dKyp);
+            fy = kPP4 * dedy4 - kPP3 * dedy3;
+            const R ve2 = (kPP4 * dedy4 - kPP3 * dedy3 - e4 * dkPP4 * dedy4 + e3 * dkPP3 * dedy3) * rdx2[j];
+            R ebc_up = -R(0.25) * Vyp * rdmx2[jp] * p.Tup;
+            R ebc_dn = R(0.25) * Vc * rdmx2[j] * p.Tbt;
+            ebc_up = ebc_up + h * rdx2[j] * kPP4 * rdmx2[jp] * p.Tup + h * rdx2[j] * dkPP4 * dedy4 * p.Tup;
+            ebc_dn = ebc_dn + h * rdx2[j] * kPP3 * rdmx2[j] * p.Tbt - h * rdx2[j] * dkPP3 * dedy3 * p.Tbt;
+            const R eACJ = h * rdx2[j] * (kPP4 * rdmx2[jp] + kPP3 * rdmx2[j] - dx2[jp] * (R(0.5) * rdmx2[jp]) * dkPP4 * dedy4 * jep + dx2[jm] * (R(0.5) * rdmx2[j]) * dkPP3 * dedy3 * jem)
+                              + (R(0.25) * Vc * rdmx2[j] - R(0.25) * Vyp * rdmx2[jp]);
+            const R eAPJ = (-h * rdx2[j] * (kPP4 * rdmx2[jp] + dx2[j] * (R(0.5) * rdmx2[jp]) * dkPP4 * dedy4) + R(0.25) * Vyp * rdmx2[jp]) * jep;
+            const R eAMJ = (-h * rdx2[j] * (kPP3 * rdmx2[j] - dx2[j] * (R(0.5) * rdmx2[j]) * dkPP3 * dedy3) - R(0.25) * Vc * rdmx2[j]) * jem;
+            rhs = rhs - R(0.25) * (Vc * dedy3 + Vyp * dedy4) + h * ve2 + (R(1.0) - jem) * ebc_dn + (R(1.0) - jep) * ebc_up
+                  - (eAPJ * Typ + eACJ * Tc + eAMJ * Tym);
+        }
+        const R dv = fx * rdx1[i] + fy * rdx2[j] + fz * rdx3[k];
         const R eACK = h * rdx3[k] * (kPP6 * rdmx3[kp] + kPP5 * rdmx3[k] - dx3[kp] * (R(0.5) * rdmx3[kp]) * dkPP6 * dedz6 + dx3[km] * (R(0.5) * rdmx3[k]) * dkPP5 * dedz5)
                           + (-R(0.25) * Wzp * rdmx3[kp] + R(0.25) * Wc * rdmx3[k]);
         const R eAPK = -h * rdx3[k] * (kPP6 * rdmx3[kp] + dx3[k] * (R(0.5) * rdmx3[kp]) * dkPP6 * dedz6) + R(0.25) * Wzp * rdmx3[kp];
         const R eAMK = -h * rdx3[k] * (kPP5 * rdmx3[k] - dx3[k] * (R(0.5) * rdmx3[k]) * dkPP5 * dedz5) - R(0.25) * Wc * rdmx3[k];
-        const R eACI = h * rdx1[i] * (kPP2 * rdmx1[ip] + kPP1 * rdmx1[i] - dx1[ip] * (R(0.5) * rdmx1[ip]) * dkPP2 * dedx2 + dx1[im] * (R(0.5) * rdmx1[i]) * dkPP1 * dedx1)
-                          + (R(0.25) * Uc * rdmx1[i] - R(0.25) * Uxp * rdmx1[ip]);
-        const R eAPI = -h * rdx1[i] * (kPP2 * rdmx1[ip] + dx1[i] * (R(0.5) * rdmx1[ip]) * dkPP2 * dedx2) + R(0.25) * Uxp * rdmx1[ip];
-        const R eAMI = -h * rdx1[i] * (kPP1 * rdmx1[i] - dx1[i] * (R(0.5) * rdmx1[i]) * dkPP1 * dedx1) - R(0.25) * Uc * rdmx1[i];
-        const R eACJ = h * rdx2[j] * (kPP4 * rdmx2[jp] + kPP3 * rdmx2[j] - dx2[jp] * (R(0.5) * rdmx2[jp]) * dkPP4 * dedy4 * jep + dx2[jm] * (R(0.5) * rdmx2[j]) * dkPP3 * dedy3 * jem)
-                          + (R(0.25) * Vc * rdmx2[j] - R(0.25) * Vyp * rdmx2[jp]);
-        const R eAPJ = (-h * rdx2[j] * (kPP4 * rdmx2[jp] + dx2[j] * (R(0.5) * rdmx2[jp]) * dkPP4 * dedy4) + R(0.25) * Vyp * rdmx2[jp]) * jep;
-        const R eAMJ = (-h * rdx2[j] * (kPP3 * rdmx2[j] - dx2[j] * (R(0.5) * rdmx2[j]) * dkPP3 * dedy3) - R(0.25) * Vc * rdmx2[j]) * jem;
-        rhs = rhs - (eAPK * Tzp + eACK * Tc + eAMK * Tzm + eAPJ * Typ + eACJ * Tc + eAMJ * Tym
-                     + eAPI * Txp + eACI * Tc + eAMI * Txm - dh * Tc * dv);
         const R dt = st.dt;
         Coef<R, 1> cf;
         cf.b = eACK * dt - R(0.5) * dh * dv * dt + R(1.0);

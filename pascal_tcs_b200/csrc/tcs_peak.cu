@@ -32,9 +32,16 @@ __global__ void __launch_bounds__(256) fp64_fma_kernel(double a, double b, doubl
 extern "C" int tcs_measure_fp64_peak(int device, double *tflops)
 {
     using namespace tcs;
-    if (!tflops) return TCS_ERR_ARG;
+    if (!tflops) return set_error(TCS_ERR_ARG, "tcs_measure_fp64_peak: null result pointer");
     *tflops = 0.0;
-    if (cudaSetDevice(device) != cudaSuccess) return TCS_ERR_CUDA;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+        cudaGetLastError();   // leave no error behind for the next launch check
+        return set_error(TCS_ERR_ARG, "tcs_measure_fp64_peak: no such device");
+    }
+    int prev = 0;
+    cudaGetDevice(&prev);   // the caller's current device is put back at the end
+    if (cudaSetDevice(device) != cudaSuccess) return set_error(TCS_ERR_CUDA, "tcs_measure_fp64_peak: cudaSetDevice failed");
     int sms = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     double *out = nullptr;
@@ -58,5 +65,6 @@ extern "C" int tcs_measure_fp64_peak(int device, double *tflops)
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
     if (out) cudaFree(out);
-    return ok ? TCS_OK : TCS_ERR_CUDA;
+    cudaSetDevice(prev);
+    return ok ? TCS_OK : set_error(TCS_ERR_CUDA, "tcs_measure_fp64_peak: the timing kernel failed");
 }

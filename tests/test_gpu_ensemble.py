@@ -41,13 +41,14 @@ def test_ensemble_matches_cases_stepped_alone(tcs, batched):
         assert b.scalars()["step"] == 5
 
 
-def test_ensemble_reports_blown_cases(tcs):
+@pytest.mark.parametrize("batched", [True, False])
+def test_ensemble_reports_blown_cases(tcs, batched):
     good = tcs.Solver(**CASES[0])
     bad = tcs.Solver(n1m=16, n2m=16, n3m=16, property_set=1, Pr=7.0, Ra=1e6, dtStart=1e-3)
     T = bad.get("T")
     T[1:-1, 1:-1, 1:-1] = np.random.default_rng(0).uniform(-5.0, 5.0, T[1:-1, 1:-1, 1:-1].shape)
     bad.set("T", T)
-    ens = tcs.Ensemble([good, bad])
+    ens = tcs.Ensemble([good, bad], batched=batched)
     assert ens.step(3) == 1
     assert good.scalars()["step"] == 3 and good.scalars()["blowup"] == 0
     assert bad.scalars()["blowup"] == 1

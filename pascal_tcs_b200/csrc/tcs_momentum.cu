@@ -101,29 +101,32 @@ struct DUZ {
         const R vu3 = (mu6 * dudz6 - mu5 * dudz5) * rdx3[k];
         const R vu12 = (mu4 * dvdx4 - mu3 * dvdx3) * rdx2[j];
         const R vu13 = (mu6 * dwdx6 - mu5 * dwdx5) * rdx3[k];
-        R rhs = ih * (R(2.0) * vu1 + vu2 + vu3 + vu12 + vu13);
+        // The reduced right-hand side (see the thermal z sweep): the explicit
+        // operator minus the implicit ones applied to U, with the x and z parts
+        // collapsed (their coefficient terms cancel in exact arithmetic) and the
+        // y part in the reference's form on the wall-adjacent planes only.
+        R rhs = R(4.0) * ih * vu1 + R(2.0) * ih * (vu3 + vu13) - R(0.5) * (u1 * dudx1 + u2 * dudx2) - R(0.5) * (w5 * dudz5 + w6 * dudz6);
         rhs = rhs - p.Cmp * invRhoc * (ld(f.P + c) - ld(f.P + c - 1)) * rdmx1[i];
         const R Tc = R(0.5) * (dx1[im] * ld(f.T + c) + dx1[i] * ld(f.T + c - 1)) * rdmx1[i];
         rhs = rhs + p.Cmt * (Tc + p.a12pera11 * (Tc * Tc) * p.DeltaT) * invRhoc;
-        R ubc_dn = R(0.25) * v3 * rdmx2[j] * p.Ubt - R(0.25) * dudy3 * (dx1[i] * p.Vbt + dx1[im] * p.Vbt) * rdmx1[i] * R(0.5);
-        R ubc_up = -R(0.25) * v4 * rdmx2[jp] * p.Uup - R(0.25) * dudy4 * (dx1[i] * p.Vup + dx1[im] * p.Vup) * rdmx1[i] * R(0.5);
-        ubc_dn = ubc_dn + ih * rdx2[j] * mu3 * rdmx2[j] * p.Ubt;
-        ubc_dn = ubc_dn - ih * rdx2[j] * mu3 * rdmx1[i] * (p.Vbt - p.Vbt);
-        ubc_up = ubc_up + ih * rdx2[j] * mu4 * rdmx2[jp] * p.Uup;
-        ubc_up = ubc_up + ih * rdx2[j] * mu4 * rdmx1[i] * (p.Vup - p.Vup);
-        rhs = rhs + (R(1.0) - jum) * ubc_dn + (R(1.0) - jup) * ubc_up;
-        const R mACI = ih * rdmx1[i] * (Mjk * rdx1[i] + Mjk * rdx1[im]) * R(2.0) + R(0.25) * (dudx2 * R(0.5) + dudx1 * R(0.5) - u2 * rdx1[i] + u1 * rdx1[im]);
-        const R mAPI = -ih * rdmx1[i] * Mjk * rdx1[i] * R(2.0) + R(0.25) * (u2 * rdx1[i] + dudx2 * R(0.5));
-        const R mAMI = -ih * rdmx1[i] * Mjk * rdx1[im] * R(2.0) + R(0.25) * (-u1 * rdx1[im] + dudx1 * R(0.5));
-        const R mACJ = ih * rdx2[j] * (mu4 * rdmx2[jp] + mu3 * rdmx2[j]) + R(0.25) * (-v4 * rdmx2[jp] + v3 * rdmx2[j]);
-        const R mAPJ = (-ih * rdx2[j] * mu4 * rdmx2[jp] + R(0.25) * (v4 * rdmx2[jp])) * jup;
-        const R mAMJ = (-ih * rdx2[j] * mu3 * rdmx2[j] + R(0.25) * (-v3 * rdmx2[j])) * jum;
+        if (j != 1 && j != g.N2) {
+            rhs = rhs + R(2.0) * ih * (vu2 + vu12) - R(0.5) * (v3 * dudy3 + v4 * dudy4);
+        } else {
+            R ubc_dn = R(0.25) * v3 * rdmx2[j] * p.Ubt - R(0.25) * dudy3 * (dx1[i] * p.Vbt + dx1[im] * p.Vbt) * rdmx1[i] * R(0.5);
+            R ubc_up = -R(0.25) * v4 * rdmx2[jp] * p.Uup - R(0.25) * dudy4 * (dx1[i] * p.Vup + dx1[im] * p.Vup) * rdmx1[i] * R(0.5);
+            ubc_dn = ubc_dn + ih * rdx2[j] * mu3 * rdmx2[j] * p.Ubt;
+            ubc_dn = ubc_dn - ih * rdx2[j] * mu3 * rdmx1[i] * (p.Vbt - p.Vbt);
+            ubc_up = ubc_up + ih * rdx2[j] * mu4 * rdmx2[jp] * p.Uup;
+            ubc_up = ubc_up + ih * rdx2[j] * mu4 * rdmx1[i] * (p.Vup - p.Vup);
+            const R mACJ = ih * rdx2[j] * (mu4 * rdmx2[jp] + mu3 * rdmx2[j]) + R(0.25) * (-v4 * rdmx2[jp] + v3 * rdmx2[j]);
+            const R mAPJ = (-ih * rdx2[j] * mu4 * rdmx2[jp] + R(0.25) * (v4 * rdmx2[jp])) * jup;
+            const R mAMJ = (-ih * rdx2[j] * mu3 * rdmx2[j] + R(0.25) * (-v3 * rdmx2[j])) * jum;
+            rhs = rhs + ih * (vu2 + vu12) + (R(1.0) - jum) * ubc_dn + (R(1.0) - jup) * ubc_up - (mAPJ * Uyp + mACJ * Uc + mAMJ * Uym)
+                  - (R(0.25) * (v4 * jup * dudy4 + v3 * jum * dudy3) - ih * rdx2[j] * (mu4 * dvdx4 * jup - mu3 * dvdx3 * jum));
+        }
         const R mACK = ih * rdx3[k] * (mu6 * rdmx3[kp] + mu5 * rdmx3[k]) + R(0.25) * (-w6 * rdmx3[kp] + w5 * rdmx3[k]);
         const R mAPK = -ih * rdx3[k] * mu6 * rdmx3[kp] + R(0.25) * (w6 * rdmx3[kp]);
         const R mAMK = -ih * rdx3[k] * mu5 * rdmx3[k] + R(0.25) * (-w5 * rdmx3[k]);
-        rhs = rhs - (mAPI * Uxp + mACI * Uc + mAMI * Uxm + mAPJ * Uyp + mACJ * Uc + mAMJ * Uym + mAPK * Uzp + mACK * Uc + mAMK * Uzm);
-        rhs = rhs - (R(0.25) * (v4 * jup * dudy4 + v3 * jum * dudy3) - ih * rdx2[j] * (mu4 * dvdx4 * jup - mu3 * dvdx3 * jum));
-        rhs = rhs - (R(0.25) * (w6 * dudz6 + w5 * dudz5) - ih * rdx3[k] * (mu6 * dwdx6 - mu5 * dwdx5));
         const R dt = st.dt;
         Coef<R, 1> cf;
         cf.b = mACK * dt + R(1.0); cf.c = mAPK * dt; cf.a = mAMK * dt; cf.d[0] = rhs * dt;
@@ -278,26 +281,26 @@ struct DVZ {
         const R vv3 = (mu6 * dvdz6 - mu5 * dvdz5) * rdx3[k];
         const R vv21 = (mu2 * dudy2 - mu1 * dudy1) * rdx1[i];
         const R vv23 = (mu6 * dwdy6 - mu5 * dwdy5) * rdx3[k];
-        R rhs = ih * (vv1 + R(2.0) * vv2 + vv3 + vv21 + vv23);
+        // The reduced right-hand side (see DUZ); the y part keeps the
+        // reference's form on the planes next to the walls (j = 2, N2).
+        R rhs = R(2.0) * ih * (vv1 + vv21 + vv3 + vv23) - R(0.5) * (u1 * dvdx1 + u2 * dvdx2) - R(0.5) * (w5 * dvdz5 + w6 * dvdz6)
+                - R(0.25) * (ddu1 * dvdx1 + ddu2 * dvdx2) + ih * rdx1[i] * (mu2 * ddudy2 - mu1 * ddudy1);
         rhs = rhs - p.Cmp * invRhoc * (ld(f.P + c) - ld(f.P + c - sj)) * rdmx2[j];
-        R vbc_dn = (R(0.25) * rdx2[jm] * v3 * p.Vbt - R(0.25) * R(0.5) * dvdy3 * p.Vbt);
-        R vbc_up = (-R(0.25) * rdx2[j] * v4 * p.Vup - R(0.25) * R(0.5) * dvdy4 * p.Vup);
-        vbc_dn = vbc_dn + ih * rdmx2[j] * Mjmk * rdx2[jm] * p.Vbt * R(2.0);
-        vbc_up = vbc_up + ih * rdmx2[j] * Mjk * rdx2[j] * p.Vup * R(2.0);
-        rhs = rhs + (R(1.0) - jvm) * vbc_dn + (R(1.0) - jvp) * vbc_up;
-        const R mACI = ih * rdx1[i] * (mu2 * rdmx1[ip] + mu1 * rdmx1[i]) + R(0.25) * (-u2 * rdmx1[ip] + u1 * rdmx1[i]);
-        const R mAPI = -ih * rdx1[i] * mu2 * rdmx1[ip] + R(0.25) * (u2 * rdmx1[ip]);
-        const R mAMI = -ih * rdx1[i] * mu1 * rdmx1[i] + R(0.25) * (-u1 * rdmx1[i]);
-        const R mACJ = ih * rdmx2[j] * (Mjk * rdx2[j] + Mjmk * rdx2[jm]) * R(2.0) + R(0.25) * (dvdy4 * R(0.5) + dvdy3 * R(0.5) - v4 * rdx2[j] + v3 * rdx2[jm]);
-        const R mAPJ = (-ih * rdmx2[j] * Mjk * rdx2[j] * R(2.0) + R(0.25) * (v4 * rdx2[j] + dvdy4 * R(0.5))) * jvp;
-        const R mAMJ = (-ih * rdmx2[j] * Mjmk * rdx2[jm] * R(2.0) + R(0.25) * (-v3 * rdx2[jm] + dvdy3 * R(0.5))) * jvm;
+        if (jvp != R(0.0) && jvm != R(0.0)) {
+            rhs = rhs + R(4.0) * ih * vv2 - R(0.5) * (v3 * dvdy3 + v4 * dvdy4);
+        } else {
+            R vbc_dn = (R(0.25) * rdx2[jm] * v3 * p.Vbt - R(0.25) * R(0.5) * dvdy3 * p.Vbt);
+            R vbc_up = (-R(0.25) * rdx2[j] * v4 * p.Vup - R(0.25) * R(0.5) * dvdy4 * p.Vup);
+            vbc_dn = vbc_dn + ih * rdmx2[j] * Mjmk * rdx2[jm] * p.Vbt * R(2.0);
+            vbc_up = vbc_up + ih * rdmx2[j] * Mjk * rdx2[j] * p.Vup * R(2.0);
+            const R mACJ = ih * rdmx2[j] * (Mjk * rdx2[j] + Mjmk * rdx2[jm]) * R(2.0) + R(0.25) * (dvdy4 * R(0.5) + dvdy3 * R(0.5) - v4 * rdx2[j] + v3 * rdx2[jm]);
+            const R mAPJ = (-ih * rdmx2[j] * Mjk * rdx2[j] * R(2.0) + R(0.25) * (v4 * rdx2[j] + dvdy4 * R(0.5))) * jvp;
+            const R mAMJ = (-ih * rdmx2[j] * Mjmk * rdx2[jm] * R(2.0) + R(0.25) * (-v3 * rdx2[jm] + dvdy3 * R(0.5))) * jvm;
+            rhs = rhs + R(2.0) * ih * vv2 + (R(1.0) - jvm) * vbc_dn + (R(1.0) - jvp) * vbc_up - (mAPJ * Vyp + mACJ * Vc + mAMJ * Vym);
+        }
         const R mACK = ih * rdx3[k] * (mu6 * rdmx3[kp] + mu5 * rdmx3[k]) + R(0.25) * (-w6 * rdmx3[kp] + w5 * rdmx3[k]);
         const R mAPK = -ih * rdx3[k] * mu6 * rdmx3[kp] + R(0.25) * (w6 * rdmx3[kp]);
         const R mAMK = -ih * rdx3[k] * mu5 * rdmx3[k] + R(0.25) * (-w5 * rdmx3[k]);
-        rhs = rhs - (mAPI * Vxp + mACI * Vc + mAMI * Vxm + mAPJ * Vyp + mACJ * Vc + mAMJ * Vym + mAPK * Vzp + mACK * Vc + mAMK * Vzm);
-        rhs = rhs - (R(0.25) * (u2 * dvdx2 + u1 * dvdx1) - ih * rdx1[i] * (mu2 * dudy2 - mu1 * dudy1));
-        rhs = rhs - (R(0.25) * (w6 * dvdz6 + w5 * dvdz5) - ih * rdx3[k] * (mu6 * dwdy6 - mu5 * dwdy5));
-        rhs = rhs - (R(0.25) * (ddu2 * dvdx2 + ddu1 * dvdx1) - ih * rdx1[i] * (mu2 * ddudy2 - mu1 * ddudy1));
         const R dt = st.dt;
         Coef<R, 1> cf;
         cf.b = mACK * dt + R(1.0); cf.c = mAPK * dt; cf.a = mAMK * dt; cf.d[0] = rhs * dt;
@@ -464,29 +467,31 @@ struct DWZ {
         const R vw3 = (Mjk * dwdz6 - Mjkm * dwdz5) * rdmx3[k];
         const R vw31 = (mu2 * dudz2 - mu1 * dudz1) * rdx1[i];
         const R vw32 = (mu4 * dvdz4 - mu3 * dvdz3) * rdx2[j];
-        R rhs = ih * (vw1 + vw2 + R(2.0) * vw3 + vw31 + vw32);
+        // The reduced right-hand side (see DUZ); the y part keeps the
+        // reference's form on the wall-adjacent planes (j = 1, N2).
+        R rhs = R(2.0) * ih * (vw1 + vw31) + R(4.0) * ih * vw3 - R(0.5) * (u1 * dwdx1 + u2 * dwdx2) - R(0.5) * (w5 * dwdz5 + w6 * dwdz6)
+                - R(0.25) * (ddu1 * dwdx1 + ddu2 * dwdx2) + ih * rdx1[i] * (mu2 * ddudz2 - mu1 * ddudz1);
         rhs = rhs - p.Cmp * invRhoc * (ld(f.P + c) - ld(f.P + c - sk)) * rdmx3[k];
-        R zbc_dn = R(0.25) * v3 * rdmx2[j] * p.Wbt - R(0.25) * dwdy3 * (dx3[km] * p.Vbt + dx3[k] * p.Vbt) * rdmx3[k] * R(0.5);
-        R zbc_up = -R(0.25) * v4 * rdmx2[jp] * p.Wup - R(0.25) * dwdy4 * (dx3[km] * p.Vup + dx3[k] * p.Vup) * rdmx3[k] * R(0.5);
-        zbc_dn = zbc_dn + ih * rdx2[j] * mu3 * rdmx2[jp] * p.Wbt;
-        zbc_up = zbc_up + ih * rdx2[j] * mu4 * rdmx2[j] * p.Wup;
-        zbc_dn = zbc_dn - ih * rdx2[j] * mu3 * rdmx3[k] * (p.Vbt - p.Vbt);
-        zbc_up = zbc_up + ih * rdx2[j] * mu4 * rdmx3[k] * (p.Vup - p.Vup);
-        rhs = rhs + (R(1.0) - jwm) * zbc_dn + (R(1.0) - jwp) * zbc_up;
-        const R mACI = ih * rdx1[i] * (mu2 * rdmx1[ip] + mu1 * rdmx1[i]) + R(0.25) * (-u2 * rdmx1[ip] + u1 * rdmx1[i]);
-        const R mAPI = -ih * rdx1[i] * mu2 * rdmx1[ip] + R(0.25) * (u2 * rdmx1[ip]);
-        const R mAMI = -ih * rdx1[i] * mu1 * rdmx1[i] + R(0.25) * (-u1 * rdmx1[i]);
-        const R mACJ = ih * rdx2[j] * (mu4 * rdmx2[jp] + mu3 * rdmx2[j]) + R(0.25) * (-v4 * rdmx2[jp] + v3 * rdmx2[j]);
-        const R mAPJ = (-ih * rdx2[j] * mu4 * rdmx2[jp] + R(0.25) * (v4 * rdmx2[jp])) * jwp;
-        const R mAMJ = (-ih * rdx2[j] * mu3 * rdmx2[j] + R(0.25) * (-v3 * rdmx2[j])) * jwm;
+        if (j != 1 && j != g.N2) {
+            rhs = rhs + R(2.0) * ih * (vw2 + vw32) - R(0.5) * (v3 * dwdy3 + v4 * dwdy4)
+                  - R(0.25) * (ddv3 * dwdy3 + ddv4 * dwdy4) + ih * rdx2[j] * (mu4 * ddvdz4 - mu3 * ddvdz3);
+        } else {
+            R zbc_dn = R(0.25) * v3 * rdmx2[j] * p.Wbt - R(0.25) * dwdy3 * (dx3[km] * p.Vbt + dx3[k] * p.Vbt) * rdmx3[k] * R(0.5);
+            R zbc_up = -R(0.25) * v4 * rdmx2[jp] * p.Wup - R(0.25) * dwdy4 * (dx3[km] * p.Vup + dx3[k] * p.Vup) * rdmx3[k] * R(0.5);
+            zbc_dn = zbc_dn + ih * rdx2[j] * mu3 * rdmx2[jp] * p.Wbt;
+            zbc_up = zbc_up + ih * rdx2[j] * mu4 * rdmx2[j] * p.Wup;
+            zbc_dn = zbc_dn - ih * rdx2[j] * mu3 * rdmx3[k] * (p.Vbt - p.Vbt);
+            zbc_up = zbc_up + ih * rdx2[j] * mu4 * rdmx3[k] * (p.Vup - p.Vup);
+            const R mACJ = ih * rdx2[j] * (mu4 * rdmx2[jp] + mu3 * rdmx2[j]) + R(0.25) * (-v4 * rdmx2[jp] + v3 * rdmx2[j]);
+            const R mAPJ = (-ih * rdx2[j] * mu4 * rdmx2[jp] + R(0.25) * (v4 * rdmx2[jp])) * jwp;
+            const R mAMJ = (-ih * rdx2[j] * mu3 * rdmx2[j] + R(0.25) * (-v3 * rdmx2[j])) * jwm;
+            rhs = rhs + ih * (vw2 + vw32) + (R(1.0) - jwm) * zbc_dn + (R(1.0) - jwp) * zbc_up - (mAPJ * Wyp + mACJ * Wc + mAMJ * Wym)
+                  - (R(0.25) * (v3 * jwm * dwdy3 + v4 * jwp * dwdy4) - ih * rdx2[j] * (mu4 * dvdz4 * jwp - mu3 * dvdz3 * jwm))
+                  - (R(0.25) * (ddv3 * jwm * dwdy3 + ddv4 * jwp * dwdy4) - ih * rdx2[j] * (mu4 * ddvdz4 * jwp - mu3 * ddvdz3 * jwm));
+        }
         const R mACK = ih * rdmx3[k] * (Mjk * rdx3[k] + Mjkm * rdx3[km]) * R(2.0) + R(0.25) * (-w6 * rdx3[k] + w5 * rdx3[km] + R(0.5) * dwdz6 + R(0.5) * dwdz5);
         const R mAPK = -ih * rdmx3[k] * Mjk * rdx3[k] * R(2.0) + R(0.25) * (w6 * rdx3[k] + R(0.5) * dwdz6);
         const R mAMK = -ih * rdmx3[k] * Mjkm * rdx3[km] * R(2.0) + R(0.25) * (-w5 * rdx3[km] + R(0.5) * dwdz5);
-        rhs = rhs - (mAPI * Wxp + mACI * Wc + mAMI * Wxm + mAPJ * Wyp + mACJ * Wc + mAMJ * Wym + mAPK * Wzp + mACK * Wc + mAMK * Wzm);
-        rhs = rhs - (R(0.25) * (u2 * dwdx2 + u1 * dwdx1) - ih * rdx1[i] * (mu2 * dudz2 - mu1 * dudz1));
-        rhs = rhs - (R(0.25) * (v3 * jwm * dwdy3 + v4 * jwp * dwdy4) - ih * rdx2[j] * (mu4 * dvdz4 * jwp - mu3 * dvdz3 * jwm));
-        rhs = rhs - (R(0.25) * (ddu2 * dwdx2 + ddu1 * dwdx1) - ih * rdx1[i] * (mu2 * ddudz2 - mu1 * ddudz1));
-        rhs = rhs - (R(0.25) * (ddv3 * jwm * dwdy3 + ddv4 * jwp * dwdy4) - ih * rdx2[j] * (mu4 * ddvdz4 * jwp - mu3 * ddvdz3 * jwm));
         const R dt = st.dt;
         Coef<R, 1> cf;
         cf.b = mACK * dt + R(1.0); cf.c = mAPK * dt; cf.a = mAMK * dt; cf.d[0] = rhs * dt;

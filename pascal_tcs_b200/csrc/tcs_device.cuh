@@ -521,8 +521,11 @@ __device__ __forceinline__ void warp_solve_line_reg(R *__restrict__ A, R *__rest
     }
 }
 
-template <class R, int NR, int MREG, bool REC>
-__device__ __forceinline__ void solve_line(R *A, R *C, R *D, int DS, const LinePlan &lp, int lane, R *F, LaneFactors<R> *lf)
+// Solve a line with the register-resident elimination when the lane's
+// partition fits MREG rows, else in shared memory.
+template <class R, int NR, int MREG, bool REC = false>
+__device__ __forceinline__ void solve_line(R *A, R *C, R *D, int DS, const LinePlan &lp, int lane, R *F = nullptr,
+                                           LaneFactors<R> *lf = nullptr)
 {
     if (MREG > 0 && lp.m0 + (lp.rem ? 1 : 0) <= MREG)
         warp_solve_line_reg<R, NR, (MREG > 0 ? MREG : 1), REC>(A, C, D, DS, lp, lane, F, lf);
@@ -660,12 +663,6 @@ struct LineOcc {
     // the x sweeps' wide shape, for lines too long to fit 4 per 128-thread block
     static constexpr int xw = f32 ? 3 : 4, nt_xw = 256, reg_xw = reg_x;
 };
-
-// Solve a line with the register-resident elimination when the lane's
-// partition fits Prob::MREG rows, else in shared memory.
-template <class R, int NR, int MREG, bool REC = false>
-__device__ __forceinline__ void solve_line(R *A, R *C, R *D, int DS, const LinePlan &lp, int lane,
-                                           R *F = nullptr, LaneFactors<R> *lf = nullptr);
 
 // The block a line problem works on, read through vbx<ITEM>() / vby<ITEM>():
 // blockIdx in a one-case launch (ITEM = 0), the work item's block in a

@@ -61,7 +61,7 @@ struct DUZ {
     __device__ Coef<R, 1> build(int l, int r, const State &st) const
     {
         const int i = li(l), j = 1 + vby<ITEM>(), k = r + 1;
-        const int im = i - 1, ip = i + 1, jm = j - 1, jp = j + 1, km = k - 1, kp = k + 1;
+        const int im = i - 1, jm = j - 1, jp = j + 1, km = k - 1, kp = k + 1;
         const PhysT<R> &p = g.ph;
         const R *dx1 = g.m1.dx, *dx2 = g.m2.dx, *dx3 = g.m3.dx;
         const R *rdx1 = g.m1.rdx, *rdx2 = g.m2.rdx, *rdx3 = g.m3.rdx;
@@ -421,7 +421,7 @@ struct DWZ {
     __device__ Coef<R, 1> build(int l, int r, const State &st) const
     {
         const int i = li(l), j = 1 + vby<ITEM>(), k = r + 1;
-        const int im = i - 1, ip = i + 1, jm = j - 1, jp = j + 1, km = k - 1, kp = k + 1;
+        const int im = i - 1, ip = i + 1, jm = j - 1, jp = j + 1, km = k - 1;
         const PhysT<R> &p = g.ph;
         const R *dx1 = g.m1.dx, *dx2 = g.m2.dx, *dx3 = g.m3.dx;
         const R *rdx1 = g.m1.rdx, *rdx2 = g.m2.rdx, *rdx3 = g.m3.rdx;

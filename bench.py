@@ -275,13 +275,12 @@ def run_reference_ensemble(args, cfg, workload, O, threads) -> int:
     cases = ensemble_cases(cfg["ensemble"], cfg["precision"])[:2]
     cells_steps, el = 0, 0.0
     for c in cases:
-        o = O.Oracle(**{k: v for k, v in c.items() if k not in ("device", "precision")})
-        t0 = time.perf_counter()
-        o.step(args.steps)
-        el += time.perf_counter() - t0
+        fresh = lambda: O.Oracle(**{k: v for k, v in c.items() if k not in ("device", "precision")})
+        el += oracle_steps(fresh, args.steps, ENSEMBLE_RESET)
         cells_steps += c["n1m"] * c["n2m"] * c["n3m"] * args.steps
     v = cells_steps / el
-    sample = f"{args.steps} steps of each of the first 2 of the {cfg['ensemble']} cases, one at a time"
+    sample = (f"{args.steps} steps of each of the first 2 of the {cfg['ensemble']} cases, one at a time, "
+              f"restarting from the seeded state every {ENSEMBLE_RESET} steps as the GPU arm does")
     line = {"impl": "reference", "metric": "cell-steps/s (batched ensemble)", "value": v, "unit": "cell-steps/s",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": None,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -293,6 +292,27 @@ def run_reference_ensemble(args, cfg, workload, O, threads) -> int:
     return 0
 
 
+def oracle_steps(fresh, k: int, reset: int, warmup: int = 0) -> float:
+    """Run the oracle for `warmup` untimed then k timed steps; with a reset
+    period, restart from the seeded state (a fresh oracle, built outside the
+    timed region) before it reaches the step at which the case blows up.
+    Returns the timed seconds."""
+    o, since, el = fresh(), 0, 0.0
+    for n_total, timed in ((warmup, False), (k, True)):
+        done = 0
+        while done < n_total:
+            n = n_total - done if not reset else min(n_total - done, reset - since)
+            t0 = time.perf_counter()
+            o.step(n)
+            if timed:
+                el += time.perf_counter() - t0
+            done += n
+            since += n
+            if reset and since == reset:
+                o, since = fresh(), 0
+    return el
+
+
 def run_reference(args, cfg, workload):
     ws, rank, _ = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
     if rank != 0:
@@ -302,12 +322,9 @@ def run_reference(args, cfg, workload):
     O.set_threads(threads)
     if "ensemble" in cfg:
         return run_reference_ensemble(args, cfg, workload, O, threads)
-    o = O.Oracle(**{k: v for k, v in cfg.items() if k not in ("device", "precision")})
-    if args.warmup:
-        o.step(args.warmup)
-    t0 = time.perf_counter()
-    o.step(args.steps)
-    el = time.perf_counter() - t0
+    fresh = lambda: O.Oracle(**{k: v for k, v in cfg.items() if k not in ("device", "precision")})
+    reset = RESET_EVERY.get(workload, 0)
+    el = oracle_steps(fresh, args.steps, reset, warmup=args.warmup)
     cells = cfg["n1m"] * cfg["n2m"] * cfg["n3m"]
     v = cells * args.steps / el
     line = {"impl": "reference", "metric": "cell-steps/s (FP64 plain, one case per process)", "value": v,
@@ -317,8 +334,11 @@ def run_reference(args, cfg, workload):
             "config": {"workload": workload, **{k: cfg[k] for k in ("n1m", "n2m", "n3m", "Ra", "Pr", "dtStart")},
                        "properties": "water", "cpu_threads": threads},
             "cpu_baseline": {"value": v, "unit": "cell-steps/s", "cores": threads, "kind": "port",
-                             "sample": f"{args.steps} full time steps after {args.warmup} warm-up steps; the Fortran/MPI/"
-                                       "FFTW reference has no toolchain on this image, so its one-rank C restatement runs"},
+                             "sample": f"{args.steps} full time steps after {args.warmup} warm-up steps"
+                                       + (f", restarting from the seeded state every {reset} steps as the GPU arm does"
+                                          if reset else "")
+                                       + "; the Fortran/MPI/FFTW reference has no toolchain on this image, so its "
+                                         "one-rank C restatement runs"},
             "e2e": {"value": v, "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0

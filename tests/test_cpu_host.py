@@ -127,3 +127,29 @@ def test_tune_shape_parser():
     from pascal_tcs_b200 import tune
     assert tune.parse("256x128x64:1") == dict(n1m=256, n2m=128, n3m=64, precision=1)
     assert tune.parse("64x64x64") == dict(n1m=64, n2m=64, n3m=64, precision=0)
+
+
+def test_reference_arm_restarts_before_blowup():
+    # The water cases blow up in the reference algorithm after about 8 steps
+    # from the seeded state: the reference arm restarts from that state every
+    # RESET_EVERY steps (as the GPU arm does) and times only the steps.
+    import bench
+
+    class FakeOracle:
+        made = 0
+
+        def __init__(self):
+            FakeOracle.made += 1
+            self.n = 0
+
+        def step(self, k):
+            self.n += k
+            if self.n > 8:
+                raise FloatingPointError("blow up")
+
+    el = bench.oracle_steps(FakeOracle, 20, 8, warmup=3)
+    assert el >= 0.0
+    assert FakeOracle.made == 1 + (3 + 20) // 8
+    FakeOracle.made = 0
+    bench.oracle_steps(FakeOracle, 5, 0)          # no reset period: one oracle
+    assert FakeOracle.made == 1

@@ -52,6 +52,7 @@ struct DUZ {
     static constexpr int MREG = LineOcc<Real>::reg_z;
     static constexpr int NT = LineOcc<Real>::nt_z;
     static constexpr bool CONTIG = false;
+    static constexpr bool PAIR = LineOcc<Real>::pair_z;
     GridT<R> g; FieldsT<R> f; int TL;
     __device__ bool skip() const { return blown(g); }
     struct State { R dt; };
@@ -228,6 +229,7 @@ struct DVZ {
     static constexpr int MREG = LineOcc<Real>::reg_z;
     static constexpr int NT = LineOcc<Real>::nt_z;
     static constexpr bool CONTIG = false;
+    static constexpr bool PAIR = LineOcc<Real>::pair_z;
     GridT<R> g; FieldsT<R> f; int TL;
     __device__ bool skip() const { return blown(g); }
     struct State { R dt; };
@@ -412,6 +414,7 @@ struct DWZ {
     static constexpr int MREG = LineOcc<Real>::reg_z;
     static constexpr int NT = LineOcc<Real>::nt_z;
     static constexpr bool CONTIG = false;
+    static constexpr bool PAIR = LineOcc<Real>::pair_z;
     GridT<R> g; FieldsT<R> f; int TL;
     __device__ bool skip() const { return blown(g); }
     struct State { R dt; };

@@ -21,6 +21,7 @@ struct ThermalZ {
     static constexpr int MREG = LineOcc<Real>::reg_z;
     static constexpr int NT = LineOcc<Real>::nt_z;
     static constexpr bool CONTIG = false;
+    static constexpr bool PAIR = LineOcc<Real>::pair_z;
     GridT<R> g; FieldsT<R> f; int TL;
     __device__ bool skip() const { return blown(g); }
     struct State { R dt; };

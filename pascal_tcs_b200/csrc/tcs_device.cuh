@@ -232,6 +232,39 @@ struct Coef {
 // relative error after its refinement pass, against 5e-7 with this).
 template <class R>
 __device__ __forceinline__ R qdiv(R a, R b) { return a / b; }
+
+// Reciprocals of the line solver.  FP64: the hardware's approximate
+// reciprocal refined by two Newton-Raphson steps y <- y + y (1 - b y), the
+// classical iteration (P. Markstein, "Computation of elementary functions on
+// the IBM RISC System/6000 processor", IBM J. Res. Develop. 34(1), 1990):
+// each step squares the relative error, so the result is within about one ulp
+// of the correctly rounded 1/b for every normal b (tcs_check_reciprocal
+// measures it against the correctly rounded quotient).  It takes a handful of
+// instructions where the correctly rounded quotient takes a few tens.  FP32
+// keeps the correctly rounded quotient (see qdiv).
+template <class R>
+__device__ __forceinline__ R qrcp(R b) { return R(1) / b; }
+template <>
+__device__ __forceinline__ double qrcp<double>(double b)
+{
+    double y;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(b));
+    double e = fma(-b, y, 1.0);
+    y = fma(y, e, y);
+    e = fma(-b, y, 1.0);
+    return fma(y, e, y);
+}
+
+// The reciprocal a line family uses: qrcp where it measured faster (FR), the
+// correctly rounded quotient elsewhere (the two agree to the last bit on every
+// value tcs_check_reciprocal has tried; the choice moves register allocation
+// and scheduling, so it is made per family by measurement).
+template <bool FR, class R>
+__device__ __forceinline__ R rcp_of(R b)
+{
+    if constexpr (FR) return qrcp(b);
+    else return qdiv(R(1), b);
+}
 // What a lane keeps from the elimination of its partition so that another
 // right-hand side can be solved with the same factors (the refinement pass).
 template <class R>
@@ -244,7 +277,7 @@ struct LaneFactors {
 // A, C: coefficient rows; D: NR right-hand sides spaced by DS.  With REC the
 // pivot reciprocals of rows 2.. are stored in F and the lane's remaining
 // factors in *lf, for warp_resolve_line.
-template <class R, int NR, bool REC = false>
+template <class R, int NR, bool REC = false, bool FR = false>
 __device__ __forceinline__ void warp_solve_line(R *__restrict__ A, R *__restrict__ C, R *__restrict__ D, int DS,
                                                 const LinePlan &lp, int lane,
                                                 R *__restrict__ F = nullptr, LaneFactors<R> *lf = nullptr)
@@ -266,7 +299,7 @@ __device__ __forceinline__ void warp_solve_line(R *__restrict__ A, R *__restrict
         for (int q = 0; q < NR; q++) dm1[q] = d[q * DS + 1];
         for (int r = 2; r < m; r++) {
             const R ar = a[r];
-            const R rr = qdiv(R(1), R(1) - ar * cm1);
+            const R rr = rcp_of<FR>(R(1) - ar * cm1);
             if (REC) F[base + r] = rr;
 #pragma unroll
             for (int q = 0; q < NR; q++) { dm1[q] = rr * (d[q * DS + r] - ar * dm1[q]); d[q * DS + r] = dm1[q]; }
@@ -290,7 +323,7 @@ __device__ __forceinline__ void warp_solve_line(R *__restrict__ A, R *__restrict
             }
             // closure of row 0 with row 1 (pascal_tdma.f90:531-535)
             c0 = c[0];
-            rr0 = qdiv(R(1), R(1) - ap1 * c0);
+            rr0 = rcp_of<FR>(R(1) - ap1 * c0);
 #pragma unroll
             for (int q = 0; q < NR; q++) D0[q] = rr0 * (d[q * DS] - c0 * dp1[q]);
             A0 = rr0 * a[0];
@@ -333,7 +366,7 @@ __device__ __forceinline__ void warp_solve_line(R *__restrict__ A, R *__restrict
         bool lo_ok = true, hi_ok = true;
         if (cyc) { lo = (lo + P) & (P - 1); hi = hi & (P - 1); }
         else { lo_ok = lo >= 0; hi_ok = hi < P; lo = lo_ok ? lo : lane; hi = hi_ok ? hi : lane; }
-        const R rbe = qdiv(R(1), be);
+        const R rbe = rcp_of<FR>(be);
         R alm = __shfl_sync(0xffffffffu, al, lo), rbm = __shfl_sync(0xffffffffu, rbe, lo), gam = __shfl_sync(0xffffffffu, ga, lo);
         R alp = __shfl_sync(0xffffffffu, al, hi), rbp = __shfl_sync(0xffffffffu, rbe, hi), gap = __shfl_sync(0xffffffffu, ga, hi);
         R dem[NR], dep[NR];
@@ -353,7 +386,7 @@ __device__ __forceinline__ void warp_solve_line(R *__restrict__ A, R *__restrict
         for (int q = 0; q < NR; q++) de[q] = de[q] - k1 * dem[q] - k2 * dep[q];
         al = nal; be = nbe; ga = nga;
     }
-    const R den = qdiv(R(1), al + be + ga);
+    const R den = rcp_of<FR>(al + be + ga);
     if (REC) { lf->A0 = A0; lf->C0 = C0; lf->Am = Am; lf->Cm = Cm; lf->rr0 = rr0; lf->c0 = c0; lf->den = den; }
     R z[NR], xl[NR];
     const int nxt = cyc ? ((lane + 1) & (P - 1)) : (lane + 1 < 32 ? lane + 1 : lane);
@@ -380,7 +413,7 @@ __device__ __forceinline__ void warp_solve_line(R *__restrict__ A, R *__restrict
 // so no shared-memory access sits on the elimination chains.  The rows are
 // read once and the solution (and, with REC, the eliminated rows and pivot
 // reciprocals the refinement replays) written once.
-template <class R, int NR, int M, bool REC = false>
+template <class R, int NR, int M, bool REC = false, bool FR = false>
 __device__ __forceinline__ void warp_solve_line_reg(R *__restrict__ A, R *__restrict__ C, R *__restrict__ D, int DS,
                                                     const LinePlan &lp, int lane,
                                                     R *__restrict__ F = nullptr, LaneFactors<R> *lf = nullptr)
@@ -403,7 +436,7 @@ __device__ __forceinline__ void warp_solve_line_reg(R *__restrict__ A, R *__rest
     for (int r = 2; r < M; r++) {
         if (r < m) {
             const R ar = a[r];
-            const R rr = qdiv(R(1), R(1) - ar * c[r - 1]);
+            const R rr = rcp_of<FR>(R(1) - ar * c[r - 1]);
             if (REC) F[base + r] = rr;
 #pragma unroll
             for (int q = 0; q < NR; q++) d[q][r] = rr * (d[q][r] - ar * d[q][r - 1]);
@@ -439,7 +472,7 @@ __device__ __forceinline__ void warp_solve_line_reg(R *__restrict__ A, R *__rest
         if (m >= 3) {
             // closure of row 0 with row 1 (pascal_tdma.f90:531-535)
             c0 = c[0];
-            rr0 = qdiv(R(1), R(1) - a[1] * c0);
+            rr0 = rcp_of<FR>(R(1) - a[1] * c0);
 #pragma unroll
             for (int q = 0; q < NR; q++) D0[q] = rr0 * (d[q][0] - c0 * d[q][1]);
             A0 = rr0 * a[0];
@@ -478,7 +511,7 @@ __device__ __forceinline__ void warp_solve_line_reg(R *__restrict__ A, R *__rest
         bool lo_ok = true, hi_ok = true;
         if (cyc) { lo = (lo + P) & (P - 1); hi = hi & (P - 1); }
         else { lo_ok = lo >= 0; hi_ok = hi < P; lo = lo_ok ? lo : lane; hi = hi_ok ? hi : lane; }
-        const R rbe = qdiv(R(1), be);
+        const R rbe = rcp_of<FR>(be);
         R alm = __shfl_sync(0xffffffffu, al, lo), rbm = __shfl_sync(0xffffffffu, rbe, lo), gam = __shfl_sync(0xffffffffu, ga, lo);
         R alp = __shfl_sync(0xffffffffu, al, hi), rbp = __shfl_sync(0xffffffffu, rbe, hi), gap = __shfl_sync(0xffffffffu, ga, hi);
         R dem[NR], dep[NR];
@@ -498,7 +531,7 @@ __device__ __forceinline__ void warp_solve_line_reg(R *__restrict__ A, R *__rest
         for (int q = 0; q < NR; q++) de[q] = de[q] - k1 * dem[q] - k2 * dep[q];
         al = nal; be = nbe; ga = nga;
     }
-    const R den = qdiv(R(1), al + be + ga);
+    const R den = rcp_of<FR>(al + be + ga);
     if (REC) { lf->A0 = A0; lf->C0 = C0; lf->Am = Am; lf->Cm = Cm; lf->rr0 = rr0; lf->c0 = c0; lf->den = den; }
     R z[NR], xl[NR];
     const int nxt = cyc ? ((lane + 1) & (P - 1)) : (lane + 1 < 32 ? lane + 1 : lane);
@@ -523,14 +556,14 @@ __device__ __forceinline__ void warp_solve_line_reg(R *__restrict__ A, R *__rest
 
 // Solve a line with the register-resident elimination when the lane's
 // partition fits MREG rows, else in shared memory.
-template <class R, int NR, int MREG, bool REC = false>
+template <class R, int NR, int MREG, bool REC = false, bool FR = false>
 __device__ __forceinline__ void solve_line(R *A, R *C, R *D, int DS, const LinePlan &lp, int lane, R *F = nullptr,
                                            LaneFactors<R> *lf = nullptr)
 {
     if (MREG > 0 && lp.m0 + (lp.rem ? 1 : 0) <= MREG)
-        warp_solve_line_reg<R, NR, (MREG > 0 ? MREG : 1), REC>(A, C, D, DS, lp, lane, F, lf);
+        warp_solve_line_reg<R, NR, (MREG > 0 ? MREG : 1), REC, FR>(A, C, D, DS, lp, lane, F, lf);
     else
-        warp_solve_line<R, NR, REC>(A, C, D, DS, lp, lane, F, lf);
+        warp_solve_line<R, NR, REC, FR>(A, C, D, DS, lp, lane, F, lf);
 }
 
 // Solve the same line for another right-hand side D (in place) with the
@@ -683,6 +716,12 @@ __host__ __device__ constexpr int line_words()
     return Refine<typename Prob::Real>::on ? 5 + 2 * Prob::NRHS : 2 + Prob::NRHS;
 }
 
+// Problems whose line solves use qrcp (Prob::FAST_RCP).
+template <class P, class = void>
+struct FastRcp { static constexpr bool on = false; };
+template <class P>
+struct FastRcp<P, std::void_t<decltype(P::FAST_RCP)>> { static constexpr bool on = P::FAST_RCP; };
+
 // Problems whose build takes row-adjacent cells in pairs (Prob::PAIR).
 template <class P, class = void>
 struct PairRows { static constexpr bool on = false; };
@@ -722,7 +761,7 @@ __device__ __forceinline__ void line_block(const Prob &prob, const LinePlan &lp)
 #pragma unroll
             for (int q = 0; q < NR; q++) cf.d[q] = R(0);
         }
-        const R rb = qdiv(R(1), cf.b);
+        const R rb = rcp_of<FastRcp<Prob>::on>(cf.b);
         const R an = cf.a * rb, cn = cf.c * rb;
         sA[pos] = an; sC[pos] = cn;
 #pragma unroll
@@ -768,14 +807,14 @@ __device__ __forceinline__ void line_block(const Prob &prob, const LinePlan &lp)
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
     for (int l = warp; l < TL; l += nw) {
         if (!REF) {
-            solve_line<R, NR, Prob::MREG>(sA + l * LS, sC + l * LS, sD + l * LS, DS, lp, lane);
+            solve_line<R, NR, Prob::MREG, false, FastRcp<Prob>::on>(sA + l * LS, sC + l * LS, sD + l * LS, DS, lp, lane);
             continue;
         }
         // FP32 rows: solve recording the factors, form the residual of the
         // solution against the rows as built in FP64 (it replaces D0), and
         // solve for the correction with the recorded factors.
         LaneFactors<R> lf;
-        solve_line<R, NR, Prob::MREG, true>(sA + l * LS, sC + l * LS, sD + l * LS, DS, lp, lane, sF + l * LS, &lf);
+        solve_line<R, NR, Prob::MREG, true, FastRcp<Prob>::on>(sA + l * LS, sC + l * LS, sD + l * LS, DS, lp, lane, sF + l * LS, &lf);
         __syncwarp();
         for (int r = lane; r < n; r += 32) {
             const int pos = l * LS + spos[r];

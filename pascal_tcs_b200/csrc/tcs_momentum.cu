@@ -140,6 +140,7 @@ template <class R, int WIDE = 0, int ITEM = 0>
 struct DUX {
     using Real = R;
     static constexpr int NRHS = 1;
+    static constexpr bool FAST_RCP = true;    // measured faster with qrcp
     static constexpr int MINB = WIDE ? LineOcc<R>::xw : LineOcc<R>::x;
     static constexpr int MREG = WIDE ? LineOcc<Real>::reg_xw : LineOcc<Real>::reg_x;
     static constexpr int NT = WIDE ? LineOcc<Real>::nt_xw : LineOcc<Real>::nt_x;
@@ -326,6 +327,7 @@ template <class R, int WIDE = 0, int ITEM = 0>
 struct DVX {
     using Real = R;
     static constexpr int NRHS = 1;
+    static constexpr bool FAST_RCP = true;    // measured faster with qrcp
     static constexpr int MINB = WIDE ? LineOcc<R>::xw : LineOcc<R>::x;
     static constexpr int MREG = WIDE ? LineOcc<Real>::reg_xw : LineOcc<Real>::reg_x;
     static constexpr int NT = WIDE ? LineOcc<Real>::nt_xw : LineOcc<Real>::nt_x;
@@ -523,6 +525,7 @@ template <class R, int WIDE = 0, int ITEM = 0>
 struct DWX {
     using Real = R;
     static constexpr int NRHS = 1;
+    static constexpr bool FAST_RCP = true;    // measured faster with qrcp
     static constexpr int MINB = WIDE ? LineOcc<R>::xw : LineOcc<R>::x;
     static constexpr int MREG = WIDE ? LineOcc<Real>::reg_xw : LineOcc<Real>::reg_x;
     static constexpr int NT = WIDE ? LineOcc<Real>::nt_xw : LineOcc<Real>::nt_x;

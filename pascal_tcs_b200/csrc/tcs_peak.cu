@@ -1,10 +1,14 @@
-// tcs_peak.cu -- the FP64 arithmetic peak of the device, measured: the
-// denominator of the FP64-pipe roofline of the line-solver kernels, whose
-// stencil builds and eliminations are FP64 arithmetic at 8-9 FLOP per byte
-// of compulsory HBM traffic (above the B200's FP64 ridge point, so these
-// kernels are bound by the FP64 pipe, not by HBM).
+// tcs_peak.cu -- device measurements behind the reported numbers:
+//  * the FP64 arithmetic peak of the device: the denominator of the FP64-pipe
+//    roofline of the line-solver kernels, whose stencil builds and
+//    eliminations are FP64 arithmetic at 5-9 FLOP per byte of compulsory HBM
+//    traffic (at or above the B200's FP64 ridge point);
+//  * the accuracy of the line solver's FP64 reciprocal (qrcp) against the
+//    correctly rounded quotient.
 #include "tcs_kernels.h"
 #include "tcs.h"
+
+#include <vector>
 
 namespace tcs {
 
@@ -27,7 +31,42 @@ __global__ void __launch_bounds__(256) fp64_fma_kernel(double a, double b, doubl
     if (s == 12345.678) out[0] = s;   // keeps the chains live; never true for these inputs
 }
 
+// |qrcp(b) - 1/b| / ulp(1/b) over n values b = +-10^x, x evenly spaced in [-6, 6]
+// and both signs; out[i] holds the error of value i in ulps of the correctly
+// rounded 1/b.
+__global__ void rcp_check_kernel(int n, double *out)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double x = -6.0 + 12.0 * (double)(i >> 1) / (double)((n >> 1) > 1 ? (n >> 1) - 1 : 1);
+    const double b = ((i & 1) ? -1.0 : 1.0) * exp10(x);
+    const double q = 1.0 / b, r = qrcp(b);
+    const double ulp = fabs(nextafter(q, 2.0 * q) - q);
+    out[i] = fabs(r - q) / ulp;
+}
+
 } // namespace tcs
+
+extern "C" int tcs_check_reciprocal(int n, double *max_ulp)
+{
+    using namespace tcs;
+    if (!max_ulp || n < 2) return set_error(TCS_ERR_ARG, "tcs_check_reciprocal: need n >= 2 and a result pointer");
+    *max_ulp = -1.0;
+    double *d = nullptr;
+    if (cudaMalloc(&d, sizeof(double) * (size_t)n) != cudaSuccess) return set_error(TCS_ERR_NOMEM, "tcs_check_reciprocal: allocation");
+    rcp_check_kernel<<<(n + 255) / 256, 256>>>(n, d);
+    int rc = record_launch_error("rcp_check") ? TCS_ERR_CUDA : TCS_OK;
+    std::vector<double> h(n);
+    if (rc == TCS_OK && cudaMemcpy(h.data(), d, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost) != cudaSuccess)
+        rc = set_error(TCS_ERR_CUDA, "tcs_check_reciprocal: copy");
+    cudaFree(d);
+    if (rc == TCS_OK) {
+        double m = 0.0;
+        for (double v : h) m = v > m ? v : m;
+        *max_ulp = m;
+    }
+    return rc;
+}
 
 extern "C" int tcs_measure_fp64_peak(int device, double *tflops)
 {

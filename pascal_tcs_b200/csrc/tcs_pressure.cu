@@ -296,6 +296,7 @@ template <class R, int ITEM = 0>
 struct Modal {
     using Real = double;
     static constexpr int NRHS = 2;
+    static constexpr bool FAST_RCP = true;    // measured faster with qrcp
     static constexpr int MINB = LineOcc<R>::modal;
     static constexpr int MREG = LineOcc<Real>::reg_modal;
     static constexpr int NT = LineOcc<Real>::nt_modal;

@@ -39,7 +39,7 @@ EXPORTS = [
     "tcs_post_div", "tcs_post_cfl", "tcs_step", "tcs_get_scalars", "tcs_get_history",
     "tcs_snapshot", "tcs_restore",
     "tcs_tdma_plan_many_create", "tcs_tdma_plan_many_destroy", "tcs_tdma_many_solve",
-    "tcs_tdma_many_solve_cycle", "tcs_tdma_many_solve_noalloc", "tcs_kernel_count", "tcs_launch_count", "tcs_measure_fp64_peak", "tcs_kernel_name", "tcs_probe_enable",
+    "tcs_tdma_many_solve_cycle", "tcs_tdma_many_solve_noalloc", "tcs_kernel_count", "tcs_launch_count", "tcs_measure_fp64_peak", "tcs_check_reciprocal", "tcs_kernel_name", "tcs_probe_enable",
     "tcs_probe_read", "tcs_probe_reset", "tcs_set_use_graph", "tcs_set_tuning", "tcs_get_tuning",
     "tcs_last_error", "tcs_precision", "tcs_ensemble_create", "tcs_ensemble_destroy", "tcs_ensemble_step",
     "tcs_ensemble_size", "tcs_ensemble_set_batched", "tcs_ensemble_form", "tcs_autotune", "tcs_write_continue", "tcs_read_continue", "tcs_extract_plane",
@@ -135,6 +135,7 @@ def load() -> ctypes.CDLL:
         "tcs_ensemble_destroy": ([vp], ip),
         "tcs_ensemble_step": ([vp, ip, ctypes.POINTER(ip)], ip),
         "tcs_measure_fp64_peak": ([ip, ctypes.POINTER(ctypes.c_double)], ip),
+        "tcs_check_reciprocal": ([ip, ctypes.POINTER(ctypes.c_double)], ip),
         "tcs_ensemble_size": ([vp], ip),
         "tcs_ensemble_set_batched": ([vp, ip], ip),
         "tcs_ensemble_form": ([vp, ctypes.POINTER(ip), ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)], ip),
@@ -407,6 +408,14 @@ def measure_fp64_peak(device: int = 0) -> float:
     """FP64 FMA throughput of the device in TFLOP/s (tcs_measure_fp64_peak)."""
     v = ctypes.c_double(0.0)
     _check(load().tcs_measure_fp64_peak(int(device), ctypes.byref(v)), "tcs_measure_fp64_peak")
+    return v.value
+
+
+def check_reciprocal(n: int = 1 << 16) -> float:
+    """Largest error (ulps) of the FP64 line solver's reciprocal against the
+    correctly rounded 1/b (tcs_check_reciprocal)."""
+    v = ctypes.c_double(0.0)
+    _check(load().tcs_check_reciprocal(int(n), ctypes.byref(v)), "tcs_check_reciprocal")
     return v.value
 
 

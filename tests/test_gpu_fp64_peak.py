@@ -18,3 +18,12 @@ def test_fp64_peak_rejects_bad_device():
     import pascal_tcs_b200 as P
     with pytest.raises(P.TcsError):
         P.measure_fp64_peak(9999)
+
+
+def test_line_solver_reciprocal_within_an_ulp():
+    # qrcp (approximate reciprocal + two Newton-Raphson steps) against the
+    # correctly rounded quotient over 10^-6 .. 10^6, both signs
+    import pascal_tcs_b200 as P
+    P.load()
+    err = P.check_reciprocal(1 << 16)
+    assert 0.0 <= err <= 1.0, err

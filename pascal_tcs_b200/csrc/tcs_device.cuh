@@ -184,12 +184,17 @@ __device__ __forceinline__ R kpp_only(const PhysT<R> &p, bool d2, R T)
 // module_solve_thermal.f90:149.  The derivative's numerator (:144-148) is
 // collected into a polynomial in t = DeltaT*T with coefficients n0..n5.
 template <class R>
+__device__ __forceinline__ R qrcp(R b);
+template <>
+__device__ __forceinline__ double qrcp<double>(double b);
+
+template <class R>
 __device__ __forceinline__ void rhocp_eval(const PhysT<R> &p, R T, R &irc, R &dirc)
 {
     const R t = p.DeltaT * T;
     const R q1 = R(1) + t * (p.a11 + t * (p.a12 + t * p.a13));
     const R q2 = R(1) + t * (p.b11 + t * (p.b12 + t * p.b13));
-    const R rq = R(1) / (q1 * q2);
+    const R rq = qrcp(q1 * q2);
     irc = p.cRC * rq;
     dirc = -(p.n0 + t * (p.n1 + t * (p.n2 + t * (p.n3 + t * (p.n4 + t * p.n5))))) * (rq * rq);
 }

@@ -198,6 +198,7 @@ __global__ void __launch_bounds__(256) prhs_fftx_kernel(GridT<R> g, FieldsT<R> f
     __syncthreads();
     const double dt = g.scal[S_DT], rdt = 1.0 / dt;
     const Phys &p = g.phd;
+    const double rdtc = rdt / p.Cmp;   // 1 / (dt Cmp), once per thread
     for (int t = threadIdx.x; t < NL * N1; t += blockDim.x) {
         const int l = (int)fp.dn.div(t), i = t - l * N1 + 1, j = j0 + l;
         // two real lines per complex FFT line: line l is the real (l even) or
@@ -244,7 +245,7 @@ __global__ void __launch_bounds__(256) prhs_fftx_kernel(GridT<R> g, FieldsT<R> f
         const double Extra = ((1.0 - iR2_) * ddpdx2 - (1.0 - iR1) * ddpdx1) * rdx1[i]
                            + ((1.0 - iR4) * ddpdy4 - (1.0 - iR3) * ddpdy3) * rdx2[j]
                            + ((1.0 - iR6) * ddpdz6 - (1.0 - iR5) * ddpdz5) * rdx3[k];
-        *slot = (DivUm - cbc) * rdt / p.Cmp + Extra;
+        *slot = (DivUm - cbc) * rdtc + Extra;
     }
     if (NL & 1)         // an odd line count leaves the last packed line without an imaginary part
         for (int t = threadIdx.x; t < N1; t += blockDim.x) b0[(NL >> 1) * N1 + t].y = 0.0;
@@ -384,11 +385,12 @@ __global__ void __launch_bounds__(256) ifftx_kernel(GridT<R> g, FieldsT<R> f, FF
     __syncthreads();
     const C *res = block_fft<1>(b0, b1, nfl, N1, fp, f.tw1);
     const double aver = g.scal[S_AVER];
+    const double scale = 1.0 / ((double)N1 * (double)g.N3);   // the unnormalised transforms' 1/(N1 N3), once per thread
     for (int t = threadIdx.x; t < NL * N1; t += blockDim.x) {
         const int l = (int)fp.dn.div(t), i = t - l * N1 + 1, j = j0 + l;
         if (j > g.N2) continue;
         const C z = res[(l >> 1) * N1 + (i - 1)];
-        const double v = ((l & 1) ? z.y : z.x) / (double)N1 / (double)g.N3 - aver;
+        const double v = ((l & 1) ? z.y : z.x) * scale - aver;
         store_periodic(g, f.dP, i, j, k, R(v));
     }
 }

@@ -1,0 +1,97 @@
+"""The 256^3 water case at full size, checked through properties that do not
+depend on the size and need no CPU oracle (which takes seconds per step at
+this size): determinism, graph and eager steps, snapshot replay, the bound
+on the divergence the projection leaves, the removed pressure mean, the FP32-mixed
+form's error against FP64, and the PaScaL_TDMA interface on a full plane of
+lines (needs a B200, about 35 GB of device memory)."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+FULL = dict(n1m=256, n2m=256, n3m=256, gamma2=1.5, property_set=1, Pr=7.0, Ra=1e8, DeltaT=10.0,
+            dtStart=2e-4, fixed_dt=1, seed=1, noise_amp=0.01)
+I = (slice(1, -1),) * 3
+
+
+@pytest.fixture(scope="module")
+def tcs():
+    import pascal_tcs_b200 as P
+    P.load()
+    return P
+
+
+def rel_l2(a, b):
+    nb = np.linalg.norm(b)
+    return np.linalg.norm(a - b) / nb if nb > 0 else np.linalg.norm(a - b)
+
+
+def test_fullsize_deterministic_graph_eager_and_replay(tcs):
+    a = tcs.Solver(**FULL)
+    b = tcs.Solver(**FULL)
+    b.use_graph(False)
+    a.snapshot()
+    a.step(3)
+    b.step(3)
+    fa = {n: a.get(n) for n in ("T", "U", "V", "W", "P")}
+    for n, v in fa.items():
+        np.testing.assert_array_equal(v, b.get(n), err_msg=n)
+    a.restore()
+    a.step(3)
+    for n, v in fa.items():
+        np.testing.assert_array_equal(a.get(n), v, err_msg=n)
+    a.close()
+    b.close()
+
+
+def test_fullsize_projection_and_pressure_mean(tcs):
+    s = tcs.Solver(**FULL)
+    s.step(4)
+    h = s.history(0, 4)
+    sc = s.scalars()
+    assert sc["blowup"] == 0 and sc["step"] == 4
+    # the divergence the projection leaves (module_post.f90:100-158): the projection of this
+    # scheme uses the extrapolated pressure dPhat in its variable-density term, so it is not
+    # round-off (3e-6..7e-6 here), but finite and far below the reference's blow-up bar 1e-3
+    assert np.all(np.isfinite(h[:, 2])) and np.all(np.abs(h[:, 2]) < 1e-4), h[:, 2]
+    # the Poisson solve removes the mean of dP every step, so the pressure keeps a zero mean
+    P = s.get("P")[I]
+    assert abs(P.mean()) <= 1e-12 * np.max(np.abs(P)) + 1e-300, (P.mean(), np.max(np.abs(P)))
+    s.close()
+
+
+def test_fullsize_mixed_close_to_fp64(tcs):
+    # the error bars of the FP32-mixed form (tests/test_gpu_mixed.py) at full size
+    a = tcs.Solver(precision=0, **FULL)
+    b = tcs.Solver(precision=1, **FULL)
+    a.step(4)
+    b.step(4)
+    for n, tol in (("U", 1e-5), ("T", 1e-5), ("V", 1e-4), ("W", 1e-4), ("P", 1e-4)):
+        e = rel_l2(b.get(n)[I], a.get(n)[I])
+        print(n, f"{e:.2e}")
+        assert e <= tol, (n, e)
+    a.close()
+    b.close()
+
+
+@pytest.mark.parametrize("cyclic", [0, 1])
+def test_fullsize_tdma_plane_residual(tcs, cyclic):
+    # a z-sweep's worth of lines (256^2 systems of 256 rows) through the
+    # PaScaL_TDMA interface: the residual of every system at round-off level
+    rng = np.random.default_rng(7 + cyclic)
+    n_sys, n_row = 256 * 256, 256
+    A = rng.uniform(-0.3, 0.3, (n_row, n_sys))
+    C = rng.uniform(-0.3, 0.3, (n_row, n_sys))
+    B = 1.0 + rng.uniform(0.0, 1.0, (n_row, n_sys))
+    D = rng.uniform(-1.0, 1.0, (n_row, n_sys))
+    plan = tcs.TdmaPlan(n_sys)
+    X = D.copy()
+    (plan.many_solve_cycle if cyclic else plan.many_solve)(A.copy(), B.copy(), C.copy(), X, n_sys, n_row)
+    R = B * X - D
+    R[1:] += A[1:] * X[:-1]
+    R[:-1] += C[:-1] * X[1:]
+    if cyclic:
+        R[0] += A[0] * X[-1]
+        R[-1] += C[-1] * X[0]
+    assert np.max(np.abs(R)) <= 1e-13 * np.max(np.abs(D)), np.max(np.abs(R))
+    plan.destroy()

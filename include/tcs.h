@@ -200,10 +200,11 @@ unsigned long long tcs_launch_count(void);           /* kernels this library has
 /* The device's FP64 FMA throughput in TFLOP/s, measured (no counterpart in the
  * reference): the denominator of the line kernels' FP64-pipe roofline. */
 int tcs_measure_fp64_peak(int device, double *tflops);
-/* The largest error, in ulps of the correctly rounded 1/b, of the FP64 line
- * solver's reciprocal over n values b = +-10^x, x in [-6, 6] (no counterpart in
- * the reference: a check of this library's arithmetic). */
-int tcs_check_reciprocal(int n, double *max_ulp);
+/* The largest error, in ulps of the correctly rounded 1/b, of the line solver's
+ * reciprocal (FP64, or FP32 when fp32 != 0) over n values b = +-10^x, x in
+ * [-6, 6] (no counterpart in the reference: a check of this library's
+ * arithmetic). */
+int tcs_check_reciprocal(int n, int fp32, double *max_ulp);
 const char *tcs_kernel_name(int kernel_id);
 /* Record a CUDA event pair around every launch of the kernels in mask (bit =
  * kernel id) on the launching stream; tcs_probe_read returns their summed

@@ -245,10 +245,18 @@ __device__ __forceinline__ R qdiv(R a, R b) { return a / b; }
 // each step squares the relative error, so the result is within about one ulp
 // of the correctly rounded 1/b for every normal b (tcs_check_reciprocal
 // measures it against the correctly rounded quotient).  It takes a handful of
-// instructions where the correctly rounded quotient takes a few tens.  FP32
-// keeps the correctly rounded quotient (see qdiv).
+// instructions where the correctly rounded quotient takes a few tens.  FP32:
+// the approximate FP32 reciprocal refined by one Newton-Raphson step (the
+// unrefined approximation cost the y sweep of solvedV accuracy, see qdiv).
 template <class R>
 __device__ __forceinline__ R qrcp(R b) { return R(1) / b; }
+template <>
+__device__ __forceinline__ float qrcp<float>(float b)
+{
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(b));
+    return fmaf(y, fmaf(-b, y, 1.0f), y);
+}
 template <>
 __device__ __forceinline__ double qrcp<double>(double b)
 {

@@ -34,27 +34,29 @@ __global__ void __launch_bounds__(256) fp64_fma_kernel(double a, double b, doubl
 // |qrcp(b) - 1/b| / ulp(1/b) over n values b = +-10^x, x evenly spaced in [-6, 6]
 // and both signs; out[i] holds the error of value i in ulps of the correctly
 // rounded 1/b.
+template <class R>
 __global__ void rcp_check_kernel(int n, double *out)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const double x = -6.0 + 12.0 * (double)(i >> 1) / (double)((n >> 1) > 1 ? (n >> 1) - 1 : 1);
-    const double b = ((i & 1) ? -1.0 : 1.0) * exp10(x);
-    const double q = 1.0 / b, r = qrcp(b);
-    const double ulp = fabs(nextafter(q, 2.0 * q) - q);
-    out[i] = fabs(r - q) / ulp;
+    const R b = (R)(((i & 1) ? -1.0 : 1.0) * exp10(x));
+    const R q = R(1) / b, r = qrcp(b);
+    const double ulp = fabs((double)nextafter(q, R(2) * q) - (double)q);
+    out[i] = fabs((double)r - (double)q) / ulp;
 }
 
 } // namespace tcs
 
-extern "C" int tcs_check_reciprocal(int n, double *max_ulp)
+extern "C" int tcs_check_reciprocal(int n, int fp32, double *max_ulp)
 {
     using namespace tcs;
     if (!max_ulp || n < 2) return set_error(TCS_ERR_ARG, "tcs_check_reciprocal: need n >= 2 and a result pointer");
     *max_ulp = -1.0;
     double *d = nullptr;
     if (cudaMalloc(&d, sizeof(double) * (size_t)n) != cudaSuccess) return set_error(TCS_ERR_NOMEM, "tcs_check_reciprocal: allocation");
-    rcp_check_kernel<<<(n + 255) / 256, 256>>>(n, d);
+    if (fp32) rcp_check_kernel<float><<<(n + 255) / 256, 256>>>(n, d);
+    else rcp_check_kernel<double><<<(n + 255) / 256, 256>>>(n, d);
     int rc = record_launch_error("rcp_check") ? TCS_ERR_CUDA : TCS_OK;
     std::vector<double> h(n);
     if (rc == TCS_OK && cudaMemcpy(h.data(), d, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost) != cudaSuccess)

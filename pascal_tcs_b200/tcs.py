@@ -135,7 +135,7 @@ def load() -> ctypes.CDLL:
         "tcs_ensemble_destroy": ([vp], ip),
         "tcs_ensemble_step": ([vp, ip, ctypes.POINTER(ip)], ip),
         "tcs_measure_fp64_peak": ([ip, ctypes.POINTER(ctypes.c_double)], ip),
-        "tcs_check_reciprocal": ([ip, ctypes.POINTER(ctypes.c_double)], ip),
+        "tcs_check_reciprocal": ([ip, ip, ctypes.POINTER(ctypes.c_double)], ip),
         "tcs_ensemble_size": ([vp], ip),
         "tcs_ensemble_set_batched": ([vp, ip], ip),
         "tcs_ensemble_form": ([vp, ctypes.POINTER(ip), ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)], ip),
@@ -411,11 +411,11 @@ def measure_fp64_peak(device: int = 0) -> float:
     return v.value
 
 
-def check_reciprocal(n: int = 1 << 16) -> float:
-    """Largest error (ulps) of the FP64 line solver's reciprocal against the
-    correctly rounded 1/b (tcs_check_reciprocal)."""
+def check_reciprocal(n: int = 1 << 16, fp32: bool = False) -> float:
+    """Largest error (ulps) of the line solver's reciprocal (FP64, or FP32)
+    against the correctly rounded 1/b (tcs_check_reciprocal)."""
     v = ctypes.c_double(0.0)
-    _check(load().tcs_check_reciprocal(int(n), ctypes.byref(v)), "tcs_check_reciprocal")
+    _check(load().tcs_check_reciprocal(int(n), 1 if fp32 else 0, ctypes.byref(v)), "tcs_check_reciprocal")
     return v.value
 
 

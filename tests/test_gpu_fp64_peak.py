@@ -27,3 +27,11 @@ def test_line_solver_reciprocal_within_an_ulp():
     P.load()
     err = P.check_reciprocal(1 << 16)
     assert 0.0 <= err <= 1.0, err
+
+
+def test_fp32_line_solver_reciprocal_within_an_ulp():
+    # the FP32 form's reciprocal (approximate + one Newton-Raphson step)
+    import pascal_tcs_b200 as P
+    P.load()
+    err = P.check_reciprocal(1 << 16, fp32=True)
+    assert 0.0 <= err <= 1.0, err

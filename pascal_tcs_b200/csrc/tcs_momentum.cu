@@ -178,6 +178,7 @@ template <class R, int ITEM = 0>
 struct DUY {
     using Real = R;
     static constexpr int NRHS = 1;
+    static constexpr bool FAST_RCP = std::is_same<R, float>::value;   // measured faster in FP32 only
     static constexpr int MINB = LineOcc<R>::y;
     static constexpr int MREG = LineOcc<Real>::reg_y;
     static constexpr int NT = LineOcc<Real>::nt_y;
@@ -226,6 +227,7 @@ template <class R, int ITEM = 0>
 struct DVZ {
     using Real = R;
     static constexpr int NRHS = 1;
+    static constexpr bool FAST_RCP = std::is_same<R, float>::value;   // measured faster in FP32 only
     static constexpr int MINB = LineOcc<R>::z;
     static constexpr int MREG = LineOcc<Real>::reg_z;
     static constexpr int NT = LineOcc<Real>::nt_z;
@@ -370,6 +372,7 @@ template <class R, int ITEM = 0>
 struct DVY {
     using Real = R;
     static constexpr int NRHS = 1;
+    static constexpr bool FAST_RCP = std::is_same<R, float>::value;   // measured faster in FP32 only
     static constexpr int MINB = LineOcc<R>::y;
     static constexpr int MREG = LineOcc<Real>::reg_y;
     static constexpr int NT = LineOcc<Real>::nt_y;
@@ -412,6 +415,7 @@ template <class R, int ITEM = 0>
 struct DWZ {
     using Real = R;
     static constexpr int NRHS = 1;
+    static constexpr bool FAST_RCP = std::is_same<R, float>::value;   // measured faster in FP32 only
     static constexpr int MINB = LineOcc<R>::z;
     static constexpr int MREG = LineOcc<Real>::reg_z;
     static constexpr int NT = LineOcc<Real>::nt_z;
@@ -569,6 +573,7 @@ template <class R, int ITEM = 0>
 struct DWY {
     using Real = R;
     static constexpr int NRHS = 1;
+    static constexpr bool FAST_RCP = std::is_same<R, float>::value;   // measured faster in FP32 only
     static constexpr int MINB = LineOcc<R>::y;
     static constexpr int MREG = LineOcc<Real>::reg_y;
     static constexpr int NT = LineOcc<Real>::nt_y;

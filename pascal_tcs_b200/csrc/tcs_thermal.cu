@@ -184,6 +184,7 @@ template <class R, int ITEM = 0>
 struct ThermalY {
     using Real = R;
     static constexpr int NRHS = 1;
+    static constexpr bool FAST_RCP = std::is_same<R, float>::value;   // measured faster in FP32 only
     static constexpr int MINB = LineOcc<R>::y;
     static constexpr int MREG = LineOcc<Real>::reg_y;
     static constexpr int NT = LineOcc<Real>::nt_y;

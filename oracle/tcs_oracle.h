@@ -3,7 +3,7 @@
  *
  * CPU restatement (C99, FP64, one rank, OpenMP over independent planes) of the
  * PaScaL_TCS per-timestep path: main.f90:82-223 and every routine it calls on
- * one MPI rank.  It is the checker for the CUDA library in pascal_tcs_b200/:
+ * one MPI rank.  It is the test oracle for the CUDA library in pascal_tcs_b200/:
  * only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg may load
  * it, and never as the product path.
  *

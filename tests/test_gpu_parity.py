@@ -4,7 +4,7 @@ Tolerances (FP64 plain form): every stage <= 1e-10 relative L2 against the
 oracle from identical inputs (typically 1e-14..1e-11; the near-singular
 lowest pressure modes set the upper end); the full 100-step run of the 64^3 constant-
 property case <= 1e-10 relative L2 on u, v, w, T, p and on the Nusselt and
-kinetic-energy series (the bar BASELINE.json sets for the FP64 form); the
+kinetic-energy series (the parity bar of the FP64 form); the
 PaScaL_TDMA interface is bit-exact.
 """
 import numpy as np

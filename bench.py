@@ -281,15 +281,62 @@ def run_reference_ensemble(args, cfg, workload, O, threads) -> int:
     v = cells_steps / el
     sample = (f"{args.steps} steps of each of the first 2 of the {cfg['ensemble']} cases, one at a time, "
               f"restarting from the seeded state every {ENSEMBLE_RESET} steps as the GPU arm does")
-    line = {"impl": "reference", "metric": "cell-steps/s (batched ensemble)", "value": v, "unit": "cell-steps/s",
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    line = {"impl": "reference", "metric": ensemble_metric(cfg), "value": v, "unit": "cell-steps/s",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": None,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (seeded conduction profiles + noise)",
-            "config": {"workload": workload, "cpu_threads": threads},
+            "higher_is_better": True, "scaling": "strong" if ws > 1 else "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic: seeded conduction profiles + uniform noise 0.01, zero velocity",
+            "config": ensemble_config(cfg, workload, ws),
             "cpu_baseline": {"value": v, "unit": "cell-steps/s", "cores": threads, "kind": "port", "sample": sample},
             "e2e": {"value": v, "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
+
+
+def form_name(cfg: dict) -> str:
+    return "FP32-mixed" if cfg.get("precision", 0) else "FP64 plain"
+
+
+def l2_note(field_mb: float, step_mb: float) -> str:
+    """How the timed steps stand against the 126 MB L2 (no flush between steps)."""
+    if field_mb > 126.0:
+        return "inputs larger than L2 (each field %.0f MB)" % field_mb
+    return "each field %.1f MB, but a step streams %.0f MB, more than the 126 MB L2" % (field_mb, step_mb)
+
+
+def single_metric(cfg: dict) -> str:
+    return f"cell-steps/s ({form_name(cfg)}, one {cfg['n1m']}x{cfg['n2m']}x{cfg['n3m']} case per GPU)"
+
+
+def single_config(cfg: dict, workload: str, ws: int) -> dict:
+    """The workload a one-case line describes (the same dict in both arms)."""
+    n1, n2, n3 = cfg["n1m"], cfg["n2m"], cfg["n3m"]
+    esize = 4 if cfg.get("precision", 0) else 8
+    return {"workload": workload, "grid": [n1, n2, n3],
+            "properties": "water" if cfg["property_set"] == 1 else "constant",
+            "Ra": cfg["Ra"], "Pr": cfg["Pr"], "dt": cfg["dtStart"], "precision": form_name(cfg),
+            "parallelism": "replicas" if ws > 1 else "single",
+            "l2": l2_note(esize * (n1 + 2) * (n2 + 2) * (n3 + 2) / 1e6, step_bytes_per_cell(esize) * n1 * n2 * n3 / 1e6),
+            "timing": "eager launches with one event-probed kernel; CUDA events on the solver stream",
+            "restart_every_steps": RESET_EVERY.get(workload, 0) or None}
+
+
+def ensemble_metric(cfg: dict) -> str:
+    return f"cell-steps/s ({form_name(cfg)}, ensemble of {cfg['ensemble']} cases)"
+
+
+def ensemble_config(cfg: dict, workload: str, ws: int) -> dict:
+    """The workload an ensemble line describes (the same dict in both arms)."""
+    allcases = ensemble_cases(cfg["ensemble"], cfg["precision"])
+    total_cells = sum(c["n1m"] * c["n2m"] * c["n3m"] for c in allcases)
+    esize = 4 if cfg["precision"] else 8
+    return {"workload": workload, "cases": len(allcases), "cases_on_rank0": len(lpt_shard(allcases, ws, 0)),
+            "grids": "each axis from {64,96,128,160,192}, seed 2026", "Ra": "log-uniform 1e5..1e7",
+            "Pr": "7 (water) or 0.71 (constant)", "dt": 2e-4, "precision": form_name(cfg),
+            "parallelism": f"LPT bin-packing of cases over {ws} GPU(s)" if ws > 1 else "single",
+            "l2": "working set of %.1f GB, larger than L2" % (total_cells * esize * 24 / 1e9 / ws),
+            "timing": "one CUDA graph per ensemble step, in the form the auto selection keeps; CUDA events around the region",
+            "restart_every_steps": ENSEMBLE_RESET}
 
 
 def oracle_steps(fresh, k: int, reset: int, warmup: int = 0) -> float:
@@ -327,12 +374,11 @@ def run_reference(args, cfg, workload):
     el = oracle_steps(fresh, args.steps, reset, warmup=args.warmup)
     cells = cfg["n1m"] * cfg["n2m"] * cfg["n3m"]
     v = cells * args.steps / el
-    line = {"impl": "reference", "metric": "cell-steps/s (FP64 plain, one case per process)", "value": v,
+    line = {"impl": "reference", "metric": single_metric(cfg), "value": v,
             "unit": "cell-steps/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded conduction profile + noise)",
-            "config": {"workload": workload, **{k: cfg[k] for k in ("n1m", "n2m", "n3m", "Ra", "Pr", "dtStart")},
-                       "properties": "water", "cpu_threads": threads},
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic: seeded conduction profile + uniform noise 0.01, zero velocity",
+            "config": single_config(cfg, workload, ws),
             "cpu_baseline": {"value": v, "unit": "cell-steps/s", "cores": threads, "kind": "port",
                              "sample": f"{args.steps} full time steps after {args.warmup} warm-up steps"
                                        + (f", restarting from the seeded state every {reset} steps as the GPU arm does"
@@ -553,18 +599,12 @@ def run_ensemble(args, cfg: dict, workload: str) -> int:
     achieved = step_bytes * args.steps / (ms * 1e-3) / 1e9
     if rank == 0:
         form = "FP32-mixed" if cfg["precision"] else "FP64 plain"
-        line = {"metric": f"cell-steps/s ({form}, ensemble of {len(allcases)} cases)", "value": value,
+        line = {"metric": ensemble_metric(cfg), "value": value,
                 "unit": "cell-steps/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "strong" if ws > 1 else "weak",
                 "vs_baseline": None, "dtype": "f32+f64" if cfg["precision"] else "f64",
                 "data": "synthetic: seeded conduction profiles + uniform noise 0.01, zero velocity",
-                "config": {"workload": workload, "cases": len(allcases), "cases_on_rank0": len(cases),
-                           "grids": "each axis from {64,96,128,160,192}, seed 2026", "Ra": "log-uniform 1e5..1e7",
-                           "Pr": "7 (water) or 0.71 (constant)", "dt": 2e-4, "precision": form,
-                           "parallelism": f"LPT bin-packing of cases over {ws} GPU(s)" if ws > 1 else "single",
-                           "l2": "working set of %.1f GB, larger than L2" % (total_cells * esize * 24 / 1e9 / ws),
-                           "timing": "one CUDA graph per ensemble step, in the form the auto selection keeps; CUDA events around the region",
-                           "restart_every_steps": reset},
+                "config": ensemble_config(cfg, workload, ws),
                 "gpu_launches": launches,
                 "roofline": {"bound": "hbm", "kernel": "whole ensemble step", "achieved": achieved, "peak": peak,
                              "unit": "GB/s", "frac": achieved / peak,
@@ -668,18 +708,12 @@ def main():
 
     if rank == 0:
         form = "FP32-mixed" if fp32 else "FP64 plain"
-        line = {"metric": f"cell-steps/s ({form}, one {n1}x{n2}x{n3} case per GPU)", "value": m["value"],
+        line = {"metric": single_metric(cfg), "value": m["value"],
                 "unit": "cell-steps/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": m["ms_per_step"], "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32+f64" if fp32 else "f64",
                 "data": "synthetic: seeded conduction profile + uniform noise 0.01, zero velocity",
-                "config": {"workload": workload, "grid": [n1, n2, n3],
-                           "properties": "water" if cfg["property_set"] == 1 else "constant",
-                           "Ra": cfg["Ra"], "Pr": cfg["Pr"], "dt": cfg["dtStart"], "precision": form,
-                           "parallelism": "replicas" if ws > 1 else "single",
-                           "l2": "inputs larger than L2 (each field %.0f MB)" % ((4 if fp32 else 8) * np.prod(s.shape) / 1e6),
-                           "timing": "eager launches with one event-probed kernel; CUDA events on the solver stream",
-                           "restart_every_steps": reset or None},
+                "config": single_config(cfg, workload, ws),
                 "gpu_launches": m["launches"], "roofline": m["roofline"], "whole_step": m["whole_step"],
                 "kernel_ms_one_step": m["kernel_ms_one_step"], "tuning": m["tuning"], "clocks": m["clocks"], "e2e": e2e,
                 "fp32_mixed": mixed, "cpu_baseline": base}

@@ -707,7 +707,6 @@ def main():
         base.pop("seconds", None)
 
     if rank == 0:
-        form = "FP32-mixed" if fp32 else "FP64 plain"
         line = {"metric": single_metric(cfg), "value": m["value"],
                 "unit": "cell-steps/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": m["ms_per_step"], "higher_is_better": True, "scaling": "weak",

@@ -800,9 +800,14 @@ __device__ __forceinline__ void line_block(const Prob &prob, const LinePlan &lp)
             // two row-adjacent cells per thread: their loads are in flight together and
             // the loads their stencils share are issued once (measured on the FP64 z
             // sweeps: dw_z -8%, thermal_z -3%; slower on the y sweeps and in FP32)
-            const int nh = (n + 1) >> 1;
-            for (int t = threadIdx.x; t < TL * nh; t += blockDim.x) {
-                const int l = t & (TL - 1), r = (t >> lgTL) << 1;
+            // Pair t = threadIdx.x + m NT of the block's TL x nh pairs is (line t mod TL,
+            // pair t / TL); NT is a multiple of TL, so a thread keeps one line and steps
+            // its pairs by NT / TL: the same cells in the same order, with less index
+            // arithmetic per cell (dw_z -3%, dv_z -2%; the same form of the unpaired
+            // loop below measured slower on the y sweeps).
+            const int nh = (n + 1) >> 1, l = threadIdx.x & (TL - 1), hstep = Prob::NT >> lgTL;
+            for (int h = threadIdx.x >> lgTL; h < nh; h += hstep) {
+                const int r = h << 1;
                 if (r + 1 < n) {   // both cells in one block, so their loads can be merged and interleaved
                     put(l, r);
                     put(l, r + 1);
@@ -859,6 +864,10 @@ __device__ __forceinline__ void line_block(const Prob &prob, const LinePlan &lp)
     if (Prob::CONTIG) {
         for (int l = 0; l < TL; l++)
             for (int r = threadIdx.x; r < n; r += blockDim.x) out(l, r);
+    } else if constexpr (PairRows<Prob>::on) {
+        // one line per thread, as in the paired build
+        const int l = threadIdx.x & (TL - 1);
+        for (int r = threadIdx.x >> lgTL; r < n; r += Prob::NT >> lgTL) out(l, r);
     } else {
         for (int t = threadIdx.x; t < TL * n; t += blockDim.x) out(t & (TL - 1), t >> lgTL);
     }

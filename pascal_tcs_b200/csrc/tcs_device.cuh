@@ -741,6 +741,15 @@ struct PairRows { static constexpr bool on = false; };
 template <class P>
 struct PairRows<P, std::void_t<decltype(P::PAIR)>> { static constexpr bool on = P::PAIR; };
 
+// Unpaired strided builds that keep one line per thread and step its rows by
+// NT / TL (Prob::LINE_PER_THREAD; default: FP32 rows).  Measured at 256^3: the
+// FP32 sweeps and the modal solves faster (modal -3% in FP64, -10% in FP32;
+// FP32 thermal_y -4%), the FP64 y sweeps and the FP32 dw_z slower (+4-8%, +3%).
+template <class P, class = void>
+struct LinePerThread { static constexpr bool on = std::is_same<typename P::Real, float>::value; };
+template <class P>
+struct LinePerThread<P, std::void_t<decltype(P::LINE_PER_THREAD)>> { static constexpr bool on = P::LINE_PER_THREAD; };
+
 template <class Prob>
 __device__ __forceinline__ void line_block(const Prob &prob, const LinePlan &lp)
 {
@@ -799,12 +808,11 @@ __device__ __forceinline__ void line_block(const Prob &prob, const LinePlan &lp)
         if constexpr (PairRows<Prob>::on) {
             // two row-adjacent cells per thread: their loads are in flight together and
             // the loads their stencils share are issued once (measured on the FP64 z
-            // sweeps: dw_z -8%, thermal_z -3%; slower on the y sweeps and in FP32)
+            // sweeps: dw_z -8%, thermal_z -3%; slower on the y sweeps and in FP32).
             // Pair t = threadIdx.x + m NT of the block's TL x nh pairs is (line t mod TL,
             // pair t / TL); NT is a multiple of TL, so a thread keeps one line and steps
             // its pairs by NT / TL: the same cells in the same order, with less index
-            // arithmetic per cell (dw_z -3%, dv_z -2%; the same form of the unpaired
-            // loop below measured slower on the y sweeps).
+            // arithmetic per cell (dw_z -2%, dv_z -1%).
             const int nh = (n + 1) >> 1, l = threadIdx.x & (TL - 1), hstep = Prob::NT >> lgTL;
             for (int h = threadIdx.x >> lgTL; h < nh; h += hstep) {
                 const int r = h << 1;
@@ -815,6 +823,11 @@ __device__ __forceinline__ void line_block(const Prob &prob, const LinePlan &lp)
                     put(l, r);
                 }
             }
+        } else if constexpr (LinePerThread<Prob>::on) {
+            // the same cells and order as below, one line per thread
+            const int l = threadIdx.x & (TL - 1), rstep = Prob::NT >> lgTL;
+#pragma unroll 2
+            for (int r = threadIdx.x >> lgTL; r < n; r += rstep) put(l, r);
         } else {
             // two cells per pass: their loads are in flight together (measured 3-7% on the FP64 z and y sweeps)
 #pragma unroll 2
@@ -864,8 +877,8 @@ __device__ __forceinline__ void line_block(const Prob &prob, const LinePlan &lp)
     if (Prob::CONTIG) {
         for (int l = 0; l < TL; l++)
             for (int r = threadIdx.x; r < n; r += blockDim.x) out(l, r);
-    } else if constexpr (PairRows<Prob>::on) {
-        // one line per thread, as in the paired build
+    } else if constexpr (PairRows<Prob>::on || LinePerThread<Prob>::on) {
+        // one line per thread, as in the build
         const int l = threadIdx.x & (TL - 1);
         for (int r = threadIdx.x >> lgTL; r < n; r += Prob::NT >> lgTL) out(l, r);
     } else {

@@ -421,6 +421,7 @@ struct DWZ {
     static constexpr int NT = LineOcc<Real>::nt_z;
     static constexpr bool CONTIG = false;
     static constexpr bool PAIR = LineOcc<Real>::pair_z;
+    static constexpr bool LINE_PER_THREAD = false;   // the unpaired FP32 build: measured slower
     GridT<R> g; FieldsT<R> f; int TL;
     __device__ bool skip() const { return blown(g); }
     struct State { R dt; };

@@ -222,7 +222,7 @@ struct LinePlan {
     int P;       // partitions (lanes) per line, <= 32; power of two when cyclic
     int m0, rem; // partition p has m0 + (p < rem) rows
     int PS;      // shared-memory stride between partitions (odd)
-    int LS;      // shared-memory stride between lines (odd)
+    int LS;      // shared-memory stride between lines (odd, or set per problem by plan_for)
     int TL;      // lines per block
     int cyclic;
 };

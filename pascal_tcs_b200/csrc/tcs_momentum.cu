@@ -620,8 +620,8 @@ template <class R>
 void launch_solve_du(const Ctx<R> &cx, cudaStream_t s)
 {
     const GridT<R> &g = cx.g;
-    LinePlan pz = make_line_plan(g.N3, true, fit_tl<DUZ<R>>(g.N3, true, cx.tl_strided, cx.lanes), cx.lanes);
-    LinePlan py = make_line_plan(g.N2, false, fit_tl<DUY<R>>(g.N2, false, cx.tl_strided, cx.lanes), cx.lanes);
+    LinePlan pz = plan_for<DUZ<R>>(g.N3, true, fit_tl<DUZ<R>>(g.N3, true, cx.tl_strided, cx.lanes), cx.lanes);
+    LinePlan py = plan_for<DUY<R>>(g.N2, false, fit_tl<DUY<R>>(g.N2, false, cx.tl_strided, cx.lanes), cx.lanes);
     launch_lines(DUZ<R>{g, cx.f, pz.TL}, pz, dim3((g.N1 + pz.TL - 1) / pz.TL, g.N2), s, K_DU_Z, cx);
     launch_x<DUX>(cx, g.N2, s, K_DU_X);
     launch_lines(DUY<R>{g, cx.f, py.TL}, py, dim3((g.N1 + py.TL - 1) / py.TL, g.N3), s, K_DU_Y, cx);
@@ -631,8 +631,8 @@ template <class R>
 void launch_solve_dv(const Ctx<R> &cx, cudaStream_t s)
 {
     const GridT<R> &g = cx.g;
-    LinePlan pz = make_line_plan(g.N3, true, fit_tl<DVZ<R>>(g.N3, true, cx.tl_strided, cx.lanes), cx.lanes);
-    LinePlan py = make_line_plan(g.N2 - 1, false, fit_tl<DVY<R>>(g.N2 - 1, false, cx.tl_strided, cx.lanes), cx.lanes);
+    LinePlan pz = plan_for<DVZ<R>>(g.N3, true, fit_tl<DVZ<R>>(g.N3, true, cx.tl_strided, cx.lanes), cx.lanes);
+    LinePlan py = plan_for<DVY<R>>(g.N2 - 1, false, fit_tl<DVY<R>>(g.N2 - 1, false, cx.tl_strided, cx.lanes), cx.lanes);
     launch_lines(DVZ<R>{g, cx.f, pz.TL}, pz, dim3((g.N1 + pz.TL - 1) / pz.TL, g.N2 - 1), s, K_DV_Z, cx);
     launch_x<DVX>(cx, g.N2 - 1, s, K_DV_X);
     launch_lines(DVY<R>{g, cx.f, py.TL}, py, dim3((g.N1 + py.TL - 1) / py.TL, g.N3), s, K_DV_Y, cx);
@@ -642,8 +642,8 @@ template <class R>
 void launch_solve_dw(const Ctx<R> &cx, cudaStream_t s)
 {
     const GridT<R> &g = cx.g;
-    LinePlan pz = make_line_plan(g.N3, true, fit_tl<DWZ<R>>(g.N3, true, cx.tl_strided, cx.lanes), cx.lanes);
-    LinePlan py = make_line_plan(g.N2, false, fit_tl<DWY<R>>(g.N2, false, cx.tl_strided, cx.lanes), cx.lanes);
+    LinePlan pz = plan_for<DWZ<R>>(g.N3, true, fit_tl<DWZ<R>>(g.N3, true, cx.tl_strided, cx.lanes), cx.lanes);
+    LinePlan py = plan_for<DWY<R>>(g.N2, false, fit_tl<DWY<R>>(g.N2, false, cx.tl_strided, cx.lanes), cx.lanes);
     launch_lines(DWZ<R>{g, cx.f, pz.TL}, pz, dim3((g.N1 + pz.TL - 1) / pz.TL, g.N2), s, K_DW_Z, cx);
     launch_x<DWX>(cx, g.N2, s, K_DW_X);
     launch_lines(DWY<R>{g, cx.f, py.TL}, py, dim3((g.N1 + py.TL - 1) / py.TL, g.N3), s, K_DW_Y, cx);

@@ -527,7 +527,7 @@ template <class R>
 void launch_modal(const Ctx<R> &cx, cudaStream_t s)
 {
     const GridT<R> &g = cx.g;
-    LinePlan pm = make_line_plan(g.N2, false, fit_tl<Modal<R>>(g.N2, false, cx.tl_modal, cx.lanes), cx.lanes);
+    LinePlan pm = plan_for<Modal<R>>(g.N2, false, fit_tl<Modal<R>>(g.N2, false, cx.tl_modal, cx.lanes), cx.lanes);
     launch_lines(Modal<R>{g, cx.f, pm.TL, cx.h1p}, pm, dim3((cx.h1p + pm.TL - 1) / pm.TL, g.N3), s, K_MODAL, cx);
 }
 

@@ -246,8 +246,8 @@ template <class R>
 void launch_thermal(const Ctx<R> &cx, cudaStream_t s)
 {
     const GridT<R> &g = cx.g;
-    LinePlan pz = make_line_plan(g.N3, true, fit_tl<ThermalZ<R>>(g.N3, true, cx.tl_strided, cx.lanes), cx.lanes);
-    LinePlan py = make_line_plan(g.N2, false, fit_tl<ThermalY<R>>(g.N2, false, cx.tl_strided, cx.lanes), cx.lanes);
+    LinePlan pz = plan_for<ThermalZ<R>>(g.N3, true, fit_tl<ThermalZ<R>>(g.N3, true, cx.tl_strided, cx.lanes), cx.lanes);
+    LinePlan py = plan_for<ThermalY<R>>(g.N2, false, fit_tl<ThermalY<R>>(g.N2, false, cx.tl_strided, cx.lanes), cx.lanes);
     ThermalZ<R> z{g, cx.f, pz.TL};
     launch_lines(z, pz, dim3((g.N1 + pz.TL - 1) / pz.TL, g.N2), s, K_THERMAL_Z, cx);
     launch_x<ThermalX>(cx, g.N2, s, K_THERMAL_X);

@@ -71,9 +71,12 @@ inline size_t line_smem(const LinePlan &lp)
 // four-byte words (FP32 rows) or 16 eight-byte words per half-warp (FP64
 // rows), puts those accesses on distinct banks.  The solve (one line per
 // warp) only uses the odd partition stride PS.  Measured at 256^3: the y
-// sweeps 2-5% and the modal solves 3-4% faster in both forms; the unpaired
-// cyclic (FP32 z) sweeps 11-43% slower with it, so they keep the odd LS, as
-// do the paired builds, which step rows by 2 (no LS avoids 2-way conflicts).
+// sweeps 2-5% and the modal solves 3-4% faster in both forms.  The unpaired
+// cyclic (FP32 z) sweeps keep the odd LS: the longer stride takes three of
+// their blocks past the 196 KB shared-memory configuration into the 228 KB
+// one, whose 28 KB of L1 (against 60 KB) cost their stencil loads 11-43%.
+// The paired builds step rows by 2, where no LS avoids 2-way conflicts; they
+// keep the odd LS too.
 template <class Prob>
 inline LinePlan plan_for(int n, bool cyclic, int tl, int pmax)
 {

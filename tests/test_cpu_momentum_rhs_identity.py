@@ -1,4 +1,6 @@
-"""The U-momentum z sweep evaluates the right-hand side of
+"""The momentum z sweeps evaluate their right-hand sides in a reduced form,
+checked here for U and W (the W form adds the dU and dV cross terms).  The
+U-momentum z sweep evaluates the right-hand side of
 module_solve_momentum.f90:281-420 (stage 1 of mpi_momentum_solvedU) in a
 reduced form: the explicit operator minus the three implicit operators
 applied to U collapses in x and z (and in y away from the walls) to
@@ -108,3 +110,88 @@ def test_identity_needs_the_row_wise_viscosity():
     ih = 0.5 * Cmu * (0.5 * (dx1m * iRjk + dx1 * iRjk) / dmx1)
     delta = ih * 2.0 * 0.3 * (Uc - Uxm) / dx1m / dmx1
     assert abs((full + delta) - red) / scale > 1e-6
+
+
+def forms_w(v, jwm, jwp):
+    """solvedW stage 1 (module_solve_momentum.f90:988-1130, as the oracle
+    restates it) against the reduced form of the W-momentum z sweep (DWZ in
+    csrc/tcs_momentum.cu), with the dU and dV cross terms of the reference."""
+    (dx1m, dx1, dx1p, dmx1, dmx1p, dx2m, dx2, dx2p, dmx2, dmx2p, dx3m, dx3, dmx3,
+     Wc, Wxm, Wxp, Wym, Wyp, Wzm, Wzp, Uc, Uzm, Uxp, Uxpzm, Vc, Vzm, Vyp, Vypzm,
+     dUc, dUzm, dUxp, dUxpzm, dVc, dVzm, dVyp, dVypzm, Pc, Pzm,
+     Mjk, Mjkm, Mjmk, Mjmkm, Mjpk, Mjpkm, iRjk, iRjkm, Cmu, Cmp, Vbt, Vup, Wbt, Wup) = v
+    w5, w6 = 0.5 * (Wc + Wzm), 0.5 * (Wc + Wzp)
+    u1 = (dx3m * Uc + dx3 * Uzm) / dmx3 * 0.5
+    u2 = (dx3m * Uxp + dx3 * Uxpzm) / dmx3 * 0.5
+    v3 = (dx3m * Vc + dx3 * Vzm) / dmx3 * 0.5
+    v4 = (dx3m * Vyp + dx3 * Vypzm) / dmx3 * 0.5
+    dwdx1, dwdx2 = (Wc - Wxm) / dmx1, (Wxp - Wc) / dmx1p
+    dwdy3, dwdy4 = (Wc - Wym) / dmx2, (Wyp - Wc) / dmx2p
+    dwdz5, dwdz6 = (Wc - Wzm) / dx3m, (Wzp - Wc) / dx3
+    dudz1, dudz2 = (Uc - Uzm) / dmx3, (Uxp - Uxpzm) / dmx3
+    dvdz3, dvdz4 = (Vc - Vzm) / dmx3, (Vyp - Vypzm) / dmx3
+    ddudz1, ddudz2 = (dUc - dUzm) / dmx3, (dUxp - dUxpzm) / dmx3
+    ddvdz3, ddvdz4 = (dVc - dVzm) / dmx3, (dVyp - dVypzm) / dmx3
+    ddu1 = (dx3m * dUc + dx3 * dUzm) / dmx3 * 0.5
+    ddu2 = (dx3m * dUxp + dx3 * dUxpzm) / dmx3 * 0.5
+    ddv3 = (dx3m * dVc + dx3 * dVzm) / dmx3 * 0.5 * jwm
+    ddv4 = (dx3m * dVyp + dx3 * dVypzm) / dmx3 * 0.5 * jwp
+    # Mu constant along i (row-wise): Mu(im) = Mu(i) = Mu(ip)
+    mxz = 0.5 * (dx3m * Mjk + dx3 * Mjkm) / dmx3
+    mu1 = 0.5 * (dx1m * mxz + dx1 * mxz) / dmx1
+    mu2 = 0.5 * (dx1p * mxz + dx1 * mxz) / dmx1p
+    mua = 0.5 * (dx3m * Mjmk + dx3 * Mjmkm) / dmx3
+    mub = 0.5 * (dx3m * Mjpk + dx3 * Mjpkm) / dmx3
+    mu3 = 0.5 * (dx2m * mxz + dx2 * mua) / dmx2
+    mu4 = 0.5 * (dx2p * mxz + dx2 * mub) / dmx2p
+    invRhoc = 0.5 * (dx3m * iRjk + dx3 * iRjkm) / dmx3
+    ih = 0.5 * Cmu * invRhoc
+    vw1 = (mu2 * dwdx2 - mu1 * dwdx1) / dx1
+    vw2 = (mu4 * dwdy4 - mu3 * dwdy3) / dx2
+    vw3 = (Mjk * dwdz6 - Mjkm * dwdz5) / dmx3
+    vw31 = (mu2 * dudz2 - mu1 * dudz1) / dx1
+    vw32 = (mu4 * dvdz4 - mu3 * dvdz3) / dx2
+    press = -Cmp * invRhoc * (Pc - Pzm) / dmx3
+    zbc_dn = 0.25 * v3 / dmx2 * Wbt - 0.25 * dwdy3 * (dx3m * Vbt + dx3 * Vbt) / dmx3 * 0.5
+    zbc_up = -0.25 * v4 / dmx2p * Wup - 0.25 * dwdy4 * (dx3m * Vup + dx3 * Vup) / dmx3 * 0.5
+    zbc_dn = zbc_dn + ih / dx2 * mu3 / dmx2p * Wbt - ih / dx2 * mu3 / dmx3 * (Vbt - Vbt)
+    zbc_up = zbc_up + ih / dx2 * mu4 / dmx2 * Wup + ih / dx2 * mu4 / dmx3 * (Vup - Vup)
+    mACI = ih / dx1 * (mu2 / dmx1p + mu1 / dmx1) + 0.25 * (-u2 / dmx1p + u1 / dmx1)
+    mAPI = -ih / dx1 * mu2 / dmx1p + 0.25 * (u2 / dmx1p)
+    mAMI = -ih / dx1 * mu1 / dmx1 + 0.25 * (-u1 / dmx1)
+    mACJ = ih / dx2 * (mu4 / dmx2p + mu3 / dmx2) + 0.25 * (-v4 / dmx2p + v3 / dmx2)
+    mAPJ = (-ih / dx2 * mu4 / dmx2p + 0.25 * (v4 / dmx2p)) * jwp
+    mAMJ = (-ih / dx2 * mu3 / dmx2 + 0.25 * (-v3 / dmx2)) * jwm
+    mACK = ih / dmx3 * (Mjk / dx3 + Mjkm / dx3m) * 2.0 + 0.25 * (-w6 / dx3 + w5 / dx3m + 0.5 * dwdz6 + 0.5 * dwdz5)
+    mAPK = -ih / dmx3 * Mjk / dx3 * 2.0 + 0.25 * (w6 / dx3 + 0.5 * dwdz6)
+    mAMK = -ih / dmx3 * Mjkm / dx3m * 2.0 + 0.25 * (-w5 / dx3m + 0.5 * dwdz5)
+    full = ih * (vw1 + vw2 + 2.0 * vw3 + vw31 + vw32) + press + (1.0 - jwm) * zbc_dn + (1.0 - jwp) * zbc_up
+    full = full - (mAPI * Wxp + mACI * Wc + mAMI * Wxm + mAPJ * Wyp + mACJ * Wc + mAMJ * Wym
+                   + mAPK * Wzp + mACK * Wc + mAMK * Wzm)
+    full = full - (0.25 * (u2 * dwdx2 + u1 * dwdx1) - ih / dx1 * (mu2 * dudz2 - mu1 * dudz1))
+    full = full - (0.25 * (v3 * jwm * dwdy3 + v4 * jwp * dwdy4) - ih / dx2 * (mu4 * dvdz4 * jwp - mu3 * dvdz3 * jwm))
+    full = full - (0.25 * (ddu2 * dwdx2 + ddu1 * dwdx1) - ih / dx1 * (mu2 * ddudz2 - mu1 * ddudz1))
+    full = full - (0.25 * (ddv3 * jwm * dwdy3 + ddv4 * jwp * dwdy4) - ih / dx2 * (mu4 * ddvdz4 * jwp - mu3 * ddvdz3 * jwm))
+    red = (2.0 * ih * (vw1 + vw31) + 4.0 * ih * vw3 - 0.5 * (u1 * dwdx1 + u2 * dwdx2) - 0.5 * (w5 * dwdz5 + w6 * dwdz6)
+           - 0.25 * (ddu1 * dwdx1 + ddu2 * dwdx2) + ih / dx1 * (mu2 * ddudz2 - mu1 * ddudz1) + press)
+    if jwm == 1.0 and jwp == 1.0:
+        red = (red + 2.0 * ih * (vw2 + vw32) - 0.5 * (v3 * dwdy3 + v4 * dwdy4)
+               - 0.25 * (ddv3 * dwdy3 + ddv4 * dwdy4) + ih / dx2 * (mu4 * ddvdz4 - mu3 * ddvdz3))
+    else:
+        red = (red + ih * (vw2 + vw32) + (1.0 - jwm) * zbc_dn + (1.0 - jwp) * zbc_up - (mAPJ * Wyp + mACJ * Wc + mAMJ * Wym)
+               - (0.25 * (v3 * jwm * dwdy3 + v4 * jwp * dwdy4) - ih / dx2 * (mu4 * dvdz4 * jwp - mu3 * dvdz3 * jwm))
+               - (0.25 * (ddv3 * jwm * dwdy3 + ddv4 * jwp * dwdy4) - ih / dx2 * (mu4 * ddvdz4 * jwp - mu3 * ddvdz3 * jwm)))
+    scale = sum(abs(t) for t in (mAPI * Wxp, mACI * Wc, mAPK * Wzp, mACK * Wc, mACJ * Wc, ih * vw1, ih * vw3, press))
+    return full, red, scale
+
+
+def test_reduced_w_momentum_rhs_matches_reference_expression():
+    rng = np.random.default_rng(23)
+    worst = 0.0
+    for _ in range(500):
+        v = np.concatenate([rng.uniform(0.5, 2.0, 13), rng.uniform(-1.0, 1.0, 25), rng.uniform(0.5, 2.0, 8),
+                            rng.uniform(0.5, 2.0, 2), rng.uniform(-1.0, 1.0, 4)])
+        for jwm, jwp in ((1.0, 1.0), (0.0, 1.0), (1.0, 0.0)):
+            full, red, scale = forms_w(v, jwm, jwp)
+            worst = max(worst, abs(full - red) / scale)
+    assert worst < 1e-13, worst

@@ -1,5 +1,5 @@
 """The momentum z sweeps evaluate their right-hand sides in a reduced form,
-checked here for U and W (the W form adds the dU and dV cross terms).  The
+checked here for U, V and W (the V and W forms add the dU and dV cross terms).  The
 U-momentum z sweep evaluates the right-hand side of
 module_solve_momentum.f90:281-420 (stage 1 of mpi_momentum_solvedU) in a
 reduced form: the explicit operator minus the three implicit operators
@@ -193,5 +193,82 @@ def test_reduced_w_momentum_rhs_matches_reference_expression():
                             rng.uniform(0.5, 2.0, 2), rng.uniform(-1.0, 1.0, 4)])
         for jwm, jwp in ((1.0, 1.0), (0.0, 1.0), (1.0, 0.0)):
             full, red, scale = forms_w(v, jwm, jwp)
+            worst = max(worst, abs(full - red) / scale)
+    assert worst < 1e-13, worst
+
+
+def forms_v(v, jvm, jvp):
+    """solvedV stage 1 (module_solve_momentum.f90:626-780, as the oracle
+    restates it) against the reduced form of the V-momentum z sweep (DVZ in
+    csrc/tcs_momentum.cu), with the reference's dU cross terms; jvm, jvp are
+    jS_BC(j+1) and jS_BC(j-1)."""
+    (dx1m, dx1, dx1p, dmx1, dmx1p, dx2m, dx2, dmx2, dx3m, dx3, dx3p, dmx3, dmx3p,
+     Vc, Vym, Vyp, Vxm, Vxp, Vzm, Vzp, Uc, Uym, Uxp, Uxpym, Wc, Wym, Wzp, Wzpym,
+     dUc, dUym, dUxp, dUxpym, Pc, Pym,
+     Mjk, Mjmk, Mjkm, Mjmkm, Mjkp, Mjmkp, iRjk, iRjmk, Cmu, Cmp, Vbt, Vup) = v
+    v3, v4 = 0.5 * (Vym + Vc), 0.5 * (Vc + Vyp)
+    u1 = (dx2m * Uc + dx2 * Uym) / dmx2 * 0.5
+    u2 = (dx2m * Uxp + dx2 * Uxpym) / dmx2 * 0.5
+    w5 = (dx2m * Wc + dx2 * Wym) / dmx2 * 0.5
+    w6 = (dx2m * Wzp + dx2 * Wzpym) / dmx2 * 0.5
+    ddu1 = (dx2m * dUc + dx2 * dUym) / dmx2 * 0.5
+    ddu2 = (dx2m * dUxp + dx2 * dUxpym) / dmx2 * 0.5
+    dvdx1, dvdx2 = (Vc - Vxm) / dmx1, (Vxp - Vc) / dmx1p
+    dvdy3, dvdy4 = (Vc - Vym) / dx2m, (Vyp - Vc) / dx2
+    dvdz5, dvdz6 = (Vc - Vzm) / dmx3, (Vzp - Vc) / dmx3p
+    dudy1, dudy2 = (Uc - Uym) / dmx2, (Uxp - Uxpym) / dmx2
+    dwdy5, dwdy6 = (Wc - Wym) / dmx2, (Wzp - Wzpym) / dmx2
+    ddudy1, ddudy2 = (dUc - dUym) / dmx2, (dUxp - dUxpym) / dmx2
+    # Mu constant along i (row-wise): the three x-neighbour averages coincide
+    mxy = 0.5 * (dx2m * Mjk + dx2 * Mjmk) / dmx2
+    mu1 = 0.5 * (dx1m * mxy + dx1 * mxy) / dmx1
+    mu2 = 0.5 * (dx1p * mxy + dx1 * mxy) / dmx1p
+    mua = 0.5 * (dx2m * Mjkm + dx2 * Mjmkm) / dmx2
+    mub = 0.5 * (dx2m * Mjkp + dx2 * Mjmkp) / dmx2
+    mu5 = 0.5 * (dx3m * mxy + dx3 * mua) / dmx3
+    mu6 = 0.5 * (dx3p * mxy + dx3 * mub) / dmx3p
+    invRhoc = 0.5 * (dx2m * iRjk + dx2 * iRjmk) / dmx2
+    ih = 0.5 * Cmu * invRhoc
+    vv1 = (mu2 * dvdx2 - mu1 * dvdx1) / dx1
+    vv2 = (Mjk * dvdy4 - Mjmk * dvdy3) / dmx2
+    vv3 = (mu6 * dvdz6 - mu5 * dvdz5) / dx3
+    vv21 = (mu2 * dudy2 - mu1 * dudy1) / dx1
+    vv23 = (mu6 * dwdy6 - mu5 * dwdy5) / dx3
+    press = -Cmp * invRhoc * (Pc - Pym) / dmx2
+    vbc_dn = 0.25 / dx2m * v3 * Vbt - 0.25 * 0.5 * dvdy3 * Vbt + ih / dmx2 * Mjmk / dx2m * Vbt * 2.0
+    vbc_up = -0.25 / dx2 * v4 * Vup - 0.25 * 0.5 * dvdy4 * Vup + ih / dmx2 * Mjk / dx2 * Vup * 2.0
+    mACI = ih / dx1 * (mu2 / dmx1p + mu1 / dmx1) + 0.25 * (-u2 / dmx1p + u1 / dmx1)
+    mAPI = -ih / dx1 * mu2 / dmx1p + 0.25 * (u2 / dmx1p)
+    mAMI = -ih / dx1 * mu1 / dmx1 + 0.25 * (-u1 / dmx1)
+    mACJ = ih / dmx2 * (Mjk / dx2 + Mjmk / dx2m) * 2.0 + 0.25 * (dvdy4 * 0.5 + dvdy3 * 0.5 - v4 / dx2 + v3 / dx2m)
+    mAPJ = (-ih / dmx2 * Mjk / dx2 * 2.0 + 0.25 * (v4 / dx2 + dvdy4 * 0.5)) * jvp
+    mAMJ = (-ih / dmx2 * Mjmk / dx2m * 2.0 + 0.25 * (-v3 / dx2m + dvdy3 * 0.5)) * jvm
+    mACK = ih / dx3 * (mu6 / dmx3p + mu5 / dmx3) + 0.25 * (-w6 / dmx3p + w5 / dmx3)
+    mAPK = -ih / dx3 * mu6 / dmx3p + 0.25 * (w6 / dmx3p)
+    mAMK = -ih / dx3 * mu5 / dmx3 + 0.25 * (-w5 / dmx3)
+    full = ih * (vv1 + 2.0 * vv2 + vv3 + vv21 + vv23) + press + (1.0 - jvm) * vbc_dn + (1.0 - jvp) * vbc_up
+    full = full - (mAPI * Vxp + mACI * Vc + mAMI * Vxm + mAPJ * Vyp + mACJ * Vc + mAMJ * Vym
+                   + mAPK * Vzp + mACK * Vc + mAMK * Vzm)
+    full = full - (0.25 * (u2 * dvdx2 + u1 * dvdx1) - ih / dx1 * (mu2 * dudy2 - mu1 * dudy1))
+    full = full - (0.25 * (w6 * dvdz6 + w5 * dvdz5) - ih / dx3 * (mu6 * dwdy6 - mu5 * dwdy5))
+    full = full - (0.25 * (ddu2 * dvdx2 + ddu1 * dvdx1) - ih / dx1 * (mu2 * ddudy2 - mu1 * ddudy1))
+    red = (2.0 * ih * (vv1 + vv21 + vv3 + vv23) - 0.5 * (u1 * dvdx1 + u2 * dvdx2) - 0.5 * (w5 * dvdz5 + w6 * dvdz6)
+           - 0.25 * (ddu1 * dvdx1 + ddu2 * dvdx2) + ih / dx1 * (mu2 * ddudy2 - mu1 * ddudy1) + press)
+    if jvp != 0.0 and jvm != 0.0:
+        red = red + 4.0 * ih * vv2 - 0.5 * (v3 * dvdy3 + v4 * dvdy4)
+    else:
+        red = red + 2.0 * ih * vv2 + (1.0 - jvm) * vbc_dn + (1.0 - jvp) * vbc_up - (mAPJ * Vyp + mACJ * Vc + mAMJ * Vym)
+    scale = sum(abs(t) for t in (mAPI * Vxp, mACI * Vc, mAPK * Vzp, mACK * Vc, mACJ * Vc, ih * vv1, ih * vv2, press))
+    return full, red, scale
+
+
+def test_reduced_v_momentum_rhs_matches_reference_expression():
+    rng = np.random.default_rng(29)
+    worst = 0.0
+    for _ in range(500):
+        v = np.concatenate([rng.uniform(0.5, 2.0, 13), rng.uniform(-1.0, 1.0, 21), rng.uniform(0.5, 2.0, 8),
+                            rng.uniform(0.5, 2.0, 2), rng.uniform(-1.0, 1.0, 2)])
+        for jvm, jvp in ((1.0, 1.0), (0.0, 1.0), (1.0, 0.0)):
+            full, red, scale = forms_v(v, jvm, jvp)
             worst = max(worst, abs(full - red) / scale)
     assert worst < 1e-13, worst

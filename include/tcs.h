@@ -106,6 +106,8 @@ int tcs_momentum_pseudoupdateUVW(tcs_ctx *ctx);        /* module_solve_momentum.
 int tcs_momentum_coeffi_clean(tcs_ctx *ctx);           /* module_solve_momentum.f90:213 (no work) */
 int tcs_pressure_RHS(tcs_ctx *ctx);                    /* module_solve_pressure.f90:140 */
 int tcs_pressure_Poisson_FFT2(tcs_ctx *ctx);           /* module_solve_pressure.f90:489 */
+int tcs_pressure_Poisson_FFT1(tcs_ctx *ctx);           /* module_solve_pressure.f90:238 (transpose scheme 1: on one
+                                                          GPU the same arithmetic and kernels as FFT2) */
 int tcs_pressure_Projection(tcs_ctx *ctx);             /* module_solve_pressure.f90:756 */
 int tcs_post_div(tcs_ctx *ctx, double *maxDivU);       /* module_post.f90:100 (also computes CFL, Nu, KE) */
 int tcs_post_cfl(tcs_ctx *ctx, double *CFL, double *dt); /* module_post.f90:168 */
@@ -152,17 +154,19 @@ int tcs_tdma_many_solve_cycle_nonblocking(tcs_tdma_plan *plan, double *A, double
  * TCS_TDMA_NOALLOC_MAX_ELEMS (TCS_ERR_UNSUPPORTED otherwise).  The array costs
  * 4 * TCS_TDMA_NOALLOC_MAX_ELEMS doubles (8 MiB) on every GPU that loads the
  * library, for the life of the process.  The first call on a device looks up
- * the array's address; make that first call before any stream capture.  All
- * calls share the array: calls that overlap on the GPU race.  Blocking; runs
- * on the legacy default stream of the current device. */
+ * the array's address, and so does the first call after that device's
+ * context was reset (cudaDeviceReset); make those calls before any stream
+ * capture.  All calls share the array: calls that overlap on the GPU race.
+ * Blocking; runs on the legacy default stream of the current device. */
 #define TCS_TDMA_NOALLOC_MAX_ELEMS (1 << 18)
 int tcs_tdma_many_solve_noalloc(double *A, double *B, double *C, double *D, int n_sys, int n_row, int cyclic);
 
 /* ---- measurement --------------------------------------------------------- */
 int tcs_kernel_count(void);
 /* Restart files and planes (module_post.f90): the continue files of
- * :1264-1454 (cont_time.bin = time, dt; cont_U/V/W/P/T.bin = the n1m*n2m*n3m
- * interior, i fastest, FP64) written and read by k-slabs straight from the
+ * :1264-1454 (cont_time.bin = time, dt; cont_U/V/W/P/THETA.bin = the n1m*n2m*n3m
+ * interior, i fastest, FP64; the reader also takes cont_T.bin for T when
+ * cont_THETA.bin is absent) written and read by k-slabs straight from the
  * device, plus cont_dPhat.bin and cont_dP0.bin so that a resumed run continues
  * bit for bit (*with_pressure_history = 0 when those two are absent).  After a
  * read the periodic ghosts are refreshed before the next stage.
@@ -215,9 +219,16 @@ int tcs_probe_reset(tcs_ctx *ctx);
 int tcs_set_use_graph(tcs_ctx *ctx, int on);
 /* launch-shape knobs (powers of two): lines per thread block of the strided
  * (y, z), contiguous (x) and modal line solvers and of the x and z FFTs, and
- * the most lanes (partitions) a tridiagonal line is split over */
+ * the most lanes (partitions) a tridiagonal line is split over.  A line-solver
+ * value is an upper bound: each launch runs the largest power of two up to it
+ * whose blocks fit the SM's shared memory at the family's blocks per SM; a
+ * value no single block could hold is refused (TCS_ERR_ARG).
+ * TCS_TUNE_LONG_LINES picks where long strided lines run as one block per SM
+ * (the same warps, lines fitted to 132 KiB of shared memory so that L1 keeps
+ * 124 KiB) when the usual blocks would leave under 60 KiB of L1 or halve
+ * their lines: 1 never, 2 the z sweeps (default), 4 the z and y sweeps. */
 enum { TCS_TUNE_TL_STRIDED = 0, TCS_TUNE_TL_CONTIG, TCS_TUNE_TL_MODAL, TCS_TUNE_FFT_LINES_X, TCS_TUNE_FFT_LINES_Z,
-       TCS_TUNE_LANES, TCS_TUNE_COUNT };
+       TCS_TUNE_LANES, TCS_TUNE_LONG_LINES, TCS_TUNE_COUNT };
 int tcs_set_tuning(tcs_ctx *ctx, int knob, int value);
 int tcs_get_tuning(tcs_ctx *ctx, int knob, int *value);
 /* Autotuner (no reference counterpart): coordinate descent over every knob,

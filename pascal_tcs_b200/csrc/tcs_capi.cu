@@ -498,6 +498,7 @@ int tcs_create(const tcs_config *cfg, tcs_ctx **out)
     c->cx.fft_lines_x = N1 <= 256 ? 4 : (N1 <= 512 ? 2 : 1);
     c->cx.fft_lines_z = N3 <= 256 ? 4 : (N3 <= 512 ? 2 : 1);
     c->cx.lanes = 32;
+    c->cx.long_lines = 2;
     c->cx.probe = &c->probe;
     sync_shapes(c);
     {   // the FP32 context shares the grid, constants, scalars, tables and history
@@ -796,6 +797,14 @@ int tcs_pressure_Poisson_FFT2(tcs_ctx *c)
     return take_launch_error();
 }
 
+// Transpose scheme 1 (module_solve_pressure.f90:238-482).  On one rank its
+// arithmetic is scheme 2's: the same r2c x and c2c z transforms in the same
+// order, dxk1 = dxk2 (both span the whole half spectrum, :118-127), the same
+// pin of mode (0,0), the same zeroing of the imaginary (0,0) and (0,h3p)
+// modes, scaling, mean removal and wall extrapolation.  With no transposes to
+// choose between on one GPU, both entry points run the same kernels.
+int tcs_pressure_Poisson_FFT1(tcs_ctx *c) { return tcs_pressure_Poisson_FFT2(c); }
+
 int tcs_pressure_Projection(tcs_ctx *c)
 {
     ENTER(c);
@@ -861,7 +870,18 @@ static void launch_step(tcs_ctx *c)
 extern "C" {
 
 // Launch-shape knobs (lines per block of the line-solver families and of the
-// FFT kernels).  Values are validated against the shared-memory budget.
+// FFT kernels).  A line-solver value is the most lines per block: every
+// launch fits it down (fit_tl halves it until the family's blocks per SM fit
+// the SM's shared memory), so the value that runs is the largest power of two
+// up to it that fits.  Values are refused only where one block of the
+// family's largest row type could not hold them at all (227 KB per block);
+// the bound takes the bank-padded line stride of the non-cyclic strided
+// problems (at most one bank row, 32 words, above the odd stride).
+static bool lines_fit_one_block(size_t rowb, int value, int LS, int n)
+{
+    return rowb * (size_t)value * (size_t)(LS + 32) + (size_t)n * sizeof(int) <= (size_t)227 * 1024;
+}
+
 int tcs_set_tuning(tcs_ctx *c, int knob, int value)
 {
     ENTER(c);
@@ -872,16 +892,16 @@ int tcs_set_tuning(tcs_ctx *c, int knob, int value)
     switch (knob) {
     case TCS_TUNE_TL_STRIDED: {
         LinePlan a = make_line_plan(g.N3, true, value), b = make_line_plan(g.N2, false, value);
-        const int LS = a.LS > b.LS ? a.LS : b.LS;
-        if (rb1 * value * LS + 4096 * 4 > 200 * 1024) return set_err(TCS_ERR_ARG, "too many lines for shared memory");
+        if (!lines_fit_one_block(rb1, value, std::max(a.LS, b.LS), std::max(g.N2, g.N3)))
+            return set_err(TCS_ERR_ARG, "too many lines for shared memory");
         x.tl_strided = value; break; }
     case TCS_TUNE_TL_CONTIG: {
         LinePlan a = make_line_plan(g.N1, true, value);
-        if (rb1 * value * a.LS + 4096 * 4 > 200 * 1024) return set_err(TCS_ERR_ARG, "too many lines for shared memory");
+        if (!lines_fit_one_block(rb1, value, a.LS, g.N1)) return set_err(TCS_ERR_ARG, "too many lines for shared memory");
         x.tl_contig = value; break; }
     case TCS_TUNE_TL_MODAL: {
         LinePlan a = make_line_plan(g.N2, false, value);
-        if (row_bytes(2, false) * value * a.LS + 4096 * 4 > 200 * 1024) return set_err(TCS_ERR_ARG, "too many lines for shared memory");
+        if (!lines_fit_one_block(row_bytes(2, false), value, a.LS, g.N2)) return set_err(TCS_ERR_ARG, "too many lines for shared memory");
         x.tl_modal = value; break; }
     case TCS_TUNE_FFT_LINES_X:
         if ((size_t)value * g.N1 * (32 + e) > 200 * 1024) return set_err(TCS_ERR_ARG, "too many lines for shared memory");
@@ -892,6 +912,9 @@ int tcs_set_tuning(tcs_ctx *c, int knob, int value)
     case TCS_TUNE_LANES:
         if (value < 2 || value > 32) return set_err(TCS_ERR_ARG, "lanes per line must be 2..32");
         x.lanes = value; break;
+    case TCS_TUNE_LONG_LINES:
+        if (value > 4) return set_err(TCS_ERR_ARG, "long-line form: 1 never, 2 z sweeps, 4 z and y sweeps");
+        x.long_lines = value; break;
     default: return set_err(TCS_ERR_ARG, "unknown tuning knob");
     }
     sync_shapes(c);
@@ -912,6 +935,7 @@ int tcs_get_tuning(tcs_ctx *c, int knob, int *value)
     case TCS_TUNE_FFT_LINES_X: *value = x.fft_lines_x; break;
     case TCS_TUNE_FFT_LINES_Z: *value = x.fft_lines_z; break;
     case TCS_TUNE_LANES: *value = x.lanes; break;
+    case TCS_TUNE_LONG_LINES: *value = x.long_lines; break;
     default: return set_err(TCS_ERR_ARG, "unknown tuning knob");
     }
     return TCS_OK;
@@ -1613,7 +1637,8 @@ int tcs_tdma_many_solve_cycle_nonblocking(tcs_tdma_plan *p, double *A, double *B
 //
 // tcs_write_continue / tcs_read_continue write and read the reference's
 // continue files (module_post.f90:1264-1454: cont_time.bin = time, dt;
-// cont_U/V/W/P/T.bin = the n1m x n2m x n3m interior, i fastest, FP64) by
+// cont_U/V/W/P/THETA.bin = the n1m x n2m x n3m interior, i fastest, FP64,
+// the names the reference's writer and reader use, :1336 and :1443) by
 // k-slabs through one device staging chunk and one pinned host chunk, and add
 // cont_dPhat.bin and cont_dP0.bin, which the reference does not save, so that
 // a resumed run continues bit for bit.  tcs_extract_plane copies one padded
@@ -1633,7 +1658,10 @@ static int io_chunk(tcs_ctx *c, size_t n)
 
 static const struct { int field; const char *name; } k_cont[] = {
     {TCS_F_U, "cont_U.bin"}, {TCS_F_V, "cont_V.bin"}, {TCS_F_W, "cont_W.bin"}, {TCS_F_P, "cont_P.bin"},
-    {TCS_F_T, "cont_T.bin"}, {TCS_F_DPHAT, "cont_dPhat.bin"}, {TCS_F_DP0, "cont_dP0.bin"}};
+    {TCS_F_T, "cont_THETA.bin"}, {TCS_F_DPHAT, "cont_dPhat.bin"}, {TCS_F_DP0, "cont_dP0.bin"}};
+// Temperature files written by earlier versions of this library, read when
+// cont_THETA.bin is absent.
+static const char *const k_cont_T_legacy = "cont_T.bin";
 
 static std::string join_path(const char *dir, const char *name)
 {
@@ -1702,6 +1730,7 @@ int tcs_read_continue(tcs_ctx *c, const char *dir, int *with_pressure_history)
     const size_t want = (size_t)g.N1 * g.N2 * g.N3;
     for (const auto &cf : k_cont) {
         FILE *fp = std::fopen(join_path(dir, cf.name).c_str(), "rb");
+        if (!fp && cf.field == TCS_F_T) fp = std::fopen(join_path(dir, k_cont_T_legacy).c_str(), "rb");
         const bool optional = cf.field == TCS_F_DPHAT || cf.field == TCS_F_DP0;
         if (!fp) {
             if (optional) { history = 0; continue; }

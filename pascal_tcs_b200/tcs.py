@@ -22,7 +22,7 @@ SCALARS = ["dt", "time", "CFL", "maxDivU", "Nu_bot", "Nu_top", "KE", "blowup",
            "aver", "step", "fixed_dt"]
 HISTORY = ["dt", "time", "maxDivU", "CFL", "Nu_bot", "Nu_top", "KE"]
 METRICS = ["x1", "dx1", "dmx1", "x2", "dx2", "dmx2", "x3", "dx3", "dmx3"]
-TUNING = ["tl_strided", "tl_contig", "tl_modal", "fft_lines_x", "fft_lines_z", "lanes"]
+TUNING = ["tl_strided", "tl_contig", "tl_modal", "fft_lines_x", "fft_lines_z", "lanes", "long_lines"]
 ERRORS = {1: "bad argument", 2: "CUDA error", 3: "unsupported", 4: "BLOW UP",
           5: "out of device memory", 6: "non-finite scalar"}
 
@@ -35,7 +35,7 @@ EXPORTS = [
     "tcs_subdomain_ghostcell_update", "tcs_momentum_coeffi", "tcs_momentum_solvedU",
     "tcs_momentum_solvedV", "tcs_momentum_solvedW", "tcs_momentum_blockLdV",
     "tcs_momentum_blockLdU", "tcs_momentum_pseudoupdateUVW", "tcs_momentum_coeffi_clean",
-    "tcs_pressure_RHS", "tcs_pressure_Poisson_FFT2", "tcs_pressure_Projection",
+    "tcs_pressure_RHS", "tcs_pressure_Poisson_FFT2", "tcs_pressure_Poisson_FFT1", "tcs_pressure_Projection",
     "tcs_post_div", "tcs_post_cfl", "tcs_step", "tcs_get_scalars", "tcs_get_history",
     "tcs_snapshot", "tcs_restore",
     "tcs_tdma_plan_many_create", "tcs_tdma_plan_many_destroy", "tcs_tdma_many_solve",
@@ -154,7 +154,8 @@ def load() -> ctypes.CDLL:
                  "tcs_momentum_coeffi", "tcs_momentum_solvedU", "tcs_momentum_solvedV",
                  "tcs_momentum_solvedW", "tcs_momentum_blockLdV", "tcs_momentum_blockLdU",
                  "tcs_momentum_pseudoupdateUVW", "tcs_momentum_coeffi_clean", "tcs_pressure_RHS",
-                 "tcs_pressure_Poisson_FFT2", "tcs_pressure_Projection", "tcs_snapshot", "tcs_restore"):
+                 "tcs_pressure_Poisson_FFT2", "tcs_pressure_Poisson_FFT1", "tcs_pressure_Projection", "tcs_snapshot",
+                 "tcs_restore"):
         sig[name] = ([vp], ip)
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -229,7 +230,7 @@ class Solver:
         _check(load().tcs_download_field_async(self._h, FIELDS[name], pinned_ptr), f"download {name}")
 
     def write_continue(self, directory: str) -> None:
-        """cont_time/U/V/W/P/T.bin (the reference's continue files) plus cont_dPhat/dP0.bin."""
+        """cont_time/U/V/W/P/THETA.bin (the reference's continue files) plus cont_dPhat/dP0.bin."""
         _check(load().tcs_write_continue(self._h, directory.encode()), "write_continue")
 
     def read_continue(self, directory: str) -> bool:
@@ -304,6 +305,7 @@ class Solver:
     def momentum_coeffi_clean(self): self._call("tcs_momentum_coeffi_clean")
     def pressure_RHS(self): self._call("tcs_pressure_RHS")
     def pressure_Poisson_FFT2(self): self._call("tcs_pressure_Poisson_FFT2")
+    def pressure_Poisson_FFT1(self): self._call("tcs_pressure_Poisson_FFT1")
     def pressure_Projection(self): self._call("tcs_pressure_Projection")
 
     def ghostcell_update(self, name: str) -> None:

@@ -84,6 +84,28 @@ def test_stage_by_stage_parity(tcs, oracle_mod, case):
         assert rel_l2(cfl, so["CFL"]) < 1e-12 and rel_l2(dt, so["dt"]) < 1e-12
 
 
+def test_poisson_fft1_equals_fft2(tcs, oracle_mod):
+    # mpi_pressure_Poisson_FFT1 (transpose scheme 1) and _FFT2 compute the same
+    # arithmetic on one rank: from identical inputs the two entry points give
+    # bit-identical dP, which matches the oracle's Poisson stage at the bar
+    cfg = dict(n1m=30, n2m=17, n3m=24, property_set=1, Pr=7.0, Ra=1e6, dtStart=5e-4, top_wall_mode=1)
+    a, o = _pair(tcs, oracle_mod, **cfg)
+    b = tcs.Solver(**cfg)
+    a.step(2); b.step(2); o.step(2)
+    for s in (a, b):
+        s.thermal_solver(); s.momentum_coeffi(); s.momentum_solvedU(); s.momentum_solvedV()
+        s.momentum_solvedW(); s.momentum_blockLdV(); s.momentum_blockLdU()
+        s.momentum_pseudoupdateUVW(); s.pressure_RHS()
+    a.pressure_Poisson_FFT2()
+    b.pressure_Poisson_FFT1()
+    np.testing.assert_array_equal(b.get("dP"), a.get("dP"))
+    for st in ("thermal", "ghost_T", "mom_coeffi", "dU", "dV", "dW", "blockLdV", "blockLdU", "pseudo", "prhs", "poisson"):
+        o.stage(st)
+    _check_fields(b, o, ["dP"], where="Poisson_FFT1")
+    b.pressure_Projection(); a.pressure_Projection()
+    np.testing.assert_array_equal(b.get("U"), a.get("U"))
+
+
 def _run_compare(tcs, oracle_mod, steps, **cfg):
     g, o = _pair(tcs, oracle_mod, **cfg)
     g.step(steps)
@@ -94,6 +116,18 @@ def _run_compare(tcs, oracle_mod, steps, **cfg):
         out[n] = rel_l2(hg[:, col], hd[:, col])
     out["dt"] = rel_l2(hg[:, 0], hd[:, 0])
     return out, g, o
+
+
+def test_long_lines_match_oracle(tcs, oracle_mod):
+    # 512-row z and y lines (16 rows per lane; the z and y sweeps in their
+    # one-block-per-SM form), water properties: whole steps against the oracle
+    err, g, _ = _run_compare(tcs, oracle_mod, 3, n1m=16, n2m=512, n3m=512, gamma2=2.0, property_set=1, Pr=7.0,
+                             Ra=1e7, DeltaT=10.0, dtStart=5e-5, fixed_dt=1, seed=2)
+    print({k: f"{v:.2e}" for k, v in err.items()})
+    for k, v in err.items():
+        assert v <= RUN_TOL, f"{k}: rel L2 {v:.3e}"
+    g.set_tuning("long_lines", 4)
+    assert g.tuning()["long_lines"] == 4
 
 
 def test_64cube_constant_properties_100_steps(tcs, oracle_mod):

@@ -18,13 +18,19 @@ def tcs():
     return P
 
 
+# field -> continue file: the names module_post.f90 writes and reads (:1336-1340, :1443-1447)
+CONT = {"U": "cont_U.bin", "V": "cont_V.bin", "W": "cont_W.bin", "P": "cont_P.bin", "T": "cont_THETA.bin",
+        "dPhat": "cont_dPhat.bin", "dP0": "cont_dP0.bin"}
+
+
 def test_continue_files_have_the_reference_layout(tcs, tmp_path):
     g = tcs.Solver(**CFG)
     g.step(3)
     g.write_continue(str(tmp_path))
     n = CFG["n1m"] * CFG["n2m"] * CFG["n3m"]
-    for f in ("U", "V", "W", "P", "T", "dPhat", "dP0"):
-        a = np.fromfile(tmp_path / f"cont_{f}.bin", dtype=np.float64)
+    assert not (tmp_path / "cont_T.bin").exists()
+    for f, name in CONT.items():
+        a = np.fromfile(tmp_path / name, dtype=np.float64)
         assert a.size == n
         # (n1m, n2m, n3m) interior, i fastest: numpy (k, j, i) order
         np.testing.assert_array_equal(a.reshape(CFG["n3m"], CFG["n2m"], CFG["n1m"]), g.get(f)[I], err_msg=f)
@@ -45,6 +51,28 @@ def test_resume_from_continue_files_is_bit_continuous(tcs, tmp_path, precision):
     b.step(2)
     for f in ("T", "U", "V", "W", "P", "dPhat", "dP0"):
         np.testing.assert_array_equal(b.get(f)[I], a.get(f)[I], err_msg=f)
+
+
+def test_reads_files_written_by_the_reference_names(tcs, tmp_path):
+    # continue files written field by field under the reference's names (as
+    # mpi_Post_FileOut_Continue_Post_Reassembly_IO does), without the dPhat/dP0
+    # extras: the reader takes them and reports the missing pressure history
+    src = tcs.Solver(**CFG)
+    src.step(2)
+    for f in ("U", "V", "W", "P", "T"):
+        np.ascontiguousarray(src.get(f)[I]).tofile(tmp_path / CONT[f])
+    s = src.scalars()
+    np.array([s["time"], s["dt"]]).tofile(tmp_path / "cont_time.bin")
+    b = tcs.Solver(**CFG)
+    assert not b.read_continue(str(tmp_path))
+    for f in ("U", "V", "W", "P", "T"):
+        np.testing.assert_array_equal(b.get(f)[I], src.get(f)[I], err_msg=f)
+    assert b.scalars()["time"] == s["time"]
+    # a temperature file under this library's earlier name is still read
+    os.rename(tmp_path / "cont_THETA.bin", tmp_path / "cont_T.bin")
+    c = tcs.Solver(**CFG)
+    c.read_continue(str(tmp_path))
+    np.testing.assert_array_equal(c.get("T")[I], src.get("T")[I])
 
 
 def test_resume_without_pressure_history_is_reported(tcs, tmp_path):

@@ -106,8 +106,63 @@ void launch_tdma_many(double *A, const double *B, double *C, double *D, int n_sy
 // ---------------------------------------------------------------------------
 static __device__ __align__(256) double g_tdma_noalloc[4 * TCS_TDMA_NOALLOC_MAX_ELEMS];
 
+// Host code needs the array's device address (the symbol's name is only a
+// host-side stand-in).  It is looked up once per device context: the slot
+// remembers the unique id of the context it was taken in, so after a
+// cudaDeviceReset (a new primary context, in which the library's module is
+// loaded again) the next call looks it up afresh instead of using the dead
+// address.  The context id comes from the driver (cuCtxGetCurrent, cuCtxGetId)
+// through the runtime's entry-point query; without it every call looks up.
+struct NoallocSlot { double *ptr; unsigned long long ctx_id; bool have_id; };
 static std::mutex g_noalloc_mu;
-static double *g_noalloc_ptr[64] = {};
+static NoallocSlot g_noalloc_slot[64] = {};
+
+typedef int (*PfnCtxGetCurrent)(void **ctx);
+typedef int (*PfnCtxGetId)(void *ctx, unsigned long long *id);
+static PfnCtxGetCurrent g_ctx_get_current = nullptr;
+static PfnCtxGetId g_ctx_get_id = nullptr;
+static std::once_flag g_ctx_fn_once;
+
+static bool current_ctx_id(unsigned long long *id)
+{
+    std::call_once(g_ctx_fn_once, [] {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            g_ctx_get_current = (PfnCtxGetCurrent)f;
+        f = nullptr;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            g_ctx_get_id = (PfnCtxGetId)f;
+        cudaGetLastError();
+    });
+    if (!g_ctx_get_current || !g_ctx_get_id) return false;
+    void *ctx = nullptr;
+    if (g_ctx_get_current(&ctx) != 0 || !ctx) return false;
+    return g_ctx_get_id(ctx, id) == 0;
+}
+
+// The array's address on the current device (set-up on a device's first call,
+// and again after its context was reset).
+static int noalloc_base(int dev, double **out)
+{
+    unsigned long long id = 0;
+    bool have = current_ctx_id(&id);
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    NoallocSlot &sl = g_noalloc_slot[dev];
+    if (!sl.ptr || !have || !sl.have_id || id != sl.ctx_id) {
+        void *p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_tdma_noalloc);
+        if (e != cudaSuccess) return set_error(TCS_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+        have = current_ctx_id(&id);        // the lookup makes the primary context current
+        sl.ptr = (double *)p;
+        sl.ctx_id = id;
+        sl.have_id = have;
+    }
+    *out = sl.ptr;
+    return TCS_OK;
+}
 
 } // namespace tcs
 
@@ -123,19 +178,9 @@ extern "C" int tcs_tdma_many_solve_noalloc(double *A, double *B, double *C, doub
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return set_error(TCS_ERR_CUDA, cudaGetErrorString(e));
     if (dev < 0 || dev >= 64) return set_error(TCS_ERR_UNSUPPORTED, "device ordinal >= 64");
-    double *base;
-    {
-        // First call on this device: host code needs the array's device address
-        // (the symbol name itself is only a host-side stand-in).
-        std::lock_guard<std::mutex> lk(g_noalloc_mu);
-        if (!g_noalloc_ptr[dev]) {
-            void *p = nullptr;
-            e = cudaGetSymbolAddress(&p, g_tdma_noalloc);
-            if (e != cudaSuccess) return set_error(TCS_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-            g_noalloc_ptr[dev] = (double *)p;
-        }
-        base = g_noalloc_ptr[dev];
-    }
+    double *base = nullptr;
+    const int r = noalloc_base(dev, &base);
+    if (r) return r;
     double *dA = base, *dB = base + n, *dC = base + 2 * n, *dD = base + 3 * n;
     const size_t bytes = n * sizeof(double);
     // Every element the kernel reads is copied in first, so nothing needs clearing.

@@ -38,6 +38,7 @@ struct Shapes {
     int tl_strided, tl_contig, tl_modal;
     int fft_lines_x, fft_lines_z;
     int lanes;                                   // at most this many partitions (lanes) per line
+    int long_lines;                              // one-block-per-SM form of long lines: 1 never, 2 z sweeps, 4 z and y sweeps
     FFTPlan fp1, fp3;
     int h1p;
     double wall_ab, wall_bb, wall_at, wall_bt;   // Pbc_a, Pbc_b of the two walls
@@ -90,13 +91,21 @@ inline LinePlan plan_for(int n, bool cyclic, int tl, int pmax)
     return lp;
 }
 
+// The shared memory (KiB) a line family lets its blocks take per SM: all of
+// it (228 KiB) by default, less for the one-block-per-SM form of long lines
+// (LongLines), whose stencil builds need the L1 that the rest leaves.
+template <class P, class = void>
+struct SmemKiB { static constexpr int v = 228; };
+template <class P>
+struct SmemKiB<P, std::void_t<decltype(P::SMEM_KIB)>> { static constexpr int v = P::SMEM_KIB; };
+
 // Lines per block: the requested count, halved until MINB blocks fit in the
-// SM's shared memory (228 KB, 1 KB reserved per block);
+// family's share of the SM's shared memory (1 KB reserved per block);
 // extra: static shared memory the kernel adds per block.
 template <class Prob>
 inline int fit_tl(int n, bool cyclic, int want, int pmax, size_t extra = 0)
 {
-    const size_t budget = (size_t)228 * 1024 / Prob::MINB - 1024 - extra;
+    const size_t budget = (size_t)SmemKiB<Prob>::v * 1024 / Prob::MINB - 1024 - extra;
     int tl = want;
     while (tl > 1 && line_smem<Prob>(plan_for<Prob>(n, cyclic, tl, pmax)) > budget) tl /= 2;
     return tl;
@@ -126,6 +135,54 @@ inline void launch_lines(const Prob &p, const LinePlan &lp, dim3 grid, cudaStrea
     line_solve_kernel<Prob><<<grid, Prob::NT, smem, s>>>(p, lp);
     probe_end(cx, kid, s);
     record_launch_error(kernel_name(kid));
+}
+
+// The SM's unified L1/shared-memory configurations: the shared-memory share
+// (KiB) the driver picks for a given demand per SM; the L1 keeps the rest of
+// the 256 KiB.
+inline int smem_config_kib(size_t per_sm_bytes)
+{
+    static const int cfg[] = {0, 8, 16, 32, 64, 100, 132, 164, 196, 228};
+    for (int c : cfg)
+        if ((size_t)c * 1024 >= per_sm_bytes) return c;
+    return 228;
+}
+
+// A line family in one block per SM: the same warps per SM (NT x MINB threads
+// in one block, so the same registers per thread) with its lines per block
+// fitted to 132 KiB of shared memory, which leaves the SM 124 KiB of L1.  The
+// z-sweep builds read every input through L1 about three times (their x and z
+// neighbours come from other threads' cells): measured on B200, forcing their
+// 256^3 blocks into the 228 KiB configuration (28 KiB of L1) made them 1.8x
+// slower, and 512-row lines put them there by themselves (two blocks of 8
+// lines x 512 rows need 213 KiB).
+template <class P>
+struct LongLines : P {
+    static constexpr int NT = P::NT * P::MINB;
+    static constexpr int MINB = 1;
+    static constexpr int SMEM_KIB = 132;
+};
+
+// A strided line sweep (z or y lines: TL consecutive i per block, gy block
+// rows).  With allow_long, the one-block-per-SM form runs instead where the
+// usual form would leave less than 60 KiB of L1 or would have to halve its
+// lines per block.  make(tl) builds the problem for tl lines per block.
+template <class P, class Make>
+inline void launch_strided(const Shapes &cx, int n, bool cyclic, int nlines, int gy, Make make, cudaStream_t s, int kid,
+                           bool allow_long)
+{
+    const LinePlan a = plan_for<P>(n, cyclic, fit_tl<P>(n, cyclic, cx.tl_strided, cx.lanes), cx.lanes);
+    if (allow_long) {
+        using L = LongLines<P>;
+        const LinePlan b = plan_for<L>(n, cyclic, fit_tl<L>(n, cyclic, cx.tl_strided, cx.lanes), cx.lanes);
+        const size_t per_sm = (size_t)P::MINB * (line_smem<P>(a) + 1024);
+        const int l1_kib = 256 - smem_config_kib(per_sm);
+        if (b.TL > a.TL || l1_kib < 60) {
+            launch_lines(L{make(b.TL)}, b, dim3((nlines + b.TL - 1) / b.TL, gy), s, kid, cx);
+            return;
+        }
+    }
+    launch_lines(make(a.TL), a, dim3((nlines + a.TL - 1) / a.TL, gy), s, kid, cx);
 }
 
 // ---------------------------------------------------------------------------

@@ -620,33 +620,27 @@ template <class R>
 void launch_solve_du(const Ctx<R> &cx, cudaStream_t s)
 {
     const GridT<R> &g = cx.g;
-    LinePlan pz = plan_for<DUZ<R>>(g.N3, true, fit_tl<DUZ<R>>(g.N3, true, cx.tl_strided, cx.lanes), cx.lanes);
-    LinePlan py = plan_for<DUY<R>>(g.N2, false, fit_tl<DUY<R>>(g.N2, false, cx.tl_strided, cx.lanes), cx.lanes);
-    launch_lines(DUZ<R>{g, cx.f, pz.TL}, pz, dim3((g.N1 + pz.TL - 1) / pz.TL, g.N2), s, K_DU_Z, cx);
+    launch_strided<DUZ<R>>(cx, g.N3, true, g.N1, g.N2, [&](int tl) { return DUZ<R>{g, cx.f, tl}; }, s, K_DU_Z, cx.long_lines >= 2);
     launch_x<DUX>(cx, g.N2, s, K_DU_X);
-    launch_lines(DUY<R>{g, cx.f, py.TL}, py, dim3((g.N1 + py.TL - 1) / py.TL, g.N3), s, K_DU_Y, cx);
+    launch_strided<DUY<R>>(cx, g.N2, false, g.N1, g.N3, [&](int tl) { return DUY<R>{g, cx.f, tl}; }, s, K_DU_Y, cx.long_lines >= 4);
 }
 
 template <class R>
 void launch_solve_dv(const Ctx<R> &cx, cudaStream_t s)
 {
     const GridT<R> &g = cx.g;
-    LinePlan pz = plan_for<DVZ<R>>(g.N3, true, fit_tl<DVZ<R>>(g.N3, true, cx.tl_strided, cx.lanes), cx.lanes);
-    LinePlan py = plan_for<DVY<R>>(g.N2 - 1, false, fit_tl<DVY<R>>(g.N2 - 1, false, cx.tl_strided, cx.lanes), cx.lanes);
-    launch_lines(DVZ<R>{g, cx.f, pz.TL}, pz, dim3((g.N1 + pz.TL - 1) / pz.TL, g.N2 - 1), s, K_DV_Z, cx);
+    launch_strided<DVZ<R>>(cx, g.N3, true, g.N1, g.N2 - 1, [&](int tl) { return DVZ<R>{g, cx.f, tl}; }, s, K_DV_Z, cx.long_lines >= 2);
     launch_x<DVX>(cx, g.N2 - 1, s, K_DV_X);
-    launch_lines(DVY<R>{g, cx.f, py.TL}, py, dim3((g.N1 + py.TL - 1) / py.TL, g.N3), s, K_DV_Y, cx);
+    launch_strided<DVY<R>>(cx, g.N2 - 1, false, g.N1, g.N3, [&](int tl) { return DVY<R>{g, cx.f, tl}; }, s, K_DV_Y, cx.long_lines >= 4);
 }
 
 template <class R>
 void launch_solve_dw(const Ctx<R> &cx, cudaStream_t s)
 {
     const GridT<R> &g = cx.g;
-    LinePlan pz = plan_for<DWZ<R>>(g.N3, true, fit_tl<DWZ<R>>(g.N3, true, cx.tl_strided, cx.lanes), cx.lanes);
-    LinePlan py = plan_for<DWY<R>>(g.N2, false, fit_tl<DWY<R>>(g.N2, false, cx.tl_strided, cx.lanes), cx.lanes);
-    launch_lines(DWZ<R>{g, cx.f, pz.TL}, pz, dim3((g.N1 + pz.TL - 1) / pz.TL, g.N2), s, K_DW_Z, cx);
+    launch_strided<DWZ<R>>(cx, g.N3, true, g.N1, g.N2, [&](int tl) { return DWZ<R>{g, cx.f, tl}; }, s, K_DW_Z, cx.long_lines >= 2);
     launch_x<DWX>(cx, g.N2, s, K_DW_X);
-    launch_lines(DWY<R>{g, cx.f, py.TL}, py, dim3((g.N1 + py.TL - 1) / py.TL, g.N3), s, K_DW_Y, cx);
+    launch_strided<DWY<R>>(cx, g.N2, false, g.N1, g.N3, [&](int tl) { return DWY<R>{g, cx.f, tl}; }, s, K_DW_Y, cx.long_lines >= 4);
 }
 
 // ---------------------------------------------------------------------------

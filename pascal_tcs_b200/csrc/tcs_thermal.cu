@@ -246,13 +246,10 @@ template <class R>
 void launch_thermal(const Ctx<R> &cx, cudaStream_t s)
 {
     const GridT<R> &g = cx.g;
-    LinePlan pz = plan_for<ThermalZ<R>>(g.N3, true, fit_tl<ThermalZ<R>>(g.N3, true, cx.tl_strided, cx.lanes), cx.lanes);
-    LinePlan py = plan_for<ThermalY<R>>(g.N2, false, fit_tl<ThermalY<R>>(g.N2, false, cx.tl_strided, cx.lanes), cx.lanes);
-    ThermalZ<R> z{g, cx.f, pz.TL};
-    launch_lines(z, pz, dim3((g.N1 + pz.TL - 1) / pz.TL, g.N2), s, K_THERMAL_Z, cx);
+    launch_strided<ThermalZ<R>>(cx, g.N3, true, g.N1, g.N2, [&](int tl) { return ThermalZ<R>{g, cx.f, tl}; }, s, K_THERMAL_Z, cx.long_lines >= 2);
     launch_x<ThermalX>(cx, g.N2, s, K_THERMAL_X);
-    ThermalY<R> y{g, cx.f, py.TL};
-    launch_lines(y, py, dim3((g.N1 + py.TL - 1) / py.TL, g.N3), s, K_THERMAL_Y, cx);
+    launch_strided<ThermalY<R>>(cx, g.N2, false, g.N1, g.N3, [&](int tl) { return ThermalY<R>{g, cx.f, tl}; }, s, K_THERMAL_Y,
+                                cx.long_lines >= 4);
 }
 
 // The same three sweeps for many cases, one launch per sweep.

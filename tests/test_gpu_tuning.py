@@ -36,7 +36,8 @@ def test_autotune_keeps_state_and_caches(tcs, tmp_path):
 
 
 @pytest.mark.parametrize("knob,value", [("lanes", 8), ("lanes", 16), ("tl_strided", 2), ("tl_contig", 16),
-                                        ("tl_modal", 1), ("fft_lines_x", 1), ("fft_lines_z", 8)])
+                                        ("tl_modal", 1), ("fft_lines_x", 1), ("fft_lines_z", 8),
+                                        ("long_lines", 1), ("long_lines", 4)])
 def test_every_knob_setting_gives_the_same_step(tcs, knob, value):
     a, b = tcs.Solver(**CFG), tcs.Solver(**CFG)
     b.set_tuning(knob, value)
@@ -45,3 +46,21 @@ def test_every_knob_setting_gives_the_same_step(tcs, knob, value):
     for n in ("T", "U", "V", "W", "P"):
         x, y = a.get(n), b.get(n)
         assert np.linalg.norm(x - y) <= 1e-12 * np.linalg.norm(x), n
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_long_line_forms_are_bit_identical(tcs, precision):
+    # 512-row z and y lines: the one-block-per-SM form (z sweeps by default, y
+    # sweeps too with long_lines = 4) runs the same arithmetic per line as the
+    # usual form, so every setting gives the same bits
+    cfg = dict(n1m=16, n2m=512, n3m=512, property_set=1, Pr=7.0, Ra=1e6, dtStart=5e-4, seed=4, precision=precision)
+    runs = []
+    for v in (1, 2, 4):
+        g = tcs.Solver(**cfg)
+        g.set_tuning("long_lines", v)
+        g.step(2)
+        runs.append({n: g.get(n) for n in ("T", "U", "V", "W", "P")})
+        g.close()
+    for r in runs[1:]:
+        for n, x in runs[0].items():
+            np.testing.assert_array_equal(r[n], x, err_msg=n)

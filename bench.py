@@ -492,11 +492,60 @@ def device_run(P, torch, cfg: dict, workload: str, args, ws: int, local: int, st
              "achieved_gbs": step_bytes / (ms / args.steps * 1e-3) / 1e9}
     whole["frac_of_peak"] = whole["achieved_gbs"] / peak
     kernel_split = {k: round(v[0], 4) for k, v in sorted(per.items(), key=lambda kv: -kv[1][0]) if v[1]}
+    # the same split under the reference's stage timers (main.f90:55-72)
+    tmap = P.timer_of_kernel()
+    stages = {t: 0.0 for t in P.timer_names()}
+    for k, v in per.items():
+        if v[1] and tmap.get(k):
+            stages[tmap[k]] += v[0]
+    stage_split = {t: round(v, 4) for t, v in stages.items()}
     if reset:
         s.restore()
     return s, {"value": ws * cells * args.steps / (ms * 1e-3), "ms_per_step": ms / args.steps, "tuning": tuned,
                "launches": launches, "roofline": roof, "whole_step": whole,
-               "kernel_ms_one_step": kernel_split, "clocks": clk.summary(), "reset": reset}
+               "kernel_ms_one_step": kernel_split, "stage_ms_one_step": stage_split, "clocks": clk.summary(),
+               "reset": reset}
+
+
+def tdma_api_timing(P, torch, n_sys: int = 256 * 256, n_row: int = 256, reps: int = 5) -> dict:
+    """The reference-facing PaScaL_TDMA interface as the reference calls it:
+    a plan created, one many-systems solve and the plan destroyed per sweep
+    (module_solve_thermal.f90:364-366), on a z sweep's worth of cyclic systems
+    (256^2 systems of 256 rows), from host arrays (4 arrays up, 3 down per
+    solve) and from device arrays.  Seconds per sweep, best of reps after one
+    untimed sweep."""
+    rng = np.random.default_rng(5)
+    A = rng.uniform(-0.3, 0.3, (n_row, n_sys)); C = rng.uniform(-0.3, 0.3, (n_row, n_sys))
+    B = 1.0 + rng.uniform(0.0, 1.0, (n_row, n_sys)); D = rng.uniform(-1.0, 1.0, (n_row, n_sys))
+    out = {"systems": n_sys, "rows": n_row, "cyclic": True}
+
+    def sweep(arrs):
+        plan = P.TdmaPlan(n_sys)
+        plan.many_solve_cycle(*arrs, n_sys, n_row)
+        plan.destroy()
+
+    host = [x.copy() for x in (A, B, C, D)]
+    best = None
+    for r in range(reps + 1):
+        for h, x in zip(host, (A, B, C, D)):
+            h[...] = x
+        t0 = time.perf_counter(); sweep(host); el = time.perf_counter() - t0
+        best = el if r and (best is None or el < best) else best
+    out["host_arrays_s_per_sweep"] = best
+    out["host_arrays_rows_per_s"] = n_sys * n_row / best
+    out["host_bytes_per_sweep"] = 7 * 8 * n_sys * n_row
+    dev = [torch.tensor(x, device="cuda") for x in (A, B, C, D)]
+    src = [d.clone() for d in dev]
+    best = None
+    for r in range(reps + 1):
+        for d, x in zip(dev, src):
+            d.copy_(x)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter(); sweep(dev); el = time.perf_counter() - t0
+        best = el if r and (best is None or el < best) else best
+    out["device_arrays_s_per_sweep"] = best
+    out["device_arrays_rows_per_s"] = n_sys * n_row / best
+    return out
 
 
 def rel_l2(a, b) -> float:
@@ -740,6 +789,8 @@ def main():
                                                                   RESET_EVERY["rb256_water_fp64"])
         del keep
 
+    tdma = tdma_api_timing(P, torch) if (workload == "rb512_water_fp64" and not args.no_extra) else None
+
     base = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         base = cpu_baseline(cfg)
@@ -753,10 +804,13 @@ def main():
                 "data": "synthetic: seeded conduction profile + uniform noise 0.01, zero velocity",
                 "config": single_config(cfg, workload, ws),
                 "gpu_launches": m["launches"], "roofline": m["roofline"], "whole_step": m["whole_step"],
-                "kernel_ms_one_step": m["kernel_ms_one_step"], "tuning": m["tuning"], "clocks": m["clocks"], "e2e": e2e,
+                "kernel_ms_one_step": m["kernel_ms_one_step"], "stage_ms_one_step": m["stage_ms_one_step"],
+                "tuning": m["tuning"], "clocks": m["clocks"], "e2e": e2e,
                 "fp32_mixed": mixed, "cpu_baseline": base}
         if extra is not None:
             line["also"] = extra
+        if tdma is not None:
+            line["tdma_api"] = tdma
         print(json.dumps(line))
     if ws > 1:
         import torch.distributed as dist

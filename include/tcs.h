@@ -216,6 +216,21 @@ const char *tcs_kernel_name(int kernel_id);
 int tcs_probe_enable(tcs_ctx *ctx, uint64_t mask);
 int tcs_probe_read(tcs_ctx *ctx, int kernel_id, double *total_ms, int *launches);
 int tcs_probe_reset(tcs_ctx *ctx);
+/* The reference's stage timers (main.f90:55-72, timer.f90): the timer (1..18)
+ * whose work a kernel does, 0 for kernels outside the time loop, -1 for a bad
+ * id; and a timer's label as the reference prints it (NULL outside 1..18).
+ * Summing probed kernel times per timer gives the reference's stage split. */
+int tcs_timer_of_kernel(int kernel_id);
+const char *tcs_timer_name(int timer);
+/* Bounds-check build (no reference counterpart; the reference's debug builds
+ * use the compiler's array checks, Makefile.inc:6-11): libtcs_bc.so, compiled
+ * with -DTCS_BOUNDS_CHECK, checks every field, table, spectrum and
+ * shared-memory row index the kernels form; an index out of range is counted
+ * and its access redirected to a valid cell, never made.  tcs_bounds_checked
+ * says whether the loaded library has the checks; tcs_bounds_violations
+ * returns the case's count so far (always 0 in the normal build). */
+int tcs_bounds_checked(void);
+int tcs_bounds_violations(tcs_ctx *ctx, double *count);
 int tcs_set_use_graph(tcs_ctx *ctx, int on);
 /* launch-shape knobs (powers of two): lines per thread block of the strided
  * (y, z), contiguous (x) and modal line solvers and of the x and z FFTs, and

@@ -17,6 +17,9 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libtcs.so")
+# the bounds-check build (-DTCS_BOUNDS_CHECK): every index the kernels form is
+# checked; used by the tests, never by the benchmark
+LIB_BC = os.path.join(HERE, "libtcs_bc.so")
 SOURCES = ["tcs_thermal.cu", "tcs_momentum.cu", "tcs_pressure.cu", "tcs_post.cu",
            "tcs_tdma.cu", "tcs_capi.cu", "tcs_peak.cu"]
 HEADERS = ["tcs_device.cuh", "tcs_fields.cuh", "tcs_kernels.h"]
@@ -47,7 +50,14 @@ def _stale(target: str, deps: list[str]) -> bool:
     return any(os.path.getmtime(d) > t for d in deps)
 
 
-def build(force: bool = False, verbose: bool = False, extra: list[str] | None = None) -> str:
+def build(force: bool = False, verbose: bool = False, extra: list[str] | None = None, bounds_check: bool = False) -> str:
+    """Compile libtcs.so (or, with bounds_check, libtcs_bc.so) and return its path."""
+    if bounds_check:
+        return _build(os.path.join(BUILD, "bc"), LIB_BC, force, verbose, ["-DTCS_BOUNDS_CHECK"] + (extra or []))
+    return _build(BUILD, LIB, force, verbose, extra)
+
+
+def _build(BUILD: str, LIB: str, force: bool, verbose: bool, extra: list[str] | None) -> str:
     os.makedirs(BUILD, exist_ok=True)
     hdrs = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(ROOT, "include", "tcs.h")]
     objs, jobs = [], []
@@ -84,5 +94,6 @@ if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("--force", action="store_true")
     ap.add_argument("--verbose", action="store_true")
+    ap.add_argument("--bounds-check", action="store_true", help="build libtcs_bc.so with index checks")
     a = ap.parse_args()
-    print(build(force=a.force, verbose=a.verbose))
+    print(build(force=a.force, verbose=a.verbose, bounds_check=a.bounds_check))

@@ -70,6 +70,26 @@ static const char *const k_names[K_COUNT] = {
 
 const char *kernel_name(int kid) { return (kid >= 0 && kid < K_COUNT) ? k_names[kid] : "?"; }
 
+// The reference's stage timers (main.f90:55-72: timer_str(1..18), stamped
+// after every call of the time loop, :129-221) and the timer each kernel's
+// work falls under.  The property evaluation of mpi_thermal_coeffi (1) is
+// fused into the thermal sweeps (2), the pseudo-update (9) into the pressure
+// right-hand side (10), the ghost-cell updates (13) into the stores of the
+// producing kernels, and mpi_Post_CFL (16) into the diagnostics kernel (15),
+// so those timers count no kernels; 0 marks kernels outside the time loop.
+static const char *const k_timer_names[19] = {
+    "", "[Main] Thermal coeff", "[Main] Thermal solve", "[Main] Momentum coeff", "[Main] Momentum solvedU",
+    "[Main] Momentum solvedV", "[Main] Momentum solvedW", "[Main] Momentum blockLdV", "[Main] Momentum blockLdU",
+    "[Main] Momentum updatePseudoUVW", "[Main] Pressure RHS", "[Main] Pressure PoissonSolve",
+    "[Main] Pressure projection", "[Main] Update GhostCell", "[Main] Clean coeff", "[Main] Post div",
+    "[Main] Post CFL", "[Main] Misc operation", "[Main] File write"};
+static const int k_timer_of[K_COUNT] = {
+    2, 2, 2, 3,                       // thermal_z, thermal_x, thermal_y, momentum_coeffi
+    4, 4, 4, 5, 5, 5, 6, 6, 6,        // du_*, dv_*, dw_*
+    7, 8, 9, 10, 11, 11, 11,          // blockld_v, blockld_u, pseudo_update, prhs_fftx, fftz_fwd, modal_tdma, mean
+    11, 11, 11, 12, 12, 15, 15, 0};   // fftz_inv, ifftx, dp_wall, projection, p_wall, post, finalize, tdma_api
+static_assert(sizeof(k_timer_of) / sizeof(int) == K_COUNT, "one timer per kernel");
+
 // ---------------------------------------------------------------------------
 // probes: CUDA event pairs on the launching stream
 // ---------------------------------------------------------------------------
@@ -374,6 +394,26 @@ const char *tcs_last_error(void) { return g_err.c_str(); }
 int tcs_kernel_count(void) { return K_COUNT; }
 unsigned long long tcs_launch_count(void) { return g_launches; }
 const char *tcs_kernel_name(int kid) { return kernel_name(kid); }
+int tcs_bounds_checked(void)
+{
+#ifdef TCS_BOUNDS_CHECK
+    return 1;
+#else
+    return 0;
+#endif
+}
+
+int tcs_bounds_violations(tcs_ctx *c, double *count)
+{
+    if (!c || !count) return set_err(TCS_ERR_ARG, "null argument");
+    cudaSetDevice(c->cfg.device);
+    CK(cudaMemcpyAsync(count, c->cx.g.scal + S_OOB, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return TCS_OK;
+}
+
+int tcs_timer_of_kernel(int kid) { return (kid >= 0 && kid < K_COUNT) ? k_timer_of[kid] : -1; }
+const char *tcs_timer_name(int timer) { return (timer >= 1 && timer <= 18) ? k_timer_names[timer] : nullptr; }
 
 int tcs_create(const tcs_config *cfg, tcs_ctx **out)
 {
@@ -427,7 +467,7 @@ int tcs_create(const tcs_config *cfg, tcs_ctx **out)
     g.d1 = g.m1; g.d2 = g.m2; g.d3 = g.m3;
     const size_t NP = (size_t)g.NP;
     c->cx.h1p = N1 / 2 + 1;
-    if (!r) r = dalloc(c, &g.scal, (size_t)S_NSCAL);
+    if (!r) r = dalloc(c, &g.scal, (size_t)S_NALLOC);
     c->partials = post_partial_count();
     if (!r) r = dalloc(c, &c->cx.f.part, (size_t)c->partials);
     c->cx.f.hist_cap = 100000;
@@ -1108,12 +1148,28 @@ int tcs_probe_reset(tcs_ctx *c)
 // ---- PaScaL_TDMA ------------------------------------------------------------
 } // extern "C"
 
-struct tcs_tdma_plan {
-    int n_sys;
+// A plan borrows a (stream, device staging buffer) slot from a per-process
+// pool and returns it when destroyed.  The reference creates and destroys a
+// plan around every sweep (module_solve_thermal.f90:364-366 and every solve of
+// module_solve_momentum.f90 and module_solve_pressure.f90), so a caller that
+// keeps the reference's solvers and swaps in only PaScaL_TDMA would otherwise
+// pay a stream creation, a cudaMalloc and a cudaFree per sweep; with the pool
+// the staging grows to the largest system seen on the device and stays.
+// Slots are per device; a slot is used by one plan at a time, so plans alive
+// at the same time (other host threads) stage through different buffers.
+struct TdmaSlot {
     int device;
     cudaStream_t stream;
     double *buf;
     size_t cap;
+    bool busy;
+};
+static std::mutex g_tdma_mu;
+static std::vector<TdmaSlot *> g_tdma_slots;
+
+struct tcs_tdma_plan {
+    int n_sys;
+    TdmaSlot *slot;
 };
 
 extern "C" {
@@ -1122,10 +1178,26 @@ int tcs_tdma_plan_many_create(tcs_tdma_plan **plan, int n_sys, int myrank, int n
 {
     if (!plan || n_sys < 1) return set_err(TCS_ERR_ARG, "bad plan arguments");
     if (nprocs != 1 || myrank != 0) return set_err(TCS_ERR_UNSUPPORTED, "one GPU holds the whole line: nprocs must be 1");
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    TdmaSlot *sl = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_tdma_mu);
+        for (TdmaSlot *t : g_tdma_slots)
+            if (!t->busy && t->device == dev) { sl = t; break; }
+        if (!sl) {
+            sl = new TdmaSlot{dev, nullptr, nullptr, 0, false};
+            if (cudaStreamCreateWithFlags(&sl->stream, cudaStreamNonBlocking) != cudaSuccess) {
+                delete sl;
+                return set_err(TCS_ERR_CUDA, "stream");
+            }
+            g_tdma_slots.push_back(sl);
+        }
+        sl->busy = true;
+    }
     tcs_tdma_plan *p = new tcs_tdma_plan();
-    p->n_sys = n_sys; p->buf = nullptr; p->cap = 0;
-    cudaGetDevice(&p->device);
-    if (cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking) != cudaSuccess) { delete p; return set_err(TCS_ERR_CUDA, "stream"); }
+    p->n_sys = n_sys;
+    p->slot = sl;
     *plan = p;
     return TCS_OK;
 }
@@ -1133,9 +1205,11 @@ int tcs_tdma_plan_many_create(tcs_tdma_plan **plan, int n_sys, int myrank, int n
 int tcs_tdma_plan_many_destroy(tcs_tdma_plan *p)
 {
     if (!p) return set_err(TCS_ERR_ARG, "null plan");
-    cudaStreamSynchronize(p->stream);
-    if (p->buf) cudaFree(p->buf);
-    cudaStreamDestroy(p->stream);
+    cudaStreamSynchronize(p->slot->stream);
+    {
+        std::lock_guard<std::mutex> lk(g_tdma_mu);
+        p->slot->busy = false;
+    }
     delete p;
     return TCS_OK;
 }
@@ -1144,34 +1218,35 @@ static int tdma_solve(tcs_tdma_plan *p, double *A, double *B, double *C, double 
 {
     if (!p || !A || !B || !C || !D) return set_err(TCS_ERR_ARG, "null argument");
     if (n_sys != p->n_sys || n_row < 2) return set_err(TCS_ERR_ARG, "n_sys must match the plan and n_row >= 2");
-    cudaSetDevice(p->device);
+    TdmaSlot *sl = p->slot;
+    cudaSetDevice(sl->device);
     cudaPointerAttributes at;
     bool dev = cudaPointerGetAttributes(&at, D) == cudaSuccess && at.type == cudaMemoryTypeDevice;
     cudaGetLastError();
     const size_t n = (size_t)n_sys * n_row;
     if (dev) {
-        launch_tdma_many(A, B, C, D, n_sys, n_row, cyclic, p->stream);
+        launch_tdma_many(A, B, C, D, n_sys, n_row, cyclic, sl->stream);
         if (take_launch_error()) return TCS_ERR_CUDA;
-        CK(cudaStreamSynchronize(p->stream));
+        CK(cudaStreamSynchronize(sl->stream));
         return TCS_OK;
     }
-    if (p->cap < 4 * n) {
-        if (p->buf) cudaFree(p->buf);
-        p->buf = nullptr; p->cap = 0;
-        CK(cudaMalloc(&p->buf, 4 * n * sizeof(double)));
-        p->cap = 4 * n;
+    if (sl->cap < 4 * n) {
+        if (sl->buf) cudaFree(sl->buf);
+        sl->buf = nullptr; sl->cap = 0;
+        CK(cudaMalloc(&sl->buf, 4 * n * sizeof(double)));
+        sl->cap = 4 * n;
     }
-    double *dA = p->buf, *dB = dA + n, *dC = dB + n, *dD = dC + n;
-    CK(cudaMemcpyAsync(dA, A, n * sizeof(double), cudaMemcpyHostToDevice, p->stream));
-    CK(cudaMemcpyAsync(dB, B, n * sizeof(double), cudaMemcpyHostToDevice, p->stream));
-    CK(cudaMemcpyAsync(dC, C, n * sizeof(double), cudaMemcpyHostToDevice, p->stream));
-    CK(cudaMemcpyAsync(dD, D, n * sizeof(double), cudaMemcpyHostToDevice, p->stream));
-    launch_tdma_many(dA, dB, dC, dD, n_sys, n_row, cyclic, p->stream);
+    double *dA = sl->buf, *dB = dA + n, *dC = dB + n, *dD = dC + n;
+    CK(cudaMemcpyAsync(dA, A, n * sizeof(double), cudaMemcpyHostToDevice, sl->stream));
+    CK(cudaMemcpyAsync(dB, B, n * sizeof(double), cudaMemcpyHostToDevice, sl->stream));
+    CK(cudaMemcpyAsync(dC, C, n * sizeof(double), cudaMemcpyHostToDevice, sl->stream));
+    CK(cudaMemcpyAsync(dD, D, n * sizeof(double), cudaMemcpyHostToDevice, sl->stream));
+    launch_tdma_many(dA, dB, dC, dD, n_sys, n_row, cyclic, sl->stream);
     if (take_launch_error()) return TCS_ERR_CUDA;
-    CK(cudaMemcpyAsync(A, dA, n * sizeof(double), cudaMemcpyDeviceToHost, p->stream));
-    CK(cudaMemcpyAsync(C, dC, n * sizeof(double), cudaMemcpyDeviceToHost, p->stream));
-    CK(cudaMemcpyAsync(D, dD, n * sizeof(double), cudaMemcpyDeviceToHost, p->stream));
-    CK(cudaStreamSynchronize(p->stream));
+    CK(cudaMemcpyAsync(A, dA, n * sizeof(double), cudaMemcpyDeviceToHost, sl->stream));
+    CK(cudaMemcpyAsync(C, dC, n * sizeof(double), cudaMemcpyDeviceToHost, sl->stream));
+    CK(cudaMemcpyAsync(D, dD, n * sizeof(double), cudaMemcpyDeviceToHost, sl->stream));
+    CK(cudaStreamSynchronize(sl->stream));
     return TCS_OK;
 }
 

@@ -69,6 +69,20 @@ enum : int {
     S_DT = 0, S_TIME, S_CFL, S_MAXDIV, S_NUBOT, S_NUTOP, S_KE, S_BLOWUP, S_AVER,
     S_STEP, S_FIXED_DT, S_NSCAL
 };
+// One more device double past the public scalars: in a build with
+// -DTCS_BOUNDS_CHECK, the number of out-of-range indices the kernels met
+// (each one recorded here and its access redirected to a valid cell instead of
+// made; the stand-in for a memory checker).  It stays 0 in the normal build.
+enum : int { S_OOB = S_NSCAL, S_NALLOC };
+
+#if defined(TCS_BOUNDS_CHECK) && defined(__CUDA_ARCH__)
+#define TCS_OOB(scal, bad, fix)                          \
+    do {                                                 \
+        if (bad) { atomicAdd((scal) + S_OOB, 1.0); fix; } \
+    } while (0)
+#else
+#define TCS_OOB(scal, bad, fix) do { } while (0)
+#endif
 
 template <class R>
 struct GridT {
@@ -121,13 +135,19 @@ inline FastDiv make_fastdiv(unsigned d)
 template <class R>
 __host__ __device__ __forceinline__ long long ix(const GridT<R> &g, int i, int j, int k)
 {
+    TCS_OOB(g.scal, (unsigned)i > (unsigned)(g.N1 + 1) || (unsigned)j > (unsigned)(g.N2 + 1) || (unsigned)k > (unsigned)(g.N3 + 1),
+            (i = 1, j = 1, k = 1));
     return (long long)i + (long long)g.P1 * ((long long)j + (long long)g.P2 * (long long)k);
 }
 
 // 2-D (j,k) tables: Mu and invRho are constant along i (module_solve_momentum.f90:156-171
 // assigns whole rows Mu(:,j,k) inside the i loop, leaving f(T(n1sub,j,k))).
 template <class R>
-__host__ __device__ __forceinline__ int ix2(const GridT<R> &g, int j, int k) { return j + g.P2 * k; }
+__host__ __device__ __forceinline__ int ix2(const GridT<R> &g, int j, int k)
+{
+    TCS_OOB(g.scal, (unsigned)j > (unsigned)(g.N2 + 1) || (unsigned)k > (unsigned)(g.N3 + 1), (j = 1, k = 1));
+    return j + g.P2 * k;
+}
 
 // Read-only loads through the non-coherent cache.
 template <class V>
@@ -774,6 +794,7 @@ __device__ __forceinline__ void line_block(const Prob &prob, const LinePlan &lp)
     }
     __syncthreads();
     auto put = [&](int l, int r) {
+        TCS_OOB(prob.g.scal, (unsigned)l >= (unsigned)TL || (unsigned)r >= (unsigned)n, return);
         const int pos = l * LS + spos[r];
         Coef<R, NR> cf;
         if (prob.line_ok(l)) {
@@ -868,6 +889,7 @@ __device__ __forceinline__ void line_block(const Prob &prob, const LinePlan &lp)
     __syncthreads();
     auto out = [&](int l, int r) {
         if (!prob.line_ok(l)) return;
+        TCS_OOB(prob.g.scal, (unsigned)l >= (unsigned)TL || (unsigned)r >= (unsigned)n, return);
         const int pos = l * LS + spos[r];
         R x[NR];
 #pragma unroll

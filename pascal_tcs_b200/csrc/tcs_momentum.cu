@@ -223,6 +223,28 @@ struct DUY {
 // by the last stage-1 iteration (i=N1, j=N2, k=N3); the y stage scales the
 // upper coefficient by jvp = jS_BC(j-1) and the lower one by jvm = jS_BC(j+1).
 // ---------------------------------------------------------------------------
+// The x difference of U's differences along d (y for solvedV, z for solvedW):
+//   (mu2 (U(i+1) - U(i+1, d-1)) - mu1 (U(i) - U(i, d-1))) rdm rdx1
+// (viscous_v21 and viscous_w31, module_solve_momentum.f90:664-665, 694 and
+// :1017-1018, 1052).  U is far larger than
+// V and W and varies slowly, so both differences cancel: in the FP32 form,
+// computed from U's FP32 high word alone, this term carried U's storage
+// rounding (6e-8 of U) into dV and dW at 1e-6..6e-6 of their size (one stage
+// on the 64^3 case).  The FP32 form therefore forms it in FP64 from U's high
+// and low words; the FP64 form keeps the reference's expression.
+template <class R>
+__device__ __forceinline__ R cross_diff(R mu1, R mu2, R dud1, R dud2, R rdm, R rdx, const R *Ulo, long long c, long long sd,
+                                        R Uc, R Um, R Uxp, R Uxpm)
+{
+    if constexpr (HasLo<R>::on) {
+        const double d1 = ((double)Uc - (double)Um) + ((double)ld(Ulo + c) - (double)ld(Ulo + c - sd));
+        const double d2 = ((double)Uxp - (double)Uxpm) + ((double)ld(Ulo + c + 1) - (double)ld(Ulo + c + 1 - sd));
+        return (R)(((double)mu2 * d2 - (double)mu1 * d1) * (double)rdm * (double)rdx);
+    } else {
+        return (mu2 * dud2 - mu1 * dud1) * rdx;
+    }
+}
+
 template <class R, int ITEM = 0>
 struct DVZ {
     using Real = R;
@@ -284,7 +306,7 @@ struct DVZ {
         const R vv1 = (mu2 * dvdx2 - mu1 * dvdx1) * rdx1[i];
         const R vv2 = (Mjk * dvdy4 - Mjmk * dvdy3) * rdmx2[j];
         const R vv3 = (mu6 * dvdz6 - mu5 * dvdz5) * rdx3[k];
-        const R vv21 = (mu2 * dudy2 - mu1 * dudy1) * rdx1[i];
+        const R vv21 = cross_diff(mu1, mu2, dudy1, dudy2, rdmx2[j], rdx1[i], f.Ulo, c, sj, Uc, Uym, Uxp, Uxpym);
         const R vv23 = (mu6 * dwdy6 - mu5 * dwdy5) * rdx3[k];
         // The reduced right-hand side (see DUZ); the y part keeps the
         // reference's form on the planes next to the walls (j = 2, N2).
@@ -475,7 +497,7 @@ struct DWZ {
         const R vw1 = (mu2 * dwdx2 - mu1 * dwdx1) * rdx1[i];
         const R vw2 = (mu4 * dwdy4 - mu3 * dwdy3) * rdx2[j];
         const R vw3 = (Mjk * dwdz6 - Mjkm * dwdz5) * rdmx3[k];
-        const R vw31 = (mu2 * dudz2 - mu1 * dudz1) * rdx1[i];
+        const R vw31 = cross_diff(mu1, mu2, dudz1, dudz2, rdmx3[k], rdx1[i], f.Ulo, c, sk, Uc, Uzm, Uxp, Uxpzm);
         const R vw32 = (mu4 * dvdz4 - mu3 * dvdz3) * rdx2[j];
         // The reduced right-hand side (see DUZ); the y part keeps the
         // reference's form on the wall-adjacent planes (j = 1, N2).

@@ -139,6 +139,8 @@ __device__ C *block_fft(C *buf0, C *buf1, int nl, int ldl, const FFTPlan &fp, co
 template <class R>
 __device__ __forceinline__ long long sidx(const GridT<R> &g, int h1p, int kx, int j, int kz)
 {
+    TCS_OOB(g.scal, (unsigned)kx >= (unsigned)h1p || (unsigned)(j - 1) >= (unsigned)g.N2 || (unsigned)kz >= (unsigned)g.N3,
+            (kx = 0, j = 1, kz = 0));
     return (long long)kx + (long long)h1p * ((long long)(j - 1) + (long long)g.N2 * (long long)kz);
 }
 

@@ -14,7 +14,9 @@ import os
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libtcs.so")
+# TCS_LIBRARY selects another build of the library (the bounds-check build
+# libtcs_bc.so in its test); the default is the in-tree libtcs.so.
+LIB_PATH = os.environ.get("TCS_LIBRARY") or os.path.join(_HERE, "libtcs.so")
 
 FIELDS = {"T": 0, "U": 1, "V": 2, "W": 3, "P": 4, "dPhat": 5, "dP0": 6,
           "dU": 7, "dV": 8, "dW": 9, "dP": 10, "Mu": 11, "invRho": 12}
@@ -39,7 +41,8 @@ EXPORTS = [
     "tcs_post_div", "tcs_post_cfl", "tcs_step", "tcs_get_scalars", "tcs_get_history",
     "tcs_snapshot", "tcs_restore",
     "tcs_tdma_plan_many_create", "tcs_tdma_plan_many_destroy", "tcs_tdma_many_solve",
-    "tcs_tdma_many_solve_cycle", "tcs_tdma_many_solve_noalloc", "tcs_kernel_count", "tcs_launch_count", "tcs_measure_fp64_peak", "tcs_check_reciprocal", "tcs_kernel_name", "tcs_probe_enable",
+    "tcs_tdma_many_solve_cycle", "tcs_tdma_many_solve_noalloc", "tcs_kernel_count", "tcs_launch_count", "tcs_measure_fp64_peak", "tcs_check_reciprocal", "tcs_kernel_name", "tcs_timer_of_kernel", "tcs_timer_name", "tcs_bounds_checked",
+    "tcs_bounds_violations", "tcs_probe_enable",
     "tcs_probe_read", "tcs_probe_reset", "tcs_set_use_graph", "tcs_set_tuning", "tcs_get_tuning",
     "tcs_last_error", "tcs_precision", "tcs_ensemble_create", "tcs_ensemble_destroy", "tcs_ensemble_step",
     "tcs_ensemble_size", "tcs_ensemble_set_batched", "tcs_ensemble_form", "tcs_autotune", "tcs_write_continue", "tcs_read_continue", "tcs_extract_plane",
@@ -123,6 +126,10 @@ def load() -> ctypes.CDLL:
         "tcs_kernel_count": ([], ip),
         "tcs_launch_count": ([], ctypes.c_ulonglong),
         "tcs_kernel_name": ([ip], ctypes.c_char_p),
+        "tcs_timer_of_kernel": ([ip], ip),
+        "tcs_timer_name": ([ip], ctypes.c_char_p),
+        "tcs_bounds_checked": ([], ip),
+        "tcs_bounds_violations": ([vp, dp], ip),
         "tcs_probe_enable": ([vp, ctypes.c_uint64], ip),
         "tcs_probe_read": ([vp, ip, dp, ctypes.POINTER(ip)], ip),
         "tcs_probe_reset": ([vp], ip),
@@ -173,6 +180,28 @@ def _check(r: int, where: str) -> None:
 def launch_count() -> int:
     """Kernels launched by libtcs in this process (CUDA-graph replays included)."""
     return int(load().tcs_launch_count())
+
+
+def timer_of_kernel() -> dict:
+    """kernel name -> the reference's stage timer label (main.f90:55-72) its
+    work falls under (None for kernels outside the time loop)."""
+    L = load()
+    out = {}
+    for k, name in enumerate(kernel_names()):
+        t = L.tcs_timer_of_kernel(k)
+        out[name] = L.tcs_timer_name(t).decode() if t > 0 else None
+    return out
+
+
+def bounds_checked() -> bool:
+    """Whether the loaded library is the bounds-check build (libtcs_bc.so)."""
+    return bool(load().tcs_bounds_checked())
+
+
+def timer_names() -> list[str]:
+    """The reference's 18 stage-timer labels, in order (main.f90:55-72)."""
+    L = load()
+    return [L.tcs_timer_name(t).decode() for t in range(1, 19)]
 
 
 def kernel_names() -> list[str]:
@@ -248,6 +277,12 @@ class Solver:
         out = np.empty((len(fields), nb, na))
         _check(load().tcs_extract_plane(self._h, int(axis), int(index), len(fields), ids, _dptr(out)), "extract_plane")
         return out
+
+    def bounds_violations(self) -> int:
+        """Out-of-range indices the kernels met so far (bounds-check build; 0 otherwise)."""
+        v = ctypes.c_double()
+        _check(load().tcs_bounds_violations(self._h, ctypes.byref(v)), "tcs_bounds_violations")
+        return int(v.value)
 
     @property
     def precision(self) -> int:

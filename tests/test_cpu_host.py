@@ -33,6 +33,27 @@ def test_kernel_names(tcs):
     assert len(names) == len(set(names)) and "thermal_z" in names and "projection" in names
 
 
+def test_stage_timers_follow_the_reference_labels(tcs):
+    # main.f90:55-72: the 18 timer labels, and every kernel of the time loop
+    # under the timer of the routine whose work it does
+    ref = ["Thermal coeff", "Thermal solve", "Momentum coeff", "Momentum solvedU", "Momentum solvedV",
+           "Momentum solvedW", "Momentum blockLdV", "Momentum blockLdU", "Momentum updatePseudoUVW", "Pressure RHS",
+           "Pressure PoissonSolve", "Pressure projection", "Update GhostCell", "Clean coeff", "Post div",
+           "Post CFL", "Misc operation", "File write"]
+    assert tcs.timer_names() == ["[Main] " + r for r in ref]
+    m = tcs.timer_of_kernel()
+    assert set(m) == set(tcs.kernel_names())
+    want = {"thermal_z": "Thermal solve", "du_y": "Momentum solvedU", "dv_x": "Momentum solvedV",
+            "dw_z": "Momentum solvedW", "momentum_coeffi": "Momentum coeff", "blockld_v": "Momentum blockLdV",
+            "blockld_u": "Momentum blockLdU", "pseudo_update": "Momentum updatePseudoUVW", "prhs_fftx": "Pressure RHS",
+            "fftz_fwd": "Pressure PoissonSolve", "modal_tdma": "Pressure PoissonSolve", "ifftx": "Pressure PoissonSolve",
+            "projection": "Pressure projection", "post": "Post div", "tdma_api": None}
+    for k, v in want.items():
+        assert m[k] == (None if v is None else "[Main] " + v), k
+    L = tcs.load()
+    assert L.tcs_timer_of_kernel(-1) == -1 and L.tcs_timer_name(0) is None and L.tcs_timer_name(19) is None
+
+
 @pytest.mark.parametrize("cfg,code", [(dict(n1m=2), 1), (dict(n1m=14), 3), (dict(n3m=22), 3)])
 def test_create_rejects_bad_configuration_without_touching_the_gpu(tcs, cfg, code):
     with pytest.raises(tcs.TcsError) as ei:

@@ -95,12 +95,12 @@ RESET_EVERY = {f"{k}_{form}": n for k, n in (("rb256_water", 8), ("rb512_water",
 
 # Compulsory-traffic model: arrays each kernel must stream once (reads +
 # writes) per interior cell; properties and tridiagonal coefficients are
-# recomputed, 1-D metrics and ghosts ignored.  Whole step: 109 arrays at 8 B
-# (872 B per cell-step) in the FP64 form.  The FP32-mixed form stores every
-# array in FP32 (its FP64 parts live in registers and shared memory) and adds
-# the velocity's low words: read and written by the pressure right-hand side
-# (6) and the projection (6), read by the diagnostics (3), so 124 arrays at
-# 4 B = 496 B per cell-step.
+# recomputed, 1-D metrics, 2-D property tables and ghosts ignored.  Whole step:
+# 109 arrays at 8 B (872 B per cell-step) in the FP64 form.  The FP32-mixed
+# form stores every array in FP32 (its FP64 parts live in registers and shared
+# memory) and adds the velocity's low words: read and written by the pressure
+# right-hand side (6) and the projection (6), read by the diagnostics (3), so
+# 124 arrays at 4 B = 496 B per cell-step.
 STEP_ARRAYS = 109
 LO_ARRAYS = {"prhs_fftx": 6, "projection": 6, "post": 3}
 

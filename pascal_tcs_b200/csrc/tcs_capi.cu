@@ -481,6 +481,11 @@ int tcs_create(const tcs_config *cfg, tcs_ctx **out)
         for (R **p : fl) if (!r) r = dalloc(c, p, NP);
         if (!r) r = dalloc(c, &F.Mu2, (size_t)(N2 + 2) * (N3 + 2));
         if (!r) r = dalloc(c, &F.iR2, (size_t)(N2 + 2) * (N3 + 2));
+        if (HasLo<R>::on) {
+            if (!r) r = dalloc(c, &F.iR2d, (size_t)(N2 + 2) * (N3 + 2));
+        } else {
+            F.iR2d = (double *)F.iR2;
+        }
         if (!r) r = dalloc(c, &F.S, (size_t)c->cx.h1p * N2 * N3);
         if (HasLo<R>::on) {
             R **lo[] = {&F.Ulo, &F.Vlo, &F.Wlo, &F.Unlo, &F.Vnlo, &F.Wnlo};
@@ -653,13 +658,14 @@ static int copy_field(tcs_ctx *c, int f, double *host, bool up, bool async)
     if (f == TCS_F_MU || f == TCS_F_INVRHO) {
         if (up) return set_err(TCS_ERR_ARG, "Mu and invRho are derived from T");
         std::vector<double> t((size_t)(g.N2 + 2) * (g.N3 + 2));
-        if (c->fp32) {
+        if (c->fp32 && f == TCS_F_MU) {
             std::vector<float> tf(t.size());
-            CK(cudaMemcpyAsync(tf.data(), f == TCS_F_MU ? c->cf.f.Mu2 : c->cf.f.iR2, tf.size() * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+            CK(cudaMemcpyAsync(tf.data(), c->cf.f.Mu2, tf.size() * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
             CK(cudaStreamSynchronize(c->stream));
             for (size_t q = 0; q < t.size(); q++) t[q] = tf[q];
-        } else {
-            CK(cudaMemcpyAsync(t.data(), f == TCS_F_MU ? c->cx.f.Mu2 : c->cx.f.iR2, t.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        } else {   // FP64: Mu, and invRho in both forms
+            const double *tab = f == TCS_F_MU ? c->cx.f.Mu2 : (c->fp32 ? c->cf.f.iR2d : c->cx.f.iR2d);
+            CK(cudaMemcpyAsync(t.data(), tab, t.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
         }
         CK(cudaStreamSynchronize(c->stream));
         for (int k = 0; k < g.N3 + 2; k++)

@@ -23,8 +23,15 @@ struct FieldsT {
     R *dU, *dV, *dW, *dP;
     // interior stage scratch (padded layout)
     R *scr;
-    // 2-D (j,k) property tables: Mu and invRho of mpi_momentum_coeffi
+    // 2-D (j,k) property tables: Mu and invRho of mpi_momentum_coeffi, in the
+    // field type (read by the line sweeps), and invRho in FP64 (the same array
+    // in the FP64 form).  invRho differs from 1 by about 1e-3 for water, and
+    // the pressure right-hand side and the projection use 1 - invRho: from an
+    // FP32 table those terms carried 6e-5 relative error, which left P 2-3e-5
+    // off the FP64 form after 5-8 steps of the 256^3 and 512^3 water cases
+    // (3-8e-6 with the FP64 table).
     R *Mu2, *iR2;
+    double *iR2d;
     // Poisson spectral work array: (h1p, N2, N3) complex, kx fastest
     cplx_t<R> *S;
     // modified wavenumbers and y coefficients of the modal solves (FP64 in both forms)

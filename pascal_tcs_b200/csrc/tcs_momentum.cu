@@ -18,17 +18,21 @@ namespace tcs {
 // ---------------------------------------------------------------------------
 // mpi_momentum_coeffi (:145-173) -> (j,k) tables from T(n1sub, j, k).
 // ---------------------------------------------------------------------------
+// Evaluated in FP64 in both forms; the FP32 form also keeps invRho in FP64
+// (FieldsT::iR2d) for the pressure right-hand side and the projection.
 template <class R>
 __global__ void momentum_coeffi_kernel(GridT<R> g, FieldsT<R> f)
 {
     const int j = blockIdx.x * blockDim.x + threadIdx.x, k = blockIdx.y;
     if (j > g.N2 + 1 || blown(g)) return;
-    const PhysT<R> &p = g.ph;
-    const R t1 = p.DeltaT * f.T[ix(g, g.N1 + 1, j, k)];
-    const R t2 = t1 * t1, t3 = t2 * t1, t4 = t3 * t1, t5 = t4 * t1;
-    const R ra = (p.a10 + p.a10 * (p.a11 * t1 + p.a12 * t2 + p.a13 * t3 + p.a14 * t4 + p.a15 * t5));
-    f.Mu2[ix2(g, j, k)] = ra * (p.d10 + p.d10 * (p.d11 * t1 + p.d12 * t2 + p.d13 * t3 + p.d14 * t4 + p.d15 * t5)) / p.Mu0;
-    f.iR2[ix2(g, j, k)] = p.Rho0 / ra;
+    const Phys &p = g.phd;
+    const double t1 = p.DeltaT * (double)f.T[ix(g, g.N1 + 1, j, k)];
+    const double t2 = t1 * t1, t3 = t2 * t1, t4 = t3 * t1, t5 = t4 * t1;
+    const double ra = (p.a10 + p.a10 * (p.a11 * t1 + p.a12 * t2 + p.a13 * t3 + p.a14 * t4 + p.a15 * t5));
+    const double ir = p.Rho0 / ra;
+    f.Mu2[ix2(g, j, k)] = (R)(ra * (p.d10 + p.d10 * (p.d11 * t1 + p.d12 * t2 + p.d13 * t3 + p.d14 * t4 + p.d15 * t5)) / p.Mu0);
+    f.iR2[ix2(g, j, k)] = (R)ir;
+    if constexpr (HasLo<R>::on) f.iR2d[ix2(g, j, k)] = ir;
 }
 
 template <class R>
@@ -223,28 +227,6 @@ struct DUY {
 // by the last stage-1 iteration (i=N1, j=N2, k=N3); the y stage scales the
 // upper coefficient by jvp = jS_BC(j-1) and the lower one by jvm = jS_BC(j+1).
 // ---------------------------------------------------------------------------
-// The x difference of U's differences along d (y for solvedV, z for solvedW):
-//   (mu2 (U(i+1) - U(i+1, d-1)) - mu1 (U(i) - U(i, d-1))) rdm rdx1
-// (viscous_v21 and viscous_w31, module_solve_momentum.f90:664-665, 694 and
-// :1017-1018, 1052).  U is far larger than
-// V and W and varies slowly, so both differences cancel: in the FP32 form,
-// computed from U's FP32 high word alone, this term carried U's storage
-// rounding (6e-8 of U) into dV and dW at 1e-6..6e-6 of their size (one stage
-// on the 64^3 case).  The FP32 form therefore forms it in FP64 from U's high
-// and low words; the FP64 form keeps the reference's expression.
-template <class R>
-__device__ __forceinline__ R cross_diff(R mu1, R mu2, R dud1, R dud2, R rdm, R rdx, const R *Ulo, long long c, long long sd,
-                                        R Uc, R Um, R Uxp, R Uxpm)
-{
-    if constexpr (HasLo<R>::on) {
-        const double d1 = ((double)Uc - (double)Um) + ((double)ld(Ulo + c) - (double)ld(Ulo + c - sd));
-        const double d2 = ((double)Uxp - (double)Uxpm) + ((double)ld(Ulo + c + 1) - (double)ld(Ulo + c + 1 - sd));
-        return (R)(((double)mu2 * d2 - (double)mu1 * d1) * (double)rdm * (double)rdx);
-    } else {
-        return (mu2 * dud2 - mu1 * dud1) * rdx;
-    }
-}
-
 template <class R, int ITEM = 0>
 struct DVZ {
     using Real = R;
@@ -306,7 +288,7 @@ struct DVZ {
         const R vv1 = (mu2 * dvdx2 - mu1 * dvdx1) * rdx1[i];
         const R vv2 = (Mjk * dvdy4 - Mjmk * dvdy3) * rdmx2[j];
         const R vv3 = (mu6 * dvdz6 - mu5 * dvdz5) * rdx3[k];
-        const R vv21 = cross_diff(mu1, mu2, dudy1, dudy2, rdmx2[j], rdx1[i], f.Ulo, c, sj, Uc, Uym, Uxp, Uxpym);
+        const R vv21 = (mu2 * dudy2 - mu1 * dudy1) * rdx1[i];
         const R vv23 = (mu6 * dwdy6 - mu5 * dwdy5) * rdx3[k];
         // The reduced right-hand side (see DUZ); the y part keeps the
         // reference's form on the planes next to the walls (j = 2, N2).
@@ -497,7 +479,7 @@ struct DWZ {
         const R vw1 = (mu2 * dwdx2 - mu1 * dwdx1) * rdx1[i];
         const R vw2 = (mu4 * dwdy4 - mu3 * dwdy3) * rdx2[j];
         const R vw3 = (Mjk * dwdz6 - Mjkm * dwdz5) * rdmx3[k];
-        const R vw31 = cross_diff(mu1, mu2, dudz1, dudz2, rdmx3[k], rdx1[i], f.Ulo, c, sk, Uc, Uzm, Uxp, Uxpzm);
+        const R vw31 = (mu2 * dudz2 - mu1 * dudz1) * rdx1[i];
         const R vw32 = (mu4 * dvdz4 - mu3 * dvdz3) * rdx2[j];
         // The reduced right-hand side (see DUZ); the y part keeps the
         // reference's form on the wall-adjacent planes (j = 1, N2).

@@ -30,7 +30,7 @@
 
 namespace tcs {
 
-#define IR(jj, kk) ld(f.iR2 + ix2(g, (jj), (kk)))
+#define IR(jj, kk) ld(f.iR2d + ix2(g, (jj), (kk)))   // FP64 invRho in both forms
 
 template <class C> struct CReal;
 template <> struct CReal<double2> { using T = double; };

@@ -5,15 +5,20 @@ The mixed form stores every field in FP32, so its results differ from the
 oracle's FP64 ones by rounding: the bars below are error bounds, stated per
 field and per diagnostic.
   * one stage from identical inputs: <= STAGE_TOL relative L2 on every output,
-    the pressure correction dP included (measured 2e-8..1.5e-6, except 5.8e-6
-    for dV of the 64^3 case, whose stencils see the velocity rounded to FP32
-    while dV itself is two orders of magnitude below U);
-  * the 64^3 constant-property case after 100 steps and a water case after 40:
-    <= RUN_TOL on the velocity vector, U, T, the Nusselt and kinetic-energy
-    series (measured 3e-8..6e-7), and <= SMALL_TOL on the components V and W
-    and on P (measured 1e-5..2.4e-5: these start from zero and stay two to
-    three orders of magnitude below U, so the FP32 rounding of the momentum
-    increments is a larger relative error);
+    the pressure correction dP included (measured 2e-8..1.4e-7, except
+    5.8e-6 for dV and 2.4e-6 for dW of the 64^3 case, whose stencils see U
+    rounded to FP32 while dV and dW are two orders of magnitude smaller);
+  * the benchmark's own cases at their step counts (256^3 water, 8 steps)
+    against the FP64 form: <= 1e-5 on every field and diagnostic (measured
+    U 7e-8, V 4e-6, W 4e-6, T 7e-8, P 8e-6);
+  * the 64^3 constant-property case after 100 steps and a 32^3 water case
+    after 40: <= RUN_TOL on the velocity vector, U, T, the Nusselt and
+    kinetic-energy series (measured 2e-8..4e-7), and the per-field bars of
+    ACCUM_TOL on V, W and P (measured V 1.0e-5 and 1.3e-5, W 9.5e-6 and
+    1.3e-5, P 2.0e-5 and 2.4e-5).  Those three grow with the step count: one
+    FP32 rounding of T in an FP64 run moves V, W and P by 1.2e-6 (measured on
+    the 256^3 and 512^3 cases), the mixed form stores T, U, V, W and P in FP32
+    every step, and the per-step offsets add up like a random walk;
   * determinism: graph and eager steps, the per-routine driver sequence and a
     snapshot replay give bit-identical results.
 """
@@ -24,7 +29,7 @@ pytestmark = pytest.mark.gpu
 
 STAGE_TOL = 1e-5
 RUN_TOL = 1e-5
-SMALL_TOL = 1e-4
+ACCUM_TOL = {"V": 2e-5, "W": 2e-5, "P": 4e-5}
 MIXED = 1
 
 
@@ -118,16 +123,16 @@ def test_mixed_64cube_100_steps_vs_oracle(tcs, oracle_mod):
     err = _run_vs_oracle(tcs, oracle_mod, 100, CASES[0])
     for k in ("velocity", "U", "T", "Nu_bot", "Nu_top", "KE"):
         assert err[k] <= RUN_TOL, f"{k}: {err[k]:.3e}"
-    for k in ("V", "W", "P"):
-        assert err[k] <= SMALL_TOL, f"{k}: {err[k]:.3e}"
+    for k, tol in ACCUM_TOL.items():
+        assert err[k] <= tol, f"{k}: {err[k]:.3e}"
 
 
 def test_mixed_water_40_steps_vs_oracle(tcs, oracle_mod):
     err = _run_vs_oracle(tcs, oracle_mod, 40, CASES[1])
     for k in ("velocity", "U", "T", "Nu_bot", "Nu_top", "KE"):
         assert err[k] <= RUN_TOL, f"{k}: {err[k]:.3e}"
-    for k in ("V", "W", "P"):
-        assert err[k] <= SMALL_TOL, f"{k}: {err[k]:.3e}"
+    for k, tol in ACCUM_TOL.items():
+        assert err[k] <= tol, f"{k}: {err[k]:.3e}"
 
 
 def test_mixed_storage(tcs):
@@ -193,3 +198,22 @@ def test_mixed_close_to_fp64_form(tcs):
     ha, hb = a.history(0, 10), b.history(0, 10)
     for col in (4, 5, 6):
         assert rel_l2(hb[:, col], ha[:, col]) <= RUN_TOL
+
+
+def test_mixed_256cube_water_every_field_within_1e_5(tcs):
+    # The benchmark's 256^3 water case (Ra 1e8, Pr 7, dt 2e-4, seed 1) at the
+    # step count the benchmark compares (it restarts from the seeded state
+    # every 8 steps): every field and diagnostic of the mixed form within 1e-5
+    # relative L2 of the FP64 form.
+    cfg = dict(n1m=256, n2m=256, n3m=256, gamma2=1.5, property_set=1, Pr=7.0, Ra=1e8, DeltaT=10.0,
+               dtStart=2e-4, fixed_dt=1, seed=1, noise_amp=0.01)
+    a, b = tcs.Solver(precision=0, **cfg), tcs.Solver(precision=MIXED, **cfg)
+    a.step(8); b.step(8)
+    err = {n: rel_l2(b.get(n)[I], a.get(n)[I]) for n in ("U", "V", "W", "T", "P")}
+    ha, hb = a.history(0, 8), b.history(0, 8)
+    for col, n in ((4, "Nu_bot"), (5, "Nu_top"), (6, "KE")):
+        err[n] = rel_l2(hb[:, col], ha[:, col])
+    print({k: f"{v:.2e}" for k, v in err.items()})
+    for k, v in err.items():
+        assert v <= 1e-5, f"{k}: {v:.3e}"
+    a.close(); b.close()

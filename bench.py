@@ -44,6 +44,10 @@ _CASES = {
     # profiling size: inputs still larger than L2, about 1.3 GB on the device
     "rb192_water": dict(n1m=192, n2m=192, n3m=192, gamma2=1.5, property_set=1, Pr=7.0, Ra=1e8,
                         DeltaT=10.0, dtStart=2e-4, fixed_dt=1, seed=1, noise_amp=0.01),
+    # profiling size of the 512^3 case's line shapes: the same 512-row z lines on
+    # 128^2 planes (67 MB per field, about 1.7 GB on the device)
+    "rbz512_water": dict(n1m=128, n2m=128, n3m=512, gamma2=2.0, property_set=1, Pr=7.0, Ra=1e9,
+                         DeltaT=10.0, dtStart=5e-5, fixed_dt=1, seed=2, noise_amp=0.01),
 }
 # precision 0: plain FP64; 1: FP32-mixed
 WORKLOADS = {f"{k}_{form}": dict(v, precision=prec) for k, v in _CASES.items()
@@ -90,7 +94,8 @@ ENSEMBLE_RESET = 8
 # ~1.6x per step at the bottom wall; the oracle restatement and this library stop at
 # the same step).  Their timed steps therefore restart from the seeded initial state,
 # kept on the device, every RESET_EVERY steps; the restore copies are timed too.
-RESET_EVERY = {f"{k}_{form}": n for k, n in (("rb256_water", 8), ("rb512_water", 5), ("rb192_water", 8))
+RESET_EVERY = {f"{k}_{form}": n for k, n in (("rb256_water", 8), ("rb512_water", 5), ("rb192_water", 8),
+                                             ("rbz512_water", 5))
                for form in ("fp64", "mixed")}
 
 # Compulsory-traffic model: arrays each kernel must stream once (reads +

@@ -581,22 +581,16 @@ def mixed_error(s64, s32, nsteps: int) -> dict:
     return out
 
 
-def run_ensemble(args, cfg: dict, workload: str) -> int:
+def ensemble_measure(P, torch, args, cfg: dict, workload: str, ws: int, rank: int, local: int) -> dict:
     """The batched ensemble: this rank's share of the cases (LPT by cell count)
     advanced together by one CUDA graph per step, against the same cases
-    stepped one at a time."""
-    ws, rank, local = dist_setup(args.gpus)
-    import torch
-    import pascal_tcs_b200 as P
-
-    torch.cuda.set_device(local)
+    stepped one at a time.  Returns the fields of the JSON line."""
     allcases = ensemble_cases(cfg["ensemble"], cfg["precision"])
     cases = lpt_shard(allcases, ws, rank)
     solvers = [P.Solver(device=local, **c) for c in cases]
     for s in solvers:
         s.snapshot()
     ens = P.Ensemble(solvers)
-    cells = sum(c["n1m"] * c["n2m"] * c["n3m"] for c in cases)
     reset = ENSEMBLE_RESET
 
     def grouped(k: int):
@@ -671,28 +665,40 @@ def run_ensemble(args, cfg: dict, workload: str) -> int:
     peak, peak_kind = measured_peaks()
     step_bytes = step_bytes_per_cell(esize) * total_cells
     achieved = step_bytes * args.steps / (ms * 1e-3) / 1e9
-    if rank == 0:
-        form = "FP32-mixed" if cfg["precision"] else "FP64 plain"
-        line = {"metric": ensemble_metric(cfg), "value": value,
-                "unit": "cell-steps/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
-                "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "strong" if ws > 1 else "weak",
-                "vs_baseline": None, "dtype": "f32+f64" if cfg["precision"] else "f64",
-                "data": "synthetic: seeded conduction profiles + uniform noise 0.01, zero velocity",
-                "config": ensemble_config(cfg, workload, ws),
-                "gpu_launches": launches,
-                "roofline": {"bound": "hbm", "kernel": "whole ensemble step", "achieved": achieved, "peak": peak,
-                             "unit": "GB/s", "frac": achieved / peak,
-                             "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
-                             "algorithmic_bytes_per_step": step_bytes, "traffic": None},
-                "form": {"chosen": "batched" if ens_form == 1 else "one branch per case",
-                         "measured_ms_per_step": {"one_branch_per_case": tune_br, "batched": tune_bat}},
-                "batched": {"value": bat, "ms_per_step": ms_bat / args.steps},
-                "one_branch_per_case": {"value": br, "ms_per_step": ms_br / args.steps},
-                "one_at_a_time": {"value": seq, "ms_per_step": ms_seq / args.steps},
-                "speedup_vs_one_at_a_time": value / seq,
-                "clocks": clk.summary(), "e2e": None, "cpu_baseline": None}
-        print(json.dumps(line))
     del ens
+    for s in solvers:
+        s.close()
+    return {"metric": ensemble_metric(cfg), "value": value,
+            "unit": "cell-steps/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "strong" if ws > 1 else "weak",
+            "vs_baseline": None, "dtype": "f32+f64" if cfg["precision"] else "f64",
+            "data": "synthetic: seeded conduction profiles + uniform noise 0.01, zero velocity",
+            "config": ensemble_config(cfg, workload, ws),
+            "gpu_launches": launches,
+            "roofline": {"bound": "hbm", "kernel": "whole ensemble step", "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak,
+                         "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                         "algorithmic_bytes_per_step": step_bytes, "traffic": None},
+            "form": {"chosen": "batched" if ens_form == 1 else "one branch per case",
+                     "measured_ms_per_step": {"one_branch_per_case": tune_br, "batched": tune_bat}},
+            "batched": {"value": bat, "ms_per_step": ms_bat / args.steps},
+            "one_branch_per_case": {"value": br, "ms_per_step": ms_br / args.steps},
+            "one_at_a_time": {"value": seq, "ms_per_step": ms_seq / args.steps},
+            "speedup_vs_one_at_a_time": value / seq,
+            "clocks": clk.summary()}
+
+
+def run_ensemble(args, cfg: dict, workload: str) -> int:
+    """The ensemble workloads (ens48_*) as the line's own workload."""
+    ws, rank, local = dist_setup(args.gpus)
+    import torch
+    import pascal_tcs_b200 as P
+
+    torch.cuda.set_device(local)
+    line = ensemble_measure(P, torch, args, cfg, workload, ws, rank, local)
+    if rank == 0:
+        line.update({"e2e": None, "cpu_baseline": None})
+        print(json.dumps(line))
     if ws > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
@@ -795,6 +801,10 @@ def main():
         del keep
 
     tdma = tdma_api_timing(P, torch) if (workload == "rb512_water_fp64" and not args.no_extra) else None
+    # the 48-case ensemble (FP64), as an extra key of the default run on one GPU
+    if extra is not None and ws == 1:
+        extra["ens48_fp64"] = ensemble_measure(P, torch, args, dict(WORKLOADS["ens48_fp64"]), "ens48_fp64", ws, rank,
+                                               local)
 
     base = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:

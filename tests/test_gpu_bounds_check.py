@@ -6,7 +6,8 @@ redirected to a valid cell, never made.  It stands in for a memory checker
 Makefile.inc:6-11).  The test runs that build in a fresh process over uneven
 sizes, both precisions, stretched and uniform grids, long lines, every
 launch-shape knob family, the per-routine driver sequence, an ensemble in
-both forms, the restart files and planes, and the PaScaL_TDMA interface, and
+both forms and a 26-case batched ensemble whose sweeps split over two
+multi-case launches, the restart files and planes, and the PaScaL_TDMA interface, and
 requires zero recorded violations (needs a B200)."""
 import os
 import subprocess
@@ -60,6 +61,21 @@ SCRIPT = textwrap.dedent("""
         e.step(2)
     for k, s in enumerate(ens):
         counts[f"ensemble case {{k}}"] = s.bounds_violations()
+    # 24 uneven cases per precision: more than one multi-case launch's parameter
+    # block holds (21 FP64 or 24 FP32 problems), so each batched sweep is split
+    rng = np.random.default_rng(3)
+    for prec in (0, 1):
+        big = [P.Solver(n1m=int(rng.choice([16, 20, 24])), n2m=int(rng.choice([12, 16, 24])),
+                        n3m=int(rng.choice([16, 20, 30])), property_set=int(k % 2), Pr=7.0, Ra=1e6, dtStart=5e-4,
+                        seed=k, precision=prec) for k in range(26)]
+        e2 = P.Ensemble(big)
+        e2.set_batched(1)
+        e2.step(3)
+        for k, s in enumerate(big):
+            counts[f"ensemble26 prec{{prec}} case {{k}}"] = s.bounds_violations()
+        e2.close()
+        for s in big:
+            s.close()
     rng = np.random.default_rng(1)
     for cyclic in (False, True):
         A = rng.uniform(-0.3, 0.3, (64, 500)); C = rng.uniform(-0.3, 0.3, (64, 500))

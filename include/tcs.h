@@ -241,9 +241,20 @@ int tcs_set_use_graph(tcs_ctx *ctx, int on);
  * TCS_TUNE_LONG_LINES picks where long strided lines run as one block per SM
  * (the same warps, lines fitted to 132 KiB of shared memory so that L1 keeps
  * 124 KiB) when the usual blocks would leave under 60 KiB of L1 or halve
- * their lines: 1 never, 2 the z sweeps (default), 4 the z and y sweeps. */
+ * their lines: 1 never, 2 the z sweeps (default), 4 the z and y sweeps.
+ * TCS_TUNE_Y_SOLVER picks the tridiagonal solver of the non-cyclic strided
+ * lines with FP64 rows: 1 the partitioned solver that every sweep uses
+ * (default: modified Thomas per lane with a parallel reduced-system solve,
+ * pascal_tdma.f90:487-578); 2 the plain Thomas elimination with one line per
+ * thread (tdmas.f90:27-50) for the FP64 form's y sweeps; 4 the same for the
+ * modal pressure solves too (FP64 rows in both forms).  2 and 4 keep c' and d'
+ * in a scratch buffer that setting the knob allocates ((1 + right-hand sides)
+ * x rows x lines doubles: 2.1 GB for the y sweeps and 2.4 GB for the modal
+ * solves at 512^3) and setting 1 frees.  Measured on B200: the one-line form
+ * is faster for the y sweeps at 512^3 (13-22% per sweep) and slower at 256^3,
+ * where 65536 lines leave the SMs short of threads. */
 enum { TCS_TUNE_TL_STRIDED = 0, TCS_TUNE_TL_CONTIG, TCS_TUNE_TL_MODAL, TCS_TUNE_FFT_LINES_X, TCS_TUNE_FFT_LINES_Z,
-       TCS_TUNE_LANES, TCS_TUNE_LONG_LINES, TCS_TUNE_COUNT };
+       TCS_TUNE_LANES, TCS_TUNE_LONG_LINES, TCS_TUNE_Y_SOLVER, TCS_TUNE_COUNT };
 int tcs_set_tuning(tcs_ctx *ctx, int knob, int value);
 int tcs_get_tuning(tcs_ctx *ctx, int knob, int *value);
 /* Autotuner (no reference counterpart): coordinate descent over every knob,

@@ -544,6 +544,8 @@ int tcs_create(const tcs_config *cfg, tcs_ctx **out)
     c->cx.fft_lines_z = N3 <= 256 ? 4 : (N3 <= 512 ? 2 : 1);
     c->cx.lanes = 32;
     c->cx.long_lines = 2;
+    c->cx.y_solver = 1;
+    c->cx.thomas_scr = nullptr;
     c->cx.probe = &c->probe;
     sync_shapes(c);
     {   // the FP32 context shares the grid, constants, scalars, tables and history
@@ -611,6 +613,7 @@ int tcs_destroy(tcs_ctx *c)
     if (c->stream) cudaStreamSynchronize(c->stream);
     for (auto &ge : c->graphs) cudaGraphExecDestroy(ge.exec);
     for (void *p : c->allocs) cudaFree(p);
+    if (c->cx.thomas_scr) cudaFree(c->cx.thomas_scr);
     if (c->io_host) cudaFreeHost(c->io_host);
     for (auto &v : c->probe.rec) for (auto &pr : v) { cudaEventDestroy(pr.first); cudaEventDestroy(pr.second); }
     for (cudaEvent_t e : c->probe.pool) cudaEventDestroy(e);
@@ -961,6 +964,29 @@ int tcs_set_tuning(tcs_ctx *c, int knob, int value)
     case TCS_TUNE_LONG_LINES:
         if (value > 4) return set_err(TCS_ERR_ARG, "long-line form: 1 never, 2 z sweeps, 4 z and y sweeps");
         x.long_lines = value; break;
+    case TCS_TUNE_Y_SOLVER: {
+        if (value > 4) return set_err(TCS_ERR_ARG, "y solver: 1 partitioned, 2 one line per thread (FP64 y sweeps), 4 also the modal solves");
+        // c', d' of every line of the largest one-line-per-thread launch: the FP64
+        // form's y sweeps (one right-hand side) and, with 4, the modal solves (two)
+        const size_t ny = (value >= 2 && !c->fp32) ? thomas_words(g.N2, g.N1, g.N3, 1) : 0;
+        const size_t words = std::max(ny, value == 4 ? thomas_words(g.N2, x.h1p, g.N3, 2) : (size_t)0);
+        if (x.thomas_scr) {
+            cudaStreamSynchronize(c->stream);
+            cudaFree(x.thomas_scr);
+            x.thomas_scr = nullptr;
+        }
+        if (words) {
+            void *q = nullptr;
+            const cudaError_t ce = cudaMalloc(&q, words * sizeof(double));
+            if (ce != cudaSuccess) {
+                cudaGetLastError();
+                x.y_solver = 1;
+                sync_shapes(c);
+                return set_err(TCS_ERR_NOMEM, std::string("y solver scratch: ") + cudaGetErrorString(ce));
+            }
+            x.thomas_scr = (double *)q;
+        }
+        x.y_solver = value; break; }
     default: return set_err(TCS_ERR_ARG, "unknown tuning knob");
     }
     sync_shapes(c);
@@ -982,6 +1008,7 @@ int tcs_get_tuning(tcs_ctx *c, int knob, int *value)
     case TCS_TUNE_FFT_LINES_Z: *value = x.fft_lines_z; break;
     case TCS_TUNE_LANES: *value = x.lanes; break;
     case TCS_TUNE_LONG_LINES: *value = x.long_lines; break;
+    case TCS_TUNE_Y_SOLVER: *value = x.y_solver; break;
     default: return set_err(TCS_ERR_ARG, "unknown tuning knob");
     }
     return TCS_OK;
@@ -1591,11 +1618,12 @@ void tune_load(const std::string &path)
     while (std::getline(in, line)) {
         std::istringstream ss(line);
         TuneKey k;
-        std::vector<int> v(TCS_TUNE_COUNT);
+        std::vector<int> v(TCS_TUNE_COUNT, 0);
         if (!(ss >> k.n1 >> k.n2 >> k.n3 >> k.prec)) continue;
-        bool ok = true;
-        for (int &x : v) ok = ok && (bool)(ss >> x);
-        if (ok) g_tune[k] = v;
+        int got = 0;
+        while (got < TCS_TUNE_COUNT && (ss >> v[got])) got++;
+        // lines written before the later knobs existed leave those knobs as they are (0)
+        if (got >= TCS_TUNE_LONG_LINES + 1) g_tune[k] = v;
     }
 }
 } // namespace
@@ -1639,7 +1667,7 @@ extern "C" int tcs_autotune(tcs_ctx *c, int trial_steps, const char *cache_path,
     int r;
     if (!best.empty()) {
         for (int k = 0; k < TCS_TUNE_COUNT; k++)
-            if ((r = tcs_set_tuning(c, k, best[k]))) return r;
+            if (best[k] && (r = tcs_set_tuning(c, k, best[k]))) return r;
         if (from_cache) *from_cache = 1;
         return TCS_OK;
     }

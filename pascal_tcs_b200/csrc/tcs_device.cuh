@@ -914,6 +914,59 @@ __global__ void __launch_bounds__(Prob::NT, Prob::MINB) line_solve_kernel(Prob p
     line_block(prob, lp);
 }
 
+// One line per thread: the plain Thomas elimination of a non-cyclic line with
+// FP64 rows (the sequential elimination of tdma_single and tdma_many,
+// PaScaL_TDMA/src/tdmas.f90:27-50 and 113-146), for the strided y lines and
+// the modal solves.  A block of THOMAS_TL threads takes THOMAS_TL consecutive
+// lines (the problem's TL is THOMAS_TL), thread l line l.  The forward sweep
+// builds each row with the problem's own build, keeps c' and d' of the current
+// row in registers and stores them for the back substitution in
+// scr[row][line] (consecutive threads, consecutive words: every store and load
+// of a warp is coalesced); the back substitution emits the rows from the last
+// to the first.  No shared memory and no barrier: the build's loads of the
+// next rows overlap the elimination of the current one.  scr holds
+// (1 + NRHS) x n x (all lines of the grid) doubles.
+template <class Prob>
+__global__ void __launch_bounds__(128) thomas_line_kernel(Prob prob, int n, double *__restrict__ scr)
+{
+    static_assert(std::is_same<typename Prob::Real, double>::value, "the one-line-per-thread solver takes FP64 rows");
+    constexpr int NR = Prob::NRHS;
+    if (prob.skip()) return;
+    const int l = threadIdx.x;
+    if (!prob.line_ok(l)) return;
+    const typename Prob::State st = prob.prepare();
+    const long long nl = (long long)gridDim.x * gridDim.y * blockDim.x;
+    const long long me = ((long long)blockIdx.y * gridDim.x + blockIdx.x) * blockDim.x + l;
+    double *const sc = scr + me, *const sd = scr + nl * n + me;
+    double cp = 0.0, dp[NR];
+#pragma unroll
+    for (int q = 0; q < NR; q++) dp[q] = 0.0;
+#pragma unroll 2
+    for (int r = 0; r < n; r++) {
+        const Coef<double, NR> cf = prob.build(l, r, st);
+        const double a = r ? cf.a : 0.0;
+        const double m = rcp_of<FastRcp<Prob>::on>(cf.b - a * cp);
+        cp = cf.c * m;
+#pragma unroll
+        for (int q = 0; q < NR; q++) dp[q] = (cf.d[q] - a * dp[q]) * m;
+        if (r < n - 1) {
+            sc[(long long)r * nl] = cp;
+#pragma unroll
+            for (int q = 0; q < NR; q++) sd[((long long)r * NR + q) * nl] = dp[q];
+        }
+    }
+    double x[NR];
+#pragma unroll
+    for (int q = 0; q < NR; q++) x[q] = dp[q];
+    prob.emit(l, n - 1, x, st);
+    for (int r = n - 2; r >= 0; r--) {
+        const double c = sc[(long long)r * nl];
+#pragma unroll
+        for (int q = 0; q < NR; q++) x[q] = sd[((long long)r * NR + q) * nl] - c * x[q];
+        prob.emit(l, r, x, st);
+    }
+}
+
 // The parameters of a multi-case line launch: the problems and plans of up to
 // K cases, held in the kernel-parameter space (32 KB) so that, as in
 // line_solve_kernel, the kernel reads their members as constant operands (a

@@ -39,6 +39,8 @@ struct Shapes {
     int fft_lines_x, fft_lines_z;
     int lanes;                                   // at most this many partitions (lanes) per line
     int long_lines;                              // one-block-per-SM form of long lines: 1 never, 2 z sweeps, 4 z and y sweeps
+    int y_solver;                                // FP64 y lines: 1 partitioned (line_block), 2 one line per thread for the y sweeps, 4 also the modal solves
+    double *thomas_scr;                          // c', d' of the one-line-per-thread solver (null unless y_solver asks for it)
     FFTPlan fp1, fp3;
     int h1p;
     double wall_ab, wall_bb, wall_at, wall_bt;   // Pbc_a, Pbc_b of the two walls
@@ -183,6 +185,41 @@ inline void launch_strided(const Shapes &cx, int n, bool cyclic, int nlines, int
         }
     }
     launch_lines(make(a.TL), a, dim3((nlines + a.TL - 1) / a.TL, gy), s, kid, cx);
+}
+
+// Lines per block of the one-line-per-thread solver (thomas_line_kernel).
+constexpr int THOMAS_TL = 128;
+
+// Doubles of c', d' scratch the one-line-per-thread solver needs for nlines
+// lines of n rows in gy block rows with nrhs right-hand sides.
+inline size_t thomas_words(int n, int nlines, int gy, int nrhs)
+{
+    return (size_t)(1 + nrhs) * n * ((size_t)(nlines + THOMAS_TL - 1) / THOMAS_TL) * THOMAS_TL * gy;
+}
+
+template <class P, class Make>
+inline void launch_thomas(const Shapes &cx, int n, int nlines, int gy, Make make, cudaStream_t s, int kid)
+{
+    probe_begin(cx, kid, s);
+    thomas_line_kernel<P><<<dim3((nlines + THOMAS_TL - 1) / THOMAS_TL, gy), THOMAS_TL, 0, s>>>(make(THOMAS_TL), n, cx.thomas_scr);
+    probe_end(cx, kid, s);
+    record_launch_error(kernel_name(kid));
+}
+
+// A y sweep (non-cyclic strided lines, nlines x gy of n rows): FP64 rows go
+// to the one-line-per-thread solver when the knob asks for it (y_solver 2 or
+// 4, scratch allocated), everything else to the partitioned line solver, in the
+// one-block-per-SM form where long_lines asks for it for the y sweeps.
+template <class P, class Make>
+inline void launch_y(const Shapes &cx, int n, int nlines, int gy, Make make, cudaStream_t s, int kid)
+{
+    if constexpr (std::is_same<typename P::Real, double>::value) {
+        if (cx.y_solver >= 2 && cx.thomas_scr) {
+            launch_thomas<P>(cx, n, nlines, gy, make, s, kid);
+            return;
+        }
+    }
+    launch_strided<P>(cx, n, false, nlines, gy, make, s, kid, cx.long_lines >= 4);
 }
 
 // ---------------------------------------------------------------------------

@@ -626,7 +626,7 @@ void launch_solve_du(const Ctx<R> &cx, cudaStream_t s)
     const GridT<R> &g = cx.g;
     launch_strided<DUZ<R>>(cx, g.N3, true, g.N1, g.N2, [&](int tl) { return DUZ<R>{g, cx.f, tl}; }, s, K_DU_Z, cx.long_lines >= 2);
     launch_x<DUX>(cx, g.N2, s, K_DU_X);
-    launch_strided<DUY<R>>(cx, g.N2, false, g.N1, g.N3, [&](int tl) { return DUY<R>{g, cx.f, tl}; }, s, K_DU_Y, cx.long_lines >= 4);
+    launch_y<DUY<R>>(cx, g.N2, g.N1, g.N3, [&](int tl) { return DUY<R>{g, cx.f, tl}; }, s, K_DU_Y);
 }
 
 template <class R>
@@ -635,7 +635,7 @@ void launch_solve_dv(const Ctx<R> &cx, cudaStream_t s)
     const GridT<R> &g = cx.g;
     launch_strided<DVZ<R>>(cx, g.N3, true, g.N1, g.N2 - 1, [&](int tl) { return DVZ<R>{g, cx.f, tl}; }, s, K_DV_Z, cx.long_lines >= 2);
     launch_x<DVX>(cx, g.N2 - 1, s, K_DV_X);
-    launch_strided<DVY<R>>(cx, g.N2 - 1, false, g.N1, g.N3, [&](int tl) { return DVY<R>{g, cx.f, tl}; }, s, K_DV_Y, cx.long_lines >= 4);
+    launch_y<DVY<R>>(cx, g.N2 - 1, g.N1, g.N3, [&](int tl) { return DVY<R>{g, cx.f, tl}; }, s, K_DV_Y);
 }
 
 template <class R>
@@ -644,7 +644,7 @@ void launch_solve_dw(const Ctx<R> &cx, cudaStream_t s)
     const GridT<R> &g = cx.g;
     launch_strided<DWZ<R>>(cx, g.N3, true, g.N1, g.N2, [&](int tl) { return DWZ<R>{g, cx.f, tl}; }, s, K_DW_Z, cx.long_lines >= 2);
     launch_x<DWX>(cx, g.N2, s, K_DW_X);
-    launch_strided<DWY<R>>(cx, g.N2, false, g.N1, g.N3, [&](int tl) { return DWY<R>{g, cx.f, tl}; }, s, K_DW_Y, cx.long_lines >= 4);
+    launch_y<DWY<R>>(cx, g.N2, g.N1, g.N3, [&](int tl) { return DWY<R>{g, cx.f, tl}; }, s, K_DW_Y);
 }
 
 // ---------------------------------------------------------------------------

@@ -529,6 +529,10 @@ template <class R>
 void launch_modal(const Ctx<R> &cx, cudaStream_t s)
 {
     const GridT<R> &g = cx.g;
+    if (cx.y_solver == 4 && cx.thomas_scr) {   // FP64 rows in both forms: the one-line-per-thread solver
+        launch_thomas<Modal<R>>(cx, g.N2, cx.h1p, g.N3, [&](int tl) { return Modal<R>{g, cx.f, tl, cx.h1p}; }, s, K_MODAL);
+        return;
+    }
     LinePlan pm = plan_for<Modal<R>>(g.N2, false, fit_tl<Modal<R>>(g.N2, false, cx.tl_modal, cx.lanes), cx.lanes);
     launch_lines(Modal<R>{g, cx.f, pm.TL, cx.h1p}, pm, dim3((cx.h1p + pm.TL - 1) / pm.TL, g.N3), s, K_MODAL, cx);
 }

@@ -47,12 +47,14 @@ SCRIPT = textwrap.dedent("""
             counts[f"case{{ci}} prec{{prec}}"] = g.bounds_violations()
             g.close()
     for knob, v in (("lanes", 4), ("tl_strided", 2), ("tl_contig", 1), ("tl_modal", 1), ("fft_lines_x", 1),
-                    ("fft_lines_z", 8), ("long_lines", 4)):
-        g = P.Solver(n1m=48, n2m=32, n3m=40, property_set=1, Pr=7.0, Ra=1e6, dtStart=5e-4)
-        g.set_tuning(knob, v)
-        g.step(2)
-        counts[f"{{knob}}={{v}}"] = g.bounds_violations()
-        g.close()
+                    ("fft_lines_z", 8), ("long_lines", 4), ("y_solver", 4)):
+        for prec in ((0, 1) if knob == "y_solver" else (0,)):
+            g = P.Solver(n1m=150 if knob == "y_solver" else 48, n2m=32, n3m=40, property_set=1, Pr=7.0, Ra=1e6,
+                         dtStart=5e-4, precision=prec)
+            g.set_tuning(knob, v)
+            g.step(2)
+            counts[f"{{knob}}={{v}} prec{{prec}}"] = g.bounds_violations()
+            g.close()
     ens = [P.Solver(n1m=n1, n2m=n2, n3m=n3, property_set=1, Pr=7.0, Ra=1e6, dtStart=5e-4, precision=prec)
            for (n1, n2, n3, prec) in ((16, 24, 20, 0), (32, 16, 12, 0), (24, 20, 16, 1), (20, 12, 30, 1))]
     e = P.Ensemble(ens)

@@ -130,6 +130,25 @@ def test_long_lines_match_oracle(tcs, oracle_mod):
     assert g.tuning()["long_lines"] == 4
 
 
+def test_one_line_per_thread_y_solver_matches_oracle(tcs, oracle_mod):
+    # the FP64 y sweeps and the modal solves on the plain Thomas elimination
+    # with one line per thread (y_solver 4); 150 lines along x leave the last
+    # block of 128 lines part-filled, water properties
+    cfg = dict(n1m=150, n2m=40, n3m=24, gamma2=1.5, property_set=1, Pr=7.0, Ra=1e7, DeltaT=10.0,
+               dtStart=2e-4, fixed_dt=1, seed=5)
+    g, o = _pair(tcs, oracle_mod, **cfg)
+    g.set_tuning("y_solver", 4)
+    g.step(12)
+    hd = o.step(12)
+    hg = g.history(0, 12)
+    err = {n: rel_l2(g.get(n)[1:-1, 1:-1, 1:-1], o.get(n)[1:-1, 1:-1, 1:-1]) for n in ("U", "V", "W", "T", "P")}
+    for col, n in ((4, "Nu_bot"), (5, "Nu_top"), (6, "KE")):
+        err[n] = rel_l2(hg[:, col], hd[:, col])
+    print({k: f"{v:.2e}" for k, v in err.items()})
+    for k, v in err.items():
+        assert v <= RUN_TOL, f"{k}: rel L2 {v:.3e}"
+
+
 def test_64cube_constant_properties_100_steps(tcs, oracle_mod):
     # The plain FP64 Rayleigh-Benard channel case: 64^3, Ra=1e5, Pr=0.71, dt=1e-3, seed 0.
     err, g, _ = _run_compare(tcs, oracle_mod, 100, n1m=64, n2m=64, n3m=64, Ra=1e5, Pr=0.71,

@@ -37,7 +37,7 @@ def test_autotune_keeps_state_and_caches(tcs, tmp_path):
 
 @pytest.mark.parametrize("knob,value", [("lanes", 8), ("lanes", 16), ("tl_strided", 2), ("tl_contig", 16),
                                         ("tl_modal", 1), ("fft_lines_x", 1), ("fft_lines_z", 8),
-                                        ("long_lines", 1), ("long_lines", 4)])
+                                        ("long_lines", 1), ("long_lines", 4), ("y_solver", 2), ("y_solver", 4)])
 def test_every_knob_setting_gives_the_same_step(tcs, knob, value):
     a, b = tcs.Solver(**CFG), tcs.Solver(**CFG)
     b.set_tuning(knob, value)
@@ -64,3 +64,23 @@ def test_long_line_forms_are_bit_identical(tcs, precision):
     for r in runs[1:]:
         for n, x in runs[0].items():
             np.testing.assert_array_equal(r[n], x, err_msg=n)
+
+
+def test_y_solver_in_the_mixed_form_moves_only_the_modal_solves(tcs):
+    # FP32 y sweeps keep the partitioned solver (their refinement needs it); the
+    # modal pressure solves have FP64 rows in both forms and switch solver, so
+    # the FP32-stored results move by rounding only
+    cfg = dict(CFG, precision=1)
+    a, b = tcs.Solver(**cfg), tcs.Solver(**cfg)
+    b.set_tuning("y_solver", 4)
+    assert b.tuning()["y_solver"] == 4
+    a.step(3); b.step(3)
+    for n in ("T", "U", "V", "W", "P"):
+        x, y = a.get(n), b.get(n)
+        assert np.linalg.norm(x - y) <= 1e-6 * np.linalg.norm(x), n
+    with pytest.raises(tcs.TcsError) as ei:
+        b.set_tuning("y_solver", 8)
+    assert ei.value.code == 1
+    b.set_tuning("y_solver", 1)                     # frees the scratch; the partitioned solver again
+    b.step(1); a.step(1)
+    assert np.linalg.norm(a.get("P") - b.get("P")) <= 1e-6 * np.linalg.norm(a.get("P"))

@@ -159,10 +159,18 @@ static int choose_tl(int n, bool cyclic, size_t rowb, int want)
     return tl;
 }
 
-bool make_fft_plan(int n, FFTPlan &fp)
+bool make_fft_plan(int n, FFTPlan &fp, int maxr)
 {
     fp.n = n; fp.npass = 0;
     int m = n;
+    // a power of 4 that is no power of 8 takes radix 4 throughout (one radix in
+    // every pass allows the z transform's one-buffer form), else radix 8 first
+    int p8 = n;
+    while (p8 % 8 == 0) p8 /= 8;
+    int p4 = n;
+    while (p4 % 4 == 0) p4 /= 4;
+    const bool only4 = p8 != 1 && p4 == 1;
+    while (maxr >= 8 && !only4 && m % 8 == 0 && fp.npass < 24) { fp.radix[fp.npass++] = 8; m /= 8; }
     while (m % 4 == 0 && fp.npass < 24) { fp.radix[fp.npass++] = 4; m /= 4; }
     while (m % 2 == 0 && fp.npass < 24) { fp.radix[fp.npass++] = 2; m /= 2; }
     while (m % 3 == 0 && fp.npass < 24) { fp.radix[fp.npass++] = 3; m /= 3; }
@@ -424,7 +432,10 @@ int tcs_create(const tcs_config *cfg, tcs_ctx **out)
         return set_err(TCS_ERR_UNSUPPORTED, "padded grid exceeds 2^31 cells");
     if (cfg->n1m > 4096 || cfg->n3m > 4096 || cfg->n2m > 4096) return set_err(TCS_ERR_UNSUPPORTED, "an axis exceeds 4096 cells");
     FFTPlan fp1, fp3;
-    if (!make_fft_plan(cfg->n1m, fp1) || !make_fft_plan(cfg->n3m, fp3))
+    // the x transforms share their kernels with the right-hand side and the
+    // inverse scaling, which keep their registers for that work: radix <= 4
+    // (a radix-8 butterfly took the right-hand side from 64 to 88 registers)
+    if (!make_fft_plan(cfg->n1m, fp1, 4) || !make_fft_plan(cfg->n3m, fp3, 8))
         return set_err(TCS_ERR_UNSUPPORTED, "n1m and n3m must factor into 2, 3 and 5 (FFT radices)");
     if (cfg->precision != TCS_PREC_FP64 && cfg->precision != TCS_PREC_FP32_MIXED)
         return set_err(TCS_ERR_ARG, "precision must be TCS_PREC_FP64 or TCS_PREC_FP32_MIXED");
@@ -541,7 +552,8 @@ int tcs_create(const tcs_config *cfg, tcs_ctx **out)
     }
     // measured on B200 at 256^3: 4 lines per block beats 1, 2, 8 and 16 for both FFT kernels
     c->cx.fft_lines_x = N1 <= 256 ? 4 : (N1 <= 512 ? 2 : 1);
-    c->cx.fft_lines_z = N3 <= 256 ? 4 : (N3 <= 512 ? 2 : 1);
+    // z transforms: 16 lines in the one-radix form (256-byte rows), else 4 (2 or 1 for long lines)
+    c->cx.fft_lines_z = fftz_form(fp3, 16) == 1 ? 16 : (N3 <= 256 ? 4 : (N3 <= 512 ? 2 : 1));
     c->cx.lanes = 32;
     c->cx.long_lines = 2;
     c->cx.y_solver = 1;
@@ -937,7 +949,7 @@ int tcs_set_tuning(tcs_ctx *c, int knob, int value)
     if (value < 1 || value > 64 || (value & (value - 1))) return set_err(TCS_ERR_ARG, "tuning value must be a power of two in 1..64");
     Ctx<double> &x = c->cx;
     const GridT<double> &g = x.g;
-    const size_t rb1 = row_bytes(1, c->fp32), e = esize(c);
+    const size_t rb1 = row_bytes(1, c->fp32);
     switch (knob) {
     case TCS_TUNE_TL_STRIDED: {
         LinePlan a = make_line_plan(g.N3, true, value), b = make_line_plan(g.N2, false, value);
@@ -953,10 +965,10 @@ int tcs_set_tuning(tcs_ctx *c, int knob, int value)
         if (!lines_fit_one_block(row_bytes(2, false), value, a.LS, g.N2)) return set_err(TCS_ERR_ARG, "too many lines for shared memory");
         x.tl_modal = value; break; }
     case TCS_TUNE_FFT_LINES_X:
-        if ((size_t)value * g.N1 * (32 + e) > 200 * 1024) return set_err(TCS_ERR_ARG, "too many lines for shared memory");
+        if ((size_t)value * g.N1 * (32 + esize(c)) > 200 * 1024) return set_err(TCS_ERR_ARG, "too many lines for shared memory");
         x.fft_lines_x = value; break;
     case TCS_TUNE_FFT_LINES_Z:
-        if ((size_t)value * g.N3 * 32 > 200 * 1024) return set_err(TCS_ERR_ARG, "too many lines for shared memory");
+        if (!fftz_form(x.fp3, value)) return set_err(TCS_ERR_ARG, "too many lines for shared memory");
         x.fft_lines_z = value; break;
     case TCS_TUNE_LANES:
         if (value < 2 || value > 32) return set_err(TCS_ERR_ARG, "lanes per line must be 2..32");

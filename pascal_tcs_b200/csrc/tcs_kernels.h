@@ -31,6 +31,27 @@ struct FFTPlan {
     FastDiv dn, dh;             // n and n/2 + 1
 };
 
+// A block's z-FFT lines in shared memory: element (line l, row q) of NL lines at
+// (q + q/8) NL + l -- lines fastest, so that the threads of a warp, which take
+// consecutive lines and then consecutive butterflies, touch consecutive
+// words; the pad row after every 8 rows spreads the strided writes of a pass
+// with span 1 over the banks.
+__host__ __device__ __forceinline__ int frow(int q) { return q + (q >> 3); }
+__host__ __device__ __forceinline__ size_t fft_buf_elems(int NL, int n) { return (size_t)NL * (size_t)frow(n); }
+
+// The form of a z transform of NL lines per block: 1 the one-radix form (every
+// pass of radix 4 or 8, one butterfly per thread: NL n / radix <= 1024 threads,
+// one buffer), 2 the general form (256 threads, two buffers), 0 neither fits
+// the 227 KB a block may take.
+inline size_t fftz_smem(const FFTPlan &fp, int NL, int form) { return (size_t)form * fft_buf_elems(NL, fp.n) * 16; }
+inline int fftz_form(const FFTPlan &fp, int NL)
+{
+    bool uni = fp.npass >= 1 && (fp.radix[0] == 8 || fp.radix[0] == 4);
+    for (int p = 1; p < fp.npass; p++) uni = uni && fp.radix[p] == fp.radix[0];
+    if (uni && (long long)NL * (fp.n / fp.radix[0]) <= 1024 && fftz_smem(fp, NL, 1) <= 227 * 1024) return 1;
+    return fftz_smem(fp, NL, 2) <= 227 * 1024 ? 2 : 0;
+}
+
 struct ProbeState;   // CUDA-event probes (tcs_capi.cu)
 
 // Launch shapes shared by both forms.
@@ -54,7 +75,7 @@ struct Ctx : Shapes {
 };
 
 LinePlan make_line_plan(int n, bool cyclic, int TL, int pmax = 32);
-bool make_fft_plan(int n, FFTPlan &fp);
+bool make_fft_plan(int n, FFTPlan &fp, int maxr);   // radices 2, 3, 4, 5 and (maxr >= 8) 8
 void probe_begin(const Shapes &cx, int kid, cudaStream_t s);
 void probe_end(const Shapes &cx, int kid, cudaStream_t s);
 int record_launch_error(const char *what);

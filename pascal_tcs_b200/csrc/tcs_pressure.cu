@@ -3,7 +3,7 @@
 // (module_solve_pressure.f90:140-231, 489-744, 756-874) on one HBM-resident
 // subdomain.  The FFTW calls of the reference (:565-567, 586-588, 660-662,
 // 681-683) are replaced by hand-written shared-memory Stockham FFTs with
-// radices 2, 3, 4 and 5; the MPI transposes disappear because every pass
+// radices 2, 3, 4, 5 and 8; the MPI transposes disappear because every pass
 // reads the spectral array S(kx, j, kz) (kx fastest) with coalesced tiles.
 //
 //   prhs_fftx   pseudo-update (+ghosts) -> PRHS -> r2c along x   -> S
@@ -85,9 +85,118 @@ template <int SIGN, class C> struct Bfly<5, SIGN, C> {
     }
 };
 
-// One Stockham pass of radix RX over nl lines (line stride ldl) in shared memory.
+template <int SIGN, class C> struct Bfly<8, SIGN, C> {
+    // even and odd halves by 4-point DFTs, joined with the eighth roots of unity
+    // w^q = exp(SIGN 2 pi i q / 8): w = (1 + SIGN i) / sqrt 2, w^2 = SIGN i, w^3 = SIGN i w
+    __device__ static C w1(C a)
+    {
+        using T = typename CReal<C>::T;
+        const T H = T(0.70710678118654752440);   // 1 / sqrt(2)
+        return SIGN > 0 ? cmk<C>((a.x - a.y) * H, (a.x + a.y) * H) : cmk<C>((a.x + a.y) * H, (a.y - a.x) * H);
+    }
+    __device__ static void run(C *v)
+    {
+        C e[4] = {v[0], v[2], v[4], v[6]}, o[4] = {v[1], v[3], v[5], v[7]};
+        Bfly<4, SIGN, C>::run(e);
+        Bfly<4, SIGN, C>::run(o);
+        o[1] = w1(o[1]);
+        o[2] = cmuli<SIGN>(o[2]);
+        o[3] = cmuli<SIGN>(w1(o[3]));
+#pragma unroll
+        for (int q = 0; q < 4; q++) { v[q] = cadd(e[q], o[q]); v[q + 4] = csub(e[q], o[q]); }
+    }
+};
+
+struct SmemLines {
+    double2 *b;
+    int NL;
+    __device__ double2 ld(int l, int q) const { return b[frow(q) * NL + l]; }
+    __device__ void st(int l, int q, double2 v) const { b[frow(q) * NL + l] = v; }
+};
+
+// Line accessors made of lambdas (global-memory ends of a block FFT).
+template <class F> struct LdFn { F f; __device__ double2 ld(int l, int q) const { return f(l, q); } };
+template <class F> struct StFn { F f; __device__ void st(int l, int q, double2 v) const { f(l, q, v); } };
+template <class F> __device__ __forceinline__ LdFn<F> ld_fn(F f) { return LdFn<F>{f}; }
+template <class F> __device__ __forceinline__ StFn<F> st_fn(F f) { return StFn<F>{f}; }
+
+// The z transforms: one Stockham pass of radix RX over NL lines (NL a power of two): butterfly
+// jb of line l reads rows jb + r n/RX through src and writes rows
+// o + r Ns, o = (jb / Ns) Ns RX + jb mod Ns, through dst; thread t takes line
+// t mod NL and butterfly t / NL.
+template <int RX, int SIGN, class Src, class Dst>
+__device__ __forceinline__ void fft_pass_lf(const Src &src, const Dst &dst, int NL, int lgNL, int n, int Ns,
+                                         const double2 *tw, const FastDiv &dns)
+{
+    using C = double2;
+    const int nb = n / RX, ts = n / (Ns * RX);
+    for (int t = threadIdx.x; t < (nb << lgNL); t += blockDim.x) {
+        const int l = t & (NL - 1), jb = t >> lgNL;
+        const int jq = (int)dns.div(jb), kk = jb - jq * Ns;
+        C v[RX];
+#pragma unroll
+        for (int r = 0; r < RX; r++) v[r] = src.ld(l, jb + r * nb);
+        if (kk) {
+#pragma unroll
+            for (int r = 1; r < RX; r++) {
+                C w = __ldg(tw + r * kk * ts);
+                if (SIGN > 0) w.y = -w.y;
+                v[r] = cmul(v[r], w);
+            }
+        }
+        Bfly<RX, SIGN, C>::run(v);
+        const int o = jq * Ns * RX + kk;
+#pragma unroll
+        for (int r = 0; r < RX; r++) dst.st(l, o + r * Ns, v[r]);
+    }
+}
+
+// A pass of the plan's radix RX (at most MAXR: the kernels that keep their
+// registers for other work compile without the radix-8 butterfly).
+template <int SIGN, int MAXR, class Src, class Dst>
+__device__ __forceinline__ void fft_pass_any(int RX, const Src &src, const Dst &dst, int NL, int lgNL, int n, int Ns,
+                                             const double2 *tw, const FastDiv &dns)
+{
+    switch (RX) {
+    case 8: if constexpr (MAXR >= 8) fft_pass_lf<8, SIGN>(src, dst, NL, lgNL, n, Ns, tw, dns); break;
+    case 4: fft_pass_lf<4, SIGN>(src, dst, NL, lgNL, n, Ns, tw, dns); break;
+    case 2: fft_pass_lf<2, SIGN>(src, dst, NL, lgNL, n, Ns, tw, dns); break;
+    case 3: fft_pass_lf<3, SIGN>(src, dst, NL, lgNL, n, Ns, tw, dns); break;
+    default: fft_pass_lf<5, SIGN>(src, dst, NL, lgNL, n, Ns, tw, dns); break;
+    }
+}
+
+// Unnormalised FFT of NL lines: the first pass reads through src, the last
+// writes through dst, and the passes between them go through the two
+// shared-memory buffers b0 and b1 (the first pass writes b0, so src may be
+// b1).  A barrier follows every pass but the last.
+template <int SIGN, int MAXR, class Src, class Dst>
+__device__ void block_fft_lf(const Src &src, const Dst &dst, double2 *b0, double2 *b1, int NL, const FFTPlan &fp,
+                          const double2 *tw)
+{
+    const int lgNL = __ffs(NL) - 1, n = fp.n, last = fp.npass - 1;
+    if (last == 0) {
+        fft_pass_any<SIGN, MAXR>(fp.radix[0], src, dst, NL, lgNL, n, 1, tw, fp.dns[0]);
+        return;
+    }
+    const SmemLines s0{b0, NL}, s1{b1, NL};
+    fft_pass_any<SIGN, MAXR>(fp.radix[0], src, s0, NL, lgNL, n, 1, tw, fp.dns[0]);
+    __syncthreads();
+    int Ns = fp.radix[0];
+    bool in0 = true;
+    for (int ps = 1; ps < last; ps++) {
+        fft_pass_any<SIGN, MAXR>(fp.radix[ps], in0 ? s0 : s1, in0 ? s1 : s0, NL, lgNL, n, Ns, tw, fp.dns[ps]);
+        __syncthreads();
+        Ns *= fp.radix[ps];
+        in0 = !in0;
+    }
+    fft_pass_any<SIGN, MAXR>(fp.radix[last], in0 ? s0 : s1, dst, NL, lgNL, n, Ns, tw, fp.dns[last]);
+}
+
+// The x transforms: lines held line-major (line stride ldl) and staged by the
+// kernel, one Stockham pass of radix RX over nl lines per call.
 template <int RX, int SIGN, class C>
-__device__ __forceinline__ void fft_pass(const C *src, C *dst, int nl, int ldl, int n, int Ns, const C *tw,
+__device__ __forceinline__ void fft_pass_lm(const C *src, C *dst, int nl, int ldl, int n, int Ns, const C *tw,
                                          const FastDiv &dnb, const FastDiv &dns)
 {
     const int nb = n / RX, ts = n / (Ns * RX);
@@ -117,17 +226,17 @@ __device__ __forceinline__ void fft_pass(const C *src, C *dst, int nl, int ldl, 
 // Unnormalised FFT of nl lines held in buf0; buf1 is scratch.  Returns the
 // buffer that holds the natural-order result.
 template <int SIGN, class C>
-__device__ C *block_fft(C *buf0, C *buf1, int nl, int ldl, const FFTPlan &fp, const C *tw)
+__device__ C *block_fft_lm(C *buf0, C *buf1, int nl, int ldl, const FFTPlan &fp, const C *tw)
 {
     C *src = buf0, *dst = buf1;
     int Ns = 1;
     for (int ps = 0; ps < fp.npass; ps++) {
         const int RX = fp.radix[ps];
         switch (RX) {
-        case 2: fft_pass<2, SIGN>(src, dst, nl, ldl, fp.n, Ns, tw, fp.dnb[ps], fp.dns[ps]); break;
-        case 3: fft_pass<3, SIGN>(src, dst, nl, ldl, fp.n, Ns, tw, fp.dnb[ps], fp.dns[ps]); break;
-        case 4: fft_pass<4, SIGN>(src, dst, nl, ldl, fp.n, Ns, tw, fp.dnb[ps], fp.dns[ps]); break;
-        default: fft_pass<5, SIGN>(src, dst, nl, ldl, fp.n, Ns, tw, fp.dnb[ps], fp.dns[ps]); break;
+        case 2: fft_pass_lm<2, SIGN>(src, dst, nl, ldl, fp.n, Ns, tw, fp.dnb[ps], fp.dns[ps]); break;
+        case 3: fft_pass_lm<3, SIGN>(src, dst, nl, ldl, fp.n, Ns, tw, fp.dnb[ps], fp.dns[ps]); break;
+        case 4: fft_pass_lm<4, SIGN>(src, dst, nl, ldl, fp.n, Ns, tw, fp.dnb[ps], fp.dns[ps]); break;
+        default: fft_pass_lm<5, SIGN>(src, dst, nl, ldl, fp.n, Ns, tw, fp.dnb[ps], fp.dns[ps]); break;
         }
         __syncthreads();
         C *t = src; src = dst; dst = t;
@@ -252,7 +361,7 @@ __global__ void __launch_bounds__(256) prhs_fftx_kernel(GridT<R> g, FieldsT<R> f
     if (NL & 1)         // an odd line count leaves the last packed line without an imaginary part
         for (int t = threadIdx.x; t < N1; t += blockDim.x) b0[(NL >> 1) * N1 + t].y = 0.0;
     __syncthreads();
-    const C *res = block_fft<-1>(b0, b1, nfl, N1, fp, f.tw1);
+    const C *res = block_fft_lm<-1>(b0, b1, nfl, N1, fp, f.tw1);
     // Z = FFT(a + i b) of real a, b: A(k) = (Z(k) + conj Z(N-k)) / 2, B(k) = (Z(k) - conj Z(N-k)) / 2i
     for (int t = threadIdx.x; t < NL * h1p; t += blockDim.x) {
         const int l = (int)fp.dh.div(t), kx = t - l * h1p, j = j0 + l;
@@ -264,29 +373,82 @@ __global__ void __launch_bounds__(256) prhs_fftx_kernel(GridT<R> g, FieldsT<R> f
     }
 }
 
-// c2c along z for NL consecutive kx at fixed j.
+// c2c along z for NL consecutive kx at fixed j (NL a power of two): the first
+// pass reads S and the last writes it, NL consecutive kx of one kz row per
+// group of NL threads.
 template <int SIGN, class R>
 __global__ void __launch_bounds__(256) fftz_kernel(GridT<R> g, FieldsT<R> f, FFTPlan fp, int NL, int h1p)
 {
     using C = double2;
     extern __shared__ __align__(16) unsigned char smraw[];
     if (blown(g)) return;
-    const int N3 = g.N3, kx0 = blockIdx.x * NL, j = 1 + blockIdx.y;
-    const int nl = min(NL, h1p - kx0), lgNL = __ffs(NL) - 1;     // NL is a power of two
-    C *b0 = reinterpret_cast<C *>(smraw), *b1 = b0 + NL * N3;
-    for (int t = threadIdx.x; t < NL * N3; t += blockDim.x) {
-        const int kz = t >> lgNL, l = t & (NL - 1);
-        if (l >= nl) continue;
-        const cplx_t<R> v = f.S[sidx(g, h1p, kx0 + l, j, kz)];
-        b0[l * N3 + kz] = make_double2(v.x, v.y);
+    const int kx0 = blockIdx.x * NL, j = 1 + blockIdx.y;
+    const int nl = min(NL, h1p - kx0);
+    C *b0 = reinterpret_cast<C *>(smraw), *b1 = b0 + fft_buf_elems(NL, g.N3);
+    cplx_t<R> *const S = f.S;
+    auto ld = [&](int l, int kz) -> C {
+        if (l >= nl) return make_double2(0.0, 0.0);
+        const cplx_t<R> v = S[sidx(g, h1p, kx0 + l, j, kz)];
+        return make_double2(v.x, v.y);
+    };
+    auto st = [&](int l, int kz, C v) {
+        if (l < nl) S[sidx(g, h1p, kx0 + l, j, kz)] = mkc<R>(R(v.x), R(v.y));
+    };
+    block_fft_lf<SIGN, 8>(ld_fn(ld), st_fn(st), b0, b1, NL, fp, f.tw3);
+}
+
+// The z transform of a plan whose passes all have radix RX (512 = 8^3,
+// 256 = 4^4, 64 = 8^2): one butterfly per thread per pass (blockDim.x =
+// NL n / RX), so one shared-memory buffer holds the lines -- a pass writes the
+// previous pass's outputs, the block waits, reads its own inputs, waits again
+// -- and up to 16 lines per block read and write 16 consecutive kx of a kz row
+// (256 bytes in FP64) together.  The first pass reads S, the last writes it.
+template <int SIGN, int RX, class R>
+__global__ void __launch_bounds__(1024, 1) fftz_uniform_kernel(GridT<R> g, FieldsT<R> f, FFTPlan fp, int NL, int h1p)
+{
+    using C = double2;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    if (blown(g)) return;
+    const int kx0 = blockIdx.x * NL, j = 1 + blockIdx.y, nl = min(NL, h1p - kx0);
+    C *const b = reinterpret_cast<C *>(smraw);
+    const int n = fp.n, nb = n / RX, lgNL = __ffs(NL) - 1;
+    const int l = threadIdx.x & (NL - 1), jb = threadIdx.x >> lgNL;   // jb < nb
+    const bool ok = l < nl;
+    cplx_t<R> *const S = f.S;
+    C v[RX];
+#pragma unroll
+    for (int r = 0; r < RX; r++) {
+        v[r] = make_double2(0.0, 0.0);
+        if (ok) {
+            const cplx_t<R> w = S[sidx(g, h1p, kx0 + l, j, jb + r * nb)];
+            v[r] = make_double2(w.x, w.y);
+        }
     }
-    __syncthreads();
-    const C *res = block_fft<SIGN>(b0, b1, nl, N3, fp, f.tw3);
-    for (int t = threadIdx.x; t < NL * N3; t += blockDim.x) {
-        const int kz = t >> lgNL, l = t & (NL - 1);
-        if (l >= nl) continue;
-        const C v = res[l * N3 + kz];
-        f.S[sidx(g, h1p, kx0 + l, j, kz)] = mkc<R>(R(v.x), R(v.y));
+    Bfly<RX, SIGN, C>::run(v);          // the first pass: span 1, no twiddles
+    int Ns = 1, o = jb * RX;            // span and output base of the pass just computed
+    for (int ps = 1; ps < fp.npass; ps++) {
+#pragma unroll
+        for (int r = 0; r < RX; r++) b[frow(o + r * Ns) * NL + l] = v[r];
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < RX; r++) v[r] = b[frow(jb + r * nb) * NL + l];
+        __syncthreads();
+        Ns *= RX;
+        const int jq = (int)fp.dns[ps].div(jb), kk = jb - jq * Ns, ts = n / (Ns * RX);
+        if (kk) {
+#pragma unroll
+            for (int r = 1; r < RX; r++) {
+                C w = __ldg(f.tw3 + r * kk * ts);
+                if (SIGN > 0) w.y = -w.y;
+                v[r] = cmul(v[r], w);
+            }
+        }
+        Bfly<RX, SIGN, C>::run(v);
+        o = jq * Ns * RX + kk;
+    }
+    if (ok) {
+#pragma unroll
+        for (int r = 0; r < RX; r++) S[sidx(g, h1p, kx0 + l, j, o + r * Ns)] = mkc<R>(R(v[r].x), R(v[r].y));
     }
 }
 
@@ -386,7 +548,7 @@ __global__ void __launch_bounds__(256) ifftx_kernel(GridT<R> g, FieldsT<R> f, FF
         b0[t] = make_double2(a.x - b.y, a.y + b.x);
     }
     __syncthreads();
-    const C *res = block_fft<1>(b0, b1, nfl, N1, fp, f.tw1);
+    const C *res = block_fft_lm<1>(b0, b1, nfl, N1, fp, f.tw1);
     const double aver = g.scal[S_AVER];
     const double scale = 1.0 / ((double)N1 * (double)g.N3);   // the unnormalised transforms' 1/(N1 N3), once per thread
     for (int t = threadIdx.x; t < NL * N1; t += blockDim.x) {
@@ -509,20 +671,42 @@ void launch_pseudo_prhs_fftx(const Ctx<R> &cx, cudaStream_t s, bool with_pseudo)
     record_launch_error("prhs_fftx");
 }
 
+// A z transform: the one-radix form where the plan and the lines per block
+// allow it (fftz_form), the general form otherwise.
+template <int SIGN, class R>
+static void launch_fftz(const Ctx<R> &cx, cudaStream_t s, int kid, const char *what)
+{
+    const GridT<R> &g = cx.g;
+    const int h1p = cx.h1p, NL = cx.fft_lines_z, form = fftz_form(cx.fp3, NL);
+    const dim3 grid((h1p + NL - 1) / NL, g.N2);
+    probe_begin(cx, kid, s);
+    if (form == 1) {
+        const int rx = cx.fp3.radix[0];
+        const size_t sm = fftz_smem(cx.fp3, NL, 1);
+        static size_t c8[64] = {}, c4[64] = {};
+        if (rx == 8) {
+            smem_opt_in((const void *)fftz_uniform_kernel<SIGN, 8, R>, sm, c8);
+            fftz_uniform_kernel<SIGN, 8, R><<<grid, NL * g.N3 / 8, sm, s>>>(g, cx.f, cx.fp3, NL, h1p);
+        } else {
+            smem_opt_in((const void *)fftz_uniform_kernel<SIGN, 4, R>, sm, c4);
+            fftz_uniform_kernel<SIGN, 4, R><<<grid, NL * g.N3 / 4, sm, s>>>(g, cx.f, cx.fp3, NL, h1p);
+        }
+    } else {
+        const size_t sm = fftz_smem(cx.fp3, NL, 2);
+        static size_t cz[64] = {};
+        smem_opt_in((const void *)fftz_kernel<SIGN, R>, sm, cz);
+        fftz_kernel<SIGN, R><<<grid, 256, sm, s>>>(g, cx.f, cx.fp3, NL, h1p);
+    }
+    probe_end(cx, kid, s);
+    record_launch_error(what);
+}
+
 // The Poisson solve after the right-hand side, in three parts so that an
 // ensemble can run the modal solves of all its cases in one launch.
 template <class R>
 void launch_poisson_fwd(const Ctx<R> &cx, cudaStream_t s)
 {
-    const GridT<R> &g = cx.g;
-    const int h1p = cx.h1p, NLz = cx.fft_lines_z;
-    const size_t smz = (size_t)NLz * g.N3 * 2 * sizeof(double2);
-    static size_t cz1[64] = {};
-    smem_opt_in((const void *)fftz_kernel<-1, R>, smz, cz1);
-    probe_begin(cx, K_FFTZ_FWD, s);
-    fftz_kernel<-1, R><<<dim3((h1p + NLz - 1) / NLz, g.N2), 256, smz, s>>>(g, cx.f, cx.fp3, NLz, h1p);
-    probe_end(cx, K_FFTZ_FWD, s);
-    record_launch_error("fftz_fwd");
+    launch_fftz<-1>(cx, s, K_FFTZ_FWD, "fftz_fwd");
 }
 
 template <class R>
@@ -541,20 +725,15 @@ template <class R>
 void launch_poisson_back(const Ctx<R> &cx, cudaStream_t s)
 {
     const GridT<R> &g = cx.g;
-    const int h1p = cx.h1p, NLz = cx.fft_lines_z, NLx = cx.fft_lines_x;
-    const size_t smz = (size_t)NLz * g.N3 * 2 * sizeof(double2);
+    const int h1p = cx.h1p, NLx = cx.fft_lines_x;
     const size_t smx = (size_t)((NLx + 1) / 2) * g.N1 * 2 * sizeof(double2);
-    static size_t cz2[64] = {}, cx2[64] = {};
-    smem_opt_in((const void *)fftz_kernel<1, R>, smz, cz2);
+    static size_t cx2[64] = {};
     smem_opt_in((const void *)ifftx_kernel<R>, smx, cx2);
     probe_begin(cx, K_MEAN, s);
     mean_kernel<R><<<1, 256, 0, s>>>(g, cx.f, h1p);
     probe_end(cx, K_MEAN, s);
     record_launch_error("mean");
-    probe_begin(cx, K_FFTZ_INV, s);
-    fftz_kernel<1, R><<<dim3((h1p + NLz - 1) / NLz, g.N2), 256, smz, s>>>(g, cx.f, cx.fp3, NLz, h1p);
-    probe_end(cx, K_FFTZ_INV, s);
-    record_launch_error("fftz_inv");
+    launch_fftz<1>(cx, s, K_FFTZ_INV, "fftz_inv");
     probe_begin(cx, K_IFFTX, s);
     ifftx_kernel<R><<<dim3((g.N2 + NLx - 1) / NLx, g.N3), 256, smx, s>>>(g, cx.f, cx.fp1, NLx, h1p);
     probe_end(cx, K_IFFTX, s);

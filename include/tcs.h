@@ -252,9 +252,12 @@ int tcs_set_use_graph(tcs_ctx *ctx, int on);
  * x rows x lines doubles: 2.1 GB for the y sweeps and 2.4 GB for the modal
  * solves at 512^3) and setting 1 frees.  Measured on B200: the one-line form
  * is faster for the y sweeps at 512^3 (13-22% per sweep) and slower at 256^3,
- * where 65536 lines leave the SMs short of threads. */
+ * where 65536 lines leave the SMs short of threads.
+ * TCS_TUNE_IFFT_LINES_X: lines per block of the inverse x transform
+ * (TCS_TUNE_FFT_LINES_X sets those of the pressure right-hand side and its
+ * forward x transform). */
 enum { TCS_TUNE_TL_STRIDED = 0, TCS_TUNE_TL_CONTIG, TCS_TUNE_TL_MODAL, TCS_TUNE_FFT_LINES_X, TCS_TUNE_FFT_LINES_Z,
-       TCS_TUNE_LANES, TCS_TUNE_LONG_LINES, TCS_TUNE_Y_SOLVER, TCS_TUNE_COUNT };
+       TCS_TUNE_LANES, TCS_TUNE_LONG_LINES, TCS_TUNE_Y_SOLVER, TCS_TUNE_IFFT_LINES_X, TCS_TUNE_COUNT };
 int tcs_set_tuning(tcs_ctx *ctx, int knob, int value);
 int tcs_get_tuning(tcs_ctx *ctx, int knob, int *value);
 /* Autotuner (no reference counterpart): coordinate descent over every knob,

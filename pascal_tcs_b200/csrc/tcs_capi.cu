@@ -431,11 +431,11 @@ int tcs_create(const tcs_config *cfg, tcs_ctx **out)
     if ((long long)(cfg->n1m + 2) * (cfg->n2m + 2) * (cfg->n3m + 2) > (1ll << 31))
         return set_err(TCS_ERR_UNSUPPORTED, "padded grid exceeds 2^31 cells");
     if (cfg->n1m > 4096 || cfg->n3m > 4096 || cfg->n2m > 4096) return set_err(TCS_ERR_UNSUPPORTED, "an axis exceeds 4096 cells");
-    FFTPlan fp1, fp3;
+    FFTPlan fp1, fp3, fp1u;
     // the x transforms share their kernels with the right-hand side and the
     // inverse scaling, which keep their registers for that work: radix <= 4
     // (a radix-8 butterfly took the right-hand side from 64 to 88 registers)
-    if (!make_fft_plan(cfg->n1m, fp1, 4) || !make_fft_plan(cfg->n3m, fp3, 8))
+    if (!make_fft_plan(cfg->n1m, fp1, 4) || !make_fft_plan(cfg->n3m, fp3, 8) || !make_fft_plan(cfg->n1m, fp1u, 8))
         return set_err(TCS_ERR_UNSUPPORTED, "n1m and n3m must factor into 2, 3 and 5 (FFT radices)");
     if (cfg->precision != TCS_PREC_FP64 && cfg->precision != TCS_PREC_FP32_MIXED)
         return set_err(TCS_ERR_ARG, "precision must be TCS_PREC_FP64 or TCS_PREC_FP32_MIXED");
@@ -542,7 +542,7 @@ int tcs_create(const tcs_config *cfg, tcs_ctx **out)
         c->cx.wall_at = s2 / (s2 - dmx2[n2sub] * dmx2[n2sub]);
         c->cx.wall_bt = dmx2[n2sub] * dmx2[n2sub] / (s2 - dmx2[n2sub] * dmx2[n2sub]);
     }
-    c->cx.fp1 = fp1; c->cx.fp3 = fp3;
+    c->cx.fp1 = fp1; c->cx.fp3 = fp3; c->cx.fp1u = fp1u;
     const size_t rb1 = row_bytes(1, c->fp32);
     c->cx.tl_contig = choose_tl(N1, true, rb1, 8);
     c->cx.tl_modal = choose_tl(N2, false, row_bytes(2, false), 8);   // modal rows are FP64 in both forms
@@ -554,6 +554,9 @@ int tcs_create(const tcs_config *cfg, tcs_ctx **out)
     c->cx.fft_lines_x = N1 <= 256 ? 4 : (N1 <= 512 ? 2 : 1);
     // z transforms: 16 lines in the one-radix form (256-byte rows), else 4 (2 or 1 for long lines)
     c->cx.fft_lines_z = fftz_form(fp3, 16) == 1 ? 16 : (N3 <= 256 ? 4 : (N3 <= 512 ? 2 : 1));
+    // inverse x transform, measured on B200: the one-radix form runs best with 2
+    // lines per block (64 or 128 threads; 256^3 and 512^3), the general form with 8
+    c->cx.ifft_lines_x = ifftx_form(fp1u, 2) == 1 ? 2 : (ifftx_form(fp1u, 8) ? 8 : 1);
     c->cx.lanes = 32;
     c->cx.long_lines = 2;
     c->cx.y_solver = 1;
@@ -970,6 +973,9 @@ int tcs_set_tuning(tcs_ctx *c, int knob, int value)
     case TCS_TUNE_FFT_LINES_Z:
         if (!fftz_form(x.fp3, value)) return set_err(TCS_ERR_ARG, "too many lines for shared memory");
         x.fft_lines_z = value; break;
+    case TCS_TUNE_IFFT_LINES_X:
+        if (!ifftx_form(x.fp1u, value)) return set_err(TCS_ERR_ARG, "too many lines for shared memory");
+        x.ifft_lines_x = value; break;
     case TCS_TUNE_LANES:
         if (value < 2 || value > 32) return set_err(TCS_ERR_ARG, "lanes per line must be 2..32");
         x.lanes = value; break;
@@ -1021,6 +1027,7 @@ int tcs_get_tuning(tcs_ctx *c, int knob, int *value)
     case TCS_TUNE_LANES: *value = x.lanes; break;
     case TCS_TUNE_LONG_LINES: *value = x.long_lines; break;
     case TCS_TUNE_Y_SOLVER: *value = x.y_solver; break;
+    case TCS_TUNE_IFFT_LINES_X: *value = x.ifft_lines_x; break;
     default: return set_err(TCS_ERR_ARG, "unknown tuning knob");
     }
     return TCS_OK;

@@ -52,17 +52,36 @@ inline int fftz_form(const FFTPlan &fp, int NL)
     return fftz_smem(fp, NL, 2) <= 227 * 1024 ? 2 : 0;
 }
 
+// The form of the inverse x transform of NL lines per block: 1 the one-radix
+// form (fpu of one radix 4 or 8, packed lines x N1 / radix <= 512 threads, one
+// line-major buffer), 2 the general form (256 threads, two buffers, the
+// radix-4 plan), 0 neither fits.
+inline size_t ifftx_smem(const FFTPlan &fpu, int NL, int form)
+{
+    const size_t nfl = (size_t)((NL + 1) / 2);
+    return form == 1 ? nfl * (size_t)frow(fpu.n) * 16 : nfl * (size_t)fpu.n * 2 * 16;
+}
+inline int ifftx_form(const FFTPlan &fpu, int NL)
+{
+    bool uni = fpu.npass >= 1 && (fpu.radix[0] == 8 || fpu.radix[0] == 4);
+    for (int p = 1; p < fpu.npass; p++) uni = uni && fpu.radix[p] == fpu.radix[0];
+    if (uni && (long long)((NL + 1) / 2) * (fpu.n / fpu.radix[0]) <= 512 && ifftx_smem(fpu, NL, 1) <= 227 * 1024) return 1;
+    return ifftx_smem(fpu, NL, 2) <= 227 * 1024 ? 2 : 0;
+}
+
 struct ProbeState;   // CUDA-event probes (tcs_capi.cu)
 
 // Launch shapes shared by both forms.
 struct Shapes {
     int tl_strided, tl_contig, tl_modal;
     int fft_lines_x, fft_lines_z;
+    int ifft_lines_x;                            // lines per block of the inverse x transform
     int lanes;                                   // at most this many partitions (lanes) per line
     int long_lines;                              // one-block-per-SM form of long lines: 1 never, 2 z sweeps, 4 z and y sweeps
     int y_solver;                                // FP64 y lines: 1 partitioned (line_block), 2 one line per thread for the y sweeps, 4 also the modal solves
     double *thomas_scr;                          // c', d' of the one-line-per-thread solver (null unless y_solver asks for it)
     FFTPlan fp1, fp3;
+    FFTPlan fp1u;                                // N1 with radices up to 8 (the inverse x transform's one-radix form)
     int h1p;
     double wall_ab, wall_bb, wall_at, wall_bt;   // Pbc_a, Pbc_b of the two walls
     ProbeState *probe;

@@ -560,6 +560,82 @@ __global__ void __launch_bounds__(256) ifftx_kernel(GridT<R> g, FieldsT<R> f, FF
     }
 }
 
+// The same for a one-radix plan of N1 (radix RX in every pass: 512 = 8^3,
+// 256 = 4^4): one butterfly per thread per pass (blockDim.x = packed lines x
+// N1 / RX), the packed lines line-major in one shared-memory buffer (row q of
+// packed line p at p frow(N1) + frow(q)), and the last pass's outputs, which
+// are consecutive i across consecutive threads, scaled and stored to dP from
+// registers.
+template <int RX, class R>
+__global__ void __launch_bounds__(512) ifftx_uniform_kernel(GridT<R> g, FieldsT<R> f, FFTPlan fp, int NL, int h1p)
+{
+    using C = double2;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    if (blown(g)) return;
+    const int N1 = g.N1, j0 = 1 + blockIdx.x * NL, k = 1 + blockIdx.y;
+    const int nfl = (NL + 1) >> 1, ldl = frow(N1), nb = N1 / RX, lgN1 = __ffs(N1) - 1, lgnb = __ffs(nb) - 1;
+    C *const b = reinterpret_cast<C *>(smraw);
+    auto herm = [&](int l, int kx) -> C {
+        const int j = j0 + l;
+        C v = make_double2(0.0, 0.0);
+        if (l < NL && j <= g.N2) {
+            if (kx < h1p) {
+                const cplx_t<R> w = f.S[sidx(g, h1p, kx, j, k - 1)];
+                v = make_double2(w.x, w.y);
+                if (kx == 0 || 2 * kx == N1) v.y = 0.0;   // c2r ignores these imaginary parts
+            } else {
+                const cplx_t<R> w = f.S[sidx(g, h1p, N1 - kx, j, k - 1)];
+                v = make_double2(w.x, -w.y);
+            }
+        }
+        return v;
+    };
+    // two lines per complex inverse FFT: Z = A + i B gives a + i b with a, b real
+    for (int t = threadIdx.x; t < (nfl << lgN1); t += blockDim.x) {
+        const int p = t >> lgN1, kx = t & (N1 - 1);
+        const C a = herm(2 * p, kx), c = herm(2 * p + 1, kx);
+        b[p * ldl + frow(kx)] = make_double2(a.x - c.y, a.y + c.x);
+    }
+    __syncthreads();
+    const int p = threadIdx.x >> lgnb, jb = threadIdx.x & (nb - 1);
+    C *const bl = b + p * ldl;
+    C v[RX];
+#pragma unroll
+    for (int r = 0; r < RX; r++) v[r] = bl[frow(jb + r * nb)];
+    Bfly<RX, 1, C>::run(v);             // the first pass: span 1, no twiddles
+    int Ns = 1, o = jb * RX;            // span and output base of the pass just computed
+    for (int ps = 1; ps < fp.npass; ps++) {
+        __syncthreads();                // every thread has read the previous pass's inputs
+#pragma unroll
+        for (int r = 0; r < RX; r++) bl[frow(o + r * Ns)] = v[r];
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < RX; r++) v[r] = bl[frow(jb + r * nb)];
+        Ns *= RX;
+        const int jq = (int)fp.dns[ps].div(jb), kk = jb - jq * Ns, ts = N1 / (Ns * RX);
+        if (kk) {
+#pragma unroll
+            for (int r = 1; r < RX; r++) {
+                C w = __ldg(f.tw1 + r * kk * ts);
+                w.y = -w.y;
+                v[r] = cmul(v[r], w);
+            }
+        }
+        Bfly<RX, 1, C>::run(v);
+        o = jq * Ns * RX + kk;
+    }
+    const double aver = g.scal[S_AVER];
+    const double scale = 1.0 / ((double)N1 * (double)g.N3);   // the unnormalised transforms' 1/(N1 N3), once per thread
+    const int ja = j0 + 2 * p, jbm = ja + 1;
+    const bool oka = 2 * p < NL && ja <= g.N2, okb = 2 * p + 1 < NL && jbm <= g.N2;
+#pragma unroll
+    for (int r = 0; r < RX; r++) {
+        const int i = o + r * Ns + 1;
+        if (oka) store_periodic(g, f.dP, i, ja, k, R(v[r].x * scale - aver));
+        if (okb) store_periodic(g, f.dP, i, jbm, k, R(v[r].y * scale - aver));
+    }
+}
+
 // dP wall extrapolation (:719-736) on every (i,k) including ghost columns,
 // which is what the extrapolation followed by ghost(dP) produces.
 template <class R>
@@ -725,17 +801,30 @@ template <class R>
 void launch_poisson_back(const Ctx<R> &cx, cudaStream_t s)
 {
     const GridT<R> &g = cx.g;
-    const int h1p = cx.h1p, NLx = cx.fft_lines_x;
-    const size_t smx = (size_t)((NLx + 1) / 2) * g.N1 * 2 * sizeof(double2);
-    static size_t cx2[64] = {};
-    smem_opt_in((const void *)ifftx_kernel<R>, smx, cx2);
+    const int h1p = cx.h1p, NLx = cx.ifft_lines_x, form = ifftx_form(cx.fp1u, NLx);
     probe_begin(cx, K_MEAN, s);
     mean_kernel<R><<<1, 256, 0, s>>>(g, cx.f, h1p);
     probe_end(cx, K_MEAN, s);
     record_launch_error("mean");
     launch_fftz<1>(cx, s, K_FFTZ_INV, "fftz_inv");
     probe_begin(cx, K_IFFTX, s);
-    ifftx_kernel<R><<<dim3((g.N2 + NLx - 1) / NLx, g.N3), 256, smx, s>>>(g, cx.f, cx.fp1, NLx, h1p);
+    const dim3 gx((g.N2 + NLx - 1) / NLx, g.N3);
+    const size_t smx = ifftx_smem(cx.fp1u, NLx, form);
+    if (form == 1) {
+        const int nt = ((NLx + 1) / 2) * (g.N1 / cx.fp1u.radix[0]);
+        static size_t c8[64] = {}, c4[64] = {};
+        if (cx.fp1u.radix[0] == 8) {
+            smem_opt_in((const void *)ifftx_uniform_kernel<8, R>, smx, c8);
+            ifftx_uniform_kernel<8, R><<<gx, nt, smx, s>>>(g, cx.f, cx.fp1u, NLx, h1p);
+        } else {
+            smem_opt_in((const void *)ifftx_uniform_kernel<4, R>, smx, c4);
+            ifftx_uniform_kernel<4, R><<<gx, nt, smx, s>>>(g, cx.f, cx.fp1u, NLx, h1p);
+        }
+    } else {
+        static size_t cx2[64] = {};
+        smem_opt_in((const void *)ifftx_kernel<R>, smx, cx2);
+        ifftx_kernel<R><<<gx, 256, smx, s>>>(g, cx.f, cx.fp1, NLx, h1p);
+    }
     probe_end(cx, K_IFFTX, s);
     record_launch_error("ifftx");
     probe_begin(cx, K_DP_WALL, s);

@@ -506,6 +506,11 @@ int tcs_create(const tcs_config *cfg, tcs_ctx **out)
     on_ctx(c, alloc_fields);
     if (c->fp32 && !r) r = dalloc(c, &c->stage, NP);
     if (r) { tcs_destroy(c); return r; }
+    // the split form of the pressure right-hand side keeps it in a free FP64
+    // array: scr (free between the momentum sweeps and the next step's thermal
+    // sweeps) in the FP64 form, the host-transfer staging array in the FP32 form
+    c->cx.f.prhs = c->fp32 ? nullptr : (double *)c->cx.f.scr;
+    c->cf.f.prhs = c->fp32 ? c->stage : nullptr;
     auto &F = c->cx.f;
 
     // wavenumbers (module_solve_pressure.f90:93-129) and modal y coefficients (:599-609)

@@ -23,6 +23,10 @@ struct FieldsT {
     R *dU, *dV, *dW, *dP;
     // interior stage scratch (padded layout)
     R *scr;
+    // the pressure right-hand side of the split form (FP64, padded layout): the
+    // FP64 form's scr, the FP32 form's FP64 staging array; null where the split
+    // form does not run
+    double *prhs;
     // 2-D (j,k) property tables: Mu and invRho of mpi_momentum_coeffi, in the
     // field type (read by the line sweeps), and invRho in FP64 (the same array
     // in the FP64 form).  invRho differs from 1 by about 1e-3 for water, and

@@ -373,6 +373,146 @@ __global__ void __launch_bounds__(256) prhs_fftx_kernel(GridT<R> g, FieldsT<R> f
     }
 }
 
+// The split form of the same stage, for a one-radix plan of N1 (512 = 8^3,
+// 256 = 4^4): prhs_kernel forms the pseudo-update and the right-hand side one
+// cell per thread and stores the right-hand side in FP64 (padded layout, in
+// f.prhs); fftx_uniform_kernel transforms its x lines.  The fused kernel above
+// keeps the right-hand side in shared memory, but its FFT's registers and
+// barriers hold its loads back (measured at 512^3: 3.55 ms FP64, 4.82 ms
+// FP32-mixed).  The new U at the x-upper neighbour (periodic) is formed again
+// from its inputs with the same arithmetic, so both forms give the same bits.
+template <class R>
+__global__ void __launch_bounds__(256) prhs_kernel(GridT<R> g, FieldsT<R> f, int with_pseudo)
+{
+    const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x, j = 1 + blockIdx.y, k = 1 + blockIdx.z;
+    if (i > g.N1 || blown(g)) return;
+    const double *dx1 = g.d1.dx, *dx2 = g.d2.dx, *dx3 = g.d3.dx;
+    const double *rdx1 = g.d1.rdx, *rdx2 = g.d2.rdx, *rdx3 = g.d3.rdx;
+    const double *rdmx1 = g.d1.rdmx, *rdmx2 = g.d2.rdmx, *rdmx3 = g.d3.rdmx;
+    const int sj = g.P1, sk = g.P1 * g.P2;   // 32-bit offsets (the padded grid is below 2^31 cells)
+    const int c = (int)ix(g, i, j, k), cxp = c + ((i == g.N1) ? 1 - g.N1 : 1);
+    // the new U at a cell, as the pseudo-update forms it
+    auto unew = [&](int cc) -> double {
+        if constexpr (HasLo<R>::on) {
+            const double u = join(ld(f.U + cc), ld(f.Ulo + cc));
+            return with_pseudo ? u + (double)ld(f.dU + cc) : u;
+        } else {
+            return with_pseudo ? (double)(ld(f.U + cc) + ld(f.dU + cc)) : (double)ld(f.U + cc);
+        }
+    };
+    const double Uc = unew(c), Uxp = unew(cxp);
+    const double jvm = (j == 1) ? 0.0 : 1.0, jvp = (j == g.N2) ? 0.0 : 1.0;
+    const int ckp = (k == g.N3) ? (int)ix(g, i, j, 1) : c + sk;
+    double Vc, Vyp, Wc, Wzp;
+    if constexpr (HasLo<R>::on) {
+        Vc = join(ld(f.V + c), ld(f.Vlo + c)); Vyp = join(ld(f.V + (c + sj)), ld(f.Vlo + (c + sj)));
+        Wc = join(ld(f.W + c), ld(f.Wlo + c)); Wzp = join(ld(f.W + ckp), ld(f.Wlo + ckp));
+        if (with_pseudo) {
+            Vc += (double)ld(f.dV + c) * jvm;
+            if (j < g.N2) Vyp += (double)ld(f.dV + (c + sj));
+            Wc += (double)ld(f.dW + c);
+            Wzp += (double)ld(f.dW + ckp);
+            float h, lo;
+            split(Uc, h, lo); store_periodic(g, f.Un, i, j, k, h); store_periodic(g, f.Unlo, i, j, k, lo);
+            split(Vc, h, lo); store_periodic(g, f.Vn, i, j, k, h); store_periodic(g, f.Vnlo, i, j, k, lo);
+            split(Wc, h, lo); store_periodic(g, f.Wn, i, j, k, h); store_periodic(g, f.Wnlo, i, j, k, lo);
+        }
+    } else if (with_pseudo) {
+        const R vn = ld(f.V + c) + ld(f.dV + c) * R(jvm), wn = ld(f.W + c) + ld(f.dW + c);
+        Vc = vn;
+        Vyp = (j < g.N2) ? ld(f.V + (c + sj)) + ld(f.dV + (c + sj)) : ld(f.V + (c + sj));
+        Wc = wn;
+        Wzp = ld(f.W + ckp) + ld(f.dW + ckp);
+        store_periodic(g, f.Un, i, j, k, R(Uc));
+        store_periodic(g, f.Vn, i, j, k, vn);
+        store_periodic(g, f.Wn, i, j, k, wn);
+    } else {
+        Vc = ld(f.V + c); Vyp = ld(f.V + (c + sj)); Wc = ld(f.W + c); Wzp = ld(f.W + ckp);
+    }
+    const double dt = g.scal[S_DT], rdt = 1.0 / dt;
+    const Phys &p = g.phd;
+    const double rdtc = rdt / p.Cmp;
+    const int im = i - 1, ip = i + 1, jm = j - 1, jp = j + 1, km = k - 1, kp = k + 1;
+    const double DivUm = (Uxp - Uc) * rdx1[i] + (jvp * Vyp - jvm * Vc) * rdx2[j] + (Wzp - Wc) * rdx3[k];
+    const double cbc = (1.0 - jvm) * p.Vbt * rdx2[j] - (1.0 - jvp) * p.Vup * rdx2[j];
+    const R *dPh = f.dPhat;
+    const double Pc = ld(dPh + c);
+    const double ddpdx1 = (Pc - (double)ld(dPh + (c - 1))) * rdmx1[i], ddpdx2 = ((double)ld(dPh + (c + 1)) - Pc) * rdmx1[ip];
+    const double ddpdy3 = (Pc - (double)ld(dPh + (c - sj))) * rdmx2[j], ddpdy4 = ((double)ld(dPh + (c + sj)) - Pc) * rdmx2[jp];
+    const double ddpdz5 = (Pc - (double)ld(dPh + (c - sk))) * rdmx3[k], ddpdz6 = ((double)ld(dPh + (c + sk)) - Pc) * rdmx3[kp];
+    const double iRjk = IR(j, k);
+    const double iR1 = 0.5 * rdmx1[i] * (dx1[im] * iRjk + dx1[i] * iRjk);
+    const double iR2_ = 0.5 * rdmx1[ip] * (dx1[ip] * iRjk + dx1[i] * iRjk);
+    const double iR3 = 0.5 * rdmx2[j] * (dx2[jm] * iRjk + dx2[j] * (double)IR(jm, k));
+    const double iR4 = 0.5 * rdmx2[jp] * (dx2[jp] * iRjk + dx2[j] * (double)IR(jp, k));
+    const double iR5 = 0.5 * rdmx3[k] * (dx3[km] * iRjk + dx3[k] * (double)IR(j, km));
+    const double iR6 = 0.5 * rdmx3[kp] * (dx3[kp] * iRjk + dx3[k] * (double)IR(j, kp));
+    const double Extra = ((1.0 - iR2_) * ddpdx2 - (1.0 - iR1) * ddpdx1) * rdx1[i]
+                       + ((1.0 - iR4) * ddpdy4 - (1.0 - iR3) * ddpdy3) * rdx2[j]
+                       + ((1.0 - iR6) * ddpdz6 - (1.0 - iR5) * ddpdz5) * rdx3[k];
+    f.prhs[c] = (DivUm - cbc) * rdtc + Extra;
+}
+
+// The forward r2c x transform of the split form: NL right-hand-side lines
+// (j0..j0+NL-1, k) packed two per complex line (real and imaginary parts),
+// one butterfly per thread per pass in one line-major buffer, then the
+// Hermitian separation into S as in the fused kernel.
+template <int RX, class R>
+__global__ void __launch_bounds__(512) fftx_uniform_kernel(GridT<R> g, FieldsT<R> f, FFTPlan fp, int NL, int h1p)
+{
+    using C = double2;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    if (blown(g)) return;
+    const int N1 = g.N1, j0 = 1 + blockIdx.x * NL, k = 1 + blockIdx.y;
+    const int nfl = (NL + 1) >> 1, ldl = frow(N1), nb = N1 / RX, lgN1 = __ffs(N1) - 1, lgnb = __ffs(nb) - 1;
+    C *const b = reinterpret_cast<C *>(smraw);
+    const double *const prhs = f.prhs;
+    for (int t = threadIdx.x; t < (nfl << lgN1); t += blockDim.x) {
+        const int p = t >> lgN1, q = t & (N1 - 1), ja = j0 + 2 * p;
+        const double re = (2 * p < NL && ja <= g.N2) ? ld(prhs + ix(g, q + 1, ja, k)) : 0.0;
+        const double im = (2 * p + 1 < NL && ja + 1 <= g.N2) ? ld(prhs + ix(g, q + 1, ja + 1, k)) : 0.0;
+        b[p * ldl + frow(q)] = make_double2(re, im);
+    }
+    __syncthreads();
+    const int p = threadIdx.x >> lgnb, jb = threadIdx.x & (nb - 1);
+    C *const bl = b + p * ldl;
+    C v[RX];
+#pragma unroll
+    for (int r = 0; r < RX; r++) v[r] = bl[frow(jb + r * nb)];
+    Bfly<RX, -1, C>::run(v);            // the first pass: span 1, no twiddles
+    int Ns = 1, o = jb * RX;            // span and output base of the pass just computed
+    for (int ps = 1; ps < fp.npass; ps++) {
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < RX; r++) bl[frow(o + r * Ns)] = v[r];
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < RX; r++) v[r] = bl[frow(jb + r * nb)];
+        Ns *= RX;
+        const int jq = (int)fp.dns[ps].div(jb), kk = jb - jq * Ns, ts = N1 / (Ns * RX);
+        if (kk) {
+#pragma unroll
+            for (int r = 1; r < RX; r++) v[r] = cmul(v[r], __ldg(f.tw1 + r * kk * ts));
+        }
+        Bfly<RX, -1, C>::run(v);
+        o = jq * Ns * RX + kk;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < RX; r++) bl[frow(o + r * Ns)] = v[r];
+    __syncthreads();
+    // Z = FFT(a + i b) of real a, b: A(k) = (Z(k) + conj Z(N-k)) / 2, B(k) = (Z(k) - conj Z(N-k)) / 2i
+    for (int t = threadIdx.x; t < NL * h1p; t += blockDim.x) {
+        const int l = (int)fp.dh.div(t), kx = t - l * h1p, j = j0 + l;
+        if (j > g.N2) continue;
+        const C *const bp = b + (l >> 1) * ldl;
+        const C z = bp[frow(kx)], zr = bp[frow(kx == 0 ? 0 : N1 - kx)];
+        const C v2 = (l & 1) ? make_double2(0.5 * (z.y + zr.y), 0.5 * (zr.x - z.x))
+                             : make_double2(0.5 * (z.x + zr.x), 0.5 * (z.y - zr.y));
+        f.S[sidx(g, h1p, kx, j, k - 1)] = mkc<R>(R(v2.x), R(v2.y));
+    }
+}
+
 // c2c along z for NL consecutive kx at fixed j (NL a power of two): the first
 // pass reads S and the last writes it, NL consecutive kx of one kz row per
 // group of NL threads.
@@ -738,6 +878,25 @@ void launch_pseudo_prhs_fftx(const Ctx<R> &cx, cudaStream_t s, bool with_pseudo)
 {
     const GridT<R> &g = cx.g;
     const int NL = cx.fft_lines_x;
+    if (cx.f.prhs && ifftx_form(cx.fp1u, NL) == 1) {   // the split form
+        const size_t sm = ifftx_smem(cx.fp1u, NL, 1);
+        const int nt = ((NL + 1) / 2) * (g.N1 / cx.fp1u.radix[0]);
+        const dim3 gx((g.N2 + NL - 1) / NL, g.N3);
+        static size_t c8[64] = {}, c4[64] = {};
+        probe_begin(cx, K_PRHS_FFTX, s);
+        prhs_kernel<R><<<dim3((g.N1 + 255) / 256, g.N2, g.N3), 256, 0, s>>>(g, cx.f, with_pseudo ? 1 : 0);
+        record_launch_error("prhs");
+        if (cx.fp1u.radix[0] == 8) {
+            smem_opt_in((const void *)fftx_uniform_kernel<8, R>, sm, c8);
+            fftx_uniform_kernel<8, R><<<gx, nt, sm, s>>>(g, cx.f, cx.fp1u, NL, cx.h1p);
+        } else {
+            smem_opt_in((const void *)fftx_uniform_kernel<4, R>, sm, c4);
+            fftx_uniform_kernel<4, R><<<gx, nt, sm, s>>>(g, cx.f, cx.fp1u, NL, cx.h1p);
+        }
+        probe_end(cx, K_PRHS_FFTX, s);
+        record_launch_error("fftx");
+        return;
+    }
     const size_t sm = fftx_smem(cx);
     static size_t conf[64] = {};
     smem_opt_in((const void *)prhs_fftx_kernel<R>, sm, conf);

@@ -251,8 +251,9 @@ int tcs_set_use_graph(tcs_ctx *ctx, int on);
  * in a scratch buffer that setting the knob allocates ((1 + right-hand sides)
  * x rows x lines doubles: 2.1 GB for the y sweeps and 2.4 GB for the modal
  * solves at 512^3) and setting 1 frees.  Measured on B200: the one-line form
- * is faster for the y sweeps at 512^3 (13-22% per sweep) and slower at 256^3,
- * where 65536 lines leave the SMs short of threads.
+ * is faster for the y sweeps at 512^3 (17-27% per sweep) and slower at 256^3,
+ * where 65536 lines leave the SMs short of threads; for the modal solves it
+ * is slower at both sizes (its scratch traffic is 1.5x the spectrum's).
  * TCS_TUNE_IFFT_LINES_X: lines per block of the inverse x transform
  * (TCS_TUNE_FFT_LINES_X sets those of the pressure right-hand side and its
  * forward x transform). */

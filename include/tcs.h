@@ -243,17 +243,18 @@ int tcs_set_use_graph(tcs_ctx *ctx, int on);
  * 124 KiB) when the usual blocks would leave under 60 KiB of L1 or halve
  * their lines: 1 never, 2 the z sweeps (default), 4 the z and y sweeps.
  * TCS_TUNE_Y_SOLVER picks the tridiagonal solver of the non-cyclic strided
- * lines with FP64 rows: 1 the partitioned solver that every sweep uses
- * (default: modified Thomas per lane with a parallel reduced-system solve,
- * pascal_tdma.f90:487-578); 2 the plain Thomas elimination with one line per
- * thread (tdmas.f90:27-50) for the FP64 form's y sweeps; 4 the same for the
- * modal pressure solves too (FP64 rows in both forms).  2 and 4 keep c' and d'
- * in a scratch buffer that setting the knob allocates ((1 + right-hand sides)
- * x rows x lines doubles: 2.1 GB for the y sweeps and 2.4 GB for the modal
+ * lines: 1 the partitioned solver that every sweep uses (default: modified
+ * Thomas per lane with a parallel reduced-system solve, pascal_tdma.f90:
+ * 487-578; in the FP32-mixed form FP32 elimination with one FP64-residual
+ * refinement pass); 2 the plain Thomas elimination with one line per thread
+ * (tdmas.f90:27-50) in FP64 for the y sweeps (rows built in the field type);
+ * 4 the same for the modal pressure solves too.  2 and 4 keep c' and d' in a
+ * scratch buffer that setting the knob allocates ((1 + right-hand sides) x
+ * rows x lines doubles: 2.1 GB for the y sweeps and 2.4 GB for the modal
  * solves at 512^3) and setting 1 frees.  Measured on B200: the one-line form
- * is faster for the y sweeps at 512^3 (17-27% per sweep) and slower at 256^3,
- * where 65536 lines leave the SMs short of threads; for the modal solves it
- * is slower at both sizes (its scratch traffic is 1.5x the spectrum's).
+ * is faster for the y sweeps at 512^3 and slower at 256^3, where 65536 lines
+ * leave the SMs short of threads; for the modal solves it is slower at both
+ * sizes (its scratch traffic is 1.5x the spectrum's).
  * TCS_TUNE_IFFT_LINES_X: lines per block of the inverse x transform
  * (TCS_TUNE_FFT_LINES_X sets those of the pressure right-hand side and its
  * forward x transform). */

@@ -988,10 +988,10 @@ int tcs_set_tuning(tcs_ctx *c, int knob, int value)
         if (value > 4) return set_err(TCS_ERR_ARG, "long-line form: 1 never, 2 z sweeps, 4 z and y sweeps");
         x.long_lines = value; break;
     case TCS_TUNE_Y_SOLVER: {
-        if (value > 4) return set_err(TCS_ERR_ARG, "y solver: 1 partitioned, 2 one line per thread (FP64 y sweeps), 4 also the modal solves");
-        // c', d' of every line of the largest one-line-per-thread launch: the FP64
-        // form's y sweeps (one right-hand side) and, with 4, the modal solves (two)
-        const size_t ny = (value >= 2 && !c->fp32) ? thomas_words(g.N2, g.N1, g.N3, 1) : 0;
+        if (value > 4) return set_err(TCS_ERR_ARG, "y solver: 1 partitioned, 2 one line per thread (y sweeps), 4 also the modal solves");
+        // c', d' of every line of the largest one-line-per-thread launch: the y
+        // sweeps (one right-hand side) and, with 4, the modal solves (two)
+        const size_t ny = value >= 2 ? thomas_words(g.N2, g.N1, g.N3, 1) : 0;
         const size_t words = std::max(ny, value == 4 ? thomas_words(g.N2, x.h1p, g.N3, 2) : (size_t)0);
         if (x.thomas_scr) {
             cudaStreamSynchronize(c->stream);

@@ -914,18 +914,6 @@ __global__ void __launch_bounds__(Prob::NT, Prob::MINB) line_solve_kernel(Prob p
     line_block(prob, lp);
 }
 
-// One line per thread: the plain Thomas elimination of a non-cyclic line with
-// FP64 rows (the sequential elimination of tdma_single and tdma_many,
-// PaScaL_TDMA/src/tdmas.f90:27-50 and 113-146), for the strided y lines and
-// the modal solves.  A block of THOMAS_TL threads takes THOMAS_TL consecutive
-// lines (the problem's TL is THOMAS_TL), thread l line l.  The forward sweep
-// builds each row with the problem's own build, keeps c' and d' of the current
-// row in registers and stores them for the back substitution in
-// scr[row][line] (consecutive threads, consecutive words: every store and load
-// of a warp is coalesced); the back substitution emits the rows from the last
-// to the first.  No shared memory and no barrier: the build's loads of the
-// next rows overlap the elimination of the current one.  scr holds
-// (1 + NRHS) x n x (all lines of the grid) doubles.
 // Blocks per SM the one-line-per-thread kernel is compiled for
 // (Prob::THOMAS_MINB; default 8, i.e. 64 registers).  Measured on B200 at
 // 512^3: the y sweeps 4-18% faster at 64 registers than uncapped (80-96), and
@@ -935,10 +923,25 @@ struct ThomasMinB { static constexpr int v = 8; };
 template <class P>
 struct ThomasMinB<P, std::void_t<decltype(P::THOMAS_MINB)>> { static constexpr int v = P::THOMAS_MINB; };
 
+// One line per thread: the plain Thomas elimination of a non-cyclic line in
+// FP64 (the sequential elimination of tdma_single and tdma_many,
+// PaScaL_TDMA/src/tdmas.f90:27-50 and 113-146), for the strided y lines and
+// the modal solves.  A block of THOMAS_TL threads takes THOMAS_TL consecutive
+// lines (the problem's TL is THOMAS_TL), thread l line l.  The forward sweep
+// builds each row with the problem's own build, keeps c' and d' of the current
+// row in registers and stores them for the back substitution in
+// scr[row][line] (consecutive threads, consecutive words: every store and load
+// of a warp is coalesced); the back substitution emits the rows from the last
+// to the first.  No shared memory and no barrier: the build's loads of the
+// next rows overlap the elimination of the current one.  scr holds
+// (1 + NRHS) x n x (all lines of the grid) doubles.  Rows built in FP32 (the
+// FP32-mixed form) are eliminated in FP64 and the solution rounded once when
+// it is emitted, which stands in for the FP32 elimination and its FP64-residual
+// refinement pass.
 template <class Prob>
 __global__ void __launch_bounds__(128, ThomasMinB<Prob>::v) thomas_line_kernel(Prob prob, int n, double *__restrict__ scr)
 {
-    static_assert(std::is_same<typename Prob::Real, double>::value, "the one-line-per-thread solver takes FP64 rows");
+    using R = typename Prob::Real;
     constexpr int NR = Prob::NRHS;
     if (prob.skip()) return;
     const int l = threadIdx.x;
@@ -952,12 +955,12 @@ __global__ void __launch_bounds__(128, ThomasMinB<Prob>::v) thomas_line_kernel(P
     for (int q = 0; q < NR; q++) dp[q] = 0.0;
 #pragma unroll 2
     for (int r = 0; r < n; r++) {
-        const Coef<double, NR> cf = prob.build(l, r, st);
-        const double a = r ? cf.a : 0.0;
-        const double m = rcp_of<FastRcp<Prob>::on>(cf.b - a * cp);
-        cp = cf.c * m;
+        const Coef<R, NR> cf = prob.build(l, r, st);
+        const double a = r ? (double)cf.a : 0.0;
+        const double m = rcp_of<FastRcp<Prob>::on>((double)cf.b - a * cp);
+        cp = (double)cf.c * m;
 #pragma unroll
-        for (int q = 0; q < NR; q++) dp[q] = (cf.d[q] - a * dp[q]) * m;
+        for (int q = 0; q < NR; q++) dp[q] = ((double)cf.d[q] - a * dp[q]) * m;
         if (r < n - 1) {
             sc[(long long)r * nl] = cp;
 #pragma unroll
@@ -965,14 +968,15 @@ __global__ void __launch_bounds__(128, ThomasMinB<Prob>::v) thomas_line_kernel(P
         }
     }
     double x[NR];
+    R xr[NR];
 #pragma unroll
-    for (int q = 0; q < NR; q++) x[q] = dp[q];
-    prob.emit(l, n - 1, x, st);
+    for (int q = 0; q < NR; q++) { x[q] = dp[q]; xr[q] = R(x[q]); }
+    prob.emit(l, n - 1, xr, st);
     for (int r = n - 2; r >= 0; r--) {
         const double c = sc[(long long)r * nl];
 #pragma unroll
-        for (int q = 0; q < NR; q++) x[q] = sd[((long long)r * NR + q) * nl] - c * x[q];
-        prob.emit(l, r, x, st);
+        for (int q = 0; q < NR; q++) { x[q] = sd[((long long)r * NR + q) * nl] - c * x[q]; xr[q] = R(x[q]); }
+        prob.emit(l, r, xr, st);
     }
 }
 

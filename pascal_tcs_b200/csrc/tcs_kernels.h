@@ -78,7 +78,7 @@ struct Shapes {
     int ifft_lines_x;                            // lines per block of the inverse x transform
     int lanes;                                   // at most this many partitions (lanes) per line
     int long_lines;                              // one-block-per-SM form of long lines: 1 never, 2 z sweeps, 4 z and y sweeps
-    int y_solver;                                // FP64 y lines: 1 partitioned (line_block), 2 one line per thread for the y sweeps, 4 also the modal solves
+    int y_solver;                                // y lines: 1 partitioned (line_block), 2 one line per thread for the y sweeps, 4 also the modal solves
     double *thomas_scr;                          // c', d' of the one-line-per-thread solver (null unless y_solver asks for it)
     FFTPlan fp1, fp3;
     FFTPlan fp1u;                                // N1 with radices up to 8 (the inverse x transform's one-radix form)
@@ -246,18 +246,16 @@ inline void launch_thomas(const Shapes &cx, int n, int nlines, int gy, Make make
     record_launch_error(kernel_name(kid));
 }
 
-// A y sweep (non-cyclic strided lines, nlines x gy of n rows): FP64 rows go
-// to the one-line-per-thread solver when the knob asks for it (y_solver 2 or
-// 4, scratch allocated), everything else to the partitioned line solver, in the
+// A y sweep (non-cyclic strided lines, nlines x gy of n rows): the
+// one-line-per-thread solver when the knob asks for it (y_solver 2 or 4,
+// scratch allocated), else the partitioned line solver, in the
 // one-block-per-SM form where long_lines asks for it for the y sweeps.
 template <class P, class Make>
 inline void launch_y(const Shapes &cx, int n, int nlines, int gy, Make make, cudaStream_t s, int kid)
 {
-    if constexpr (std::is_same<typename P::Real, double>::value) {
-        if (cx.y_solver >= 2 && cx.thomas_scr) {
-            launch_thomas<P>(cx, n, nlines, gy, make, s, kid);
-            return;
-        }
+    if (cx.y_solver >= 2 && cx.thomas_scr) {
+        launch_thomas<P>(cx, n, nlines, gy, make, s, kid);
+        return;
     }
     launch_strided<P>(cx, n, false, nlines, gy, make, s, kid, cx.long_lines >= 4);
 }

@@ -103,8 +103,9 @@ def test_mixed_each_stage_from_identical_inputs(tcs, oracle_mod, case):
     check(["U", "V", "W", "P", "dPhat", "dP0"], "projection")
 
 
-def _run_vs_oracle(tcs, oracle_mod, steps, cfg):
+def _run_vs_oracle(tcs, oracle_mod, steps, cfg, y_solver=1):
     g = tcs.Solver(precision=MIXED, **cfg)
+    g.set_tuning("y_solver", y_solver)
     o = oracle_mod.Oracle(**_oracle_cfg(g))
     g.step(steps)
     hd = o.step(steps)
@@ -119,16 +120,19 @@ def _run_vs_oracle(tcs, oracle_mod, steps, cfg):
     return err
 
 
-def test_mixed_64cube_100_steps_vs_oracle(tcs, oracle_mod):
-    err = _run_vs_oracle(tcs, oracle_mod, 100, CASES[0])
+# y_solver 2: the y sweeps' FP32-built rows eliminated in FP64, one line per thread
+@pytest.mark.parametrize("y_solver", [1, 2])
+def test_mixed_64cube_100_steps_vs_oracle(tcs, oracle_mod, y_solver):
+    err = _run_vs_oracle(tcs, oracle_mod, 100, CASES[0], y_solver)
     for k in ("velocity", "U", "T", "Nu_bot", "Nu_top", "KE"):
         assert err[k] <= RUN_TOL, f"{k}: {err[k]:.3e}"
     for k, tol in ACCUM_TOL.items():
         assert err[k] <= tol, f"{k}: {err[k]:.3e}"
 
 
-def test_mixed_water_40_steps_vs_oracle(tcs, oracle_mod):
-    err = _run_vs_oracle(tcs, oracle_mod, 40, CASES[1])
+@pytest.mark.parametrize("y_solver", [1, 2])
+def test_mixed_water_40_steps_vs_oracle(tcs, oracle_mod, y_solver):
+    err = _run_vs_oracle(tcs, oracle_mod, 40, CASES[1], y_solver)
     for k in ("velocity", "U", "T", "Nu_bot", "Nu_top", "KE"):
         assert err[k] <= RUN_TOL, f"{k}: {err[k]:.3e}"
     for k, tol in ACCUM_TOL.items():

@@ -257,9 +257,15 @@ int tcs_set_use_graph(tcs_ctx *ctx, int on);
  * sizes (its scratch traffic is 1.5x the spectrum's).
  * TCS_TUNE_IFFT_LINES_X: lines per block of the inverse x transform
  * (TCS_TUNE_FFT_LINES_X sets those of the pressure right-hand side and its
- * forward x transform). */
+ * forward x transform).
+ * TCS_TUNE_MIXED_ROWS (FP32-mixed form; no effect in the FP64 form): 1 the x
+ * and z sweeps eliminate their FP32 rows in FP32 with one FP64-residual
+ * refinement pass (default); 2 the x sweeps eliminate their FP32-built rows
+ * in FP64 instead (no refinement pass; the solution is rounded once to FP32);
+ * 4 the x and z sweeps. */
 enum { TCS_TUNE_TL_STRIDED = 0, TCS_TUNE_TL_CONTIG, TCS_TUNE_TL_MODAL, TCS_TUNE_FFT_LINES_X, TCS_TUNE_FFT_LINES_Z,
-       TCS_TUNE_LANES, TCS_TUNE_LONG_LINES, TCS_TUNE_Y_SOLVER, TCS_TUNE_IFFT_LINES_X, TCS_TUNE_COUNT };
+       TCS_TUNE_LANES, TCS_TUNE_LONG_LINES, TCS_TUNE_Y_SOLVER, TCS_TUNE_IFFT_LINES_X, TCS_TUNE_MIXED_ROWS,
+       TCS_TUNE_COUNT };
 int tcs_set_tuning(tcs_ctx *ctx, int knob, int value);
 int tcs_get_tuning(tcs_ctx *ctx, int knob, int *value);
 /* Autotuner (no reference counterpart): coordinate descent over every knob,

@@ -566,6 +566,7 @@ int tcs_create(const tcs_config *cfg, tcs_ctx **out)
     c->cx.long_lines = 2;
     c->cx.y_solver = 1;
     c->cx.thomas_scr = nullptr;
+    c->cx.mixed_rows = 1;
     c->cx.probe = &c->probe;
     sync_shapes(c);
     {   // the FP32 context shares the grid, constants, scalars, tables and history
@@ -981,6 +982,9 @@ int tcs_set_tuning(tcs_ctx *c, int knob, int value)
     case TCS_TUNE_IFFT_LINES_X:
         if (!ifftx_form(x.fp1u, value)) return set_err(TCS_ERR_ARG, "too many lines for shared memory");
         x.ifft_lines_x = value; break;
+    case TCS_TUNE_MIXED_ROWS:
+        if (value > 4) return set_err(TCS_ERR_ARG, "mixed rows: 1 FP32 elimination, 2 FP64 rows in the x sweeps, 4 x and z sweeps");
+        x.mixed_rows = value; break;
     case TCS_TUNE_LANES:
         if (value < 2 || value > 32) return set_err(TCS_ERR_ARG, "lanes per line must be 2..32");
         x.lanes = value; break;
@@ -1033,6 +1037,7 @@ int tcs_get_tuning(tcs_ctx *c, int knob, int *value)
     case TCS_TUNE_LONG_LINES: *value = x.long_lines; break;
     case TCS_TUNE_Y_SOLVER: *value = x.y_solver; break;
     case TCS_TUNE_IFFT_LINES_X: *value = x.ifft_lines_x; break;
+    case TCS_TUNE_MIXED_ROWS: *value = x.mixed_rows; break;
     default: return set_err(TCS_ERR_ARG, "unknown tuning knob");
     }
     return TCS_OK;

@@ -80,6 +80,7 @@ struct Shapes {
     int long_lines;                              // one-block-per-SM form of long lines: 1 never, 2 z sweeps, 4 z and y sweeps
     int y_solver;                                // y lines: 1 partitioned (line_block), 2 one line per thread for the y sweeps, 4 also the modal solves
     double *thomas_scr;                          // c', d' of the one-line-per-thread solver (null unless y_solver asks for it)
+    int mixed_rows;                              // FP32-mixed form: 1 FP32 elimination + refinement, 2 FP64 rows in the x sweeps, 4 x and z sweeps
     FFTPlan fp1, fp3;
     FFTPlan fp1u;                                // N1 with radices up to 8 (the inverse x transform's one-radix form)
     int h1p;
@@ -227,6 +228,36 @@ inline void launch_strided(const Shapes &cx, int n, bool cyclic, int nlines, int
     launch_lines(make(a.TL), a, dim3((nlines + a.TL - 1) / a.TL, gy), s, kid, cx);
 }
 
+// An FP32 line problem whose rows are eliminated in FP64 (Shapes::mixed_rows):
+// the problem's own build in the field type, its coefficients widened to FP64
+// in shared memory, the partitioned solve in FP64 without the refinement pass
+// (Refine<double> is off), and the solution rounded once to the field type when
+// the problem emits it.  Launch shape of the FP64 family of the same axis
+// (AX: 0 the z sweeps, 1 the x sweeps).
+template <class P, int AX>
+struct FP64Rows : P {
+    using Real = double;
+    static constexpr int MINB = AX ? LineOcc<double>::x : LineOcc<double>::z;
+    static constexpr int MREG = AX ? LineOcc<double>::reg_x : LineOcc<double>::reg_z;
+    static constexpr int NT = AX ? LineOcc<double>::nt_x : LineOcc<double>::nt_z;
+    __device__ Coef<double, P::NRHS> build(int l, int r, const typename P::State &st) const
+    {
+        const auto c = P::build(l, r, st);
+        Coef<double, P::NRHS> d;
+        d.a = c.a; d.b = c.b; d.c = c.c;
+#pragma unroll
+        for (int q = 0; q < P::NRHS; q++) d.d[q] = c.d[q];
+        return d;
+    }
+    __device__ void emit(int l, int r, const double *x, const typename P::State &st) const
+    {
+        typename P::Real xr[P::NRHS];
+#pragma unroll
+        for (int q = 0; q < P::NRHS; q++) xr[q] = (typename P::Real)x[q];
+        P::emit(l, r, xr, st);
+    }
+};
+
 // Lines per block of the one-line-per-thread solver (thomas_line_kernel).
 constexpr int THOMAS_TL = 128;
 
@@ -244,6 +275,21 @@ inline void launch_thomas(const Shapes &cx, int n, int nlines, int gy, Make make
     thomas_line_kernel<P><<<dim3((nlines + THOMAS_TL - 1) / THOMAS_TL, gy), THOMAS_TL, 0, s>>>(make(THOMAS_TL), n, cx.thomas_scr);
     probe_end(cx, kid, s);
     record_launch_error(kernel_name(kid));
+}
+
+// A z sweep (cyclic strided lines, nlines x gy of n rows): in the FP32-mixed
+// form with mixed_rows 4 its FP32-built rows are eliminated in FP64.
+template <class P, class Make>
+inline void launch_z(const Shapes &cx, int n, int nlines, int gy, Make make, cudaStream_t s, int kid)
+{
+    if constexpr (std::is_same<typename P::Real, float>::value) {
+        if (cx.mixed_rows >= 4) {
+            using Q = FP64Rows<P, 0>;
+            launch_strided<Q>(cx, n, true, nlines, gy, [&](int tl) { return Q{make(tl)}; }, s, kid, cx.long_lines >= 2);
+            return;
+        }
+    }
+    launch_strided<P>(cx, n, true, nlines, gy, make, s, kid, cx.long_lines >= 2);
 }
 
 // A y sweep (non-cyclic strided lines, nlines x gy of n rows): the
@@ -384,11 +430,20 @@ inline void multi_x(const std::vector<Ctx<R> *> &cs, MultiArena &A, cudaStream_t
 }
 
 // An x sweep: lines along i, one block row per (j-range, k).  FP32 runs the
-// 128-thread shape when at least 4 lines fit a block, else the wide shape.
+// 128-thread shape when at least 4 lines fit a block, else the wide shape;
+// with mixed_rows >= 2 the FP32-built rows are eliminated in FP64 instead.
 template <template <class, int, int> class X, class R>
 inline void launch_x(const Ctx<R> &cx, int nlines, cudaStream_t s, int kid)
 {
     const GridT<R> &g = cx.g;
+    if constexpr (LineOcc<R>::f32) {
+        if (cx.mixed_rows >= 2) {   // FP32-built rows eliminated in FP64
+            using P = FP64Rows<X<R, 0, 0>, 1>;
+            const LinePlan p = make_line_plan(g.N1, true, fit_tl<P>(g.N1, true, cx.tl_contig, cx.lanes), cx.lanes);
+            launch_lines(P{X<R, 0, 0>{g, cx.f, p.TL}}, p, dim3((nlines + p.TL - 1) / p.TL, g.N3), s, kid, cx);
+            return;
+        }
+    }
     const int tl = fit_tl<X<R, 0, 0>>(g.N1, true, cx.tl_contig, cx.lanes);
     if constexpr (LineOcc<R>::f32) {
         if (tl < 4) {

@@ -624,7 +624,7 @@ template <class R>
 void launch_solve_du(const Ctx<R> &cx, cudaStream_t s)
 {
     const GridT<R> &g = cx.g;
-    launch_strided<DUZ<R>>(cx, g.N3, true, g.N1, g.N2, [&](int tl) { return DUZ<R>{g, cx.f, tl}; }, s, K_DU_Z, cx.long_lines >= 2);
+    launch_z<DUZ<R>>(cx, g.N3, g.N1, g.N2, [&](int tl) { return DUZ<R>{g, cx.f, tl}; }, s, K_DU_Z);
     launch_x<DUX>(cx, g.N2, s, K_DU_X);
     launch_y<DUY<R>>(cx, g.N2, g.N1, g.N3, [&](int tl) { return DUY<R>{g, cx.f, tl}; }, s, K_DU_Y);
 }
@@ -633,7 +633,7 @@ template <class R>
 void launch_solve_dv(const Ctx<R> &cx, cudaStream_t s)
 {
     const GridT<R> &g = cx.g;
-    launch_strided<DVZ<R>>(cx, g.N3, true, g.N1, g.N2 - 1, [&](int tl) { return DVZ<R>{g, cx.f, tl}; }, s, K_DV_Z, cx.long_lines >= 2);
+    launch_z<DVZ<R>>(cx, g.N3, g.N1, g.N2 - 1, [&](int tl) { return DVZ<R>{g, cx.f, tl}; }, s, K_DV_Z);
     launch_x<DVX>(cx, g.N2 - 1, s, K_DV_X);
     launch_y<DVY<R>>(cx, g.N2 - 1, g.N1, g.N3, [&](int tl) { return DVY<R>{g, cx.f, tl}; }, s, K_DV_Y);
 }
@@ -642,7 +642,7 @@ template <class R>
 void launch_solve_dw(const Ctx<R> &cx, cudaStream_t s)
 {
     const GridT<R> &g = cx.g;
-    launch_strided<DWZ<R>>(cx, g.N3, true, g.N1, g.N2, [&](int tl) { return DWZ<R>{g, cx.f, tl}; }, s, K_DW_Z, cx.long_lines >= 2);
+    launch_z<DWZ<R>>(cx, g.N3, g.N1, g.N2, [&](int tl) { return DWZ<R>{g, cx.f, tl}; }, s, K_DW_Z);
     launch_x<DWX>(cx, g.N2, s, K_DW_X);
     launch_y<DWY<R>>(cx, g.N2, g.N1, g.N3, [&](int tl) { return DWY<R>{g, cx.f, tl}; }, s, K_DW_Y);
 }

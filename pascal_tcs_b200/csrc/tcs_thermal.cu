@@ -246,7 +246,7 @@ template <class R>
 void launch_thermal(const Ctx<R> &cx, cudaStream_t s)
 {
     const GridT<R> &g = cx.g;
-    launch_strided<ThermalZ<R>>(cx, g.N3, true, g.N1, g.N2, [&](int tl) { return ThermalZ<R>{g, cx.f, tl}; }, s, K_THERMAL_Z, cx.long_lines >= 2);
+    launch_z<ThermalZ<R>>(cx, g.N3, g.N1, g.N2, [&](int tl) { return ThermalZ<R>{g, cx.f, tl}; }, s, K_THERMAL_Z);
     launch_x<ThermalX>(cx, g.N2, s, K_THERMAL_X);
     launch_y<ThermalY<R>>(cx, g.N2, g.N1, g.N3, [&](int tl) { return ThermalY<R>{g, cx.f, tl}; }, s, K_THERMAL_Y);
 }

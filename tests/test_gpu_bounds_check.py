@@ -47,8 +47,8 @@ SCRIPT = textwrap.dedent("""
             counts[f"case{{ci}} prec{{prec}}"] = g.bounds_violations()
             g.close()
     for knob, v in (("lanes", 4), ("tl_strided", 2), ("tl_contig", 1), ("tl_modal", 1), ("fft_lines_x", 1),
-                    ("fft_lines_z", 8), ("long_lines", 4), ("y_solver", 4)):
-        for prec in ((0, 1) if knob == "y_solver" else (0,)):
+                    ("fft_lines_z", 8), ("long_lines", 4), ("y_solver", 4), ("mixed_rows", 4), ("ifft_lines_x", 8)):
+        for prec in ((0, 1) if knob in ("y_solver", "mixed_rows") else (0,)):
             g = P.Solver(n1m=150 if knob == "y_solver" else 48, n2m=32, n3m=40, property_set=1, Pr=7.0, Ra=1e6,
                          dtStart=5e-4, precision=prec)
             g.set_tuning(knob, v)

@@ -103,9 +103,10 @@ def test_mixed_each_stage_from_identical_inputs(tcs, oracle_mod, case):
     check(["U", "V", "W", "P", "dPhat", "dP0"], "projection")
 
 
-def _run_vs_oracle(tcs, oracle_mod, steps, cfg, y_solver=1):
+def _run_vs_oracle(tcs, oracle_mod, steps, cfg, solvers=(1, 1)):
     g = tcs.Solver(precision=MIXED, **cfg)
-    g.set_tuning("y_solver", y_solver)
+    g.set_tuning("y_solver", solvers[0])
+    g.set_tuning("mixed_rows", solvers[1])
     o = oracle_mod.Oracle(**_oracle_cfg(g))
     g.step(steps)
     hd = o.step(steps)
@@ -120,19 +121,24 @@ def _run_vs_oracle(tcs, oracle_mod, steps, cfg, y_solver=1):
     return err
 
 
-# y_solver 2: the y sweeps' FP32-built rows eliminated in FP64, one line per thread
-@pytest.mark.parametrize("y_solver", [1, 2])
-def test_mixed_64cube_100_steps_vs_oracle(tcs, oracle_mod, y_solver):
-    err = _run_vs_oracle(tcs, oracle_mod, 100, CASES[0], y_solver)
+# (y_solver, mixed_rows): (1, 1) FP32 eliminations with FP64-residual
+# refinement; (2, 4) the FP32-built rows of every sweep eliminated in FP64 (the
+# y sweeps one line per thread, the x and z sweeps on the partitioned solver)
+SOLVERS = [(1, 1), (2, 4)]
+
+
+@pytest.mark.parametrize("solvers", SOLVERS)
+def test_mixed_64cube_100_steps_vs_oracle(tcs, oracle_mod, solvers):
+    err = _run_vs_oracle(tcs, oracle_mod, 100, CASES[0], solvers)
     for k in ("velocity", "U", "T", "Nu_bot", "Nu_top", "KE"):
         assert err[k] <= RUN_TOL, f"{k}: {err[k]:.3e}"
     for k, tol in ACCUM_TOL.items():
         assert err[k] <= tol, f"{k}: {err[k]:.3e}"
 
 
-@pytest.mark.parametrize("y_solver", [1, 2])
-def test_mixed_water_40_steps_vs_oracle(tcs, oracle_mod, y_solver):
-    err = _run_vs_oracle(tcs, oracle_mod, 40, CASES[1], y_solver)
+@pytest.mark.parametrize("solvers", SOLVERS)
+def test_mixed_water_40_steps_vs_oracle(tcs, oracle_mod, solvers):
+    err = _run_vs_oracle(tcs, oracle_mod, 40, CASES[1], solvers)
     for k in ("velocity", "U", "T", "Nu_bot", "Nu_top", "KE"):
         assert err[k] <= RUN_TOL, f"{k}: {err[k]:.3e}"
     for k, tol in ACCUM_TOL.items():

@@ -37,7 +37,8 @@ def test_autotune_keeps_state_and_caches(tcs, tmp_path):
 
 @pytest.mark.parametrize("knob,value", [("lanes", 8), ("lanes", 16), ("tl_strided", 2), ("tl_contig", 16),
                                         ("tl_modal", 1), ("fft_lines_x", 1), ("fft_lines_z", 8),
-                                        ("long_lines", 1), ("long_lines", 4), ("y_solver", 2), ("y_solver", 4)])
+                                        ("long_lines", 1), ("long_lines", 4), ("y_solver", 2), ("y_solver", 4),
+                                        ("ifft_lines_x", 8), ("mixed_rows", 4)])
 def test_every_knob_setting_gives_the_same_step(tcs, knob, value):
     a, b = tcs.Solver(**CFG), tcs.Solver(**CFG)
     b.set_tuning(knob, value)
@@ -66,25 +67,27 @@ def test_long_line_forms_are_bit_identical(tcs, precision):
             np.testing.assert_array_equal(r[n], x, err_msg=n)
 
 
-@pytest.mark.parametrize("value", [2, 4])
-def test_y_solver_in_the_mixed_form(tcs, value):
-    # 2: the y sweeps' FP32-built rows eliminated in FP64 with one line per
-    # thread instead of the FP32 elimination and its refinement; 4: the modal
-    # pressure solves (FP64 rows in both forms) too.  Both runs store their
-    # fields in FP32 and each lies within a few 1e-6 of the FP64 form, so they
-    # agree to the mixed form's 1e-5 bar (measured: V 2.3e-6 apart after 3
-    # steps, V being the smallest component here).
+@pytest.mark.parametrize("knob,value", [("y_solver", 2), ("y_solver", 4), ("mixed_rows", 2), ("mixed_rows", 4)])
+def test_solver_knobs_in_the_mixed_form(tcs, knob, value):
+    # y_solver 2: the y sweeps' FP32-built rows eliminated in FP64 with one line
+    # per thread instead of the FP32 elimination and its refinement; 4: the
+    # modal pressure solves (FP64 rows in both forms) too.  mixed_rows 2 / 4:
+    # the x (and z) sweeps' FP32-built rows eliminated in FP64 on the
+    # partitioned solver.  Both runs store their fields in FP32 and each lies
+    # within a few 1e-6 of the FP64 form, so they agree to the mixed form's 1e-5
+    # bar (measured: V 2.3e-6 apart after 3 steps, V being the smallest
+    # component here).
     cfg = dict(CFG, precision=1)
     a, b = tcs.Solver(**cfg), tcs.Solver(**cfg)
-    b.set_tuning("y_solver", value)
-    assert b.tuning()["y_solver"] == value
+    b.set_tuning(knob, value)
+    assert b.tuning()[knob] == value
     a.step(3); b.step(3)
     for n in ("T", "U", "V", "W", "P"):
         x, y = a.get(n), b.get(n)
         assert np.linalg.norm(x - y) <= 1e-5 * np.linalg.norm(x), n
     with pytest.raises(tcs.TcsError) as ei:
-        b.set_tuning("y_solver", 8)
+        b.set_tuning(knob, 8)
     assert ei.value.code == 1
-    b.set_tuning("y_solver", 1)                     # frees the scratch; the partitioned solver again
+    b.set_tuning(knob, 1)                           # the partitioned FP32 eliminations again (frees any scratch)
     b.step(1); a.step(1)
     assert np.linalg.norm(a.get("P") - b.get("P")) <= 1e-5 * np.linalg.norm(a.get("P"))

@@ -262,10 +262,15 @@ int tcs_set_use_graph(tcs_ctx *ctx, int on);
  * and z sweeps eliminate their FP32 rows in FP32 with one FP64-residual
  * refinement pass (default); 2 the x sweeps eliminate their FP32-built rows
  * in FP64 instead (no refinement pass; the solution is rounded once to FP32);
- * 4 the x and z sweeps. */
+ * 4 the x and z sweeps.
+ * TCS_TUNE_Z_STAGING (FP64 form): 1 the z sweep of solvedW reads its stencil
+ * inputs from global memory (default); 2 it stages them into shared memory with
+ * tensor-memory-accelerator (TMA) box copies one pass of 64 k-planes ahead
+ * (same arithmetic, same results; refused, TCS_ERR_ARG, unless the form is
+ * FP64, N3 a multiple of 64 and N1 even). */
 enum { TCS_TUNE_TL_STRIDED = 0, TCS_TUNE_TL_CONTIG, TCS_TUNE_TL_MODAL, TCS_TUNE_FFT_LINES_X, TCS_TUNE_FFT_LINES_Z,
        TCS_TUNE_LANES, TCS_TUNE_LONG_LINES, TCS_TUNE_Y_SOLVER, TCS_TUNE_IFFT_LINES_X, TCS_TUNE_MIXED_ROWS,
-       TCS_TUNE_COUNT };
+       TCS_TUNE_Z_STAGING, TCS_TUNE_COUNT };
 int tcs_set_tuning(tcs_ctx *ctx, int knob, int value);
 int tcs_get_tuning(tcs_ctx *ctx, int knob, int *value);
 /* Autotuner (no reference counterpart): coordinate descent over every knob,

@@ -567,6 +567,7 @@ int tcs_create(const tcs_config *cfg, tcs_ctx **out)
     c->cx.y_solver = 1;
     c->cx.thomas_scr = nullptr;
     c->cx.mixed_rows = 1;
+    c->cx.z_staging = 1;
     c->cx.probe = &c->probe;
     sync_shapes(c);
     {   // the FP32 context shares the grid, constants, scalars, tables and history
@@ -985,6 +986,11 @@ int tcs_set_tuning(tcs_ctx *c, int knob, int value)
     case TCS_TUNE_MIXED_ROWS:
         if (value > 4) return set_err(TCS_ERR_ARG, "mixed rows: 1 FP32 elimination, 2 FP64 rows in the x sweeps, 4 x and z sweeps");
         x.mixed_rows = value; break;
+    case TCS_TUNE_Z_STAGING:
+        if (value > 2) return set_err(TCS_ERR_ARG, "z staging: 1 global loads, 2 TMA-staged inputs for dw_z");
+        if (value == 2 && (c->fp32 || !dwz_staging_possible(x)))
+            return set_err(TCS_ERR_ARG, "z staging needs the FP64 form, N3 a multiple of 64 and an even N1");
+        x.z_staging = value; break;
     case TCS_TUNE_LANES:
         if (value < 2 || value > 32) return set_err(TCS_ERR_ARG, "lanes per line must be 2..32");
         x.lanes = value; break;
@@ -1038,6 +1044,7 @@ int tcs_get_tuning(tcs_ctx *c, int knob, int *value)
     case TCS_TUNE_Y_SOLVER: *value = x.y_solver; break;
     case TCS_TUNE_IFFT_LINES_X: *value = x.ifft_lines_x; break;
     case TCS_TUNE_MIXED_ROWS: *value = x.mixed_rows; break;
+    case TCS_TUNE_Z_STAGING: *value = x.z_staging; break;
     default: return set_err(TCS_ERR_ARG, "unknown tuning knob");
     }
     return TCS_OK;

@@ -69,11 +69,13 @@ enum : int {
     S_DT = 0, S_TIME, S_CFL, S_MAXDIV, S_NUBOT, S_NUTOP, S_KE, S_BLOWUP, S_AVER,
     S_STEP, S_FIXED_DT, S_NSCAL
 };
-// One more device double past the public scalars: in a build with
+// Device doubles past the public scalars: S_OOB, in a build with
 // -DTCS_BOUNDS_CHECK, the number of out-of-range indices the kernels met
 // (each one recorded here and its access redirected to a valid cell instead of
-// made; the stand-in for a memory checker).  It stays 0 in the normal build.
-enum : int { S_OOB = S_NSCAL, S_NALLOC };
+// made; the stand-in for a memory checker; 0 in the normal build); S_TIMEOUT,
+// the number of bounded waits on asynchronous copies that ran out (a kernel
+// that records one also sets S_BLOWUP, so the step stops and reports).
+enum : int { S_OOB = S_NSCAL, S_TIMEOUT, S_NALLOC };
 
 #if defined(TCS_BOUNDS_CHECK) && defined(__CUDA_ARCH__)
 #define TCS_OOB(scal, bad, fix)                          \

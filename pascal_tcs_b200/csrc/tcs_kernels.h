@@ -81,6 +81,7 @@ struct Shapes {
     int y_solver;                                // y lines: 1 partitioned (line_block), 2 one line per thread for the y sweeps, 4 also the modal solves
     double *thomas_scr;                          // c', d' of the one-line-per-thread solver (null unless y_solver asks for it)
     int mixed_rows;                              // FP32-mixed form: 1 FP32 elimination + refinement, 2 FP64 rows in the x sweeps, 4 x and z sweeps
+    int z_staging;                               // FP64 dw_z: 1 loads from global memory, 2 inputs staged by TMA
     FFTPlan fp1, fp3;
     FFTPlan fp1u;                                // N1 with radices up to 8 (the inverse x transform's one-radix form)
     int h1p;
@@ -463,6 +464,7 @@ template <class R> void launch_momentum_coeffi(const Ctx<R> &cx, cudaStream_t s)
 template <class R> void launch_solve_du(const Ctx<R> &cx, cudaStream_t s);
 template <class R> void launch_solve_dv(const Ctx<R> &cx, cudaStream_t s);
 template <class R> void launch_solve_dw(const Ctx<R> &cx, cudaStream_t s);
+bool dwz_staging_possible(const Ctx<double> &cx);   // the TMA-staged dw_z can run this case
 template <class R> void launch_blockld_v(const Ctx<R> &cx, cudaStream_t s);
 template <class R> void launch_blockld_u(const Ctx<R> &cx, cudaStream_t s);
 template <class R> void launch_pseudo_update(const Ctx<R> &cx, cudaStream_t s);   // standalone (Un = U + dU, ...)

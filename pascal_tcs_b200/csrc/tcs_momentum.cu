@@ -9,6 +9,7 @@
 // reference assigns whole rows Mu(:,j,k) inside its i loop (:156-171), so every
 // value along i equals the one computed from T(n1sub,j,k).
 #include "tcs_kernels.h"
+#include "tcs_tma.cuh"
 
 namespace tcs {
 
@@ -432,7 +433,18 @@ struct DWZ {
     __device__ State prepare() const { return State{R(g.scal[S_DT])}; }
     __device__ int li(int l) const { return 1 + vbx<ITEM>() * TL + l; }
     __device__ bool line_ok(int l) const { return li(l) <= g.N1; }
+    // The stencil inputs of a cell, read through val(array, di, dj, dk): from
+    // global memory (build) or from the staged tiles (dwz_staged_kernel), with
+    // the same arithmetic after them.
+    enum : int { A_W = 0, A_U, A_V, A_DU, A_DV, A_P };
     __device__ Coef<R, 1> build(int l, int r, const State &st) const
+    {
+        const long long c = ix(g, li(l), 1 + vby<ITEM>(), r + 1), sj = g.P1, sk = (long long)g.P1 * g.P2;
+        const R *const arr[6] = {f.W, f.U, f.V, f.dU, f.dV, f.P};
+        return build_with([&](int a, int di, int dj, int dk) { return ld(arr[a] + (c + di + dj * sj + dk * sk)); }, l, r, st);
+    }
+    template <class Val>
+    __device__ __forceinline__ Coef<R, 1> build_with(const Val &val, int l, int r, const State &st) const
     {
         const int i = li(l), j = 1 + vby<ITEM>(), k = r + 1;
         const int im = i - 1, ip = i + 1, jm = j - 1, jp = j + 1, km = k - 1;
@@ -440,15 +452,13 @@ struct DWZ {
         const R *dx1 = g.m1.dx, *dx2 = g.m2.dx, *dx3 = g.m3.dx;
         const R *rdx1 = g.m1.rdx, *rdx2 = g.m2.rdx, *rdx3 = g.m3.rdx;
         const R *rdmx1 = g.m1.rdmx, *rdmx2 = g.m2.rdmx, *rdmx3 = g.m3.rdmx;
-        const long long c = ix(g, i, j, k), sj = g.P1, sk = (long long)g.P1 * g.P2;
-        const R *U = f.U, *V = f.V, *W = f.W, *dU = f.dU, *dV = f.dV;
         const R jwm = (j == 1) ? R(0.0) : R(1.0), jwp = (j == g.N2) ? R(0.0) : R(1.0);
-        const R Wc = ld(W + c), Wzm = ld(W + c - sk), Wzp = ld(W + c + sk), Wxm = ld(W + c - 1), Wxp = ld(W + c + 1);
-        const R Wym = ld(W + c - sj), Wyp = ld(W + c + sj);
-        const R Uc = ld(U + c), Uzm = ld(U + c - sk), Uxp = ld(U + c + 1), Uxpzm = ld(U + c + 1 - sk);
-        const R Vc = ld(V + c), Vzm = ld(V + c - sk), Vyp = ld(V + c + sj), Vypzm = ld(V + c + sj - sk);
-        const R dUc = ld(dU + c), dUzm = ld(dU + c - sk), dUxp = ld(dU + c + 1), dUxpzm = ld(dU + c + 1 - sk);
-        const R dVc = ld(dV + c), dVzm = ld(dV + c - sk), dVyp = ld(dV + c + sj), dVypzm = ld(dV + c + sj - sk);
+        const R Wc = val(A_W, 0, 0, 0), Wzm = val(A_W, 0, 0, -1), Wzp = val(A_W, 0, 0, 1), Wxm = val(A_W, -1, 0, 0), Wxp = val(A_W, 1, 0, 0);
+        const R Wym = val(A_W, 0, -1, 0), Wyp = val(A_W, 0, 1, 0);
+        const R Uc = val(A_U, 0, 0, 0), Uzm = val(A_U, 0, 0, -1), Uxp = val(A_U, 1, 0, 0), Uxpzm = val(A_U, 1, 0, -1);
+        const R Vc = val(A_V, 0, 0, 0), Vzm = val(A_V, 0, 0, -1), Vyp = val(A_V, 0, 1, 0), Vypzm = val(A_V, 0, 1, -1);
+        const R dUc = val(A_DU, 0, 0, 0), dUzm = val(A_DU, 0, 0, -1), dUxp = val(A_DU, 1, 0, 0), dUxpzm = val(A_DU, 1, 0, -1);
+        const R dVc = val(A_DV, 0, 0, 0), dVzm = val(A_DV, 0, 0, -1), dVyp = val(A_DV, 0, 1, 0), dVypzm = val(A_DV, 0, 1, -1);
         const R Mjk = MU(j, k), Mjkm = MU(j, km), Mjmk = MU(jm, k), Mjmkm = MU(jm, km), Mjpk = MU(jp, k), Mjpkm = MU(jp, km);
         const R iRjk = IR(j, k), iRjkm = IR(j, km);
         const R w5 = R(0.5) * (Wc + Wzm), w6 = R(0.5) * (Wc + Wzp);
@@ -485,7 +495,7 @@ struct DWZ {
         // reference's form on the wall-adjacent planes (j = 1, N2).
         R rhs = R(2.0) * ih * (vw1 + vw31) + R(4.0) * ih * vw3 - R(0.5) * (u1 * dwdx1 + u2 * dwdx2) - R(0.5) * (w5 * dwdz5 + w6 * dwdz6)
                 - R(0.25) * (ddu1 * dwdx1 + ddu2 * dwdx2) + ih * rdx1[i] * (mu2 * ddudz2 - mu1 * ddudz1);
-        rhs = rhs - p.Cmp * invRhoc * (ld(f.P + c) - ld(f.P + c - sk)) * rdmx3[k];
+        rhs = rhs - p.Cmp * invRhoc * (val(A_P, 0, 0, 0) - val(A_P, 0, 0, -1)) * rdmx3[k];
         if (j != 1 && j != g.N2) {
             rhs = rhs + R(2.0) * ih * (vw2 + vw32) - R(0.5) * (v3 * dwdy3 + v4 * dwdy4)
                   - R(0.25) * (ddv3 * dwdy3 + ddv4 * dwdy4) + ih * rdx2[j] * (mu4 * ddvdz4 - mu3 * ddvdz3);
@@ -620,6 +630,201 @@ struct DWY {
     __device__ void emit(int l, int r, const R *x, const State &st) const { store_periodic(g, f.dW, li(l), r + 1, 1 + vby<ITEM>(), x[0]); }
 };
 
+// ---------------------------------------------------------------------------
+// solvedW's z sweep with its stencil inputs staged by TMA (FP64 form,
+// TCS_TUNE_Z_STAGING 2).  The same lines, rows, arithmetic and solve as the
+// DWZ line-solver launch (DWZ::build_with is shared, so the results are the
+// same bits); only where the stencil inputs come from differs.  A block of
+// 512 threads owns 8 lines (i0..i0+7) of one j; the rows are built in passes of
+// ZS_CH = 64 k-planes, one cell per thread per pass, from shared-memory boxes
+// of the six input arrays that the tensor memory accelerator copies one pass
+// ahead (two buffers):
+//   W       i0-1..i0+8 x j-1..j+1 x k-1..k+64      (x and y neighbours, k +-1)
+//   U, dU   i0-1..i0+8 x j        x k-1..k+63
+//   V, dV   i0-1..i0+8 x j..j+1   x k-1..k+63
+//   P       i0-1..i0+8 x j        x k-1..k+63
+// Every box starts at x = i0-1 = 8 bx, an even element, so its first byte is
+// 16-byte aligned as TMA requires, and is 10 doubles (80 bytes) wide.  It
+// requires N3 a multiple of ZS_CH and an even N1 (the row pitch a multiple of
+// 16 bytes); launch_solve_dw checks both.
+// ---------------------------------------------------------------------------
+constexpr int ZS_CH = 64, ZS_TL = 8, ZS_NT = 512;
+constexpr int ZS_WAIT = 1 << 22;   // polls of a bounded wait (each try_wait suspends briefly)
+__host__ __device__ constexpr int zs_rows(int a) { return a == 0 ? 3 : ((a == 2 || a == 4) ? 2 : 1); }
+__host__ __device__ constexpr int zs_planes(int a) { return a == 0 ? ZS_CH + 2 : ZS_CH + 1; }
+__host__ __device__ constexpr int zs_bytes(int a) { return 10 * zs_rows(a) * zs_planes(a) * 8; }
+__host__ __device__ constexpr int zs_off(int a) { return a == 0 ? 0 : zs_off(a - 1) + (zs_bytes(a - 1) + 127) / 128 * 128; }
+constexpr int ZS_BUF = zs_off(6);
+constexpr int ZS_TX = zs_bytes(0) + zs_bytes(1) + zs_bytes(2) + zs_bytes(3) + zs_bytes(4) + zs_bytes(5);
+
+struct alignas(64) DWZMaps {
+    CUtensorMap m[6];   // DWZ's A_W, A_U, A_V, A_DU, A_DV, A_P
+};
+
+// Dynamic shared memory: two box buffers, the rows (A, C, D), the row map, two mbarriers.
+inline size_t zs_smem(const LinePlan &lp)
+{
+    const size_t rows = (size_t)3 * ZS_TL * lp.LS * sizeof(double) + (size_t)lp.n * sizeof(int);
+    return 2 * (size_t)ZS_BUF + ((rows + 15) & ~(size_t)15) + 2 * sizeof(uint64_t);
+}
+
+__global__ void __launch_bounds__(ZS_NT, 1) dwz_staged_kernel(const __grid_constant__ DWZ<double> prob,
+                                                              const __grid_constant__ DWZMaps maps, LinePlan lp)
+{
+    using P = DWZ<double>;
+    extern __shared__ __align__(128) unsigned char smraw[];
+    if (prob.skip()) return;
+    const P::State st = prob.prepare();
+    const int n = lp.n, LS = lp.LS, DS = ZS_TL * LS, nch = n / ZS_CH;
+    double *const sA = reinterpret_cast<double *>(smraw + 2 * ZS_BUF), *const sC = sA + DS, *const sD = sC + DS;
+    int *const spos = reinterpret_cast<int *>(sD + DS);
+    const size_t rows = (size_t)3 * DS * sizeof(double) + (size_t)n * sizeof(int);
+    uint64_t *const bar = reinterpret_cast<uint64_t *>(smraw + 2 * ZS_BUF + ((rows + 15) & ~(size_t)15));
+    const int x0 = ZS_TL * blockIdx.x, j = 1 + blockIdx.y;
+    if (smem_u32(smraw) & 127) {   // the boxes need 128-byte aligned destinations: record and stop, copy nothing
+        if (threadIdx.x == 0) {
+            atomicAdd(prob.g.scal + S_TIMEOUT, 1.0);
+            prob.g.scal[S_BLOWUP] = 1.0;
+        }
+        return;
+    }
+    if (threadIdx.x == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        mbar_init_fence();
+    }
+    if (threadIdx.x < lp.P) {
+        const int p = threadIdx.x, m = lp.m0 + (p < lp.rem ? 1 : 0), start = p * lp.m0 + (p < lp.rem ? p : lp.rem);
+        for (int q = 0; q < m; q++) spos[start + q] = p * lp.PS + q;
+    }
+    __syncthreads();
+    auto issue = [&](int c) {   // thread 0: the boxes of pass c into buffer c & 1
+        uint64_t *b = &bar[c & 1];
+        unsigned char *dst = smraw + (c & 1) * ZS_BUF;
+        mbar_arrive_expect_tx(b, ZS_TX);
+#pragma unroll
+        for (int a = 0; a < 6; a++) tma_load_3d(dst + zs_off(a), &maps.m[a], b, x0, a == P::A_W ? j - 1 : j, c * ZS_CH);
+    };
+    if (threadIdx.x == 0) {
+        issue(0);
+        if (nch > 1) issue(1);
+    }
+    const int l = threadIdx.x & (ZS_TL - 1), rr = threadIdx.x >> 3;   // one cell per thread per pass
+    int c = 0;
+    bool ok = true;
+    for (; c < nch; c++) {
+        const bool got = mbar_wait(&bar[c & 1], (c >> 1) & 1, ZS_WAIT);
+        if (__syncthreads_or(!got)) { ok = false; break; }
+        const double *const t = reinterpret_cast<const double *>(smraw + (c & 1) * ZS_BUF);
+        // row r = c ZS_CH + rr is plane k = r + 1, plane k + dk of a box at z = rr + 1 + dk
+        auto val = [&](int a, int di, int dj, int dk) -> double {
+            const int z = rr + 1 + dk, y = (a == P::A_W) ? 1 + dj : dj;
+            return t[zs_off(a) / 8 + (z * zs_rows(a) + y) * 10 + (l + 1 + di)];
+        };
+        const int r = c * ZS_CH + rr;
+        Coef<double, 1> cf;
+        if (prob.line_ok(l)) {
+            cf = prob.build_with(val, l, r, st);
+        } else {
+            cf.a = 0.0; cf.b = 1.0; cf.c = 0.0; cf.d[0] = 0.0;
+        }
+        const double rb = rcp_of<FastRcp<P>::on>(cf.b);
+        const int pos = l * LS + spos[r];
+        sA[pos] = cf.a * rb; sC[pos] = cf.c * rb; sD[pos] = cf.d[0] * rb;
+        __syncthreads();   // every thread is done with this buffer
+        if (threadIdx.x == 0 && c + 2 < nch) {
+            fence_proxy_async();
+            issue(c + 2);
+        }
+    }
+    if (!ok) {
+        // a copy did not arrive in time: record it, stop the step, and wait
+        // (bounded) for this block's copies still in flight before leaving
+        if (threadIdx.x == 0) {
+            atomicAdd(prob.g.scal + S_TIMEOUT, 1.0);
+            prob.g.scal[S_BLOWUP] = 1.0;
+            for (int d = c; d < c + 2 && d < nch; d++) mbar_wait(&bar[d & 1], (d >> 1) & 1, ZS_WAIT);
+        }
+        return;
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int ll = warp; ll < ZS_TL; ll += ZS_NT / 32)
+        solve_line<double, 1, P::MREG, false, FastRcp<P>::on>(sA + ll * LS, sC + ll * LS, sD + ll * LS, DS, lp, lane);
+    __syncthreads();
+    if (prob.line_ok(l))
+        for (int r = rr; r < n; r += ZS_NT / ZS_TL) {
+            const double x = sD[l * LS + spos[r]];
+            prob.emit(l, r, &x, st);
+        }
+}
+
+// The tensor maps of the staged z sweep: one 3-D map (x = i, y = j, z = k over
+// the padded array) per input array with that array's box.
+typedef CUresult (*PfnTensorMapEncodeTiled)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                            const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                            CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+static PfnTensorMapEncodeTiled tensor_map_encoder()
+{
+    static PfnTensorMapEncodeTiled fn = [] {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &f, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess) {
+            cudaGetLastError();
+            f = nullptr;
+        }
+        return (PfnTensorMapEncodeTiled)f;
+    }();
+    return fn;
+}
+
+static bool dwz_maps(const Ctx<double> &cx, DWZMaps &mp)
+{
+    const GridT<double> &g = cx.g;
+    PfnTensorMapEncodeTiled enc = tensor_map_encoder();
+    if (!enc) return false;
+    const double *src[6] = {cx.f.W, cx.f.U, cx.f.V, cx.f.dU, cx.f.dV, cx.f.P};
+    const cuuint64_t dims[3] = {(cuuint64_t)g.P1, (cuuint64_t)g.P2, (cuuint64_t)g.N3 + 2};
+    const cuuint64_t strides[2] = {(cuuint64_t)g.P1 * 8, (cuuint64_t)g.P1 * g.P2 * 8};
+    const cuuint32_t es[3] = {1, 1, 1};
+    for (int a = 0; a < 6; a++) {
+        const cuuint32_t box[3] = {10, (cuuint32_t)zs_rows(a), (cuuint32_t)zs_planes(a)};
+        if (enc(&mp.m[a], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, (void *)src[a], dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+            return false;
+    }
+    return true;
+}
+
+// Whether the staged form can run this case (shape, shared memory, tensor-map encoder).
+bool dwz_staging_possible(const Ctx<double> &cx)
+{
+    const GridT<double> &g = cx.g;
+    if (g.N3 % ZS_CH || (g.P1 * 8) % 16) return false;
+    if (zs_smem(make_line_plan(g.N3, true, ZS_TL, cx.lanes)) > 227 * 1024) return false;
+    DWZMaps mp;
+    return dwz_maps(cx, mp);
+}
+
+// Launches the staged form if the knob asks for it and the shape allows it.
+static bool launch_dwz_staged(const Ctx<double> &cx, cudaStream_t s)
+{
+    const GridT<double> &g = cx.g;
+    if (cx.z_staging != 2 || g.N3 % ZS_CH || (g.P1 * 8) % 16) return false;
+    const LinePlan lp = make_line_plan(g.N3, true, ZS_TL, cx.lanes);
+    const size_t sm = zs_smem(lp);
+    if (sm > 227 * 1024) return false;
+    DWZMaps mp;
+    if (!dwz_maps(cx, mp)) return false;
+    static size_t conf[64] = {};
+    smem_opt_in((const void *)dwz_staged_kernel, sm, conf);
+    probe_begin(cx, K_DW_Z, s);
+    dwz_staged_kernel<<<dim3((g.N1 + ZS_TL - 1) / ZS_TL, g.N2), ZS_NT, sm, s>>>(DWZ<double>{g, cx.f, ZS_TL}, mp, lp);
+    probe_end(cx, K_DW_Z, s);
+    record_launch_error(kernel_name(K_DW_Z));
+    return true;
+}
+
 template <class R>
 void launch_solve_du(const Ctx<R> &cx, cudaStream_t s)
 {
@@ -642,7 +847,9 @@ template <class R>
 void launch_solve_dw(const Ctx<R> &cx, cudaStream_t s)
 {
     const GridT<R> &g = cx.g;
-    launch_z<DWZ<R>>(cx, g.N3, g.N1, g.N2, [&](int tl) { return DWZ<R>{g, cx.f, tl}; }, s, K_DW_Z);
+    bool staged = false;
+    if constexpr (std::is_same<R, double>::value) staged = launch_dwz_staged(cx, s);
+    if (!staged) launch_z<DWZ<R>>(cx, g.N3, g.N1, g.N2, [&](int tl) { return DWZ<R>{g, cx.f, tl}; }, s, K_DW_Z);
     launch_x<DWX>(cx, g.N2, s, K_DW_X);
     launch_y<DWY<R>>(cx, g.N2, g.N1, g.N3, [&](int tl) { return DWY<R>{g, cx.f, tl}; }, s, K_DW_Y);
 }

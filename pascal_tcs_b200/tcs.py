@@ -24,7 +24,7 @@ SCALARS = ["dt", "time", "CFL", "maxDivU", "Nu_bot", "Nu_top", "KE", "blowup",
            "aver", "step", "fixed_dt"]
 HISTORY = ["dt", "time", "maxDivU", "CFL", "Nu_bot", "Nu_top", "KE"]
 METRICS = ["x1", "dx1", "dmx1", "x2", "dx2", "dmx2", "x3", "dx3", "dmx3"]
-TUNING = ["tl_strided", "tl_contig", "tl_modal", "fft_lines_x", "fft_lines_z", "lanes", "long_lines", "y_solver", "ifft_lines_x", "mixed_rows"]
+TUNING = ["tl_strided", "tl_contig", "tl_modal", "fft_lines_x", "fft_lines_z", "lanes", "long_lines", "y_solver", "ifft_lines_x", "mixed_rows", "z_staging"]
 ERRORS = {1: "bad argument", 2: "CUDA error", 3: "unsupported", 4: "BLOW UP",
           5: "out of device memory", 6: "non-finite scalar"}
 

@@ -65,6 +65,11 @@ SCRIPT = textwrap.dedent("""
         counts[f"ensemble case {{k}}"] = s.bounds_violations()
     # 24 uneven cases per precision: more than one multi-case launch's parameter
     # block holds (21 FP64 or 24 FP32 problems), so each batched sweep is split
+    g = P.Solver(n1m=36, n2m=20, n3m=64, property_set=1, Pr=7.0, Ra=1e6, dtStart=5e-4)
+    g.set_tuning("z_staging", 2)
+    g.step(2)
+    counts["z_staging=2"] = g.bounds_violations()
+    g.close()
     rng = np.random.default_rng(3)
     for prec in (0, 1):
         big = [P.Solver(n1m=int(rng.choice([16, 20, 24])), n2m=int(rng.choice([12, 16, 24])),

@@ -91,3 +91,24 @@ def test_solver_knobs_in_the_mixed_form(tcs, knob, value):
     b.set_tuning(knob, 1)                           # the partitioned FP32 eliminations again (frees any scratch)
     b.step(1); a.step(1)
     assert np.linalg.norm(a.get("P") - b.get("P")) <= 1e-5 * np.linalg.norm(a.get("P"))
+
+
+def test_tma_staged_dwz_gives_the_same_bits(tcs):
+    # solvedW's z sweep with its inputs staged by TMA (z_staging 2) runs the same
+    # arithmetic on the same values as the global-load form: the same bits, over
+    # whole water steps, on a grid whose N3 is two passes of 64 planes and whose
+    # last x block is part-filled (N1 = 36)
+    cfg = dict(n1m=36, n2m=24, n3m=128, property_set=1, Pr=7.0, Ra=1e6, DeltaT=10.0, dtStart=5e-4, seed=9)
+    a, b = tcs.Solver(**cfg), tcs.Solver(**cfg)
+    b.set_tuning("z_staging", 2)
+    assert b.tuning()["z_staging"] == 2
+    a.step(3); b.step(3)
+    for n in ("T", "U", "V", "W", "P", "dW"):
+        np.testing.assert_array_equal(b.get(n), a.get(n), err_msg=n)
+    # refused where it cannot run: the FP32 form, N3 not a multiple of 64, odd N1
+    for bad in (dict(cfg, precision=1), dict(cfg, n3m=96), dict(cfg, n1m=45)):
+        g = tcs.Solver(**bad)
+        with pytest.raises(tcs.TcsError) as ei:
+            g.set_tuning("z_staging", 2)
+        assert ei.value.code == 1
+        g.close()

@@ -262,7 +262,8 @@ int tcs_set_use_graph(tcs_ctx *ctx, int on);
  * and z sweeps eliminate their FP32 rows in FP32 with one FP64-residual
  * refinement pass (default); 2 the x sweeps eliminate their FP32-built rows
  * in FP64 instead (no refinement pass; the solution is rounded once to FP32);
- * 4 the x and z sweeps.
+ * 4 the x and z sweeps; 8 the same with the z sweeps at three blocks per SM
+ * (shared-memory elimination; faster at 256^3, slower at 512^3).
  * TCS_TUNE_Z_STAGING (FP64 form): 1 the z sweep of solvedW reads its stencil
  * inputs from global memory (default); 2 it stages them into shared memory with
  * tensor-memory-accelerator (TMA) box copies one pass of 64 k-planes ahead

@@ -984,7 +984,7 @@ int tcs_set_tuning(tcs_ctx *c, int knob, int value)
         if (!ifftx_form(x.fp1u, value)) return set_err(TCS_ERR_ARG, "too many lines for shared memory");
         x.ifft_lines_x = value; break;
     case TCS_TUNE_MIXED_ROWS:
-        if (value > 4) return set_err(TCS_ERR_ARG, "mixed rows: 1 FP32 elimination, 2 FP64 rows in the x sweeps, 4 x and z sweeps");
+        if (value > 8) return set_err(TCS_ERR_ARG, "mixed rows: 1 FP32 elimination, 2 FP64 rows in the x sweeps, 4 x and z sweeps, 8 z at 3 blocks per SM");
         x.mixed_rows = value; break;
     case TCS_TUNE_Z_STAGING:
         if (value > 2) return set_err(TCS_ERR_ARG, "z staging: 1 global loads, 2 TMA-staged inputs for dw_z");

@@ -123,8 +123,9 @@ def _run_vs_oracle(tcs, oracle_mod, steps, cfg, solvers=(1, 1)):
 
 # (y_solver, mixed_rows): (1, 1) FP32 eliminations with FP64-residual
 # refinement; (2, 4) the FP32-built rows of every sweep eliminated in FP64 (the
-# y sweeps one line per thread, the x and z sweeps on the partitioned solver)
-SOLVERS = [(1, 1), (2, 4)]
+# y sweeps one line per thread, the x and z sweeps on the partitioned solver);
+# (1, 8) FP64 rows for x and z, the z sweeps in their three-block shape
+SOLVERS = [(1, 1), (2, 4), (1, 8)]
 
 
 @pytest.mark.parametrize("solvers", SOLVERS)

@@ -67,7 +67,8 @@ def test_long_line_forms_are_bit_identical(tcs, precision):
             np.testing.assert_array_equal(r[n], x, err_msg=n)
 
 
-@pytest.mark.parametrize("knob,value", [("y_solver", 2), ("y_solver", 4), ("mixed_rows", 2), ("mixed_rows", 4)])
+@pytest.mark.parametrize("knob,value", [("y_solver", 2), ("y_solver", 4), ("mixed_rows", 2), ("mixed_rows", 4),
+                                        ("mixed_rows", 8)])
 def test_solver_knobs_in_the_mixed_form(tcs, knob, value):
     # y_solver 2: the y sweeps' FP32-built rows eliminated in FP64 with one line
     # per thread instead of the FP32 elimination and its refinement; 4: the
@@ -86,7 +87,7 @@ def test_solver_knobs_in_the_mixed_form(tcs, knob, value):
         x, y = a.get(n), b.get(n)
         assert np.linalg.norm(x - y) <= 1e-5 * np.linalg.norm(x), n
     with pytest.raises(tcs.TcsError) as ei:
-        b.set_tuning(knob, 8)
+        b.set_tuning(knob, 16)
     assert ei.value.code == 1
     b.set_tuning(knob, 1)                           # the partitioned FP32 eliminations again (frees any scratch)
     b.step(1); a.step(1)

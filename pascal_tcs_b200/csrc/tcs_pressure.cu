@@ -381,22 +381,17 @@ __global__ void __launch_bounds__(256) prhs_fftx_kernel(GridT<R> g, FieldsT<R> f
 // barriers hold its loads back (measured at 512^3: 3.55 ms FP64, 4.82 ms
 // FP32-mixed).  The new U at the x-upper neighbour (periodic) is formed again
 // from its inputs with the same arithmetic, so both forms give the same bits.
-template <class R, int KZ>
+template <class R>
 __global__ void __launch_bounds__(256) prhs_kernel(GridT<R> g, FieldsT<R> f, int with_pseudo)
 {
-    // KZ consecutive k-planes per thread: the new W of the plane above each cell
-    // is the next plane's own (formed once); the new U of the x-upper neighbour
-    // comes from the next lane (threads take consecutive i), else is formed again
-    if (blown(g)) return;
-    const int i0 = 1 + blockIdx.x * blockDim.x + threadIdx.x, j = 1 + blockIdx.y, k0 = 1 + KZ * blockIdx.z;
-    const bool act = i0 <= g.N1;
-    const int i = act ? i0 : g.N1, lane = threadIdx.x & 31;   // idle lanes shadow a valid cell for the shuffles
-    const int nq = min(KZ, g.N3 - k0 + 1);                     // planes of this thread (the same in the whole block)
+    const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x, j = 1 + blockIdx.y, k = 1 + blockIdx.z;
+    if (i > g.N1 || blown(g)) return;
     const double *dx1 = g.d1.dx, *dx2 = g.d2.dx, *dx3 = g.d3.dx;
     const double *rdx1 = g.d1.rdx, *rdx2 = g.d2.rdx, *rdx3 = g.d3.rdx;
     const double *rdmx1 = g.d1.rdmx, *rdmx2 = g.d2.rdmx, *rdmx3 = g.d3.rdmx;
     const int sj = g.P1, sk = g.P1 * g.P2;   // 32-bit offsets (the padded grid is below 2^31 cells)
-    // the new U and W at a cell, as the pseudo-update forms them
+    const int c = (int)ix(g, i, j, k), cxp = c + ((i == g.N1) ? 1 - g.N1 : 1);
+    // the new U at a cell, as the pseudo-update forms it
     auto unew = [&](int cc) -> double {
         if constexpr (HasLo<R>::on) {
             const double u = join(ld(f.U + cc), ld(f.Ulo + cc));
@@ -405,78 +400,57 @@ __global__ void __launch_bounds__(256) prhs_kernel(GridT<R> g, FieldsT<R> f, int
             return with_pseudo ? (double)(ld(f.U + cc) + ld(f.dU + cc)) : (double)ld(f.U + cc);
         }
     };
-    auto wnew = [&](int cc) -> double {
-        if constexpr (HasLo<R>::on) {
-            const double w = join(ld(f.W + cc), ld(f.Wlo + cc));
-            return with_pseudo ? w + (double)ld(f.dW + cc) : w;
-        } else {
-            return with_pseudo ? (double)(ld(f.W + cc) + ld(f.dW + cc)) : (double)ld(f.W + cc);
-        }
-    };
-    const int c0 = (int)ix(g, i, j, k0);
-    double wn[KZ + 1];
-#pragma unroll
-    for (int q = 0; q <= KZ; q++) {
-        if (q > nq) break;
-        wn[q] = wnew((k0 + q == g.N3 + 1) ? (int)ix(g, i, j, 1) : c0 + q * sk);
-    }
+    const double Uc = unew(c), Uxp = unew(cxp);
     const double jvm = (j == 1) ? 0.0 : 1.0, jvp = (j == g.N2) ? 0.0 : 1.0;
+    const int ckp = (k == g.N3) ? (int)ix(g, i, j, 1) : c + sk;
+    double Vc, Vyp, Wc, Wzp;
+    if constexpr (HasLo<R>::on) {
+        Vc = join(ld(f.V + c), ld(f.Vlo + c)); Vyp = join(ld(f.V + (c + sj)), ld(f.Vlo + (c + sj)));
+        Wc = join(ld(f.W + c), ld(f.Wlo + c)); Wzp = join(ld(f.W + ckp), ld(f.Wlo + ckp));
+        if (with_pseudo) {
+            Vc += (double)ld(f.dV + c) * jvm;
+            if (j < g.N2) Vyp += (double)ld(f.dV + (c + sj));
+            Wc += (double)ld(f.dW + c);
+            Wzp += (double)ld(f.dW + ckp);
+            float h, lo;
+            split(Uc, h, lo); store_periodic(g, f.Un, i, j, k, h); store_periodic(g, f.Unlo, i, j, k, lo);
+            split(Vc, h, lo); store_periodic(g, f.Vn, i, j, k, h); store_periodic(g, f.Vnlo, i, j, k, lo);
+            split(Wc, h, lo); store_periodic(g, f.Wn, i, j, k, h); store_periodic(g, f.Wnlo, i, j, k, lo);
+        }
+    } else if (with_pseudo) {
+        const R vn = ld(f.V + c) + ld(f.dV + c) * R(jvm), wn = ld(f.W + c) + ld(f.dW + c);
+        Vc = vn;
+        Vyp = (j < g.N2) ? ld(f.V + (c + sj)) + ld(f.dV + (c + sj)) : ld(f.V + (c + sj));
+        Wc = wn;
+        Wzp = ld(f.W + ckp) + ld(f.dW + ckp);
+        store_periodic(g, f.Un, i, j, k, R(Uc));
+        store_periodic(g, f.Vn, i, j, k, vn);
+        store_periodic(g, f.Wn, i, j, k, wn);
+    } else {
+        Vc = ld(f.V + c); Vyp = ld(f.V + (c + sj)); Wc = ld(f.W + c); Wzp = ld(f.W + ckp);
+    }
     const double dt = g.scal[S_DT], rdt = 1.0 / dt;
     const Phys &p = g.phd;
     const double rdtc = rdt / p.Cmp;
+    const int im = i - 1, ip = i + 1, jm = j - 1, jp = j + 1, km = k - 1, kp = k + 1;
+    const double DivUm = (Uxp - Uc) * rdx1[i] + (jvp * Vyp - jvm * Vc) * rdx2[j] + (Wzp - Wc) * rdx3[k];
     const double cbc = (1.0 - jvm) * p.Vbt * rdx2[j] - (1.0 - jvp) * p.Vup * rdx2[j];
-    const int im = i - 1, ip = i + 1, jm = j - 1, jp = j + 1;
-#pragma unroll
-    for (int q = 0; q < KZ; q++) {
-        if (q >= nq) break;
-        const int k = k0 + q, c = c0 + q * sk, km = k - 1, kp = k + 1;
-        const double Uc = unew(c);
-        const double Ush = __shfl_down_sync(0xffffffffu, Uc, 1);
-        const double Uxp = (lane < 31 && i0 < g.N1) ? Ush : unew(c + ((i == g.N1) ? 1 - g.N1 : 1));
-        const double Wc = wn[q], Wzp = wn[q + 1];
-        double Vc, Vyp;
-        if constexpr (HasLo<R>::on) {
-            Vc = join(ld(f.V + c), ld(f.Vlo + c)); Vyp = join(ld(f.V + (c + sj)), ld(f.Vlo + (c + sj)));
-            if (with_pseudo) {
-                Vc += (double)ld(f.dV + c) * jvm;
-                if (j < g.N2) Vyp += (double)ld(f.dV + (c + sj));
-                if (act) {
-                    float h, lo;
-                    split(Uc, h, lo); store_periodic(g, f.Un, i, j, k, h); store_periodic(g, f.Unlo, i, j, k, lo);
-                    split(Vc, h, lo); store_periodic(g, f.Vn, i, j, k, h); store_periodic(g, f.Vnlo, i, j, k, lo);
-                    split(Wc, h, lo); store_periodic(g, f.Wn, i, j, k, h); store_periodic(g, f.Wnlo, i, j, k, lo);
-                }
-            }
-        } else if (with_pseudo) {
-            const R vn = ld(f.V + c) + ld(f.dV + c) * R(jvm);
-            Vc = vn;
-            Vyp = (j < g.N2) ? ld(f.V + (c + sj)) + ld(f.dV + (c + sj)) : ld(f.V + (c + sj));
-            if (act) {
-                store_periodic(g, f.Un, i, j, k, R(Uc));
-                store_periodic(g, f.Vn, i, j, k, vn);
-                store_periodic(g, f.Wn, i, j, k, R(Wc));
-            }
-        } else {
-            Vc = ld(f.V + c); Vyp = ld(f.V + (c + sj));
-        }
-        const double DivUm = (Uxp - Uc) * rdx1[i] + (jvp * Vyp - jvm * Vc) * rdx2[j] + (Wzp - Wc) * rdx3[k];
-        const R *dPh = f.dPhat;
-        const double Pc = ld(dPh + c);
-        const double ddpdx1 = (Pc - (double)ld(dPh + (c - 1))) * rdmx1[i], ddpdx2 = ((double)ld(dPh + (c + 1)) - Pc) * rdmx1[ip];
-        const double ddpdy3 = (Pc - (double)ld(dPh + (c - sj))) * rdmx2[j], ddpdy4 = ((double)ld(dPh + (c + sj)) - Pc) * rdmx2[jp];
-        const double ddpdz5 = (Pc - (double)ld(dPh + (c - sk))) * rdmx3[k], ddpdz6 = ((double)ld(dPh + (c + sk)) - Pc) * rdmx3[kp];
-        const double iRjk = IR(j, k);
-        const double iR1 = 0.5 * rdmx1[i] * (dx1[im] * iRjk + dx1[i] * iRjk);
-        const double iR2_ = 0.5 * rdmx1[ip] * (dx1[ip] * iRjk + dx1[i] * iRjk);
-        const double iR3 = 0.5 * rdmx2[j] * (dx2[jm] * iRjk + dx2[j] * (double)IR(jm, k));
-        const double iR4 = 0.5 * rdmx2[jp] * (dx2[jp] * iRjk + dx2[j] * (double)IR(jp, k));
-        const double iR5 = 0.5 * rdmx3[k] * (dx3[km] * iRjk + dx3[k] * (double)IR(j, km));
-        const double iR6 = 0.5 * rdmx3[kp] * (dx3[kp] * iRjk + dx3[k] * (double)IR(j, kp));
-        const double Extra = ((1.0 - iR2_) * ddpdx2 - (1.0 - iR1) * ddpdx1) * rdx1[i]
-                           + ((1.0 - iR4) * ddpdy4 - (1.0 - iR3) * ddpdy3) * rdx2[j]
-                           + ((1.0 - iR6) * ddpdz6 - (1.0 - iR5) * ddpdz5) * rdx3[k];
-        if (act) f.prhs[c] = (DivUm - cbc) * rdtc + Extra;
-    }
+    const R *dPh = f.dPhat;
+    const double Pc = ld(dPh + c);
+    const double ddpdx1 = (Pc - (double)ld(dPh + (c - 1))) * rdmx1[i], ddpdx2 = ((double)ld(dPh + (c + 1)) - Pc) * rdmx1[ip];
+    const double ddpdy3 = (Pc - (double)ld(dPh + (c - sj))) * rdmx2[j], ddpdy4 = ((double)ld(dPh + (c + sj)) - Pc) * rdmx2[jp];
+    const double ddpdz5 = (Pc - (double)ld(dPh + (c - sk))) * rdmx3[k], ddpdz6 = ((double)ld(dPh + (c + sk)) - Pc) * rdmx3[kp];
+    const double iRjk = IR(j, k);
+    const double iR1 = 0.5 * rdmx1[i] * (dx1[im] * iRjk + dx1[i] * iRjk);
+    const double iR2_ = 0.5 * rdmx1[ip] * (dx1[ip] * iRjk + dx1[i] * iRjk);
+    const double iR3 = 0.5 * rdmx2[j] * (dx2[jm] * iRjk + dx2[j] * (double)IR(jm, k));
+    const double iR4 = 0.5 * rdmx2[jp] * (dx2[jp] * iRjk + dx2[j] * (double)IR(jp, k));
+    const double iR5 = 0.5 * rdmx3[k] * (dx3[km] * iRjk + dx3[k] * (double)IR(j, km));
+    const double iR6 = 0.5 * rdmx3[kp] * (dx3[kp] * iRjk + dx3[k] * (double)IR(j, kp));
+    const double Extra = ((1.0 - iR2_) * ddpdx2 - (1.0 - iR1) * ddpdx1) * rdx1[i]
+                       + ((1.0 - iR4) * ddpdy4 - (1.0 - iR3) * ddpdy3) * rdx2[j]
+                       + ((1.0 - iR6) * ddpdz6 - (1.0 - iR5) * ddpdz5) * rdx3[k];
+    f.prhs[c] = (DivUm - cbc) * rdtc + Extra;
 }
 
 // The forward r2c x transform of the split form: NL right-hand-side lines
@@ -910,7 +884,7 @@ void launch_pseudo_prhs_fftx(const Ctx<R> &cx, cudaStream_t s, bool with_pseudo)
         const dim3 gx((g.N2 + NL - 1) / NL, g.N3);
         static size_t c8[64] = {}, c4[64] = {};
         probe_begin(cx, K_PRHS_FFTX, s);
-        prhs_kernel<R, 2><<<dim3((g.N1 + 255) / 256, g.N2, (g.N3 + 1) / 2), 256, 0, s>>>(g, cx.f, with_pseudo ? 1 : 0);
+        prhs_kernel<R><<<dim3((g.N1 + 255) / 256, g.N2, g.N3), 256, 0, s>>>(g, cx.f, with_pseudo ? 1 : 0);
         record_launch_error("prhs");
         if (cx.fp1u.radix[0] == 8) {
             smem_opt_in((const void *)fftx_uniform_kernel<8, R>, sm, c8);

@@ -995,7 +995,7 @@ int tcs_set_tuning(tcs_ctx *c, int knob, int value)
         if (value < 2 || value > 32) return set_err(TCS_ERR_ARG, "lanes per line must be 2..32");
         x.lanes = value; break;
     case TCS_TUNE_LONG_LINES:
-        if (value > 8) return set_err(TCS_ERR_ARG, "long-line form: 1 never, 2 z sweeps, 4 z and y sweeps, 8 also the modal solves");
+        if (value > 4) return set_err(TCS_ERR_ARG, "long-line form: 1 never, 2 z sweeps, 4 z and y sweeps");
         x.long_lines = value; break;
     case TCS_TUNE_Y_SOLVER: {
         if (value > 4) return set_err(TCS_ERR_ARG, "y solver: 1 partitioned, 2 one line per thread (y sweeps), 4 also the modal solves");

@@ -952,12 +952,6 @@ void launch_modal(const Ctx<R> &cx, cudaStream_t s)
         launch_thomas<Modal<R>>(cx, g.N2, cx.h1p, g.N3, [&](int tl) { return Modal<R>{g, cx.f, tl, cx.h1p}; }, s, K_MODAL);
         return;
     }
-    if (cx.long_lines >= 8) {   // one block per SM: 8 kx lines (128-byte rows of S in FP64) where 3 blocks fit 4
-        using L = LongLines<Modal<R>>;
-        LinePlan pl = plan_for<L>(g.N2, false, fit_tl<L>(g.N2, false, cx.tl_modal, cx.lanes), cx.lanes);
-        launch_lines(L{Modal<R>{g, cx.f, pl.TL, cx.h1p}}, pl, dim3((cx.h1p + pl.TL - 1) / pl.TL, g.N3), s, K_MODAL, cx);
-        return;
-    }
     LinePlan pm = plan_for<Modal<R>>(g.N2, false, fit_tl<Modal<R>>(g.N2, false, cx.tl_modal, cx.lanes), cx.lanes);
     launch_lines(Modal<R>{g, cx.f, pm.TL, cx.h1p}, pm, dim3((cx.h1p + pm.TL - 1) / pm.TL, g.N3), s, K_MODAL, cx);
 }

@@ -718,8 +718,10 @@ __global__ void __launch_bounds__(ZS_NT, 1) dwz_staged_kernel(const __grid_const
         const double *const t = reinterpret_cast<const double *>(smraw + (c & 1) * ZS_BUF);
         // row r = c ZS_CH + rr is plane k = r + 1, plane k + dk of a box at z = rr + 1 + dk
         auto val = [&](int a, int di, int dj, int dk) -> double {
-            const int z = rr + 1 + dk, y = (a == P::A_W) ? 1 + dj : dj;
-            return t[zs_off(a) / 8 + (z * zs_rows(a) + y) * 10 + (l + 1 + di)];
+            int z = rr + 1 + dk, y = (a == P::A_W) ? 1 + dj : dj, x = l + 1 + di;
+            TCS_OOB(prob.g.scal, (unsigned)z >= (unsigned)zs_planes(a) || (unsigned)y >= (unsigned)zs_rows(a) || (unsigned)x >= 10u,
+                    (z = 0, y = 0, x = 0));
+            return t[zs_off(a) / 8 + (z * zs_rows(a) + y) * 10 + x];
         };
         const int r = c * ZS_CH + rr;
         Coef<double, 1> cf;

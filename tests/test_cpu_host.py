@@ -28,6 +28,24 @@ def test_library_exports_every_declared_symbol(tcs):
     assert declared == set(tcs.EXPORTS)
 
 
+def test_tuning_knobs_follow_the_header(tcs):
+    # the Python binding addresses knobs by their index in include/tcs.h's
+    # TCS_TUNE_* enum: the two lists must agree name for name and in order,
+    # and every line of the committed tune cache must carry at most that many
+    # knob columns (older lines may stop early; the library keeps the rest)
+    hdr = open(os.path.join(ROOT, "include", "tcs.h")).read()
+    body = re.search(r"enum\s*\{\s*(TCS_TUNE_TL_STRIDED[^}]*)\}", hdr).group(1)
+    names = [n.strip().split("=")[0].strip() for n in body.split(",") if n.strip()]
+    assert names[-1] == "TCS_TUNE_COUNT"
+    assert [n[len("TCS_TUNE_"):].lower() for n in names[:-1]] == tcs.tcs.TUNING
+    with open(os.path.join(ROOT, "pascal_tcs_b200", "tune_cache.txt")) as f:
+        for line in f:
+            v = line.split()
+            if v:
+                assert 4 + 7 <= len(v) <= 4 + len(tcs.tcs.TUNING), line
+                assert all(int(x) > 0 for x in v[:3] + v[4:]) and v[3] in ("0", "1"), line
+
+
 def test_kernel_names(tcs):
     names = tcs.kernel_names()
     assert len(names) == len(set(names)) and "thermal_z" in names and "projection" in names
